@@ -1,0 +1,238 @@
+/*
+ * mfree_b200: C ABI of the B200-native explicit 2D SPH cutting step.
+ *
+ * One context (mf_ctx) owns one particle system on one GPU: the particle_gpu state, the
+ * cell-list grid (grid_gpu_green / grid_gpu_rothlin semantics), the leap_frog stepper,
+ * the constants and the rigid tool. Every entry point returns an int status (MF_OK = 0,
+ * negative on error); no entry point exits the process or prints.
+ *
+ * Units and layouts are the reference's: cm, g, microseconds; vector fields interleaved
+ * (pos = x0 y0 x1 y1 ..., S = Sxx Sxy Syy Szz per particle), flags as 0/1 doubles.
+ * The comment above each function names the reference interface it replaces
+ * (file:line within the reference project iwf-inspire/mfree_iwf-ul_cut_gpu).
+ */
+#ifndef MFREE_B200_H
+#define MFREE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MF_ABI_VERSION 1
+
+/* ---- status codes ---- */
+#define MF_OK 0
+#define MF_ERR_INVALID (-1)     /* bad argument (null pointer, size, enum, flag value) */
+#define MF_ERR_CUDA (-2)        /* a CUDA runtime call failed (see mf_last_cuda_error) */
+#define MF_ERR_STATE (-3)       /* call out of order (e.g. step before particles/grid) */
+#define MF_ERR_RANGE (-4)       /* size beyond a documented maximum / grid budget exceeded */
+#define MF_ERR_NOMEM (-5)       /* device or host allocation failed */
+#define MF_ERR_NO_DEVICE (-6)   /* no CUDA device (the product has no CPU fallback) */
+#define MF_ERR_DEVICE_FAULT (-7) /* a kernel reported an internal error (bounded wait expired) */
+
+/* ---- particle fields (particle_gpu.h:33-87) ---- */
+#define MF_FIELD_POS 0        /* 2 doubles */
+#define MF_FIELD_VEL 1        /* 2 */
+#define MF_FIELD_H 2          /* 1 */
+#define MF_FIELD_RHO 3        /* 1 */
+#define MF_FIELD_P 4          /* 1: pressure of the last predictor (0 for tool particles) */
+#define MF_FIELD_S 5          /* 4: Sxx Sxy Syy Szz */
+#define MF_FIELD_R 6          /* 4: artificial stress Rxx Rxy Ryy 0 (0 for tool particles) */
+#define MF_FIELD_FC 7         /* 2 */
+#define MF_FIELD_FT 8         /* 2 */
+#define MF_FIELD_N 9          /* 2: contact normal, indexed by array position (not permuted) */
+#define MF_FIELD_FIXED 10     /* 1: 0/1 */
+#define MF_FIELD_BLANKED 11   /* 1: 0/1 */
+#define MF_FIELD_TOOL 12      /* 1: 0/1 (tool_particle) */
+#define MF_FIELD_EPS_PL 13    /* 1 */
+#define MF_FIELD_EPS_PL_DOT 14 /* 1 */
+#define MF_FIELD_T 15         /* 1 */
+#define MF_FIELD_POS_T 16     /* 2 */
+#define MF_FIELD_VEL_T 17     /* 2 */
+#define MF_FIELD_RHO_T 18     /* 1 */
+#define MF_FIELD_S_T 19       /* 4 */
+#define MF_FIELD_T_T 20       /* 1 */
+#define MF_FIELD_S_DER 21     /* 4: only with MF_OPT_KEEP_DERIVATIVES */
+#define MF_FIELD_V_DER 22     /* 4: only with MF_OPT_KEEP_DERIVATIVES */
+#define MF_FIELD_IDX 23       /* 1 int: Green = sort permutation, Rothlin = persistent id */
+#define MF_FIELD_HASH 24      /* 1 int: cell hash of the last sort, in array order */
+#define MF_NUM_FIELDS 25
+
+/* ---- enums ---- */
+#define MF_GRID_GREEN 0        /* grid_gpu_green.h:38-91 */
+#define MF_GRID_ROTHLIN 1      /* grid_gpu_rothlin.h:55-91 */
+#define MF_THERMAL_BROOKSHAW 0 /* types.h:94 */
+#define MF_THERMAL_PSE 1       /* types.h:95 */
+#define MF_JC_JOHNSON_COOK 0   /* plasticity.cuh:30-46 */
+#define MF_JC_TANH 1           /* plasticity.cuh:48-70 (used by the secant solve, as m_s_yield) */
+#define MF_PRECISION_FP64 0    /* plain FP64 */
+#define MF_PRECISION_MIXED 1   /* FP32 pair sums on cell-relative coordinates, FP64 integration */
+
+/* option bits for mf_set_flags */
+#define MF_OPT_KEEP_DERIVATIVES 1 /* also store S_der / v_der (the reference's public arrays) */
+#define MF_OPT_NO_GRAPHS 2        /* launch kernels directly instead of replaying CUDA graphs */
+
+/* ---- constants (constants_structs.h:25-82), same member order ---- */
+typedef struct { double E, nu, rho0, K, G, mass, mass_tool; } mf_phys_constants;
+typedef struct { double cp, tq, k, alpha, T_init, eta; } mf_trml_constants;
+typedef struct { double wdeltap, stresseps, xspheps, alpha, beta, eta; } mf_corr_constants;
+typedef struct {
+  double A, B, C, n, m, Tmelt, Tref, eps_dot_ref, tanh_a, tanh_b, tanh_c, tanh_d;
+} mf_joco_constants;
+
+/* ---- rigid tool (tool_gpu.cuh:32-52 + the __constant__ block of tool_gpu.cu:21-27) ---- */
+typedef struct {
+  double left[2], right[2];
+  double a, b;  /* line y = a x + b, or x = b if vertical */
+  int vertical;
+  double n[2];  /* outward normal (not updated when the tool moves, as in the reference) */
+} mf_segment;
+typedef struct { double r, t1, t2, p[2]; } mf_fillet;
+typedef struct {
+  int num_seg;        /* 0 (no tool), 4, or 5 (5 means segment 2 is the fillet) */
+  mf_segment seg[5];
+  int has_fillet;
+  mf_fillet fillet;
+  double mu;            /* friction coefficient */
+  double contact_alpha; /* penalty factor */
+  double slave_mass;    /* workpiece particle mass */
+  double vel[2];        /* tool velocity */
+} mf_tool_state;
+
+/* ---- run-time status (replaces printf / exit diagnostics) ---- */
+typedef struct {
+  long long steps;            /* steps taken by this context */
+  long long blanked;          /* particles currently blanked */
+  long long newly_blanked;    /* blanked by invalidate() since the last status read */
+  long long out_of_grid;      /* hashes outside [0, num_cell) clamped since creation */
+  long long secant_cap_hits;  /* JC secant solves that hit the iteration cap */
+  int max_cell_occupancy;     /* largest particles-per-cell seen in the last sort */
+  int error_flags;            /* bit 0: a bounded wait in the cell scan expired */
+} mf_status;
+
+typedef struct mf_ctx mf_ctx;
+
+/* ---- context ---- */
+int mf_version(void);
+const char *mf_error_string(int code);
+int mf_last_cuda_error(const mf_ctx *ctx);            /* cudaError_t of the last failure */
+int mf_ctx_create(int device, mf_ctx **out);
+int mf_ctx_destroy(mf_ctx *ctx);
+int mf_ctx_stream(mf_ctx *ctx, void **cuda_stream);   /* the stream all work is queued on */
+int mf_set_flags(mf_ctx *ctx, int flags);
+int mf_synchronize(mf_ctx *ctx);
+
+/* ---- particles: particle_gpu(...) constructors (particle_gpu.h:81-86, particle_gpu.cu:97-125).
+   pos, vel, rho and h are required; T, fixed, tool_p and S may be NULL (zero). Flag arrays
+   must hold exactly 0 or 1. ---- */
+int mf_particles_create(mf_ctx *ctx, int N, const double *pos, const double *vel, const double *rho,
+                        const double *T, const double *h, const double *fixed, const double *tool_p,
+                        const double *S);
+int mf_particles_count(const mf_ctx *ctx, int *N);
+/* copy a field to / from host memory: N * width doubles (ints for IDX and HASH) */
+int mf_get_field(mf_ctx *ctx, int field, void *host);
+int mf_set_field(mf_ctx *ctx, int field, const void *host);
+
+/* ---- grid: grid_gpu_green(N, bbmin, bbmax, h) / grid_gpu_rothlin(...) locked geometry
+   (grid.cu:139-158), or the adaptive grid(max_cell, N) (grid.cu:97-136,160-162) ---- */
+int mf_grid_create_locked(mf_ctx *ctx, int kind, double bbmin_x, double bbmin_y, double bbmax_x,
+                          double bbmax_y, double h);
+int mf_grid_create_adaptive(mf_ctx *ctx, int kind, int max_cell);
+/* grid_base accessors (grid.h:51-72): out5 = bbmin_x bbmin_y bbmax_x bbmax_y dx */
+int mf_grid_geometry(mf_ctx *ctx, int *nx, int *ny, int *num_cell, double *out5);
+/* update_geometry + assign_hashes + sort (leap_frog.cu:106-108) without stepping */
+int mf_grid_build(mf_ctx *ctx);
+/* get_cells (grid_gpu_green.cu:207-210 / grid_gpu_rothlin.cu:129-136) into host arrays of
+   num_cell ints. Green: empty cells have start = -1 (their end is -1 here; the reference
+   leaves it stale). Rothlin: start[c] = #particles with hash < c, end[c] = start[c+1]. */
+int mf_grid_get_cells(mf_ctx *ctx, int *start, int *end);
+
+/* ---- constants: actions_setup_* (actions_gpu.cu:438-469) and interactions_setup_*
+   (interactions_gpu.cu:433-459) in one call. joco NULL = no plasticity; trml_* NULL = 0. */
+int mf_set_constants(mf_ctx *ctx, const mf_phys_constants *phys, const mf_corr_constants *corr,
+                     const mf_joco_constants *joco, const mf_trml_constants *trml_wp,
+                     const mf_trml_constants *trml_tool);
+int mf_set_options(mf_ctx *ctx, int thermal_solver, int jc_model, int precision);
+int mf_set_dt(mf_ctx *ctx, double dt); /* global_dt (benchmarks.cpp:20) */
+
+/* ---- tool: tool_gpu_set_up_tool (tool_gpu.cu:224-271); the per-step tool_gpu_update_tool
+   (tool_gpu.cu:275-316) happens on the device inside mf_step. NULL or num_seg = 0: no tool. */
+int mf_tool_set(mf_ctx *ctx, const mf_tool_state *tool);
+int mf_tool_get(mf_ctx *ctx, mf_tool_state *tool);
+
+/* ---- stepping: leap_frog::step (leap_frog.cu:94-155), n times, queued asynchronously ---- */
+int mf_step(mf_ctx *ctx, int n_steps);
+/* parts of one step, for parity tests: 0 grid (sort), 1 predictor (init, predict, eos,
+   artificial stress), 2 interactions + rates, 3 corrector .. invalidate. */
+int mf_step_stage(mf_ctx *ctx, int stage);
+/* report_force (output.cu:31-39): sum of fc + ft after the last step, compensated */
+int mf_report_force(mf_ctx *ctx, double out[2]);
+/* per-step force log since the last call (or creation), at most max entries of 2 doubles */
+int mf_force_log(mf_ctx *ctx, double *out, int max_entries, int *n_out);
+int mf_status_get(mf_ctx *ctx, mf_status *status);
+
+/* ---- host scene setup: setup_ref_cut (benchmarks.cpp:255-537) and its generalisation ---- */
+typedef struct {
+  int N, n_workpiece, n_tool;
+  double *pos, *vel, *rho, *T, *h, *fixed, *tool_p; /* host arrays owned by the scene */
+  mf_phys_constants phys;
+  mf_corr_constants corr;
+  mf_joco_constants joco;
+  mf_trml_constants trml_wp, trml_tool;
+  int has_joco;
+  mf_tool_state tool;
+  double grid_bbmin[2], grid_bbmax[2], grid_h;
+  double dt, t_final;
+  double feed, speed;
+} mf_scene;
+
+typedef struct {
+  /* lattice: reference mode (nx_lattice == 0): ny rows spanning [hi_y - 3 feed, hi_y]
+     (benchmarks.cpp:266-273); explicit mode: nx_lattice x ny rows at spacing dx from lo. */
+  int ny;
+  int nx_lattice;
+  double dx;
+  double lo_x, lo_y, hi_x, hi_y;
+  double hdx;
+  double jitter;            /* uniform jitter amplitude as a fraction of dx (0 = none) */
+  unsigned long long seed;
+  /* tool (tool.cpp:342-375; positioning benchmarks.cpp:398-414) */
+  double rake, clear, chamfer, speed, feed, mu_fric, contact_alpha;
+  double tool_tl_x, tool_tl_y, tool_length, tool_height;
+  double tool_front_x;      /* explicit mode: translate the tool so front() = this x */
+  int sample_tool;          /* add thermal-only tool particles (benchmarks.cpp:425-459) */
+  int use_thermals;
+  /* material */
+  double E, nu, rho0, rho_tool;
+  mf_joco_constants joco;
+  mf_trml_constants trml_wp, trml_tool;
+  mf_corr_constants corr;   /* wdeltap is computed */
+  double cfl;               /* dt = cfl*hdx*dx/(sqrt(K/rho0) + sqrt(speed)) (benchmarks.cpp:530) */
+  double cutting_distance;
+} mf_cut_params;
+
+/* parameters that reproduce setup_ref_cut(ny, grid, rake, clear, chamfer, speed, feed) */
+int mf_cut_params_reference(mf_cut_params *p, int ny, double rake, double clear, double chamfer,
+                            double speed, double feed);
+int mf_scene_cut(const mf_cut_params *p, mf_scene **out);
+int mf_scene_setup_ref_cut(int ny, double rake, double clear, double chamfer, double speed, double feed,
+                           mf_scene **out);
+int mf_scene_free(mf_scene *scene);
+/* particles + locked Green/Rothlin grid + constants + tool + dt from a scene */
+int mf_scene_upload(mf_ctx *ctx, const mf_scene *scene, int grid_kind);
+
+/* ---- host tool geometry (tool.cpp): the (tl, length, height, rake, clear, r, mu) constructor,
+   sample_tool (tool.cpp:121-144) and update_tool (tool.cpp:211-221) ---- */
+int mf_tool_construct(double tl_x, double tl_y, double length, double height, double rake, double clear,
+                      double r, double mu, mf_tool_state *out);
+int mf_tool_sample(const mf_tool_state *tool, double dx, double *xy_out, int capacity, int *n_out);
+int mf_tool_translate(mf_tool_state *tool, double dt); /* tool::update_tool with tool->vel */
+
+/* ---- output: vtk_writer_write (vtk_writer.cpp:20-178, 185-264), legacy ASCII ---- */
+int mf_vtk_write_particles(mf_ctx *ctx, const char *path);
+int mf_vtk_write_tool(const mf_tool_state *tool, const char *path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,796 @@
+// C ABI of the B200 SPH step (include/mfree_b200.h): context, device buffers, launches and
+// CUDA-graph replay of leap_frog::step (leap_frog.cu:94-155).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "mf_kernels.cuh"
+#include "mf_mixed.cuh"
+#include "mfree_b200.h"
+
+using namespace mf;
+
+struct mf_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int last_cuda_err = 0;
+  int flags = 0;
+  // particles
+  int N = 0;
+  bool has_particles = false;
+  // grid
+  bool has_grid = false;
+  int grid_kind = MF_GRID_GREEN;
+  geom G{};
+  // constants / options
+  params P{};
+  bool has_constants = false;
+  mf_tool_state tool{};
+  // device memory
+  dev_buffers D{};
+  state_set set[2]{};
+  int cur = 0;          // set holding the current state
+  bool mid_step = false; // stages 1-2 ran: reads see the step's buffer
+  int scan_tiles = 0;   // tiles for max_cell + 1 entries
+  int finish_blocks = 0;
+  int bbox_blocks = 0;
+  std::vector<void *> particle_allocs, grid_allocs, fixed_allocs;
+  // graphs: one per parity of the double buffer
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  bool graph_valid = false;
+  long long steps = 0;
+  unsigned long long force_read_head = 0;
+  unsigned long long status_newly_blanked_seen = 0;
+};
+
+namespace {
+
+#define CK(call)                                    \
+  do {                                              \
+    cudaError_t e_ = (call);                        \
+    if (e_ != cudaSuccess) {                        \
+      ctx->last_cuda_err = (int)e_;                 \
+      return MF_ERR_CUDA;                           \
+    }                                               \
+  } while (0)
+
+int set_device(mf_ctx *ctx) {
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) { ctx->last_cuda_err = (int)e; return MF_ERR_CUDA; }
+  return MF_OK;
+}
+
+template <class T>
+int dalloc(mf_ctx *ctx, std::vector<void *> &list, T **ptr, size_t count) {
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, count ? count * sizeof(T) : sizeof(T));
+  if (e != cudaSuccess) {
+    ctx->last_cuda_err = (int)e;
+    return e == cudaErrorMemoryAllocation ? MF_ERR_NOMEM : MF_ERR_CUDA;
+  }
+  e = cudaMemset(p, 0, count ? count * sizeof(T) : sizeof(T));
+  if (e != cudaSuccess) { ctx->last_cuda_err = (int)e; return MF_ERR_CUDA; }
+  list.push_back(p);
+  *ptr = (T *)p;
+  return MF_OK;
+}
+
+void free_list(std::vector<void *> &list) {
+  for (void *p : list) cudaFree(p);
+  list.clear();
+}
+
+void drop_graphs(mf_ctx *ctx) {
+  for (int k = 0; k < 2; ++k)
+    if (ctx->graph[k]) { cudaGraphExecDestroy(ctx->graph[k]); ctx->graph[k] = nullptr; }
+  ctx->graph_valid = false;
+}
+
+#define TRY(x)                 \
+  do {                         \
+    int r_ = (x);              \
+    if (r_ != MF_OK) return r_; \
+  } while (0)
+
+int alloc_set(mf_ctx *ctx, state_set &s, int N) {
+  auto &L = ctx->particle_allocs;
+  TRY(dalloc(ctx, L, &s.pos, N)); TRY(dalloc(ctx, L, &s.vel, N)); TRY(dalloc(ctx, L, &s.fc, N));
+  TRY(dalloc(ctx, L, &s.ft, N)); TRY(dalloc(ctx, L, &s.pos_t, N)); TRY(dalloc(ctx, L, &s.vel_t, N));
+  TRY(dalloc(ctx, L, &s.rho, N)); TRY(dalloc(ctx, L, &s.T, N)); TRY(dalloc(ctx, L, &s.eps_pl, N));
+  TRY(dalloc(ctx, L, &s.eps_pl_dot, N)); TRY(dalloc(ctx, L, &s.h, N)); TRY(dalloc(ctx, L, &s.rho_t, N));
+  TRY(dalloc(ctx, L, &s.T_t, N)); TRY(dalloc(ctx, L, &s.S, N)); TRY(dalloc(ctx, L, &s.S_t, N));
+  TRY(dalloc(ctx, L, &s.flags, N)); TRY(dalloc(ctx, L, &s.idx, N));
+  return MF_OK;
+}
+
+int alloc_particles(mf_ctx *ctx, int N) {
+  drop_graphs(ctx);
+  free_list(ctx->particle_allocs);
+  auto &L = ctx->particle_allocs;
+  TRY(alloc_set(ctx, ctx->set[0], N));
+  TRY(alloc_set(ctx, ctx->set[1], N));
+  dev_buffers &D = ctx->D;
+  TRY(dalloc(ctx, L, &D.n, N));
+  TRY(dalloc(ctx, L, &D.rec, (size_t)N * R_WIDTH));
+  TRY(dalloc(ctx, L, &D.recf, (size_t)N * F_WIDTH));
+  TRY(dalloc(ctx, L, &D.pp, N));
+  TRY(dalloc(ctx, L, &D.S_der, N));
+  TRY(dalloc(ctx, L, &D.v_der, N));
+  TRY(dalloc(ctx, L, &D.hash_cur, N));
+  TRY(dalloc(ctx, L, &D.hash_new, N));
+  TRY(dalloc(ctx, L, &D.slot, N));
+  TRY(dalloc(ctx, L, &D.perm_u, N));
+  TRY(dalloc(ctx, L, &D.perm, N));
+  ctx->finish_blocks = (N + BLOCK - 1) / BLOCK;
+  ctx->bbox_blocks = std::min(ctx->finish_blocks, 148 * 4);
+  TRY(dalloc(ctx, L, &D.partials, (size_t)std::max(ctx->finish_blocks, 1) * 8));
+  ctx->N = N;
+  return MF_OK;
+}
+
+int alloc_grid(mf_ctx *ctx, int max_cell) {
+  drop_graphs(ctx);
+  free_list(ctx->grid_allocs);
+  auto &L = ctx->grid_allocs;
+  TRY(dalloc(ctx, L, &ctx->D.count, (size_t)max_cell));
+  TRY(dalloc(ctx, L, &ctx->D.off, (size_t)max_cell + 1));
+  ctx->scan_tiles = (max_cell + SCAN_TILE - 1) / SCAN_TILE + 1;
+  TRY(dalloc(ctx, L, &ctx->D.scan_status, (size_t)ctx->scan_tiles));
+  return MF_OK;
+}
+
+int upload_geom(mf_ctx *ctx) {
+  CK(cudaMemcpyAsync(ctx->D.g, &ctx->G, sizeof(geom), cudaMemcpyHostToDevice, ctx->stream));
+  return MF_OK;
+}
+
+void bind_sets(mf_ctx *ctx) {
+  ctx->D.A = ctx->set[ctx->cur];
+  ctx->D.B = ctx->set[ctx->cur ^ 1];
+}
+
+bool ready(const mf_ctx *ctx) { return ctx->has_particles && ctx->has_grid && ctx->has_constants; }
+
+// cell-list build into the other buffer (k_hash_count .. k_reorder); PREDICT adds the
+// predictor of the step
+int launch_cells(mf_ctx *ctx, bool step_mode) {
+  const int N = ctx->N;
+  const int nb = (N + BLOCK - 1) / BLOCK;
+  bind_sets(ctx);
+  if (!ctx->G.locked)
+    k_bbox<<<ctx->bbox_blocks, BLOCK, 0, ctx->stream>>>(N, ctx->D.A.pos, ctx->D.A.h, ctx->D);
+  const int hash_blocks = std::max(nb, (ctx->scan_tiles + BLOCK - 1) / BLOCK);
+  k_hash_count<<<hash_blocks, BLOCK, 0, ctx->stream>>>(N, ctx->D.A, ctx->D, ctx->scan_tiles,
+                                                        step_mode && ctx->P.has_tool ? 1 : 0, ctx->P.dt);
+  k_scan<<<ctx->scan_tiles, SCAN_THREADS, 0, ctx->stream>>>(ctx->D, N);
+  k_scatter<<<nb, BLOCK, 0, ctx->stream>>>(N, ctx->D);
+  return MF_OK;
+}
+
+int launch_stage(mf_ctx *ctx, int stage) {
+  const int N = ctx->N;
+  const int nb = (N + BLOCK - 1) / BLOCK;
+  const int npb = (N + PAIR_BLOCK - 1) / PAIR_BLOCK;
+  bind_sets(ctx);
+  const bool mixed = ctx->P.precision == MF_PRECISION_MIXED;
+  switch (stage) {
+    case 0:
+      TRY(launch_cells(ctx, true));
+      break;
+    case 1:
+      if (mixed) k_reorder<true, true><<<nb, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      else k_reorder<true, false><<<nb, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      break;
+    case 2:
+      if (mixed) k_pair_mixed<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      else k_pair_fp64<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      if (ctx->P.thermal_solver == MF_THERMAL_PSE && ctx->P.thermal_wp)
+        k_pse<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      break;
+    case 3:
+      k_finish<<<ctx->finish_blocks, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      break;
+    default:
+      return MF_ERR_INVALID;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { ctx->last_cuda_err = (int)e; return MF_ERR_CUDA; }
+  return MF_OK;
+}
+
+int launch_step(mf_ctx *ctx) {
+  for (int s = 0; s < 4; ++s) TRY(launch_stage(ctx, s));
+  return MF_OK;
+}
+
+int build_graphs(mf_ctx *ctx) {
+  drop_graphs(ctx);
+  const int saved = ctx->cur;
+  for (int k = 0; k < 2; ++k) {
+    ctx->cur = k;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = launch_step(ctx);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc != MF_OK) { if (g) cudaGraphDestroy(g); ctx->cur = saved; return rc; }
+    if (e != cudaSuccess) { ctx->last_cuda_err = (int)e; ctx->cur = saved; return MF_ERR_CUDA; }
+    e = cudaGraphInstantiate(&ctx->graph[k], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { ctx->last_cuda_err = (int)e; ctx->cur = saved; return MF_ERR_CUDA; }
+  }
+  ctx->cur = saved;
+  ctx->graph_valid = true;
+  return MF_OK;
+}
+
+// field storage: 0 current set, 1 position-indexed array, 2 derived
+struct field_desc {
+  int width;
+  bool is_int;
+};
+field_desc describe(int f) {
+  switch (f) {
+    case MF_FIELD_POS: case MF_FIELD_VEL: case MF_FIELD_FC: case MF_FIELD_FT: case MF_FIELD_N:
+    case MF_FIELD_POS_T: case MF_FIELD_VEL_T:
+      return {2, false};
+    case MF_FIELD_S: case MF_FIELD_R: case MF_FIELD_S_T: case MF_FIELD_S_DER: case MF_FIELD_V_DER:
+      return {4, false};
+    case MF_FIELD_IDX: case MF_FIELD_HASH:
+      return {1, true};
+    default:
+      return {1, false};
+  }
+}
+
+int view_set(const mf_ctx *ctx) { return ctx->mid_step ? (ctx->cur ^ 1) : ctx->cur; }
+
+void *field_ptr(mf_ctx *ctx, int f) {
+  state_set &s = ctx->set[view_set(ctx)];
+  switch (f) {
+    case MF_FIELD_POS: return s.pos;
+    case MF_FIELD_VEL: return s.vel;
+    case MF_FIELD_H: return s.h;
+    case MF_FIELD_RHO: return s.rho;
+    case MF_FIELD_P: return ctx->D.pp;
+    case MF_FIELD_S: return s.S;
+    case MF_FIELD_FC: return s.fc;
+    case MF_FIELD_FT: return s.ft;
+    case MF_FIELD_N: return ctx->D.n;
+    case MF_FIELD_EPS_PL: return s.eps_pl;
+    case MF_FIELD_EPS_PL_DOT: return s.eps_pl_dot;
+    case MF_FIELD_T: return s.T;
+    case MF_FIELD_POS_T: return s.pos_t;
+    case MF_FIELD_VEL_T: return s.vel_t;
+    case MF_FIELD_RHO_T: return s.rho_t;
+    case MF_FIELD_S_T: return s.S_t;
+    case MF_FIELD_T_T: return s.T_t;
+    case MF_FIELD_S_DER: return ctx->D.S_der;
+    case MF_FIELD_V_DER: return ctx->D.v_der;
+    case MF_FIELD_IDX: return s.idx;
+    case MF_FIELD_HASH: return ctx->D.hash_cur;
+    default: return nullptr;
+  }
+}
+
+unsigned flag_bit(int f) {
+  return f == MF_FIELD_FIXED ? FLAG_FIXED : f == MF_FIELD_BLANKED ? FLAG_BLANKED : f == MF_FIELD_TOOL ? FLAG_TOOL : 0u;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mf_version(void) { return MF_ABI_VERSION; }
+
+const char *mf_error_string(int code) {
+  switch (code) {
+    case MF_OK: return "ok";
+    case MF_ERR_INVALID: return "invalid argument";
+    case MF_ERR_CUDA: return "CUDA runtime error";
+    case MF_ERR_STATE: return "call out of order";
+    case MF_ERR_RANGE: return "size out of range";
+    case MF_ERR_NOMEM: return "out of memory";
+    case MF_ERR_NO_DEVICE: return "no CUDA device";
+    case MF_ERR_DEVICE_FAULT: return "a kernel reported an internal error";
+    default: return "unknown error";
+  }
+}
+
+int mf_last_cuda_error(const mf_ctx *ctx) { return ctx ? ctx->last_cuda_err : 0; }
+
+int mf_ctx_create(int device, mf_ctx **out) {
+  if (!out) return MF_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) return MF_ERR_NO_DEVICE;
+  if (device < 0 || device >= count) return MF_ERR_INVALID;
+  mf_ctx *ctx = new (std::nothrow) mf_ctx;
+  if (!ctx) return MF_ERR_NOMEM;
+  ctx->device = device;
+  int rc = set_device(ctx);
+  if (rc == MF_OK) {
+    cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) rc = MF_ERR_CUDA;
+  }
+  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.g, 1);
+  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.st, 1);
+  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.tool, 1);
+  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.ticket, 4);
+  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.scan_done, 1);
+  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.force_log, (size_t)FORCE_LOG_CAP * 2);
+  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.force_last, 2);
+  if (rc != MF_OK) { mf_ctx_destroy(ctx); return rc; }
+  ctx->P.corr.wdeltap = 1.;  // make_corr_constants (constants_structs.cpp:31-35)
+  *out = ctx;
+  return MF_OK;
+}
+
+int mf_ctx_destroy(mf_ctx *ctx) {
+  if (!ctx) return MF_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  drop_graphs(ctx);
+  free_list(ctx->particle_allocs);
+  free_list(ctx->grid_allocs);
+  free_list(ctx->fixed_allocs);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return MF_OK;
+}
+
+int mf_ctx_stream(mf_ctx *ctx, void **stream) {
+  if (!ctx || !stream) return MF_ERR_INVALID;
+  *stream = (void *)ctx->stream;
+  return MF_OK;
+}
+
+int mf_set_flags(mf_ctx *ctx, int flags) {
+  if (!ctx) return MF_ERR_INVALID;
+  ctx->flags = flags;
+  ctx->P.keep_derivs = (flags & MF_OPT_KEEP_DERIVATIVES) ? 1 : 0;
+  drop_graphs(ctx);
+  return MF_OK;
+}
+
+int mf_synchronize(mf_ctx *ctx) {
+  if (!ctx) return MF_ERR_INVALID;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_particles_create(mf_ctx *ctx, int N, const double *pos, const double *vel, const double *rho, const double *T,
+                        const double *h, const double *fixed, const double *tool_p, const double *S) {
+  if (!ctx || N <= 0 || !pos || !vel || !rho || !h) return MF_ERR_INVALID;
+  for (const double *fl : {fixed, tool_p})
+    if (fl)
+      for (int i = 0; i < N; ++i)
+        if (!(fl[i] == 0. || fl[i] == 1.)) return MF_ERR_INVALID;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  TRY(alloc_particles(ctx, N));
+  ctx->cur = 0;
+  state_set &s = ctx->set[0];
+  CK(cudaMemcpy(s.pos, pos, sizeof(double) * 2 * (size_t)N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s.vel, vel, sizeof(double) * 2 * (size_t)N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s.rho, rho, sizeof(double) * (size_t)N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s.h, h, sizeof(double) * (size_t)N, cudaMemcpyHostToDevice));
+  if (T) CK(cudaMemcpy(s.T, T, sizeof(double) * (size_t)N, cudaMemcpyHostToDevice));
+  if (S) CK(cudaMemcpy(s.S, S, sizeof(double) * 4 * (size_t)N, cudaMemcpyHostToDevice));
+  std::vector<unsigned> fl((size_t)N, 0u);
+  std::vector<int> idx((size_t)N);
+  for (int i = 0; i < N; ++i) {
+    if (fixed && fixed[i] == 1.) fl[i] |= FLAG_FIXED;
+    if (tool_p && tool_p[i] == 1.) fl[i] |= FLAG_TOOL;
+    idx[i] = i;  // particle_gpu.cu:53-54
+  }
+  CK(cudaMemcpy(s.flags, fl.data(), sizeof(unsigned) * (size_t)N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s.idx, idx.data(), sizeof(int) * (size_t)N, cudaMemcpyHostToDevice));
+  ctx->has_particles = true;
+  ctx->P.N = N;
+  return MF_OK;
+}
+
+int mf_particles_count(const mf_ctx *ctx, int *N) {
+  if (!ctx || !N) return MF_ERR_INVALID;
+  *N = ctx->has_particles ? ctx->N : 0;
+  return MF_OK;
+}
+
+int mf_get_field(mf_ctx *ctx, int field, void *host) {
+  if (!ctx || !host || field < 0 || field >= MF_NUM_FIELDS) return MF_ERR_INVALID;
+  if (!ctx->has_particles) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const size_t N = (size_t)ctx->N;
+  unsigned bit = flag_bit(field);
+  if (bit) {
+    std::vector<unsigned> fl(N);
+    CK(cudaMemcpy(fl.data(), ctx->set[view_set(ctx)].flags, sizeof(unsigned) * N, cudaMemcpyDeviceToHost));
+    double *o = (double *)host;
+    for (size_t i = 0; i < N; ++i) o[i] = (fl[i] & bit) ? 1. : 0.;
+    return MF_OK;
+  }
+  if (field == MF_FIELD_R) {
+    std::vector<double> rec(N * R_WIDTH);
+    CK(cudaMemcpy(rec.data(), ctx->D.rec, sizeof(double) * N * R_WIDTH, cudaMemcpyDeviceToHost));
+    double *o = (double *)host;
+    for (size_t i = 0; i < N; ++i) {
+      o[4 * i] = rec[i * R_WIDTH + R_RXX];
+      o[4 * i + 1] = rec[i * R_WIDTH + R_RXY];
+      o[4 * i + 2] = rec[i * R_WIDTH + R_RYY];
+      o[4 * i + 3] = 0.;
+    }
+    return MF_OK;
+  }
+  field_desc d = describe(field);
+  void *src = field_ptr(ctx, field);
+  if (!src) return MF_ERR_INVALID;
+  size_t bytes = N * d.width * (d.is_int ? sizeof(int) : sizeof(double));
+  CK(cudaMemcpy(host, src, bytes, cudaMemcpyDeviceToHost));
+  return MF_OK;
+}
+
+int mf_set_field(mf_ctx *ctx, int field, const void *host) {
+  if (!ctx || !host || field < 0 || field >= MF_NUM_FIELDS) return MF_ERR_INVALID;
+  if (!ctx->has_particles) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const size_t N = (size_t)ctx->N;
+  unsigned bit = flag_bit(field);
+  if (bit) {
+    const double *in = (const double *)host;
+    for (size_t i = 0; i < N; ++i)
+      if (!(in[i] == 0. || in[i] == 1.)) return MF_ERR_INVALID;
+    std::vector<unsigned> fl(N);
+    CK(cudaMemcpy(fl.data(), ctx->set[ctx->cur].flags, sizeof(unsigned) * N, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < N; ++i) fl[i] = in[i] == 1. ? (fl[i] | bit) : (fl[i] & ~bit);
+    CK(cudaMemcpy(ctx->set[ctx->cur].flags, fl.data(), sizeof(unsigned) * N, cudaMemcpyHostToDevice));
+    return MF_OK;
+  }
+  if (field == MF_FIELD_R) return MF_ERR_INVALID;  // recomputed every step
+  field_desc d = describe(field);
+  void *dst = field_ptr(ctx, field);
+  if (!dst) return MF_ERR_INVALID;
+  size_t bytes = N * d.width * (d.is_int ? sizeof(int) : sizeof(double));
+  CK(cudaMemcpy(dst, host, bytes, cudaMemcpyHostToDevice));
+  return MF_OK;
+}
+
+int mf_grid_create_locked(mf_ctx *ctx, int kind, double bbmin_x, double bbmin_y, double bbmax_x, double bbmax_y,
+                          double h) {
+  if (!ctx || (kind != MF_GRID_GREEN && kind != MF_GRID_ROTHLIN) || !(h > 0.)) return MF_ERR_INVALID;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  // grid_base::set_geometry (grid.cu:139-158)
+  geom G{};
+  G.bbmin_x = bbmin_x - 1e-6;
+  G.bbmin_y = bbmin_y - 1e-6;
+  G.bbmax_x = bbmax_x + 1e-6;
+  G.bbmax_y = bbmax_y + 1e-6;
+  double kernel_width = 2.;
+  G.dx = h * kernel_width / 2.;
+  double lx = G.bbmax_x - G.bbmin_x, ly = G.bbmax_y - G.bbmin_y;
+  double fnx = std::ceil(lx / G.dx), fny = std::ceil(ly / G.dx);
+  if (!(fnx >= 1. && fny >= 1.) || fnx * fny > 2.0e9) return MF_ERR_RANGE;
+  G.nx = (int)(unsigned)fnx;
+  G.ny = (int)(unsigned)fny;
+  G.num_cell = G.nx * G.ny;
+  G.max_cell = G.num_cell;
+  G.locked = 1;
+  TRY(alloc_grid(ctx, G.max_cell));
+  ctx->G = G;
+  ctx->grid_kind = kind;
+  ctx->P.grid_kind = kind;
+  ctx->has_grid = true;
+  TRY(upload_geom(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_grid_create_adaptive(mf_ctx *ctx, int kind, int max_cell) {
+  if (!ctx || (kind != MF_GRID_GREEN && kind != MF_GRID_ROTHLIN) || max_cell < 2) return MF_ERR_INVALID;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  geom G{};
+  G.nx = 1; G.ny = 1; G.num_cell = 1; G.max_cell = max_cell; G.dx = 1.; G.locked = 0;
+  TRY(alloc_grid(ctx, max_cell));
+  ctx->G = G;
+  ctx->grid_kind = kind;
+  ctx->P.grid_kind = kind;
+  ctx->has_grid = true;
+  TRY(upload_geom(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_grid_geometry(mf_ctx *ctx, int *nx, int *ny, int *num_cell, double *out5) {
+  if (!ctx) return MF_ERR_INVALID;
+  if (!ctx->has_grid) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  geom G;
+  CK(cudaMemcpy(&G, ctx->D.g, sizeof(geom), cudaMemcpyDeviceToHost));
+  if (nx) *nx = G.nx;
+  if (ny) *ny = G.ny;
+  if (num_cell) *num_cell = G.num_cell;
+  if (out5) { out5[0] = G.bbmin_x; out5[1] = G.bbmin_y; out5[2] = G.bbmax_x; out5[3] = G.bbmax_y; out5[4] = G.dx; }
+  return MF_OK;
+}
+
+int mf_grid_build(mf_ctx *ctx) {
+  if (!ctx) return MF_ERR_INVALID;
+  if (!ctx->has_particles || !ctx->has_grid || ctx->mid_step) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  ctx->P.N = ctx->N;
+  TRY(launch_cells(ctx, false));
+  const int nb = (ctx->N + BLOCK - 1) / BLOCK;
+  k_reorder<false, false><<<nb, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { ctx->last_cuda_err = (int)e; return MF_ERR_CUDA; }
+  ctx->cur ^= 1;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_grid_get_cells(mf_ctx *ctx, int *start, int *end) {
+  if (!ctx || !start || !end) return MF_ERR_INVALID;
+  if (!ctx->has_grid) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  geom G;
+  CK(cudaMemcpy(&G, ctx->D.g, sizeof(geom), cudaMemcpyDeviceToHost));
+  std::vector<int> off((size_t)G.num_cell + 1);
+  CK(cudaMemcpy(off.data(), ctx->D.off, sizeof(int) * off.size(), cudaMemcpyDeviceToHost));
+  for (int c = 0; c < G.num_cell; ++c) {
+    if (ctx->grid_kind == MF_GRID_ROTHLIN) {
+      start[c] = off[c];
+      end[c] = off[c + 1];
+    } else if (off[c + 1] > off[c]) {
+      start[c] = off[c];
+      end[c] = off[c + 1];
+    } else {
+      start[c] = -1;
+      end[c] = -1;
+    }
+  }
+  return MF_OK;
+}
+
+int mf_set_constants(mf_ctx *ctx, const mf_phys_constants *phys, const mf_corr_constants *corr,
+                     const mf_joco_constants *joco, const mf_trml_constants *trml_wp,
+                     const mf_trml_constants *trml_tool) {
+  if (!ctx || !phys || !corr) return MF_ERR_INVALID;
+  params &P = ctx->P;
+  P.phys = *phys;
+  P.corr = *corr;
+  P.plastic = joco ? 1 : 0;
+  if (joco) P.joco = *joco;
+  else std::memset(&P.joco, 0, sizeof(P.joco));
+  std::memset(&P.trml_wp, 0, sizeof(P.trml_wp));
+  std::memset(&P.trml_tool, 0, sizeof(P.trml_tool));
+  if (trml_wp) P.trml_wp = *trml_wp;
+  if (trml_tool) P.trml_tool = *trml_tool;
+  P.fric_heat = P.trml_wp.eta != 0. ? 1 : 0;         // actions_gpu.cu:457-460
+  P.thermal_bc = P.trml_tool.alpha != 0. ? 1 : 0;    // actions_gpu.cu:466-468
+  P.thermal_wp = P.trml_wp.alpha != 0. ? 1 : 0;      // interactions_gpu.cu:443
+  P.thermal_tool_on = P.trml_tool.alpha != 0. ? 1 : 0; // interactions_gpu.cu:453
+  ctx->has_constants = true;
+  drop_graphs(ctx);
+  return MF_OK;
+}
+
+int mf_set_options(mf_ctx *ctx, int thermal_solver, int jc_model, int precision) {
+  if (!ctx) return MF_ERR_INVALID;
+  if (thermal_solver != MF_THERMAL_BROOKSHAW && thermal_solver != MF_THERMAL_PSE) return MF_ERR_INVALID;
+  if (jc_model != MF_JC_JOHNSON_COOK && jc_model != MF_JC_TANH) return MF_ERR_INVALID;
+  if (precision != MF_PRECISION_FP64 && precision != MF_PRECISION_MIXED) return MF_ERR_INVALID;
+  ctx->P.thermal_solver = thermal_solver;
+  ctx->P.jc_model = jc_model;
+  ctx->P.precision = precision;
+  drop_graphs(ctx);
+  return MF_OK;
+}
+
+int mf_set_dt(mf_ctx *ctx, double dt) {
+  if (!ctx || !(dt > 0.) || !std::isfinite(dt)) return MF_ERR_INVALID;
+  ctx->P.dt = dt;
+  drop_graphs(ctx);
+  return MF_OK;
+}
+
+int mf_tool_set(mf_ctx *ctx, const mf_tool_state *tool) {
+  if (!ctx) return MF_ERR_INVALID;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  mf_tool_state t;
+  std::memset(&t, 0, sizeof(t));
+  if (tool) {
+    if (tool->num_seg < 0 || tool->num_seg > 5 || tool->num_seg == 1 || tool->num_seg == 2 || tool->num_seg == 3)
+      if (tool->num_seg != 0) return MF_ERR_INVALID;
+    t = *tool;
+  }
+  ctx->tool = t;
+  ctx->P.has_tool = t.num_seg > 0 ? 1 : 0;
+  CK(cudaMemcpy(ctx->D.tool, &t, sizeof(t), cudaMemcpyHostToDevice));
+  drop_graphs(ctx);
+  return MF_OK;
+}
+
+int mf_tool_get(mf_ctx *ctx, mf_tool_state *tool) {
+  if (!ctx || !tool) return MF_ERR_INVALID;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy(tool, ctx->D.tool, sizeof(*tool), cudaMemcpyDeviceToHost));
+  return MF_OK;
+}
+
+int mf_step(mf_ctx *ctx, int n_steps) {
+  if (!ctx || n_steps < 0) return MF_ERR_INVALID;
+  if (!ready(ctx)) return MF_ERR_STATE;
+  if (!(ctx->P.dt > 0.) || ctx->mid_step) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  ctx->P.N = ctx->N;
+  const bool graphs = !(ctx->flags & MF_OPT_NO_GRAPHS);
+  if (graphs && !ctx->graph_valid) TRY(build_graphs(ctx));
+  for (int k = 0; k < n_steps; ++k) {
+    if (graphs) {
+      CK(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
+    } else {
+      TRY(launch_step(ctx));
+    }
+    ctx->cur ^= 1;
+    ctx->steps++;
+  }
+  return MF_OK;
+}
+
+int mf_step_stage(mf_ctx *ctx, int stage) {
+  if (!ctx || stage < 0 || stage > 3) return MF_ERR_INVALID;
+  if (!ready(ctx)) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  ctx->P.N = ctx->N;
+  // stages 1..2 leave the half-built step in the other buffer; reads during the step see it
+  if (stage == 0 && ctx->mid_step) return MF_ERR_STATE;
+  TRY(launch_stage(ctx, stage));
+  if (stage == 1) ctx->mid_step = true;
+  if (stage == 3) {
+    ctx->cur ^= 1;
+    ctx->steps++;
+    ctx->mid_step = false;
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_report_force(mf_ctx *ctx, double out[2]) {
+  if (!ctx || !out) return MF_ERR_INVALID;
+  if (!ctx->has_particles) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  state_set &s = ctx->set[ctx->cur];
+  k_force_only<<<1, BLOCK, 0, ctx->stream>>>(ctx->N, s.fc, s.ft, ctx->D);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, ctx->D.force_last, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_force_log(mf_ctx *ctx, double *out, int max_entries, int *n_out) {
+  if (!ctx || !n_out || max_entries < 0) return MF_ERR_INVALID;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  dev_status st;
+  CK(cudaMemcpy(&st, ctx->D.st, sizeof(st), cudaMemcpyDeviceToHost));
+  unsigned long long head = st.force_log_head;
+  unsigned long long first = ctx->force_read_head;
+  if (head - first > (unsigned long long)FORCE_LOG_CAP) first = head - FORCE_LOG_CAP;
+  unsigned long long n = head - first;
+  if (n > (unsigned long long)max_entries) n = (unsigned long long)max_entries;
+  if (n > 0 && out) {
+    std::vector<double> all((size_t)FORCE_LOG_CAP * 2);
+    CK(cudaMemcpy(all.data(), ctx->D.force_log, sizeof(double) * all.size(), cudaMemcpyDeviceToHost));
+    for (unsigned long long k = 0; k < n; ++k) {
+      unsigned long long slot = (first + k) % FORCE_LOG_CAP;
+      out[2 * k] = all[2 * slot];
+      out[2 * k + 1] = all[2 * slot + 1];
+    }
+  }
+  ctx->force_read_head = first + n;
+  *n_out = (int)n;
+  return MF_OK;
+}
+
+int mf_status_get(mf_ctx *ctx, mf_status *out) {
+  if (!ctx || !out) return MF_ERR_INVALID;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  dev_status st;
+  CK(cudaMemcpy(&st, ctx->D.st, sizeof(st), cudaMemcpyDeviceToHost));
+  out->steps = ctx->steps;
+  out->blanked = 0;
+  if (ctx->has_particles) {
+    std::vector<unsigned> fl((size_t)ctx->N);
+    CK(cudaMemcpy(fl.data(), ctx->set[ctx->cur].flags, sizeof(unsigned) * fl.size(), cudaMemcpyDeviceToHost));
+    long long b = 0;
+    for (unsigned f : fl) b += (f & FLAG_BLANKED) ? 1 : 0;
+    out->blanked = b;
+  }
+  out->newly_blanked = (long long)(st.newly_blanked - ctx->status_newly_blanked_seen);
+  ctx->status_newly_blanked_seen = st.newly_blanked;
+  out->out_of_grid = (long long)st.out_of_grid;
+  out->secant_cap_hits = (long long)st.secant_cap_hits;
+  out->max_cell_occupancy = st.max_cell_occupancy;
+  out->error_flags = st.error_flags;
+  return MF_OK;
+}
+
+int mf_scene_upload(mf_ctx *ctx, const mf_scene *s, int grid_kind) {
+  if (!ctx || !s) return MF_ERR_INVALID;
+  TRY(mf_particles_create(ctx, s->N, s->pos, s->vel, s->rho, s->T, s->h, s->fixed, s->tool_p, nullptr));
+  TRY(mf_grid_create_locked(ctx, grid_kind, s->grid_bbmin[0], s->grid_bbmin[1], s->grid_bbmax[0], s->grid_bbmax[1],
+                            s->grid_h));
+  TRY(mf_set_constants(ctx, &s->phys, &s->corr, s->has_joco ? &s->joco : nullptr, &s->trml_wp, &s->trml_tool));
+  TRY(mf_tool_set(ctx, &s->tool));
+  TRY(mf_set_dt(ctx, s->dt));
+  return MF_OK;
+}
+
+// vtk_writer_write(const particle_gpu*, int) (vtk_writer.cpp:20-178): the unblanked particles
+int mf_vtk_write_particles(mf_ctx *ctx, const char *path) {
+  if (!ctx || !path) return MF_ERR_INVALID;
+  if (!ctx->has_particles) return MF_ERR_STATE;
+  const int n = ctx->N;
+  std::vector<double> pos(2 * (size_t)n), vel(2 * (size_t)n), rho(n), p(n), T(n), eps(n), S(4 * (size_t)n), fixed(n),
+      blanked(n), tool(n);
+  TRY(mf_get_field(ctx, MF_FIELD_POS, pos.data()));
+  TRY(mf_get_field(ctx, MF_FIELD_VEL, vel.data()));
+  TRY(mf_get_field(ctx, MF_FIELD_RHO, rho.data()));
+  TRY(mf_get_field(ctx, MF_FIELD_P, p.data()));
+  TRY(mf_get_field(ctx, MF_FIELD_T, T.data()));
+  TRY(mf_get_field(ctx, MF_FIELD_EPS_PL, eps.data()));
+  TRY(mf_get_field(ctx, MF_FIELD_S, S.data()));
+  TRY(mf_get_field(ctx, MF_FIELD_FIXED, fixed.data()));
+  TRY(mf_get_field(ctx, MF_FIELD_BLANKED, blanked.data()));
+  TRY(mf_get_field(ctx, MF_FIELD_TOOL, tool.data()));
+  FILE *fp = std::fopen(path, "w+");
+  if (!fp) return MF_ERR_INVALID;
+  int m = 0;
+  for (int i = 0; i < n; ++i) m += blanked[i] != 1.;
+  std::fprintf(fp, "# vtk DataFile Version 2.0\nmfree iwf\nASCII\n\nDATASET UNSTRUCTURED_GRID\n");
+  std::fprintf(fp, "POINTS %d float\n", m);
+  for (int i = 0; i < n; ++i) if (blanked[i] != 1.) std::fprintf(fp, "%f %f %f\n", pos[2 * i], pos[2 * i + 1], 0.);
+  std::fprintf(fp, "\nCELLS %d %d\n", m, 2 * m);
+  for (int i = 0; i < n; ++i) if (blanked[i] != 1.) std::fprintf(fp, "%d %d\n", 1, i);
+  std::fprintf(fp, "\nCELL_TYPES %d\n", m);
+  for (int i = 0; i < n; ++i) if (blanked[i] != 1.) std::fprintf(fp, "%d\n", 1);
+  std::fprintf(fp, "\nPOINT_DATA %d\n", m);
+  auto scalars = [&](const char *name, const std::vector<double> &v) {
+    std::fprintf(fp, "SCALARS %s float 1\nLOOKUP_TABLE default\n", name);
+    for (int i = 0; i < n; ++i) if (blanked[i] != 1.) std::fprintf(fp, "%f\n", v[i]);
+    std::fprintf(fp, "\n");
+  };
+  scalars("density", rho);
+  scalars("Temperature", T);
+  scalars("Fixed", fixed);
+  scalars("Tool", tool);
+  scalars("EquivAccumPlasticStrain", eps);
+  std::fprintf(fp, "VECTORS Velocity float\n");
+  for (int i = 0; i < n; ++i) if (blanked[i] != 1.) std::fprintf(fp, "%f %f %f\n", vel[2 * i], vel[2 * i + 1], 0.);
+  std::fprintf(fp, "\nSCALARS SvM float 1\nLOOKUP_TABLE default\n");
+  for (int i = 0; i < n; ++i) {
+    if (blanked[i] == 1.) continue;
+    double cxx = S[4 * i] - p[i], cyy = S[4 * i + 2] - p[i], czz = S[4 * i + 3] - p[i], cxy = S[4 * i + 1];
+    double svm2 = (cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy;
+    std::fprintf(fp, "%f\n", svm2 > 0 ? std::sqrt(svm2) : 0.);
+  }
+  std::fprintf(fp, "\n");
+  std::fclose(fp);
+  return MF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,835 @@
+// sm_100a kernels of one leap-frog step (leap_frog.cu:94-155).
+//
+// Per step, on one stream (captured once into a CUDA graph):
+//   k_bbox        adaptive grid only: min/max reduction -> geometry     (grid.cu:97-136)
+//   k_hash_count  cell hash per particle + atomic per-cell count;       (grid.cu:34-51)
+//                 block 0 also advances the rigid tool                  (tool.cpp:211-221)
+//   k_scan        single-pass decoupled look-back exclusive scan of the
+//                 counts -> cell offsets (the cell_start/cell_end lists)
+//   k_scatter     particle -> slot inside its cell
+//   k_reorder     stable rank fix-up inside each cell (equal to thrust's stable sort_by_key),
+//                 gather of the persistent state into the other buffer, and - in a step - the
+//                 predictor, EOS, artificial stress and the neighbour pair records
+//                 (grid_gpu_green.cu:22-116, leap_frog.cu:30-66, actions_gpu.cu:41-97)
+//   k_pair_fp64   the pair sums over the 5x5 cell window (interactions_gpu.cu:147-345) and the
+//                 rates: Jaumann, continuity, momentum, advection (actions_gpu.cu:99-224)
+//   k_pse         PSE heat Laplacian (interactions_gpu.cu:88-144), PSE solver only
+//   k_finish      corrector, friction heat, JC plasticity, tool particles, contact, boundary
+//                 conditions, invalidation and the compensated tool-force reduction
+//                 (leap_frog.cu:68-92, actions_gpu.cu:135-162,226-349, tool_gpu.cu:151-221,
+//                 output.cu:31-39)
+#pragma once
+
+#include "mf_device.cuh"
+
+namespace mf {
+
+struct state_set {
+  double2 *pos, *vel, *fc, *ft, *pos_t, *vel_t;
+  double *rho, *T, *eps_pl, *eps_pl_dot, *h, *rho_t, *T_t;
+  double4 *S, *S_t;
+  unsigned *flags;
+  int *idx;
+};
+
+struct dev_buffers {
+  state_set A, B;       // A: state at the start of the step (previous order), B: new order
+  double2 *n;           // contact normal, indexed by array position (never permuted)
+  double *rec;          // FP64 pair records, R_WIDTH doubles per particle
+  float *recf;          // FP32 pair records (mixed form), F_WIDTH floats per particle
+  double *pp;           // predictor pressure (the reference's particles->p)
+  double4 *S_der, *v_der;
+  int *hash_cur;        // cell hash per array position (sorted order)
+  int *hash_new, *slot, *perm_u, *perm;
+  int *count;           // per-cell counts (max_cell)
+  int *off;             // cell offsets (max_cell + 1)
+  unsigned long long *scan_status;
+  unsigned *scan_done;
+  double *partials;     // per-block partial sums (force / bbox)
+  unsigned *ticket;     // last-block tickets: [0] force, [1] bbox
+  double *force_log;    // FORCE_LOG_CAP x 2
+  double *force_last;   // 2
+  mf_tool_state *tool;
+  geom *g;
+  dev_status *st;
+};
+
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+constexpr int BLOCK = 256;
+constexpr int PAIR_BLOCK = 128;
+constexpr unsigned long long SCAN_FLAG_AGG = 1ull << 62;
+constexpr unsigned long long SCAN_FLAG_PREFIX = 2ull << 62;
+constexpr long long SCAN_SPIN_LIMIT = 1ll << 24;
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+// ---------------------------------------------------------------------------------------
+// adaptive geometry (grid_base::update_geometry, grid.cu:97-136)
+__device__ __forceinline__ void bbox_merge(double *a, const double *b) {
+  a[0] = fmin(a[0], b[0]);
+  a[1] = fmin(a[1], b[1]);
+  a[2] = fmax(a[2], b[2]);
+  a[3] = fmax(a[3], b[3]);
+  a[4] = fmax(a[4], b[4]);
+}
+
+__global__ void __launch_bounds__(BLOCK) k_bbox(int N, const double2 *__restrict__ pos,
+                                                const double *__restrict__ h, dev_buffers D) {
+  __shared__ double sm[BLOCK / 32][5];
+  __shared__ bool last;
+  const double BIG = 1.7976931348623157e+308;
+  double v[5] = {BIG, BIG, -BIG, -BIG, -BIG};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    double2 p = pos[i];
+    double hh = h[i];
+    if (isfinite(p.x)) { v[0] = fmin(v[0], p.x); v[2] = fmax(v[2], p.x); }
+    if (isfinite(p.y)) { v[1] = fmin(v[1], p.y); v[3] = fmax(v[3], p.y); }
+    if (isfinite(hh)) v[4] = fmax(v[4], hh);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    double w[5];
+    for (int k = 0; k < 5; ++k) w[k] = __shfl_down_sync(0xffffffffu, v[k], o);
+    bbox_merge(v, w);
+  }
+  if (lane_id() == 0)
+    for (int k = 0; k < 5; ++k) sm[threadIdx.x >> 5][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) bbox_merge(v, sm[w]);
+    for (int k = 0; k < 5; ++k) D.partials[blockIdx.x * 8 + k] = v[k];
+    __threadfence();
+    unsigned t = atomicAdd(&D.ticket[1], 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  double r[5] = {BIG, BIG, -BIG, -BIG, -BIG};
+  for (unsigned b = 0; b < gridDim.x; ++b) {
+    double w[5];
+    for (int k = 0; k < 5; ++k) w[k] = ((volatile double *)D.partials)[b * 8 + k];
+    bbox_merge(r, w);
+  }
+  D.ticket[1] = 0;
+  geom g = *D.g;
+  double bbmin_x = r[0] - 1e-6, bbmin_y = r[1] - 1e-6, bbmax_x = r[2] + 1e-6, bbmax_y = r[3] + 1e-6;
+  double dx = r[4] * 2.0 / 2;
+  double lx = bbmax_x - bbmin_x, ly = bbmax_y - bbmin_y;
+  unsigned nx = (unsigned)ceil(lx / dx), ny = (unsigned)ceil(ly / dx);
+  unsigned long long nc = (unsigned long long)nx * ny;
+  if (!(N > 0) || !(dx > 0.) || !(nc < (unsigned long long)g.max_cell)) {
+    atomicOr(&D.st->error_flags, ERR_GRID_BUDGET);
+    return;  // keep the previous geometry; out-of-range hashes are clamped and counted
+  }
+  g.bbmin_x = bbmin_x; g.bbmin_y = bbmin_y; g.bbmax_x = bbmax_x; g.bbmax_y = bbmax_y;
+  g.dx = dx; g.nx = (int)nx; g.ny = (int)ny; g.num_cell = (int)nc;
+  *D.g = g;
+}
+
+// ---------------------------------------------------------------------------------------
+// cell hash + count (compute_hashes, grid.cu:34-51)
+__global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A, dev_buffers D, int num_scan_tiles,
+                                                      int advance_tool, double dt) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (advance_tool && gid == 0) {
+    mf_tool_state T = *D.tool;
+    tool_translate_rn(T, dt);
+    *D.tool = T;
+  }
+  for (int t = gid; t < num_scan_tiles; t += gridDim.x * blockDim.x) D.scan_status[t] = 0ull;
+  unsigned oog = 0;
+  if (gid < N) {
+    const geom g = *D.g;
+    int hsh;
+    if (A.flags[gid] & FLAG_BLANKED) {
+      hsh = D.hash_cur[gid];  // blanked particles keep their previous hash (grid.cu:39-41)
+    } else {
+      double2 p = A.pos[gid];
+      int ix = __double2int_rz((p.x - g.bbmin_x) / g.dx);
+      int iy = __double2int_rz((p.y - g.bbmin_y) / g.dx);
+      long long hh = (long long)ix * (long long)g.ny + (long long)iy;
+      if (hh < 0) { hh = 0; oog = 1; }
+      else if (hh >= g.num_cell) { hh = g.num_cell - 1; oog = 1; }
+      hsh = (int)hh;
+    }
+    D.hash_new[gid] = hsh;
+    D.slot[gid] = atomicAdd(&D.count[hsh], 1);
+  }
+  unsigned any = __ballot_sync(0xffffffffu, oog);
+  if (any && lane_id() == 0) atomicAdd(&D.st->out_of_grid, (unsigned long long)__popc(any));
+}
+
+// ---------------------------------------------------------------------------------------
+// exclusive scan of the cell counts -> offsets, single pass with decoupled look-back.
+// Tile ids come from an atomic ticket, so every tile waits only on tiles that are already
+// running; the wait is bounded and reports ERR_SCAN_WAIT instead of hanging.
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int N) {
+  __shared__ int s_tile;
+  __shared__ int s_warp[SCAN_THREADS / 32];
+  __shared__ int s_excl;
+  __shared__ int s_max[SCAN_THREADS / 32];
+  const int num_cell = D.g->num_cell;
+  const int num_tiles = (num_cell + SCAN_TILE - 1) / SCAN_TILE;
+  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&D.st->scan_tile_counter, 1u);
+  __syncthreads();
+  const int tile = s_tile;
+  if (tile < num_tiles) {
+    const int base = tile * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    int tsum = 0, tmax = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      int c = base + k;
+      int x = c < num_cell ? D.count[c] : 0;
+      v[k] = tsum;
+      tsum += x;
+      tmax = max(tmax, x);
+    }
+    // warp inclusive scan of thread sums
+    int incl = tsum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if ((int)lane_id() >= o) incl += y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tmax = max(tmax, __shfl_down_sync(0xffffffffu, tmax, o));
+    if (lane_id() == 31) s_warp[threadIdx.x >> 5] = incl;
+    if (lane_id() == 0) s_max[threadIdx.x >> 5] = tmax;
+    __syncthreads();
+    int warp_excl = 0, agg = 0, bmax = 0;
+    for (int w = 0; w < SCAN_THREADS / 32; ++w) {
+      if (w < (int)(threadIdx.x >> 5)) warp_excl += s_warp[w];
+      agg += s_warp[w];
+      bmax = max(bmax, s_max[w]);
+    }
+    const int thread_excl = warp_excl + incl - tsum;
+    if (threadIdx.x == 0) {
+      if (bmax > 0) atomicMax(&D.st->max_cell_occupancy, bmax);
+      int excl = 0;
+      if (tile == 0) {
+        atomicExch(&D.scan_status[0], SCAN_FLAG_PREFIX | (unsigned long long)(unsigned)agg);
+      } else {
+        atomicExch(&D.scan_status[tile], SCAN_FLAG_AGG | (unsigned long long)(unsigned)agg);
+        int t = tile - 1;
+        long long spins = 0;
+        while (t >= 0) {
+          unsigned long long w = *((volatile unsigned long long *)&D.scan_status[t]);
+          unsigned long long flag = w & (3ull << 62);
+          if (flag == 0ull) {
+            if (++spins > SCAN_SPIN_LIMIT) {
+              atomicOr(&D.st->error_flags, ERR_SCAN_WAIT);
+              break;
+            }
+            continue;
+          }
+          excl += (int)(unsigned)(w & 0xffffffffull);
+          if (flag == SCAN_FLAG_PREFIX) break;
+          --t;
+        }
+        atomicExch(&D.scan_status[tile], SCAN_FLAG_PREFIX | (unsigned long long)(unsigned)(excl + agg));
+      }
+      s_excl = excl;
+    }
+    __syncthreads();
+    const int excl = s_excl + thread_excl;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      int c = base + k;
+      if (c < num_cell) {
+        D.off[c] = excl + v[k];
+        D.count[c] = 0;  // ready for the next step
+      }
+    }
+    if (tile == num_tiles - 1 && threadIdx.x == 0) D.off[num_cell] = s_excl + agg;
+  }
+  // the last block to finish re-arms the tile ticket
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned d = atomicAdd(D.scan_done, 1u);
+    if (d == gridDim.x - 1) {
+      D.st->scan_tile_counter = 0u;
+      *D.scan_done = 0u;
+    }
+  }
+  (void)N;
+}
+
+__global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  D.perm_u[D.off[D.hash_new[q]] + D.slot[q]] = q;
+}
+
+// ---------------------------------------------------------------------------------------
+// stable rank fix-up: inside a cell, the atomics gave the members in arbitrary order; the
+// stable sort wants them by previous array position. Position q of the sorted order holds
+// the member with exactly (q - cell_start) smaller previous positions.
+__device__ __forceinline__ int stable_member(const dev_buffers &D, int q) {
+  const int pu = D.perm_u[q];
+  const int c = D.hash_new[pu];
+  const int s = D.off[c], e = D.off[c + 1];
+  if (e - s == 1) return pu;
+  const int k = q - s;
+  for (int m = s; m < e; ++m) {
+    const int v = D.perm_u[m];
+    int less = 0;
+    for (int m2 = s; m2 < e; ++m2) less += D.perm_u[m2] < v;
+    if (less == k) return v;
+  }
+  return pu;  // unreachable for a consistent cell list
+}
+
+// gather into the new order (grid_gpu_green.cu:22-116) and, if PREDICT, the predictor
+// (leap_frog.cu:30-66), EOS (actions_gpu.cu:41-51), artificial stress (:53-97) and the
+// neighbour records read by the pair kernel.
+template <bool PREDICT, bool MIXED>
+__global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers D) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= P.N) return;
+  const int p = stable_member(D, q);
+  const state_set &A = D.A;
+  const state_set &B = D.B;
+  D.perm[q] = p;
+  B.idx[q] = P.grid_kind == MF_GRID_GREEN ? p : A.idx[p];
+  const int hsh = D.hash_new[p];
+  D.hash_cur[q] = hsh;
+
+  double2 pos = A.pos[p], vel = A.vel[p];
+  double4 S = A.S[p];
+  double rho = A.rho[p], T = A.T[p];
+  double2 pos_t = A.pos_t[p], vel_t = A.vel_t[p];
+  double4 S_t = A.S_t[p];
+  double rho_t = A.rho_t[p], T_t = A.T_t[p];
+  const unsigned f = A.flags[p];
+  const double h = A.h[p];
+  B.eps_pl[q] = A.eps_pl[p];
+  B.eps_pl_dot[q] = A.eps_pl_dot[p];
+  B.fc[q] = A.fc[p];
+  // the Rothlin grid does not gather ft (grid_gpu_rothlin.cu:138-250): it stays in place
+  B.ft[q] = P.grid_kind == MF_GRID_GREEN ? A.ft[p] : A.ft[q];
+  B.h[q] = h;
+  B.pos_t[q] = pos_t;
+  B.vel_t[q] = vel_t;
+  B.S_t[q] = S_t;
+  B.rho_t[q] = rho_t;
+  B.T_t[q] = T_t;
+
+  const bool blanked = f & FLAG_BLANKED;
+  const bool tool = f & FLAG_TOOL;
+  if (PREDICT && !blanked) {
+    const double dt = P.dt;
+    pos.x = pos.x + 0.5 * dt * pos_t.x;
+    pos.y = pos.y + 0.5 * dt * pos_t.y;
+    vel.x = vel.x + 0.5 * dt * vel_t.x;
+    vel.y = vel.y + 0.5 * dt * vel_t.y;
+    S.x = S.x + 0.5 * dt * S_t.x;
+    S.y = S.y + 0.5 * dt * S_t.y;
+    S.z = S.z + 0.5 * dt * S_t.z;
+    S.w = S.w + 0.5 * dt * S_t.w;
+    rho = rho + 0.5 * dt * rho_t;
+    T = T + 0.5 * dt * T_t;
+  }
+  B.pos[q] = pos;
+  B.vel[q] = vel;
+  B.S[q] = S;
+  B.rho[q] = rho;
+  B.T[q] = T;
+  B.flags[q] = f;
+  if (!PREDICT) return;
+
+  const double mass = P.phys.mass, K = P.phys.K;
+  double prs = 0., Rxx = 0., Rxy = 0., Ryy = 0.;
+  if (!tool) {
+    const double rho0 = P.phys.rho0;
+    const double c0 = (double)sqrtf((float)(K / rho0));
+    prs = c0 * c0 * (rho - rho0);
+    artificial_stress(rho, prs, S.x, S.y, S.z, P.corr.stresseps, Rxx, Rxy, Ryy);
+  }
+  D.pp[q] = prs;
+  const double rho21 = 1. / (rho * rho);
+  const double sxx = (S.x - prs) * rho21, sxy = S.y * rho21, syy = (S.z - prs) * rho21;
+  const double c = (double)sqrtf((float)(K / rho));
+  const double vol = mass / rho;
+  double r[R_WIDTH] = {pos.x, pos.y, vel.x, vel.y, sxx, sxy, syy, Rxx, Rxy, Ryy, h, rho, c, vol, T, 0.};
+  unsigned rf = f & (FLAG_BLANKED | FLAG_TOOL | FLAG_FIXED);
+  bool finite = true;
+#pragma unroll
+  for (int k = 0; k < R_FLAGS; ++k) finite = finite && isfinite(r[k]);
+  if (!finite) rf |= FLAG_NONFINITE;
+  r[R_FLAGS] = __longlong_as_double((long long)rf);
+  double2 *dst = reinterpret_cast<double2 *>(D.rec + (size_t)q * R_WIDTH);
+#pragma unroll
+  for (int k = 0; k < R_WIDTH / 2; ++k) dst[k] = make_double2(r[2 * k], r[2 * k + 1]);
+
+  if (MIXED) {
+    // FP32 record: position relative to the origin of the particle's own cell
+    const geom g = *D.g;
+    const int ci = hsh / g.ny, cj = hsh - ci * g.ny;
+    const double ox = g.bbmin_x + ci * g.dx, oy = g.bbmin_y + cj * g.dx;
+    float fr[F_WIDTH] = {(float)(pos.x - ox), (float)(pos.y - oy), (float)vel.x, (float)vel.y, (float)sxx,
+                         (float)sxy, (float)syy, (float)Rxx, (float)Rxy, (float)Ryy, (float)h, (float)rho,
+                         (float)c, (float)vol, (float)T,
+                         __int_as_float((int)(rf | ((unsigned)cj << 8)))};
+    float4 *fd = reinterpret_cast<float4 *>(D.recf + (size_t)q * F_WIDTH);
+#pragma unroll
+    for (int k = 0; k < F_WIDTH / 4; ++k) fd[k] = make_float4(fr[4 * k], fr[4 * k + 1], fr[4 * k + 2], fr[4 * k + 3]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// pair sums over the 5x5 cell window + rates, plain FP64 (interactions_gpu.cu:147-345,
+// actions_gpu.cu:99-224). With hash = ix*ny + iy, the five cells of one window column are
+// consecutive hashes, so their particles form one contiguous range of the sorted order;
+// visiting the columns in x order and each range in array order is the reference's
+// neighbour order (x-cell outer, y-cell inner, sorted order within a cell).
+__device__ __forceinline__ void load_rec(const double *__restrict__ rec, int j, double *r) {
+  const double2 *s = reinterpret_cast<const double2 *>(rec + (size_t)j * R_WIDTH);
+#pragma unroll
+  for (int k = 0; k < R_WIDTH / 2; ++k) {
+    double2 v = __ldg(s + k);
+    r[2 * k] = v.x;
+    r[2 * k + 1] = v.y;
+  }
+}
+
+__global__ void __launch_bounds__(PAIR_BLOCK) k_pair_fp64(params P, dev_buffers D) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= P.N) return;
+  const double *__restrict__ rec = D.rec;
+  double ri[R_WIDTH];
+  load_rec(rec, q, ri);
+  const unsigned fi = (unsigned)__double_as_longlong(ri[R_FLAGS]);
+  if (fi & FLAG_BLANKED) return;
+  const bool tool_i = fi & FLAG_TOOL;
+  const bool brookshaw = P.thermal_solver == MF_THERMAL_BROOKSHAW;
+  if (!brookshaw && tool_i) return;  // PSE build: tool particles return early (:160-162)
+
+  const double mass = P.phys.mass;
+  const double wdeltap = P.corr.wdeltap, alpha = P.corr.alpha, beta = P.corr.beta, eta = P.corr.eta;
+  const double eps = P.corr.xspheps;
+  double thermal_alpha = 0.;
+  if (brookshaw) thermal_alpha = !tool_i ? P.trml_wp.alpha : (P.thermal_tool_on ? P.trml_tool.alpha : 0.);
+  const bool thermal = thermal_alpha != 0.;
+
+  const double xi = ri[R_X], yi = ri[R_Y], vxi = ri[R_VX], vyi = ri[R_VY];
+  const double sxxi = ri[R_SXX], sxyi = ri[R_SXY], syyi = ri[R_SYY];
+  const double Rxxi = ri[R_RXX], Rxyi = ri[R_RXY], Ryyi = ri[R_RYY];
+  const double hi = ri[R_H], rhoi = ri[R_RHO], ci = ri[R_C];
+  const double Ti = thermal ? ri[R_T] : 0.;
+  const double h1 = 1 / hi;
+  const double fourh2 = 4 * hi * hi;
+  const bool nonfinite_i = fi & FLAG_NONFINITE;
+
+  const geom g = *D.g;
+  const int hashi = D.hash_cur[q];
+  const int gi = hashi / g.ny;
+  const int gj = hashi - gi * g.ny;
+  const int low_i = gi - 2 < 0 ? 0 : gi - 2;
+  const int low_j = gj - 2 < 0 ? 0 : gj - 2;
+  const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
+  const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
+
+  double vdx = 0., vdy = 0., vdz = 0., vdw = 0.;  // v_der
+  double sdx = 0., sdy = 0., sdz = 0., sdw = 0.;  // S_der
+  double vtx = 0., vty = 0., xtx = 0., xty = 0.;   // vel_t (AV), pos_t (XSPH)
+  double T_lapl = 0.;
+
+  for (int ii = low_i; ii < high_i; ++ii) {
+    const int j0 = __ldg(D.off + ii * g.ny + low_j);
+    const int j1 = __ldg(D.off + ii * g.ny + high_j);
+    for (int j = j0; j < j1; ++j) {
+      const double2 *sj = reinterpret_cast<const double2 *>(rec + (size_t)j * R_WIDTH);
+      const double2 fx = __ldg(sj + 7);  // T, flags (R_T, R_FLAGS)
+      const unsigned fj = (unsigned)__double_as_longlong(fx.y);
+      if (fj & FLAG_BLANKED) continue;
+      const double2 xy = __ldg(sj + 0);
+      const double xij = xi - xy.x;
+      const double yij = yi - xy.y;
+      const double rr2 = xij * xij + yij * yij;
+      const bool in_support = !(rr2 >= fourh2 || rr2 < 1e-8);
+      // Outside the support the reference adds terms multiplied by W = 0: they change no
+      // finite sum, but a NaN/Inf operand turns the sum into NaN. Skip only when finite.
+      if (!in_support && !(nonfinite_i || (fj & FLAG_NONFINITE))) continue;
+      double w = 0., w_x = 0., w_y = 0.;
+      if (in_support) cubic_spline_fp64(xij, yij, rr2, h1, w, w_x, w_y);
+      const double Tj = thermal ? fx.x : 0.;
+      const double2 v = __ldg(sj + 1);
+      const double2 s01 = __ldg(sj + 2);  // sxx, sxy
+      const double2 s2r0 = __ldg(sj + 3); // syy, Rxx
+      const double2 r12 = __ldg(sj + 4);  // Rxy, Ryy
+      const double2 hrho = __ldg(sj + 5); // h, rho
+      const double2 cvol = __ldg(sj + 6); // c, vol
+      const double rhoj = hrho.y, volj = cvol.y;
+      const bool tool_j = fj & FLAG_TOOL;
+      if (!tool_i && !tool_j) {
+        vdx += (v.x - vxi) * w_x * volj;
+        vdy += (v.x - vxi) * w_y * volj;
+        vdz += (v.y - vyi) * w_x * volj;
+        vdw += (v.y - vyi) * w_y * volj;
+        double fab = w / wdeltap;
+        fab *= fab;
+        fab *= fab;
+        const double Rx = fab * (Rxxi + s2r0.y);
+        const double Ry = fab * (Rxyi + r12.x);
+        const double Rz = fab * (Ryyi + r12.y);
+        sdx += mass * (sxxi + s01.x + Rx) * w_x;
+        sdy += mass * (sxyi + s01.y + Ry) * w_y;
+        sdz += mass * (sxyi + s01.y + Ry) * w_x;
+        sdw += mass * (syyi + s2r0.x + Rz) * w_y;
+        const double vijx = vxi - v.x;
+        const double vijy = vyi - v.y;
+        const double vijposij = vijx * xij + vijy * yij;
+        const double rhoij = 0.5 * (rhoi + rhoj);
+        if (vijposij < 0.) {
+          const double cij = 0.5 * (ci + cvol.x);
+          const double hij = 0.5 * (hi + hrho.x);
+          const double muij = (hij * vijposij) / (rr2 + eta * eta * hij * hij);
+          const double piij = (-alpha * cij * muij + beta * muij * muij) / rhoij;
+          vtx += -mass * piij * w_x;
+          vty += -mass * piij * w_y;
+        }
+        xtx += -eps * w * mass / rhoij * vijx;
+        xty += -eps * w * mass / rhoij * vijy;
+      }
+      if (thermal) {
+        const double rij = sqrt(rr2);
+        if (rij > 1e-8) {
+          const double eijx = xij / rij;
+          const double eijy = yij / rij;
+          const double rij1 = 1. / rij;
+          T_lapl += 2.0 * volj * (Ti - Tj) * rij1 * (eijx * w_x + eijy * w_y);
+        }
+      }
+    }
+  }
+
+  const state_set &B = D.B;
+  if (P.keep_derivs) {
+    D.S_der[q] = make_double4(sdx, sdy, sdz, sdw);
+    D.v_der[q] = make_double4(vdx, vdy, vdz, vdw);
+  }
+  if (!tool_i) {
+    const double4 S = B.S[q];  // predicted stress
+    double tx, ty, tz, tw;
+    jaumann(P.phys.G, vdx, vdy, vdz, vdw, S.x, S.y, S.z, S.w, tx, ty, tz, tw);
+    B.S_t[q] = make_double4(tx, ty, tz, tw);
+    B.rho_t[q] = -rhoi * (vdx + vdw);
+    const double2 fc = B.fc[q], ft = B.ft[q];
+    double2 vel_t;
+    vel_t.x = vtx + (sdx + sdy + fc.x / mass + ft.x / mass);
+    vel_t.y = vty + (sdz + sdw + fc.y / mass + ft.y / mass);
+    B.vel_t[q] = vel_t;
+    B.pos_t[q] = make_double2(xtx + vxi, xty + vyi);
+  } else {
+    B.vel_t[q] = make_double2(vtx, vty);
+    B.pos_t[q] = make_double2(xtx, xty);
+  }
+  if (thermal) B.T_t[q] = thermal_alpha * T_lapl;
+}
+
+// PSE heat Laplacian (interactions_gpu.cu:88-144): every particle of the window, blanked
+// ones included; alpha taken through the reference's half-length texture binding (:405).
+__global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers D) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= P.N) return;
+  const double *__restrict__ rec = D.rec;
+  const double2 *si = reinterpret_cast<const double2 *>(rec + (size_t)q * R_WIDTH);
+  const double2 fx = __ldg(si + 7);
+  const unsigned fi = (unsigned)__double_as_longlong(fx.y);
+  if (fi & FLAG_BLANKED) return;
+  const double2 xy = __ldg(si + 0);
+  const double hi = __ldg(si + 5).x;
+  const double Ti = fx.x;
+  const double mass = P.phys.mass;
+  const long long tex_elems = ((long long)sizeof(int) * P.N) / 8;
+  const bool tool_i = q < tex_elems ? (fi & FLAG_TOOL) != 0 : false;
+  const double alpha = tool_i ? P.trml_tool.alpha : P.trml_wp.alpha;
+  const geom g = *D.g;
+  const int hashi = D.hash_cur[q];
+  const int gi = hashi / g.ny;
+  const int gj = hashi - gi * g.ny;
+  const int low_i = gi - 2 < 0 ? 0 : gi - 2;
+  const int low_j = gj - 2 < 0 ? 0 : gj - 2;
+  const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
+  const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
+  double T_ti = 0.;
+  for (int ii = low_i; ii < high_i; ++ii) {
+    const int j0 = __ldg(D.off + ii * g.ny + low_j);
+    const int j1 = __ldg(D.off + ii * g.ny + high_j);
+    for (int j = j0; j < j1; ++j) {
+      const double2 *sj = reinterpret_cast<const double2 *>(rec + (size_t)j * R_WIDTH);
+      const double2 pj = __ldg(sj + 0);
+      const double Tj = __ldg(sj + 7).x;
+      const double rhoj = __ldg(sj + 5).y;
+      const double w2 = lapl_pse_fp64(xy.x - pj.x, xy.y - pj.y, hi);
+      T_ti += (Tj - Ti) * w2 * mass / rhoj;
+    }
+  }
+  D.B.T_t[q] = alpha * T_ti;
+}
+
+// ---------------------------------------------------------------------------------------
+// corrector .. invalidate, per particle, plus the tool force (leap_frog.cu:68-92,
+// actions_gpu.cu:135-162,226-349, tool_gpu.cu:151-221, output.cu:31-39)
+__global__ void __launch_bounds__(BLOCK) k_finish(params P, dev_buffers D) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  ksum fcx{0., 0.}, fcy{0., 0.}, ftx{0., 0.}, fty{0., 0.};
+  unsigned newly_blanked = 0, capped = 0, blanked_now = 0;
+  if (q < P.N) {
+    const state_set &A = D.A;
+    const state_set &B = D.B;
+    const double dt = P.dt;
+    unsigned f = B.flags[q];
+    const bool blanked = f & FLAG_BLANKED;
+    const bool tool = f & FLAG_TOOL;
+    const bool fixed = f & FLAG_FIXED;
+    double2 pos = B.pos[q], vel = B.vel[q];
+    double4 S = B.S[q];
+    double rho = B.rho[q], T = B.T[q];
+    double2 pos_t = B.pos_t[q], vel_t = B.vel_t[q];
+    const double4 S_t = B.S_t[q];
+    const double rho_t = B.rho_t[q], T_t = B.T_t[q];
+    if (!blanked) {  // correct (leap_frog.cu:68-92) from the state at the start of the step
+      const int p = D.perm[q];
+      const double2 pos0 = A.pos[p], vel0 = A.vel[p];
+      const double4 S0 = A.S[p];
+      const double rho0 = A.rho[p], T0 = A.T[p];
+      pos.x = pos0.x + dt * pos_t.x;
+      pos.y = pos0.y + dt * pos_t.y;
+      vel.x = vel0.x + dt * vel_t.x;
+      vel.y = vel0.y + dt * vel_t.y;
+      S.x = S0.x + dt * S_t.x;
+      S.y = S0.y + dt * S_t.y;
+      S.z = S0.z + dt * S_t.z;
+      S.w = S0.w + dt * S_t.w;
+      rho = rho0 + dt * rho_t;
+      T = T0 + dt * T_t;
+    }
+    double eps_pl = B.eps_pl[q], eps_pl_dot = B.eps_pl_dot[q];
+    double2 fc = B.fc[q], ft = B.ft[q];
+    const mf_tool_state &TL = *D.tool;
+    // friction heat (actions_gpu.cu:135-162), previous step's ft and n
+    if (P.has_tool && P.fric_heat && !tool) {
+      const double f_fric_mag = (double)sqrtf((float)(ft.x * ft.x + ft.y * ft.y));
+      if (f_fric_mag != 0.) {
+        const double2 normal = D.n[q];
+        const double vdx = vel.x - TL.vel[0], vdy = vel.y - TL.vel[1];
+        const double vdn = vdx * normal.x + vdy * normal.y;
+        const double vrx = vdx - vdn, vry = vdy - vdn;
+        const double v_rel_mag = (double)sqrtf((float)(vrx * vrx + vry * vry));
+        T += P.trml_wp.eta * dt * f_fric_mag * v_rel_mag / (P.trml_wp.cp * P.phys.mass);
+      }
+    }
+    // JC plasticity, radial return (actions_gpu.cu:226-285)
+    if (P.plastic && !tool) {
+      const double mu = P.phys.G;
+      const double Sxx = S.x, Syy = S.z, Szz = S.w, Sxy = S.y;
+      const double norm_Strial = (double)sqrtf((float)(Sxx * Sxx + Syy * Syy + Szz * Szz + Sxy * Sxy));
+      const double pr = D.pp[q];
+      const double cxx = Sxx - pr, cyy = Syy - pr, czz = Szz - pr, cxy = Sxy;
+      const double svm = (double)sqrtf(
+          (float)((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy));
+      const double sigma_Y = sigma_yield(P.joco, eps_pl, eps_pl_dot, T);
+      if (svm < sigma_Y) {
+        eps_pl_dot = 0.;
+      } else {
+        bool cap = false;
+        const double delta_lambda = solve_secant(P.joco, P.jc_model, fmax(eps_pl_dot * dt * sqrt(2. / 3.), 1e-8),
+                                                 1e-6, norm_Strial, eps_pl, T, dt, P.phys.G, cap);
+        capped = cap ? 1u : 0u;
+        const float s23f = sqrtf((float)(2.0 / 3.0));
+        const double eps_pl_new = eps_pl + (double)(s23f * fmaxf((float)delta_lambda, 0.f));
+        const double eps_pl_dot_new = (double)(s23f * fmaxf((float)delta_lambda, 0.f)) / dt;
+        S.x = Sxx - Sxx / norm_Strial * delta_lambda * 2. * mu;
+        S.z = Syy - Syy / norm_Strial * delta_lambda * 2. * mu;
+        S.w = Szz - Szz / norm_Strial * delta_lambda * 2. * mu;
+        S.y = Sxy - Sxy / norm_Strial * delta_lambda * 2. * mu;
+        if (P.trml_wp.tq != 0.) {
+          const double delta_eps_pl = eps_pl_new - eps_pl;
+          const double sY = sigma_yield(P.joco, eps_pl_new, eps_pl_dot_new, T);
+          T += P.trml_wp.tq / (P.trml_wp.cp * rho) * delta_eps_pl * sY;
+        }
+        eps_pl = eps_pl_new;
+        eps_pl_dot = eps_pl_dot_new;
+      }
+    }
+    // tool particles move with the tool (tool_gpu.cu:210-221); contact (:151-207)
+    if (P.has_tool) {
+      if (tool) {
+        pos.x += dt * TL.vel[0];
+        pos.y += dt * TL.vel[1];
+      } else {
+        double cpx = 0., cpy = 0., nx = 0., ny = 0.;
+        const bool inside = establish_contact(TL, pos.x, pos.y, cpx, cpy, nx, ny);
+        if (!inside) {
+          fc = make_double2(0., 0.);
+          ft = make_double2(0., 0.);
+          D.n[q] = make_double2(0., 0.);
+        } else {
+          const double dt2 = dt * dt;
+          const double gN = (pos.x - cpx) * nx + (pos.y - cpy) * ny;
+          const double sc = -TL.slave_mass * gN;
+          double2 fN = make_double2(sc * nx, sc * ny);
+          fN.x = fN.x / dt2 * TL.contact_alpha;
+          fN.y = fN.y / dt2 * TL.contact_alpha;
+          double2 fT = make_double2(0., 0.);
+          if (TL.mu != 0.) {
+            const double vx = vel.x - TL.vel[0], vy = vel.y - TL.vel[1];
+            const double vrx = vx - vx * nx, vry = vy - vy * ny;
+            const double ks = TL.contact_alpha * TL.slave_mass;
+            const double kx = ks * vrx / dt, ky = ks * vry / dt;
+            const double fy = TL.mu * sqrt(fN.x * fN.x + fN.y * fN.y);
+            const double fsx = ft.x - kx, fsy = ft.y - ky;
+            const double lfs = sqrt(fsx * fsx + fsy * fsy);
+            if (lfs > fy) {
+              fT.x = fy * fsx / lfs;
+              fT.y = fy * fsy / lfs;
+            } else {
+              fT = make_double2(fsx, fsy);
+            }
+          }
+          fc = fN;
+          ft = fT;
+          D.n[q] = make_double2(nx, ny);
+        }
+      }
+    }
+    // boundary conditions (actions_gpu.cu:287-311)
+    if (!tool && fixed) {
+      vel = make_double2(0., 0.);
+      fc = make_double2(0., 0.);
+      pos_t = make_double2(0., 0.);
+      vel_t = make_double2(0., 0.);
+      B.pos_t[q] = pos_t;
+      B.vel_t[q] = vel_t;
+    }
+    if (P.thermal_bc && fixed) T = P.trml_wp.T_init;
+    // invalidate (actions_gpu.cu:317-349)
+    if (!blanked) {
+      bool invalid = isnaninf(pos_t.x) || isnaninf(pos_t.y) || isnaninf(vel_t.x) || isnaninf(vel_t.y) ||
+                     isnaninf(S_t.x) || isnaninf(S_t.y) || isnaninf(S_t.z) || isnaninf(S_t.w) ||
+                     isnaninf(rho_t) || isnaninf(T_t);
+      if (invalid) {
+        f |= FLAG_BLANKED;
+        newly_blanked = 1;
+        B.flags[q] = f;
+      }
+    }
+    blanked_now = (f & FLAG_BLANKED) ? 1u : 0u;
+    B.pos[q] = pos;
+    B.vel[q] = vel;
+    B.S[q] = S;
+    B.rho[q] = rho;
+    B.T[q] = T;
+    B.eps_pl[q] = eps_pl;
+    B.eps_pl_dot[q] = eps_pl_dot;
+    B.fc[q] = fc;
+    B.ft[q] = ft;
+    fcx.s = fc.x; fcy.s = fc.y; ftx.s = ft.x; fty.s = ft.y;
+  }
+  // block reduction of the force (compensated) and of the counters
+  __shared__ ksum sm[BLOCK / 32][4];
+  __shared__ unsigned smc[BLOCK / 32][3];
+  __shared__ bool last;
+  for (int o = 16; o > 0; o >>= 1) {
+    ksum a{__shfl_down_sync(0xffffffffu, fcx.s, o), __shfl_down_sync(0xffffffffu, fcx.c, o)};
+    ksum b{__shfl_down_sync(0xffffffffu, fcy.s, o), __shfl_down_sync(0xffffffffu, fcy.c, o)};
+    ksum c{__shfl_down_sync(0xffffffffu, ftx.s, o), __shfl_down_sync(0xffffffffu, ftx.c, o)};
+    ksum d{__shfl_down_sync(0xffffffffu, fty.s, o), __shfl_down_sync(0xffffffffu, fty.c, o)};
+    ksum_merge(fcx, a); ksum_merge(fcy, b); ksum_merge(ftx, c); ksum_merge(fty, d);
+  }
+  const unsigned nb = __popc(__ballot_sync(0xffffffffu, newly_blanked));
+  const unsigned nc = __popc(__ballot_sync(0xffffffffu, capped));
+  const unsigned nbl = __popc(__ballot_sync(0xffffffffu, blanked_now));
+  if (lane_id() == 0) {
+    sm[threadIdx.x >> 5][0] = fcx; sm[threadIdx.x >> 5][1] = fcy;
+    sm[threadIdx.x >> 5][2] = ftx; sm[threadIdx.x >> 5][3] = fty;
+    smc[threadIdx.x >> 5][0] = nb; smc[threadIdx.x >> 5][1] = nc; smc[threadIdx.x >> 5][2] = nbl;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ksum r[4] = {sm[0][0], sm[0][1], sm[0][2], sm[0][3]};
+    unsigned cnt[3] = {smc[0][0], smc[0][1], smc[0][2]};
+    for (int w = 1; w < BLOCK / 32; ++w) {
+      for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
+      for (int k = 0; k < 3; ++k) cnt[k] += smc[w][k];
+    }
+    for (int k = 0; k < 4; ++k) {
+      D.partials[blockIdx.x * 8 + 2 * k] = r[k].s;
+      D.partials[blockIdx.x * 8 + 2 * k + 1] = r[k].c;
+    }
+    if (cnt[0]) atomicAdd(&D.st->newly_blanked, (unsigned long long)cnt[0]);
+    if (cnt[1]) atomicAdd(&D.st->secant_cap_hits, (unsigned long long)cnt[1]);
+    if (cnt[2]) atomicAdd(&D.st->blanked, (unsigned long long)cnt[2]);
+    __threadfence();
+    const unsigned t = atomicAdd(&D.ticket[0], 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  // last block: fixed-order reduction of all block partials
+  __threadfence();
+  ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    const volatile double *pr = D.partials + (size_t)b * 8;
+    for (int k = 0; k < 4; ++k) {
+      ksum x{pr[2 * k], pr[2 * k + 1]};
+      ksum_merge(r[k], x);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 4; ++k) {
+      ksum x{__shfl_down_sync(0xffffffffu, r[k].s, o), __shfl_down_sync(0xffffffffu, r[k].c, o)};
+      ksum_merge(r[k], x);
+    }
+  __syncthreads();
+  if (lane_id() == 0)
+    for (int k = 0; k < 4; ++k) sm[threadIdx.x >> 5][k] = r[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < BLOCK / 32; ++w)
+      for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
+    // report_force: total contact force plus total friction force
+    const double Fx = (r[0].s + r[0].c) + (r[2].s + r[2].c);
+    const double Fy = (r[1].s + r[1].c) + (r[3].s + r[3].c);
+    D.force_last[0] = Fx;
+    D.force_last[1] = Fy;
+    const unsigned long long hd = D.st->force_log_head;
+    D.force_log[2 * (hd % FORCE_LOG_CAP)] = Fx;
+    D.force_log[2 * (hd % FORCE_LOG_CAP) + 1] = Fy;
+    D.st->force_log_head = hd + 1;
+    D.st->steps += 1;
+    D.ticket[0] = 0u;
+  }
+}
+
+// report_force on the current state without stepping (output.cu:31-39)
+__global__ void __launch_bounds__(BLOCK) k_force_only(int N, const double2 *__restrict__ fc,
+                                                      const double2 *__restrict__ ft, dev_buffers D) {
+  __shared__ ksum sm[BLOCK / 32][4];
+  ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    double2 a = fc[i], b = ft[i];
+    ksum_add(r[0], a.x); ksum_add(r[1], a.y); ksum_add(r[2], b.x); ksum_add(r[3], b.y);
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 4; ++k) {
+      ksum x{__shfl_down_sync(0xffffffffu, r[k].s, o), __shfl_down_sync(0xffffffffu, r[k].c, o)};
+      ksum_merge(r[k], x);
+    }
+  if (lane_id() == 0)
+    for (int k = 0; k < 4; ++k) sm[threadIdx.x >> 5][k] = r[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < BLOCK / 32; ++w)
+      for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
+    D.force_last[0] = (r[0].s + r[0].c) + (r[2].s + r[2].c);
+    D.force_last[1] = (r[1].s + r[1].c) + (r[3].s + r[3].c);
+  }
+}
+
+}  // namespace mf

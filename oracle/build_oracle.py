@@ -1,0 +1,96 @@
+"""Build recipe for the oracle (test infrastructure; never part of the product path).
+
+Two artefacts:
+
+* ``oracle/_build/liboracle.so``: the CPU restatement of the reference step
+  (``oracle/sph_oracle.c``), plain C11 + OpenMP, built with gcc.
+* ``oracle/_ref/libref_host.so``: the reference's own host-compilable sources, compiled
+  where they lie (``<reference>/src``) against the project's GLM-subset shim
+  (``oracle/ref_shim``), plus the recording harness ``oracle/ref_host_harness.cu`` and the
+  host build of ``plasticity.cuh`` (``oracle/ref_host_plasticity.cpp``). It is only built
+  when the reference tree is present; the GPU machines use the prebuilt file or skip.
+
+Both are loaded with ctypes by ``tests/`` and by ``bench.py``'s CPU-baseline leg only.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REF_SRC = Path(os.environ.get("MF_REFERENCE_SRC", "/root/reference/src"))
+NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+CUDA_HOME = Path(NVCC).resolve().parent.parent
+
+ORACLE_LIB = HERE / "_build" / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libref_host.so"
+
+
+def _run(cmd, cwd=None):
+    r = subprocess.run(cmd, cwd=cwd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(str(c) for c in cmd) + "\n" + r.stdout + "\n")
+        raise RuntimeError(f"build step failed: {cmd[0]} ({r.returncode})")
+    return r.stdout
+
+
+def _stale(target: Path, sources) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(Path(s).stat().st_mtime > t for s in sources)
+
+
+def build_oracle(force: bool = False) -> Path:
+    """gcc -O2 -fopenmp the C restatement into a shared library (no FMA contraction)."""
+    srcs = [HERE / "sph_oracle.c", HERE / "sph_oracle.h"]
+    if force or _stale(ORACLE_LIB, srcs):
+        ORACLE_LIB.parent.mkdir(parents=True, exist_ok=True)
+        _run([
+            "gcc", "-std=gnu11", "-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
+            "-fno-fast-math", "-Wall", "-Wno-unused-function",
+            "-o", str(ORACLE_LIB), str(HERE / "sph_oracle.c"), "-lm",
+        ])
+    return ORACLE_LIB
+
+
+def build_ref(force: bool = False) -> Path | None:
+    """Compile the reference's host-side sources (where they lie) into oracle/_ref."""
+    if not REF_SRC.is_dir():
+        return REF_LIB if REF_LIB.exists() else None
+    ref_files = ["benchmarks.cpp", "tool.cpp", "geometric_primitives.cpp", "constants_structs.cpp",
+                 "grid.cu", "tool_wear.cu"]
+    srcs = [HERE / "ref_host_harness.cu", HERE / "ref_host_plasticity.cpp",
+            HERE / "ref_shim" / "glm" / "glm.hpp"] + [REF_SRC / f for f in ref_files]
+    if not (force or _stale(REF_LIB, srcs)):
+        return REF_LIB
+    obj = HERE / "_ref" / "obj"
+    obj.mkdir(parents=True, exist_ok=True)
+    inc = ["-I", str(HERE / "ref_shim"), "-I", str(REF_SRC)]
+    # the reference's Release flags were -O3 -std=c++11; host code keeps x87-free SSE2
+    # arithmetic and no FMA contraction, as gcc does by default for x86-64.
+    nv = [NVCC, "-O3", "-std=c++14", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+          "-gencode", "arch=compute_100a,code=sm_100a", "-w", "-x", "cu", "-c"]
+    objs = []
+    for f in ["ref_host_harness.cu"]:
+        o = obj / (Path(f).stem + ".o")
+        _run(nv + inc + ["-o", str(o), str(HERE / f)])
+        objs.append(o)
+    for f in ref_files:
+        o = obj / ("ref_" + Path(f).stem + ".o")
+        _run(nv + inc + ["-o", str(o), str(REF_SRC / f)])
+        objs.append(o)
+    o = obj / "ref_host_plasticity.o"
+    _run(["g++", "-O3", "-std=c++14", "-fPIC", "-ffp-contract=off", "-w", "-c",
+          "-I", str(CUDA_HOME / "include")] + inc + ["-o", str(o), str(HERE / "ref_host_plasticity.cpp")])
+    objs.append(o)
+    _run([NVCC, "-shared", "-Xcompiler", "-fPIC", "-o", str(REF_LIB)] + [str(x) for x in objs])
+    return REF_LIB
+
+
+if __name__ == "__main__":
+    print(build_oracle(force="--force" in sys.argv))
+    print(build_ref(force="--force" in sys.argv))

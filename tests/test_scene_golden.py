@@ -1,0 +1,106 @@
+"""The product's host code against the reference: setup_ref_cut, the tool, the grid box.
+
+All of it runs on the CPU through the C ABI (no device needed for the host scene code).
+"""
+import numpy as np
+import pytest
+
+from conftest import bits_equal
+
+SCENES = ("ref_cut_default", "ref_cut_ny12_rake0", "ref_cut_sharp")
+ARRAYS = ("pos", "vel", "rho", "T", "h", "fixed", "tool_p")
+
+
+def scene_constants(mf, s):
+    v = [getattr(s.phys, f) for f, _ in mf.Phys._fields_]
+    v += [getattr(s.corr, f) for f, _ in mf.Corr._fields_]
+    v += [getattr(s.joco, f) for f, _ in mf.Joco._fields_]
+    v += [getattr(s.trml_wp, f) for f, _ in mf.Trml._fields_]
+    v += [getattr(s.trml_tool, f) for f, _ in mf.Trml._fields_]
+    v += [s.dt, s.t_final, s.tool.contact_alpha, 1.0]
+    return np.array(v)
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_setup_ref_cut_bitwise(mf, golden, name):
+    g = golden(name)
+    sc = mf.Scene.ref_cut(*[float(x) if i else int(x) for i, x in enumerate(g["args"])])
+    assert sc.N == int(g["N"])
+    for k in ARRAYS:
+        assert bits_equal(sc.array(k).reshape(-1), g[k]), k
+    assert bits_equal(scene_constants(mf, sc.s), g["constants"])
+    t = mf.tool_to_array(sc.s.tool)
+    assert bits_equal(t["seg"], g["tool_seg"])
+    assert bits_equal(t["fillet"], g["tool_fillet"])
+    assert bits_equal(t["vel"], g["tool_vel"])
+    assert t["mu"] == g["tool_misc"][2]
+    assert sc.s.tool.slave_mass == sc.s.phys.mass
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_grid_box_gives_reference_geometry(mf, orc, golden, name):
+    """The scene's box through grid_base::set_geometry (grid.cu:139-158) = the reference grid."""
+    g = golden(name)
+    sc = mf.Scene.ref_cut(*[float(x) if i else int(x) for i, x in enumerate(g["args"])])
+    o = orc.Oracle(sc.N)
+    s = sc.s
+    o.L.orc_set_grid_locked(o.s, 0, s.grid_bbmin[0], s.grid_bbmin[1], s.grid_bbmax[0], s.grid_bbmax[1], s.grid_h)
+    geo = o.geometry()
+    nx, ny, bx0, by0, bx1, by1, dx, nc, locked = g["grid"]
+    assert (geo["nx"], geo["ny"], geo["num_cell"]) == (int(nx), int(ny), int(nc))
+    assert bits_equal([geo["bbmin_x"], geo["bbmin_y"], geo["bbmax_x"], geo["bbmax_y"], geo["dx"]],
+                      [bx0, by0, bx1, by1, dx])
+
+
+def test_tool_construct_sample_translate(mf, golden):
+    g = golden("ref_tools")
+    k = 0
+    while f"t{k}_seg" in g:
+        a = g[f"t{k}_args"]
+        t = mf.tool_construct((a[0], a[1]), a[2], a[3], a[4], a[5], a[6], a[7])
+        arr = mf.tool_to_array(t)
+        assert bits_equal(arr["seg"], g[f"t{k}_seg"]), k
+        assert bits_equal(arr["fillet"], g[f"t{k}_fillet"]), k
+        xy = mf.tool_sample(t, 0.0014)
+        assert bits_equal(xy, g[f"t{k}_sample"]), k
+        t.vel[0], t.vel[1] = 1.16667e-4, 0.0
+        for _ in range(50):
+            mf.tool_translate(t, 1.17e-3)
+        arr = mf.tool_to_array(t)
+        assert bits_equal(arr["seg"], g[f"t{k}_seg_moved"]), k
+        if t.has_fillet:
+            assert bits_equal(arr["fillet"], g[f"t{k}_fillet_moved"]), k
+        k += 1
+    assert k == 4
+
+
+def test_generalised_scene_explicit_lattice(mf):
+    """The benchmark scenes: explicit nx x ny lattice, jitter, tool front placed at x."""
+    p = mf.reference_cut_params()
+    p.nx_lattice, p.ny, p.dx = 143, 43, 1.4e-3
+    p.lo_x, p.lo_y = 0.0, 0.0
+    p.jitter, p.seed = 0.005, 1
+    p.tool_front_x = -0.1 * 1.4e-3
+    p.feed, p.rake, p.clear, p.chamfer = 0.005, 0.0, 7.0, 5e-4
+    p.cfl = 0.3
+    p.sample_tool = 0
+    p.use_thermals = 0
+    sc = mf.Scene.from_params(p)
+    assert sc.s.n_workpiece == 143 * 43 and sc.s.n_tool == 0
+    pos = sc.array("pos")
+    lattice_x = np.repeat(np.arange(143) * 1.4e-3, 43)
+    assert np.max(np.abs(pos[:, 0] - lattice_x)) <= 0.005 * 1.4e-3 * (1 + 1e-12)
+    # deterministic
+    sc2 = mf.Scene.from_params(p)
+    assert bits_equal(sc2.array("pos"), pos)
+    # bottom row fixed
+    fixed = sc.array("fixed")
+    assert np.all(fixed.reshape(143, 43)[:, 0] == 1.0)
+    # tool front at the requested x, low point at hi_y - feed
+    t = mf.tool_to_array(sc.s.tool)
+    hi_y = 42 * 1.4e-3
+    low = t["fillet"][4] - t["fillet"][0]
+    assert abs(low - (hi_y - 0.005)) < 1e-12
+    # dt = cfl*hdx*dx/(sqrt(K/rho0) + sqrt(v))
+    s = sc.s
+    assert abs(s.dt - 0.3 * 1.5 * 1.4e-3 / (np.sqrt(s.phys.K / s.phys.rho0) + np.sqrt(s.speed))) < 1e-18
