@@ -1,0 +1,422 @@
+"""Benchmark: particle-steps/s of the explicit 2D SPH cutting step on B200.
+
+Workload (one "step" = one leap-frog step of the whole particle system): the ~150k-particle
+orthogonal cut with the Brookshaw thermal solver and thermal contact (tool particles):
+Ti6Al4V workpiece 2.0 mm x 0.6 mm on a 714 x 214 lattice, dx = 2.8 um, seeded jitter
++-0.5% dx, h = 1.5 dx, rigid tool (rake 0, clearance 7 deg, edge radius 5 um, depth of cut
+50 um, 70 m/min, mu = 0.35), CFL 0.3. Synthetic inputs, generated by the project's scene
+setup (a generalisation of the reference's setup_ref_cut).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Both forms run: plain FP64 and mixed FP32/FP64; the headline value is the mixed form.
+Each timed step is bracketed by CUDA events on the library's stream, with the L2 flushed
+(256 MiB written) between timed steps. Under torchrun (N > 1) every rank steps its own
+replica of the scene (replicas only: the step has no data-path exchange); the time is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "mfree_iwf-ul_cut_gpu_b200"
+METRIC = "particle-steps/s at ~150k particles w/ thermal contact: mixed vs FP64, same B200"
+ALGO_BYTES_PER_PARTICLE_STEP = 480.0  # canonical FP64 bytes per particle-step
+FLUSH_BYTES = 256 << 20
+
+
+def load_package():
+    name = "mfree_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def cut_params(mf, nx=714, ny=214, dx=2.8e-4):
+    """The ~150k-particle cut (dx 2.8 um, 714 x 214) with thermal contact."""
+    p = mf.reference_cut_params()
+    p.nx_lattice, p.ny, p.dx = nx, ny, dx
+    p.lo_x, p.lo_y = 0.0, 0.0
+    p.jitter, p.seed = 0.005, 1
+    p.rake, p.clear, p.chamfer = 0.0, 7.0, 5e-4
+    p.feed = 0.005
+    p.speed = 70.0 * 100.0 / 60.0e6  # 70 m/min in cm/us
+    p.mu_fric = 0.35
+    p.tool_front_x = -0.1 * dx
+    p.sample_tool = 1
+    p.use_thermals = 1
+    p.E, p.nu, p.rho0 = 1.1, 0.35, 4.43
+    jc = p.joco
+    jc.A, jc.B, jc.n, jc.C, jc.m = 0.01098, 0.01092, 0.93, 0.014, 1.1
+    jc.eps_dot_ref, jc.Tref, jc.Tmelt = 1e-6, 300.0, 1878.0
+    p.trml_wp.cp, p.trml_wp.k, p.trml_wp.tq, p.trml_wp.eta = 553e-8, 7.1e-13, 0.9, 0.9
+    p.cfl = 0.3
+    return p
+
+
+WORKLOAD = {"workload": "orthogonal cut, Ti6Al4V 2.0 x 0.6 mm, 714x214 lattice dx=2.8um + sampled tool "
+                        "particles, Brookshaw thermal solver, thermal contact",
+            "lattice": [714, 214], "dx_um": 2.8, "thermal_solver": "brookshaw", "grid": "green (locked)"}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """Max of a per-rank float over all ranks (identity at world size 1)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(value: float, world: int, device=None) -> float:
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.dev), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def time_form(mf, torch, scene, precision, steps, warmup, device):
+    """Per-step CUDA-event times (ms) of mf_step(1) with the L2 flushed between steps, plus the
+    pair kernel's own duration (mf_step_stage(2) bracketed by events)."""
+    ctx = mf.Context(device)
+    ctx.upload_scene(scene, mf.GRID_GREEN)
+    ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    ctx.step(warmup)
+    ctx.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            ctx.step(1)
+            ev[k][1].record(stream)
+    torch.cuda.synchronize(device)
+    step_ms = np.array([a.elapsed_time(b) for a, b in ev])
+    # pair kernel alone (stage 2), a few samples, cold L2 as above
+    pair = []
+    with torch.cuda.stream(stream):
+        for _ in range(max(5, min(20, steps // 4))):
+            ctx.stage(0)
+            ctx.stage(1)
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ctx.stage(2)
+            b.record(stream)
+            ctx.stage(3)
+            torch.cuda.synchronize(device)
+            pair.append(a.elapsed_time(b))
+    st = ctx.status()
+    ctx.close()
+    return step_ms, np.array(pair), st
+
+
+def e2e_form(mf, scene, precision, steps, device):
+    """End to end through the C ABI with host buffers: upload of the scene from host memory,
+    `steps` x (mf_step(1) + read of that step's tool force to the host), download of the
+    final state; wall clock around all of it."""
+    import torch
+
+    ctx = mf.Context(device)
+    ctx.upload_scene(scene, mf.GRID_GREEN)
+    ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
+    ctx.step(2)  # graph instantiation outside the timed region
+    ctx.synchronize()
+    n = scene.N
+    fields = ("pos", "vel", "S", "rho", "T", "eps_pl")
+    t0 = time.perf_counter()
+    ctx.upload_scene(scene, mf.GRID_GREEN)
+    ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
+    h2d = n * 8 * (2 + 2 + 1 + 1 + 1 + 1 + 1)  # pos vel rho T h fixed tool_p
+    for _ in range(steps):
+        ctx.step(1)
+        ctx.force_log(1)
+    out = {f: ctx.get(f) for f in fields}
+    t1 = time.perf_counter()
+    d2h_state = sum(v.nbytes for v in out.values())
+    ctx.close()
+    del torch
+    return (t1 - t0), h2d, d2h_state
+
+
+def cpu_baseline(mf, scene, seconds=12.0, max_steps=50):
+    """The oracle port (C, OpenMP, all host threads) on the same scene: bounded sample."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    sys.path.insert(0, str(ROOT / "tests"))
+    import binding as orc
+    import build_oracle
+    from helpers import load_oracle
+
+    build_oracle.build_oracle()
+    st = scene_state(mf, scene)
+    o = load_oracle(orc, st)
+    o.L.orc_step(o.s)  # warm-up (first-touch of the pages)
+    t0 = time.perf_counter()
+    o.L.orc_step(o.s)
+    t1 = time.perf_counter() - t0
+    k = int(max(1, min(max_steps, seconds / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    o.L.orc_steps(o.s, k)
+    dt = time.perf_counter() - t0
+    return {"value": scene.N * k / dt, "unit": "particle-steps/s", "cores": int(orc.lib().orc_get_threads()),
+            "kind": "port", "sample": f"{k} steps of the full {scene.N}-particle scene after 1 warm-up step "
+                                      f"(oracle C restatement, OpenMP), {dt:.1f} s"}
+
+
+def scene_state(mf, scene):
+    """The scene as the state dict tests/helpers.load_oracle expects."""
+    import ctypes as C
+
+    s = scene.s
+    N = scene.N
+    st = {"N": N}
+    for k in ("pos", "vel", "rho", "T", "h", "fixed", "tool_p"):
+        st[k] = scene.array(k).copy()
+    z1, z2, z4 = np.zeros(N), np.zeros((N, 2)), np.zeros((N, 4))
+    st.update({"S": z4, "eps_pl": z1, "eps_pl_dot": z1, "fc": z2, "ft": z2, "n": z2, "pos_t": z2, "vel_t": z2,
+               "rho_t": z1, "S_t": z4, "T_t": z1, "blanked": z1})
+    st.update({"phys": s.phys, "corr": s.corr, "joco": s.joco, "trml_wp": s.trml_wp, "trml_tool": s.trml_tool,
+               "dt": s.dt, "grid": (tuple(s.grid_bbmin), tuple(s.grid_bbmax), s.grid_h)})
+    t = mf.ToolState()
+    C.memmove(C.byref(t), C.byref(s.tool), C.sizeof(mf.ToolState))
+    st["tool"] = t
+    return st
+
+
+def kernels_per_step(mf, precision):
+    return 6  # hash+count, scan, scatter, reorder/predict, pair, finish (locked grid, Brookshaw)
+
+
+def run_reference(args):
+    """--impl reference: the reference path's CPU restatement on the host cores."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    mf = load_package()
+    scene = mf.Scene.from_params(cut_params(mf))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    sys.path.insert(0, str(ROOT / "tests"))
+    import binding as orc
+    import build_oracle
+    from helpers import load_oracle
+
+    build_oracle.build_oracle()
+    o = load_oracle(orc, scene_state(mf, scene))
+    # each "step" is one full oracle step; bound the run to a few minutes
+    o.L.orc_step(o.s)
+    t0 = time.perf_counter()
+    o.L.orc_step(o.s)
+    t1 = time.perf_counter() - t0
+    budget = 150.0
+    warm = min(args.warmup, max(0, int(budget * 0.2 / max(t1, 1e-6))))
+    steps = max(1, min(args.steps, int(budget * 0.8 / max(t1, 1e-6))))
+    for _ in range(warm):
+        o.L.orc_step(o.s)
+    t0 = time.perf_counter()
+    o.L.orc_steps(o.s, steps)
+    dt = time.perf_counter() - t0
+    v = scene.N * steps / dt
+    cores = int(orc.lib().orc_get_threads())
+    line = {"metric": METRIC, "value": v, "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": warm, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": dict(WORKLOAD, n_particles=scene.N, n_tool=scene.s.n_tool),
+            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+                             "sample": f"{steps} full steps of the {scene.N}-particle scene (requested "
+                                       f"{args.steps}), C restatement of the reference step, OpenMP"},
+            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=100)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    world, rank, local = dist_env()
+    device = local if world > 1 else 0
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", device))
+    mf = load_package()
+    scene = mf.Scene.from_params(cut_params(mf))
+    N = scene.N
+
+    results = {}
+    clocks = None
+    for name, prec in (("fp64", mf.PRECISION_FP64), ("mixed", mf.PRECISION_MIXED)):
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(device)
+        with ClockSampler(device) as cs:
+            step_ms, pair_ms, st = time_form(mf, torch, scene, prec, args.steps, args.warmup, device)
+        if name == "mixed":
+            clocks = cs.summary()
+        total_ms = max_over_ranks(float(step_ms.sum()), world, device=f"cuda:{device}")
+        particles = sum_over_ranks(float(N), world, device=f"cuda:{device}")
+        value = particles * args.steps / (total_ms * 1e-3)
+        pair_mean = float(pair_ms.mean())
+        results[name] = {"value": value, "ms_per_step": total_ms / args.steps,
+                         "pair_kernel_ms": pair_mean, "status": st}
+    # roofline of the dominant kernel (the pair kernel) on the canonical per-particle bytes
+    peaks_file = ROOT / "MEASURED_PEAKS.json"
+    if peaks_file.exists():
+        peak = float(json.loads(peaks_file.read_text())["hbm_gbs"])
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    head = results["mixed"]
+    achieved = ALGO_BYTES_PER_PARTICLE_STEP * N / (head["pair_kernel_ms"] * 1e-3) / 1e9
+    step_achieved = ALGO_BYTES_PER_PARTICLE_STEP * N / (head["ms_per_step"] * 1e-3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "pair_kernel_traffic.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get("mixed_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    e2e = None
+    if rank == 0:
+        secs, h2d, d2h = e2e_form(mf, scene, mf.PRECISION_MIXED, args.e2e_steps, device)
+        e2e = {"value": N * args.e2e_steps / secs, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": h2d / args.e2e_steps, "d2h_bytes_per_step": 16 + d2h / args.e2e_steps,
+               "steps": args.e2e_steps,
+               "what": "host scene upload + per-step mf_step(1) and force read-back + final state download"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(mf, scene)
+    if world > 1:
+        torch.distributed.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": head["value"], "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed",
+            "data": "synthetic",
+            "config": dict(WORKLOAD, n_particles=N, n_workpiece=scene.s.n_workpiece, n_tool=scene.s.n_tool,
+                           parallelism=f"replicas x{world}", l2="flushed between timed steps (256 MiB write)",
+                           global_particles=N * world),
+            "forms": {"fp64": {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
+                               "pair_kernel_ms": results["fp64"]["pair_kernel_ms"]},
+                      "mixed": {"value": results["mixed"]["value"], "ms_per_step": results["mixed"]["ms_per_step"],
+                                "pair_kernel_ms": results["mixed"]["pair_kernel_ms"]},
+                      "mixed_over_fp64": results["mixed"]["value"] / results["fp64"]["value"]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                         "kernel": "k_pair_mixed", "algorithmic_bytes_per_particle": ALGO_BYTES_PER_PARTICLE_STEP,
+                         "step_achieved": step_achieved, "step_frac": step_achieved / peak},
+            "gpu_launches": kernels_per_step(mf, mf.PRECISION_MIXED) * args.steps,
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "status": {k: v for k, v in results["mixed"]["status"].items()},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

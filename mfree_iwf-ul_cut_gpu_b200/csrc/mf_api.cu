@@ -692,12 +692,13 @@ int mf_force_log(mf_ctx *ctx, double *out, int max_entries, int *n_out) {
   unsigned long long n = head - first;
   if (n > (unsigned long long)max_entries) n = (unsigned long long)max_entries;
   if (n > 0 && out) {
-    std::vector<double> all((size_t)FORCE_LOG_CAP * 2);
-    CK(cudaMemcpy(all.data(), ctx->D.force_log, sizeof(double) * all.size(), cudaMemcpyDeviceToHost));
-    for (unsigned long long k = 0; k < n; ++k) {
-      unsigned long long slot = (first + k) % FORCE_LOG_CAP;
-      out[2 * k] = all[2 * slot];
-      out[2 * k + 1] = all[2 * slot + 1];
+    // at most two contiguous pieces of the ring
+    unsigned long long done = 0;
+    while (done < n) {
+      unsigned long long slot = (first + done) % FORCE_LOG_CAP;
+      unsigned long long len = std::min(n - done, (unsigned long long)FORCE_LOG_CAP - slot);
+      CK(cudaMemcpy(out + 2 * done, ctx->D.force_log + 2 * slot, sizeof(double) * 2 * len, cudaMemcpyDeviceToHost));
+      done += len;
     }
   }
   ctx->force_read_head = first + n;

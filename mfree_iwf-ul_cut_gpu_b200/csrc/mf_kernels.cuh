@@ -142,18 +142,19 @@ __global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A, dev_bu
   unsigned oog = 0;
   if (gid < N) {
     const geom g = *D.g;
-    int hsh;
+    long long hh;
     if (A.flags[gid] & FLAG_BLANKED) {
-      hsh = D.hash_cur[gid];  // blanked particles keep their previous hash (grid.cu:39-41)
+      hh = D.hash_cur[gid];  // blanked particles keep their previous hash (grid.cu:39-41)
     } else {
       double2 p = A.pos[gid];
       int ix = __double2int_rz((p.x - g.bbmin_x) / g.dx);
       int iy = __double2int_rz((p.y - g.bbmin_y) / g.dx);
-      long long hh = (long long)ix * (long long)g.ny + (long long)iy;
-      if (hh < 0) { hh = 0; oog = 1; }
-      else if (hh >= g.num_cell) { hh = g.num_cell - 1; oog = 1; }
-      hsh = (int)hh;
+      hh = (long long)ix * (long long)g.ny + (long long)iy;
     }
+    // outside [0, num_cell) the reference writes out of bounds; clamp and count instead
+    if (hh < 0) { hh = 0; oog = 1; }
+    else if (hh >= g.num_cell) { hh = g.num_cell - 1; oog = 1; }
+    const int hsh = (int)hh;
     D.hash_new[gid] = hsh;
     D.slot[gid] = atomicAdd(&D.count[hsh], 1);
   }

@@ -291,10 +291,14 @@ static int trunc_sat(double v) {
 static void assign_hashes(orc_state *s) {
   long long oog = 0;
   for (int i = 0; i < s->N; ++i) {
-    if (s->blanked[i] == 1.) continue;
-    int ix = trunc_sat((s->pos[i].x - s->bbmin_x) / s->dx);
-    int iy = trunc_sat((s->pos[i].y - s->bbmin_y) / s->dx);
-    long long hsh = (long long)ix * (long long)s->ny + (long long)iy;
+    long long hsh;
+    if (s->blanked[i] == 1.) {
+      hsh = s->hash[i];
+    } else {
+      int ix = trunc_sat((s->pos[i].x - s->bbmin_x) / s->dx);
+      int iy = trunc_sat((s->pos[i].y - s->bbmin_y) / s->dx);
+      hsh = (long long)ix * (long long)s->ny + (long long)iy;
+    }
     if (hsh < 0) { hsh = 0; ++oog; }
     else if (hsh >= s->num_cell) { hsh = s->num_cell - 1; ++oog; }
     s->hash[i] = (int)hsh;
