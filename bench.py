@@ -193,35 +193,41 @@ def time_form(mf, torch, scene, precision, steps, warmup, device):
     return step_ms, np.array(pair), st
 
 
-def e2e_form(mf, scene, precision, steps, device):
-    """End to end through the C ABI with host buffers: upload of the scene from host memory,
-    `steps` x (mf_step(1) + read of that step's tool force to the host), download of the
-    final state; wall clock around all of it."""
-    import torch
-
+def e2e_form(mf, torch, scene, precision, steps, device):
+    """End to end through the C ABI with host buffers. Outside the timed region: context,
+    device buffers and the step graphs (created once per run). Inside: the particle state
+    copied in from pinned host memory (mf_set_field), `steps` x (mf_step(1) + a copy of that
+    step's tool force to pinned host memory), and the final state copied back to the host."""
     ctx = mf.Context(device)
     ctx.upload_scene(scene, mf.GRID_GREEN)
     ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
-    ctx.step(2)  # graph instantiation outside the timed region
+    ctx.step(2)  # builds the graphs
     ctx.synchronize()
     n = scene.N
-    fields = ("pos", "vel", "S", "rho", "T", "eps_pl")
+    init = {}
+    for f, w in (("pos", 2), ("vel", 2), ("rho", 1), ("T", 1), ("S", 4), ("eps_pl", 1), ("eps_pl_dot", 1),
+                 ("fc", 2), ("ft", 2), ("pos_t", 2), ("vel_t", 2), ("rho_t", 1), ("S_t", 4), ("T_t", 1)):
+        src = scene.array(f) if f in ("pos", "vel", "rho", "T") else np.zeros((n, w) if w > 1 else n)
+        init[f] = torch.from_numpy(np.ascontiguousarray(src, dtype=np.float64)).pin_memory()
+    forces = torch.zeros((steps, 2), dtype=torch.float64).pin_memory()
+    out_fields = ("pos", "vel", "S", "rho", "T", "eps_pl")
     t0 = time.perf_counter()
-    ctx.upload_scene(scene, mf.GRID_GREEN)
-    ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
-    h2d = n * 8 * (2 + 2 + 1 + 1 + 1 + 1 + 1)  # pos vel rho T h fixed tool_p
-    for _ in range(steps):
+    for f, t in init.items():
+        ctx.set(f, t.numpy())
+    for k in range(steps):
         ctx.step(1)
-        ctx.force_log(1)
-    out = {f: ctx.get(f) for f in fields}
+        ctx.force_last_async(forces[k].data_ptr())
+    ctx.synchronize()
+    out = {f: ctx.get(f) for f in out_fields}
     t1 = time.perf_counter()
-    d2h_state = sum(v.nbytes for v in out.values())
+    h2d = sum(t.numel() * 8 for t in init.values())
+    d2h = sum(v.nbytes for v in out.values())
+    assert np.isfinite(forces.numpy()).all()
     ctx.close()
-    del torch
-    return (t1 - t0), h2d, d2h_state
+    return (t1 - t0), h2d, d2h
 
 
-def cpu_baseline(mf, scene, seconds=12.0, max_steps=50):
+def cpu_baseline(mf, scene, seconds=12.0, max_steps=5000):
     """The oracle port (C, OpenMP, all host threads) on the same scene: bounded sample."""
     sys.path.insert(0, str(ROOT / "oracle"))
     sys.path.insert(0, str(ROOT / "tests"))
@@ -318,7 +324,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--e2e-steps", type=int, default=500)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -376,11 +382,12 @@ def main():
 
     e2e = None
     if rank == 0:
-        secs, h2d, d2h = e2e_form(mf, scene, mf.PRECISION_MIXED, args.e2e_steps, device)
+        secs, h2d, d2h = e2e_form(mf, torch, scene, mf.PRECISION_MIXED, args.e2e_steps, device)
         e2e = {"value": N * args.e2e_steps / secs, "unit": "particle-steps/s",
                "h2d_bytes_per_step": h2d / args.e2e_steps, "d2h_bytes_per_step": 16 + d2h / args.e2e_steps,
                "steps": args.e2e_steps,
-               "what": "host scene upload + per-step mf_step(1) and force read-back + final state download"}
+               "what": "state in from pinned host memory, per step mf_step(1) + tool force to pinned host "
+                       "memory, final state out; wall clock"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(mf, scene)

@@ -167,6 +167,9 @@ int mf_step(mf_ctx *ctx, int n_steps);
 int mf_step_stage(mf_ctx *ctx, int stage);
 /* report_force (output.cu:31-39): sum of fc + ft after the last step, compensated */
 int mf_report_force(mf_ctx *ctx, double out[2]);
+/* queue a copy of the last step's tool force (2 doubles) to host memory; with pinned host
+   memory the copy is asynchronous and complete after the next mf_synchronize */
+int mf_force_last_async(mf_ctx *ctx, double *host_out2);
 /* per-step force log since the last call (or creation), at most max entries of 2 doubles */
 int mf_force_log(mf_ctx *ctx, double *out, int max_entries, int *n_out);
 int mf_status_get(mf_ctx *ctx, mf_status *status);

@@ -136,7 +136,7 @@ def lib():
         "mf_set_options": ([vp, i, i, i], i), "mf_set_dt": ([vp, d], i),
         "mf_tool_set": ([vp, C.POINTER(ToolState)], i), "mf_tool_get": ([vp, C.POINTER(ToolState)], i),
         "mf_step": ([vp, i], i), "mf_step_stage": ([vp, i], i), "mf_report_force": ([vp, vp], i),
-        "mf_force_log": ([vp, vp, i, ip], i), "mf_status_get": ([vp, C.POINTER(Status)], i),
+        "mf_force_log": ([vp, vp, i, ip], i), "mf_force_last_async": ([vp, vp], i), "mf_status_get": ([vp, C.POINTER(Status)], i),
         "mf_cut_params_reference": ([C.POINTER(CutParams), i, d, d, d, d, d], i),
         "mf_scene_cut": ([C.POINTER(CutParams), C.POINTER(C.POINTER(SceneStruct))], i),
         "mf_scene_setup_ref_cut": ([i, d, d, d, d, d, C.POINTER(C.POINTER(SceneStruct))], i),
@@ -337,6 +337,10 @@ class Context:
         out = np.zeros(2)
         self._check(self.L.mf_report_force(self.h, _ptr(out)), "mf_report_force")
         return out
+
+    def force_last_async(self, host_ptr: int):
+        """Queue a copy of the last step's force (2 doubles) to host memory at host_ptr."""
+        self._check(self.L.mf_force_last_async(self.h, C.c_void_p(host_ptr)), "mf_force_last_async")
 
     def force_log(self, max_entries=1 << 16):
         out = np.zeros(2 * max_entries)

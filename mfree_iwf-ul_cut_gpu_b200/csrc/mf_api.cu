@@ -680,6 +680,13 @@ int mf_report_force(mf_ctx *ctx, double out[2]) {
   return MF_OK;
 }
 
+int mf_force_last_async(mf_ctx *ctx, double *host_out2) {
+  if (!ctx || !host_out2) return MF_ERR_INVALID;
+  TRY(set_device(ctx));
+  CK(cudaMemcpyAsync(host_out2, ctx->D.force_last, sizeof(double) * 2, cudaMemcpyDeviceToHost, ctx->stream));
+  return MF_OK;
+}
+
 int mf_force_log(mf_ctx *ctx, double *out, int max_entries, int *n_out) {
   if (!ctx || !n_out || max_entries < 0) return MF_ERR_INVALID;
   TRY(set_device(ctx));

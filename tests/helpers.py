@@ -68,9 +68,14 @@ def perturbed_scene(mf, ny=12, seed=0, tensile=False, blank_frac=0.0, tool_push_
     st["grid"] = (tuple(s.grid_bbmin), tuple(s.grid_bbmax), s.grid_h)
     tool = mf.ToolState()
     C.memmove(C.byref(tool), C.byref(s.tool), C.sizeof(mf.ToolState))
-    # push the tool into the workpiece so that particles are inside it
+    # push the tool into the workpiece so that particles are inside it: close the gap
+    # between the tool's front and the workpiece's left edge, then tool_push_dx cells more
     if tool_push_dx:
-        t_push = tool_push_dx * dx / tool.vel[0]
+        xs = [tool.seg[i].left[0] for i in range(tool.num_seg)] + [tool.seg[i].right[0] for i in range(tool.num_seg)]
+        if tool.has_fillet:
+            xs.append(tool.fillet.p[0] + tool.fillet.r)
+        gap = float(st["pos"][wp, 0].min()) - max(xs)
+        t_push = (gap + tool_push_dx * dx) / tool.vel[0]
         mf.tool_translate(tool, t_push)
         st["pos"][~wp] += t_push * np.array([tool.vel[0], tool.vel[1]])
     st["tool"] = tool

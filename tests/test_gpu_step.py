@@ -6,7 +6,10 @@ Tolerances (norm-wise, max|a-b| / max|b| per field):
     versions and glibc's differ by a few float ulps);
   * pair sums / rates given identical inputs: 1e-12;
   * corrector .. contact given identical inputs: 1e-12;
-  * full steps with compressive states (R = 0): 1e-11.
+  * full steps with compressive states (R = 0): 1e-11;
+  * eps_pl_dot: 1e-7, because the reference rounds the plastic multiplier to float
+    (fmaxf, actions_gpu.cu:264-265): a last-bit difference of the secant result between
+    CUDA's and glibc's pow/log moves it by one float ulp.
 Cell lists, flags, permutations and the tool are compared bit for bit.
 """
 import ctypes as C
@@ -23,16 +26,20 @@ STATE = ("pos", "vel", "S", "rho", "T", "eps_pl", "eps_pl_dot", "fc", "ft", "n")
 RATES = ("pos_t", "vel_t", "S_t", "rho_t", "T_t")
 
 
+FLOAT_ROUNDED = {"eps_pl_dot": 1e-7}
+
+
 def check(ctx, o, fields, tol, mask=None):
     worst = {}
     for f in fields:
+        ftol = max(tol, FLOAT_ROUNDED.get(f, 0.0))
         a, b = ctx.get(f), o.get(f)
         if mask is not None:
             a, b = a[mask], b[mask]
         e = rel_err(a, b)
         worst[f] = e
         assert np.isfinite(a).all() == np.isfinite(b).all(), f
-        assert e <= tol, (f, e)
+        assert e <= ftol, (f, e)
     return worst
 
 
