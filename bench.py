@@ -193,11 +193,16 @@ def time_form(mf, torch, scene, precision, steps, warmup, device):
     return step_ms, np.array(pair), st
 
 
+E2E_FIELDS = ("pos", "vel", "h", "rho", "T", "fixed", "blanked", "tool_p", "S", "eps_pl", "eps_pl_dot", "fc", "ft",
+              "n", "pos_t", "vel_t", "rho_t", "S_t", "T_t")
+
+
 def e2e_form(mf, torch, scene, precision, steps, device):
     """End to end through the C ABI with host buffers. Outside the timed region: context,
-    device buffers and the step graphs (created once per run). Inside: the particle state
-    copied in from pinned host memory (mf_set_field), `steps` x (mf_step(1) + a copy of that
-    step's tool force to pinned host memory), and the final state copied back to the host."""
+    device buffers and the step graphs (created once per run). Inside: the complete particle
+    state copied in from pinned host memory (mf_set_field, all per-particle fields, in one
+    consistent order), `steps` x (mf_step(1) + a copy of that step's tool force to pinned
+    host memory), and the final state copied back to the host."""
     ctx = mf.Context(device)
     ctx.upload_scene(scene, mf.GRID_GREEN)
     ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
@@ -205,9 +210,12 @@ def e2e_form(mf, torch, scene, precision, steps, device):
     ctx.synchronize()
     n = scene.N
     init = {}
-    for f, w in (("pos", 2), ("vel", 2), ("rho", 1), ("T", 1), ("S", 4), ("eps_pl", 1), ("eps_pl_dot", 1),
-                 ("fc", 2), ("ft", 2), ("pos_t", 2), ("vel_t", 2), ("rho_t", 1), ("S_t", 4), ("T_t", 1)):
-        src = scene.array(f) if f in ("pos", "vel", "rho", "T") else np.zeros((n, w) if w > 1 else n)
+    for f in E2E_FIELDS:
+        w = mf.FIELDS[f][1]
+        if f in ("pos", "vel", "h", "rho", "T", "fixed", "tool_p"):
+            src = scene.array(f)
+        else:
+            src = np.zeros((n, w) if w > 1 else n)
         init[f] = torch.from_numpy(np.ascontiguousarray(src, dtype=np.float64)).pin_memory()
     forces = torch.zeros((steps, 2), dtype=torch.float64).pin_memory()
     out_fields = ("pos", "vel", "S", "rho", "T", "eps_pl")
@@ -222,9 +230,9 @@ def e2e_form(mf, torch, scene, precision, steps, device):
     t1 = time.perf_counter()
     h2d = sum(t.numel() * 8 for t in init.values())
     d2h = sum(v.nbytes for v in out.values())
-    assert np.isfinite(forces.numpy()).all()
+    finite = bool(np.isfinite(forces.numpy()).all())
     ctx.close()
-    return (t1 - t0), h2d, d2h
+    return (t1 - t0), h2d, d2h, finite
 
 
 def cpu_baseline(mf, scene, seconds=12.0, max_steps=5000):
@@ -325,6 +333,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=500)
+    ap.add_argument("--lattice-scale", type=float, default=1.0,
+                    help="lattice points per dimension relative to 714 x 214 (same 2.0 x 0.6 mm body); "
+                         "values below 1 give the smaller profiling case")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -343,7 +354,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", device))
     mf = load_package()
-    scene = mf.Scene.from_params(cut_params(mf))
+    sc = args.lattice_scale
+    scene = mf.Scene.from_params(cut_params(mf, nx=int(round(714 * sc)), ny=int(round(214 * sc)), dx=2.8e-4 / sc))
     N = scene.N
 
     results = {}
@@ -382,7 +394,9 @@ def main():
 
     e2e = None
     if rank == 0:
-        secs, h2d, d2h = e2e_form(mf, torch, scene, mf.PRECISION_MIXED, args.e2e_steps, device)
+        secs, h2d, d2h, finite = e2e_form(mf, torch, scene, mf.PRECISION_MIXED, args.e2e_steps, device)
+        if not finite:
+            raise SystemExit("e2e: non-finite tool force in the end-to-end run")
         e2e = {"value": N * args.e2e_steps / secs, "unit": "particle-steps/s",
                "h2d_bytes_per_step": h2d / args.e2e_steps, "d2h_bytes_per_step": 16 + d2h / args.e2e_steps,
                "steps": args.e2e_steps,

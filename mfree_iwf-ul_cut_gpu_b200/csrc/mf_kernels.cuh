@@ -75,7 +75,7 @@ __device__ __forceinline__ void bbox_merge(double *a, const double *b) {
   a[4] = fmax(a[4], b[4]);
 }
 
-__global__ void __launch_bounds__(BLOCK) k_bbox(int N, const double2 *__restrict__ pos,
+static __global__ void __launch_bounds__(BLOCK) k_bbox(int N, const double2 *__restrict__ pos,
                                                 const double *__restrict__ h, dev_buffers D) {
   __shared__ double sm[BLOCK / 32][5];
   __shared__ bool last;
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(BLOCK) k_bbox(int N, const double2 *__restrict
 
 // ---------------------------------------------------------------------------------------
 // cell hash + count (compute_hashes, grid.cu:34-51)
-__global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A, dev_buffers D, int num_scan_tiles,
+static __global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A, dev_buffers D, int num_scan_tiles,
                                                       int advance_tool, double dt) {
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   if (advance_tool && gid == 0) {
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A, dev_bu
 // exclusive scan of the cell counts -> offsets, single pass with decoupled look-back.
 // Tile ids come from an atomic ticket, so every tile waits only on tiles that are already
 // running; the wait is bounded and reports ERR_SCAN_WAIT instead of hanging.
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int N) {
+static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int N) {
   __shared__ int s_tile;
   __shared__ int s_warp[SCAN_THREADS / 32];
   __shared__ int s_excl;
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int N) {
   (void)N;
 }
 
-__global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D) {
+static __global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= N) return;
   D.perm_u[D.off[D.hash_new[q]] + D.slot[q]] = q;
@@ -288,7 +288,7 @@ __device__ __forceinline__ int stable_member(const dev_buffers &D, int q) {
 // (leap_frog.cu:30-66), EOS (actions_gpu.cu:41-51), artificial stress (:53-97) and the
 // neighbour records read by the pair kernel.
 template <bool PREDICT, bool MIXED>
-__global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers D) {
+static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const int p = stable_member(D, q);
@@ -367,13 +367,14 @@ __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers D) {
   for (int k = 0; k < R_WIDTH / 2; ++k) dst[k] = make_double2(r[2 * k], r[2 * k + 1]);
 
   if (MIXED) {
-    // FP32 record: position relative to the origin of the particle's own cell
+    // FP32 record: position relative to the origin of the particle's own cell, temperature
+    // relative to the initial temperature (only differences of T enter the pair sums)
     const geom g = *D.g;
     const int ci = hsh / g.ny, cj = hsh - ci * g.ny;
     const double ox = g.bbmin_x + ci * g.dx, oy = g.bbmin_y + cj * g.dx;
     float fr[F_WIDTH] = {(float)(pos.x - ox), (float)(pos.y - oy), (float)vel.x, (float)vel.y, (float)sxx,
                          (float)sxy, (float)syy, (float)Rxx, (float)Rxy, (float)Ryy, (float)h, (float)rho,
-                         (float)c, (float)vol, (float)T,
+                         (float)c, (float)vol, (float)(T - P.trml_wp.T_init),
                          __int_as_float((int)(rf | ((unsigned)cj << 8)))};
     float4 *fd = reinterpret_cast<float4 *>(D.recf + (size_t)q * F_WIDTH);
 #pragma unroll
@@ -397,7 +398,7 @@ __device__ __forceinline__ void load_rec(const double *__restrict__ rec, int j, 
   }
 }
 
-__global__ void __launch_bounds__(PAIR_BLOCK) k_pair_fp64(params P, dev_buffers D) {
+static __global__ void __launch_bounds__(PAIR_BLOCK) k_pair_fp64(params P, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const double *__restrict__ rec = D.rec;
@@ -534,7 +535,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pair_fp64(params P, dev_buffers 
 
 // PSE heat Laplacian (interactions_gpu.cu:88-144): every particle of the window, blanked
 // ones included; alpha taken through the reference's half-length texture binding (:405).
-__global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers D) {
+static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const double *__restrict__ rec = D.rec;
@@ -576,7 +577,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers D) {
 // ---------------------------------------------------------------------------------------
 // corrector .. invalidate, per particle, plus the tool force (leap_frog.cu:68-92,
 // actions_gpu.cu:135-162,226-349, tool_gpu.cu:151-221, output.cu:31-39)
-__global__ void __launch_bounds__(BLOCK) k_finish(params P, dev_buffers D) {
+static __global__ void __launch_bounds__(BLOCK) k_finish(params P, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   ksum fcx{0., 0.}, fcy{0., 0.}, ftx{0., 0.}, fty{0., 0.};
   unsigned newly_blanked = 0, capped = 0, blanked_now = 0;
@@ -809,7 +810,7 @@ __global__ void __launch_bounds__(BLOCK) k_finish(params P, dev_buffers D) {
 }
 
 // report_force on the current state without stepping (output.cu:31-39)
-__global__ void __launch_bounds__(BLOCK) k_force_only(int N, const double2 *__restrict__ fc,
+static __global__ void __launch_bounds__(BLOCK) k_force_only(int N, const double2 *__restrict__ fc,
                                                       const double2 *__restrict__ ft, dev_buffers D) {
   __shared__ ksum sm[BLOCK / 32][4];
   ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};

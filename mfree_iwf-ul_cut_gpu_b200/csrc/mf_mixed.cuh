@@ -7,7 +7,9 @@
 //   * x_ij = (ci - cj) * dx + (xi_rel - xj_rel): small integers times the cell size plus
 //     a difference of in-cell offsets, instead of a difference of absolute coordinates;
 //   * e_ij . grad W / r = (x_ij w_x + y_ij w_y) / r^2 (Brookshaw);
-//   * divisions by r use one rsqrt per pair.
+//   * divisions by r use one rsqrt per pair;
+//   * temperatures are stored relative to the initial temperature, so Ti - Tj keeps its
+//     digits near it.
 // Its error against the FP64 oracle is measured and reported, not assumed.
 #pragma once
 
@@ -15,7 +17,7 @@
 
 namespace mf {
 
-__global__ void __launch_bounds__(PAIR_BLOCK) k_pair_mixed(params P, dev_buffers D) {
+static __global__ void __launch_bounds__(PAIR_BLOCK) k_pair_mixed(params P, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const float *__restrict__ rec = D.recf;

@@ -13,6 +13,7 @@ Tolerances (norm-wise, max|a-b| / max|b| per field):
 Cell lists, flags, permutations and the tool are compared bit for bit.
 """
 import ctypes as C
+import math
 
 import numpy as np
 import pytest
@@ -108,8 +109,14 @@ def test_full_steps_compressive(mf, orc, grid_kind):
         check(ctx, o, STATE + RATES, tol)
         assert np.array_equal(ctx.get("blanked"), o.get("blanked"))
     assert tool_bits(mf, orc, ctx, o)
-    f1, f2 = ctx.report_force(), o.report_force()
-    assert rel_err(f1, f2) <= 1e-10
+    # per-particle forces matched above; the net force cancels, so check the reduction
+    # itself: the compensated device sum against the exact sum of the device's own forces
+    f1 = ctx.report_force()
+    fc, ft = ctx.get("fc"), ctx.get("ft")
+    exact = np.array([math.fsum(np.concatenate([fc[:, k], ft[:, k]])) for k in range(2)])
+    scale = np.abs(fc).sum(axis=0) + np.abs(ft).sum(axis=0)
+    assert np.all(np.abs(f1 - exact) <= 1e-15 * scale)
+    assert rel_err(f1, o.report_force()) <= 1e-8
 
 
 def test_graphs_match_direct_launches(mf):
