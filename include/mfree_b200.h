@@ -174,6 +174,23 @@ int mf_force_last_async(mf_ctx *ctx, double *host_out2);
 int mf_force_log(mf_ctx *ctx, double *out, int max_entries, int *n_out);
 int mf_status_get(mf_ctx *ctx, mf_status *status);
 
+/* ---- cell list without device allocation (no counterpart in the reference) ----
+   For callers that cannot allocate device memory (a host that reserves all device memory at
+   start-up and allows no driver allocation later, or a foreign-language binding that passes
+   device pointers but has no access to the CUDA allocator): the hash, stable permutation and
+   grid_gpu_green-format cell bounds that mf_grid_build computes for a locked grid, from
+   caller-owned device buffers only (d_pos: 2N doubles; d_hash_sorted, d_idx: N ints;
+   d_cell_start, d_cell_end: nx*ny ints, -1 on empty cells), queued on `stream`. The grid is
+   given directly (origin bbmin, cell size dx, nx x ny cells, as mf_grid_geometry reports).
+   Scratch is one fixed device array inside the library, so N is limited to
+   MF_NOALLOC_MAX_PARTICLES and nx*ny to MF_NOALLOC_MAX_CELLS (MF_ERR_RANGE beyond). The first
+   call on a device looks up that array's address; make it before any stream capture. Calls
+   share the array: calls that overlap on the GPU race. No cudaMalloc/cudaFree is made. */
+#define MF_NOALLOC_MAX_PARTICLES (1 << 19)
+#define MF_NOALLOC_MAX_CELLS (1 << 21)
+int mf_cells_build_noalloc(const double *d_pos, int N, double bbmin_x, double bbmin_y, double dx, int nx, int ny,
+                           int *d_hash_sorted, int *d_idx, int *d_cell_start, int *d_cell_end, void *stream);
+
 /* ---- host scene setup: setup_ref_cut (benchmarks.cpp:255-537) and its generalisation ---- */
 typedef struct {
   int N, n_workpiece, n_tool;
