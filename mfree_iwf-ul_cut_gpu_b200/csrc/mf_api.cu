@@ -36,9 +36,15 @@ struct mf_ctx {
   state_set set[2]{};
   int cur = 0;          // set holding the current state
   bool mid_step = false; // stages 1-2 ran: reads see the step's buffer
+  bool last_staged = false; // the last predictor ran staged (all intermediates stored)
   int scan_tiles = 0;   // tiles for max_cell + 1 entries
   int finish_blocks = 0;
   int bbox_blocks = 0;
+  int sm_count = 148;
+  mf_tool_state *tool_buf[2] = {nullptr, nullptr};  // tool after the last step, by parity
+  // k_finish of the last step already hashed and counted the particles for the next one
+  // (locked grid): the next step starts at the scan
+  bool counts_ready = false;
   std::vector<void *> particle_allocs, grid_allocs, fixed_allocs;
   // graphs: one per parity of the double buffer
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -108,6 +114,15 @@ int alloc_set(mf_ctx *ctx, state_set &s, int N) {
   return MF_OK;
 }
 
+// the counts the last step's k_finish prepared are stale once the host changes the state
+int invalidate_counts(mf_ctx *ctx) {
+  if (ctx->counts_ready && ctx->D.count) {
+    CK(cudaMemsetAsync(ctx->D.count, 0, sizeof(int) * (size_t)ctx->G.max_cell, ctx->stream));
+  }
+  ctx->counts_ready = false;
+  return MF_OK;
+}
+
 int alloc_particles(mf_ctx *ctx, int N) {
   drop_graphs(ctx);
   free_list(ctx->particle_allocs);
@@ -126,9 +141,10 @@ int alloc_particles(mf_ctx *ctx, int N) {
   TRY(dalloc(ctx, L, &D.slot, N));
   TRY(dalloc(ctx, L, &D.perm_u, N));
   TRY(dalloc(ctx, L, &D.perm, N));
-  ctx->finish_blocks = (N + BLOCK - 1) / BLOCK;
-  ctx->bbox_blocks = std::min(ctx->finish_blocks, 148 * 4);
-  TRY(dalloc(ctx, L, &D.partials, (size_t)std::max(ctx->finish_blocks, 1) * 8));
+  ctx->finish_blocks = std::min((N + BLOCK - 1) / BLOCK, ctx->sm_count * FINISH_BLOCKS_PER_SM);
+  ctx->bbox_blocks = std::min((N + BLOCK - 1) / BLOCK, ctx->sm_count * 4);
+  TRY(dalloc(ctx, L, &D.partials, (size_t)std::max(std::max(ctx->finish_blocks, ctx->bbox_blocks), 1) * 8));
+  TRY(invalidate_counts(ctx));
   ctx->N = N;
   return MF_OK;
 }
@@ -141,8 +157,10 @@ int alloc_grid(mf_ctx *ctx, int max_cell) {
   TRY(dalloc(ctx, L, &ctx->D.off, (size_t)max_cell + 1));
   ctx->scan_tiles = (max_cell + SCAN_TILE - 1) / SCAN_TILE + 1;
   TRY(dalloc(ctx, L, &ctx->D.scan_status, (size_t)ctx->scan_tiles));
+  ctx->counts_ready = false;
   return MF_OK;
 }
+
 
 int upload_geom(mf_ctx *ctx) {
   CK(cudaMemcpyAsync(ctx->D.g, &ctx->G, sizeof(geom), cudaMemcpyHostToDevice, ctx->stream));
@@ -152,7 +170,13 @@ int upload_geom(mf_ctx *ctx) {
 void bind_sets(mf_ctx *ctx) {
   ctx->D.A = ctx->set[ctx->cur];
   ctx->D.B = ctx->set[ctx->cur ^ 1];
+  ctx->D.tool_prev = ctx->tool_buf[ctx->cur];
+  ctx->D.tool_next = ctx->tool_buf[ctx->cur ^ 1];
 }
+
+// the steady-state step of a locked grid starts at the scan: the previous step's k_finish
+// hashed and counted the particles
+bool fused_step(const mf_ctx *ctx) { return ctx->G.locked && !ctx->P.staged; }
 
 bool ready(const mf_ctx *ctx) { return ctx->has_particles && ctx->has_grid && ctx->has_constants; }
 
@@ -164,9 +188,10 @@ int launch_cells(mf_ctx *ctx, bool step_mode) {
   bind_sets(ctx);
   if (!ctx->G.locked)
     k_bbox<<<ctx->bbox_blocks, BLOCK, 0, ctx->stream>>>(N, ctx->D.A.pos, ctx->D.A.h, ctx->D);
-  const int hash_blocks = std::max(nb, (ctx->scan_tiles + BLOCK - 1) / BLOCK);
-  k_hash_count<<<hash_blocks, BLOCK, 0, ctx->stream>>>(N, ctx->D.A, ctx->D, ctx->scan_tiles,
-                                                        step_mode && ctx->P.has_tool ? 1 : 0, ctx->P.dt);
+  if (!(step_mode && fused_step(ctx))) {
+    const int hash_blocks = std::max(nb, (ctx->scan_tiles + BLOCK - 1) / BLOCK);
+    k_hash_count<<<hash_blocks, BLOCK, 0, ctx->stream>>>(N, ctx->D.A, ctx->D, ctx->scan_tiles);
+  }
   k_scan<<<ctx->scan_tiles, SCAN_THREADS, 0, ctx->stream>>>(ctx->D, N);
   k_scatter<<<nb, BLOCK, 0, ctx->stream>>>(N, ctx->D);
   return MF_OK;
@@ -193,7 +218,8 @@ int launch_stage(mf_ctx *ctx, int stage) {
         k_pse<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
       break;
     case 3:
-      k_finish<<<ctx->finish_blocks, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      if (fused_step(ctx)) k_finish<true><<<ctx->finish_blocks, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D, ctx->scan_tiles);
+      else k_finish<false><<<ctx->finish_blocks, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D, ctx->scan_tiles);
       break;
     default:
       return MF_ERR_INVALID;
@@ -205,6 +231,19 @@ int launch_stage(mf_ctx *ctx, int stage) {
 
 int launch_step(mf_ctx *ctx) {
   for (int s = 0; s < 4; ++s) TRY(launch_stage(ctx, s));
+  return MF_OK;
+}
+
+// hash + count for the first fused step (afterwards each step's k_finish prepares them)
+int prime_counts(mf_ctx *ctx) {
+  if (!fused_step(ctx) || ctx->counts_ready) return MF_OK;
+  bind_sets(ctx);
+  const int nb = (ctx->N + BLOCK - 1) / BLOCK;
+  const int hash_blocks = std::max(nb, (ctx->scan_tiles + BLOCK - 1) / BLOCK);
+  k_hash_count<<<hash_blocks, BLOCK, 0, ctx->stream>>>(ctx->N, ctx->D.A, ctx->D, ctx->scan_tiles);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { ctx->last_cuda_err = (int)e; return MF_ERR_CUDA; }
+  ctx->counts_ready = true;
   return MF_OK;
 }
 
@@ -319,7 +358,13 @@ int mf_ctx_create(int device, mf_ctx **out) {
   }
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.g, 1);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.st, 1);
-  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.tool, 1);
+  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->tool_buf[0], 1);
+  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->tool_buf[1], 1);
+  if (rc == MF_OK) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
+      ctx->sm_count = sms;
+  }
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.ticket, 4);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.scan_done, 1);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.force_log, (size_t)FORCE_LOG_CAP * 2);
@@ -374,6 +419,9 @@ int mf_particles_create(mf_ctx *ctx, int N, const double *pos, const double *vel
   TRY(set_device(ctx));
   CK(cudaStreamSynchronize(ctx->stream));
   TRY(alloc_particles(ctx, N));
+  // the tool set so far stays the current one when the parity restarts at 0
+  if (ctx->cur != 0)
+    CK(cudaMemcpy(ctx->tool_buf[0], ctx->tool_buf[ctx->cur], sizeof(mf_tool_state), cudaMemcpyDeviceToDevice));
   ctx->cur = 0;
   state_set &s = ctx->set[0];
   CK(cudaMemcpy(s.pos, pos, sizeof(double) * 2 * (size_t)N, cudaMemcpyHostToDevice));
@@ -417,9 +465,21 @@ int mf_get_field(mf_ctx *ctx, int field, void *host) {
     return MF_OK;
   }
   if (field == MF_FIELD_R) {
+    double *o = (double *)host;
+    if (ctx->P.precision == MF_PRECISION_MIXED && ctx->P.thermal_solver != MF_THERMAL_PSE && !ctx->last_staged) {
+      // mixed form: R lives only in the FP32 pair records
+      std::vector<float> rec(N * F_WIDTH);
+      CK(cudaMemcpy(rec.data(), ctx->D.recf, sizeof(float) * N * F_WIDTH, cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < N; ++i) {
+        o[4 * i] = rec[i * F_WIDTH + F_RXX];
+        o[4 * i + 1] = rec[i * F_WIDTH + F_RXY];
+        o[4 * i + 2] = rec[i * F_WIDTH + F_RYY];
+        o[4 * i + 3] = 0.;
+      }
+      return MF_OK;
+    }
     std::vector<double> rec(N * R_WIDTH);
     CK(cudaMemcpy(rec.data(), ctx->D.rec, sizeof(double) * N * R_WIDTH, cudaMemcpyDeviceToHost));
-    double *o = (double *)host;
     for (size_t i = 0; i < N; ++i) {
       o[4 * i] = rec[i * R_WIDTH + R_RXX];
       o[4 * i + 1] = rec[i * R_WIDTH + R_RXY];
@@ -440,6 +500,7 @@ int mf_set_field(mf_ctx *ctx, int field, const void *host) {
   if (!ctx || !host || field < 0 || field >= MF_NUM_FIELDS) return MF_ERR_INVALID;
   if (!ctx->has_particles) return MF_ERR_STATE;
   TRY(set_device(ctx));
+  TRY(invalidate_counts(ctx));
   CK(cudaStreamSynchronize(ctx->stream));
   const size_t N = (size_t)ctx->N;
   unsigned bit = flag_bit(field);
@@ -528,6 +589,7 @@ int mf_grid_build(mf_ctx *ctx) {
   if (!ctx->has_particles || !ctx->has_grid || ctx->mid_step) return MF_ERR_STATE;
   TRY(set_device(ctx));
   ctx->P.N = ctx->N;
+  TRY(invalidate_counts(ctx));
   TRY(launch_cells(ctx, false));
   const int nb = (ctx->N + BLOCK - 1) / BLOCK;
   k_reorder<false, false><<<nb, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
@@ -617,7 +679,7 @@ int mf_tool_set(mf_ctx *ctx, const mf_tool_state *tool) {
   }
   ctx->tool = t;
   ctx->P.has_tool = t.num_seg > 0 ? 1 : 0;
-  CK(cudaMemcpy(ctx->D.tool, &t, sizeof(t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->tool_buf[ctx->cur], &t, sizeof(t), cudaMemcpyHostToDevice));
   drop_graphs(ctx);
   return MF_OK;
 }
@@ -626,7 +688,9 @@ int mf_tool_get(mf_ctx *ctx, mf_tool_state *tool) {
   if (!ctx || !tool) return MF_ERR_INVALID;
   TRY(set_device(ctx));
   CK(cudaStreamSynchronize(ctx->stream));
-  CK(cudaMemcpy(tool, ctx->D.tool, sizeof(*tool), cudaMemcpyDeviceToHost));
+  // during a staged step the tool advances in stage 3 (tool_gpu_update_tool after the
+  // plasticity, leap_frog.cu:142-145): until then this is the tool at the start of the step
+  CK(cudaMemcpy(tool, ctx->tool_buf[ctx->cur], sizeof(*tool), cudaMemcpyDeviceToHost));
   return MF_OK;
 }
 
@@ -638,6 +702,8 @@ int mf_step(mf_ctx *ctx, int n_steps) {
   ctx->P.N = ctx->N;
   const bool graphs = !(ctx->flags & MF_OPT_NO_GRAPHS);
   if (graphs && !ctx->graph_valid) TRY(build_graphs(ctx));
+  if (n_steps > 0) ctx->last_staged = false;
+  if (n_steps > 0) TRY(prime_counts(ctx));
   for (int k = 0; k < n_steps; ++k) {
     if (graphs) {
       CK(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
@@ -657,8 +723,12 @@ int mf_step_stage(mf_ctx *ctx, int stage) {
   ctx->P.N = ctx->N;
   // stages 1..2 leave the half-built step in the other buffer; reads during the step see it
   if (stage == 0 && ctx->mid_step) return MF_ERR_STATE;
-  TRY(launch_stage(ctx, stage));
-  if (stage == 1) ctx->mid_step = true;
+  if (stage == 0) TRY(invalidate_counts(ctx));
+  ctx->P.staged = 1;
+  int rc_stage = launch_stage(ctx, stage);
+  ctx->P.staged = 0;
+  TRY(rc_stage);
+  if (stage == 1) { ctx->mid_step = true; ctx->last_staged = true; }
   if (stage == 3) {
     ctx->cur ^= 1;
     ctx->steps++;

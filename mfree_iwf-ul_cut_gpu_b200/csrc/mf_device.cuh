@@ -27,9 +27,10 @@ enum : int {
 };
 
 // FP32 pair record of the mixed form (16 floats = 64 bytes): coordinates relative to the
-// origin of the particle's own cell
+// origin of the particle's own cell; the first 16 bytes (x, y, flags | cell_y << 8, vx) are
+// all the distance test needs
 enum : int {
-  F_X = 0, F_Y, F_VX, F_VY, F_SXX, F_SXY, F_SYY, F_RXX, F_RXY, F_RYY, F_H, F_RHO, F_C, F_VOL, F_T, F_FLAGS,
+  F_X = 0, F_Y, F_FLAGS, F_VX, F_VY, F_SXX, F_SXY, F_SYY, F_RXX, F_RXY, F_RYY, F_H, F_RHO, F_C, F_VOL, F_T,
   F_WIDTH
 };
 
@@ -40,6 +41,7 @@ struct params {
   int jc_model;
   int precision;
   int plastic, fric_heat, thermal_bc, thermal_wp, thermal_tool_on, has_tool, keep_derivs;
+  int staged;  // step run stage by stage (mf_step_stage): keep every intermediate array
   double dt;
   mf_phys_constants phys;
   mf_corr_constants corr;
@@ -76,8 +78,10 @@ constexpr int ERR_GRID_BUDGET = 2;
 // SPH kernel function: cubic spline (kernels.cuh:30-70). hi enters through h1 = 1/hi and
 // fourh2 = 4*hi*hi, computed once per particle i exactly as the reference computes them
 // per pair. Returns false (w = 0) outside the support or for r^2 < 1e-8.
+// Also returns dwr = der*fac, the radial factor of the gradient (grad W = dwr * x_ij), which
+// is (e_ij . grad W) / r of the Brookshaw Laplacian.
 __device__ __forceinline__ void cubic_spline_fp64(double xij, double yij, double rr2, double h1,
-                                                  double &w, double &w_x, double &w_y) {
+                                                  double &w, double &w_x, double &w_y, double &dwr) {
   constexpr double PI_FAC = 0.454728408833987;
   double der, val;
   double rad = (double)sqrtf((float)rr2);
@@ -95,6 +99,7 @@ __device__ __forceinline__ void cubic_spline_fp64(double xij, double yij, double
   w = val * fac;
   w_x = der * xij * fac;
   w_y = der * yij * fac;
+  dwr = der * fac;
 }
 
 // PSE Laplacian kernel (kernels.cuh:72-89)
@@ -156,8 +161,10 @@ __device__ __forceinline__ void jaumann(double G, double vx_x, double vx_y, doub
 }
 
 // ---------------------------------------------------------------------------------------
-// Johnson-Cook flow stress (plasticity.cuh:30-46) and the tanh variant (:48-70)
-__device__ __forceinline__ double sigma_yield(const mf_joco_constants &jc, double eps_pl, double eps_pl_dot,
+// Johnson-Cook flow stress (plasticity.cuh:30-46) and the tanh variant (:48-70). Kept out of
+// line: each call holds several pow/log expansions, and one copy keeps the instruction cache
+// and the caller's register budget small.
+static __device__ __noinline__ double sigma_yield(const mf_joco_constants &jc, double eps_pl, double eps_pl_dot,
                                               double t) {
   double theta = (t - jc.Tref) / (jc.Tmelt - jc.Tref);
   double Term_A = jc.A + jc.B * pow(eps_pl, jc.n);
@@ -169,7 +176,7 @@ __device__ __forceinline__ double sigma_yield(const mf_joco_constants &jc, doubl
   return Term_A * Term_B * Term_C;
 }
 
-__device__ __forceinline__ double sigma_yield_tanh(const mf_joco_constants &jc, double eps_pl, double eps_dot_pl,
+static __device__ __noinline__ double sigma_yield_tanh(const mf_joco_constants &jc, double eps_pl, double eps_dot_pl,
                                                    double t) {
   double theta = (t - jc.Tref) / (jc.Tmelt - jc.Tref);
   double Term_A = jc.A + jc.B * pow(eps_pl, jc.n) * 1.0 / exp(pow(eps_pl, jc.tanh_a));
@@ -196,8 +203,8 @@ __device__ __forceinline__ double opt_fun(const mf_joco_constants &jc, int model
   return norm_Strial - 2 * mu * delta_lambda - s23 * sigmaY;
 }
 
-// secant iteration (plasticity.cuh:85-119): at most 102 evaluations pairs; capped -> flag
-__device__ __forceinline__ double solve_secant(const mf_joco_constants &jc, int model, double init, double tol,
+// secant iteration (plasticity.cuh:85-119): at most 102 evaluation pairs; capped -> flag
+static __device__ __noinline__ double solve_secant(const mf_joco_constants &jc, int model, double init, double tol,
                                                double norm_Strial, double eps_pl_init, double t, double delta_t,
                                                double mu, bool &capped) {
   double delta_lambda = init;

@@ -2,8 +2,9 @@
 //
 // Per step, on one stream (captured once into a CUDA graph):
 //   k_bbox        adaptive grid only: min/max reduction -> geometry     (grid.cu:97-136)
-//   k_hash_count  cell hash per particle + atomic per-cell count;       (grid.cu:34-51)
-//                 block 0 also advances the rigid tool                  (tool.cpp:211-221)
+//   k_hash_count  cell hash per particle + atomic per-cell count       (grid.cu:34-51);
+//                 with a locked grid only before the first step, after that k_finish of
+//                 the previous step has done it
 //   k_scan        single-pass decoupled look-back exclusive scan of the
 //                 counts -> cell offsets (the cell_start/cell_end lists)
 //   k_scatter     particle -> slot inside its cell
@@ -14,10 +15,11 @@
 //   k_pair_fp64   the pair sums over the 5x5 cell window (interactions_gpu.cu:147-345) and the
 //                 rates: Jaumann, continuity, momentum, advection (actions_gpu.cu:99-224)
 //   k_pse         PSE heat Laplacian (interactions_gpu.cu:88-144), PSE solver only
-//   k_finish      corrector, friction heat, JC plasticity, tool particles, contact, boundary
-//                 conditions, invalidation and the compensated tool-force reduction
-//                 (leap_frog.cu:68-92, actions_gpu.cu:135-162,226-349, tool_gpu.cu:151-221,
-//                 output.cu:31-39)
+//   k_finish      corrector, friction heat, JC plasticity, the rigid tool's advance, tool
+//                 particles, contact, boundary conditions, invalidation and the compensated
+//                 tool-force reduction; with a locked grid also the next step's hashes and
+//                 counts (leap_frog.cu:68-92, actions_gpu.cu:135-162,226-349, tool.cpp:211-221,
+//                 tool_gpu.cu:151-221, output.cu:31-39)
 #pragma once
 
 #include "mf_device.cuh"
@@ -49,7 +51,8 @@ struct dev_buffers {
   unsigned *ticket;     // last-block tickets: [0] force, [1] bbox
   double *force_log;    // FORCE_LOG_CAP x 2
   double *force_last;   // 2
-  mf_tool_state *tool;
+  mf_tool_state *tool_prev;  // tool after the previous step (read)
+  mf_tool_state *tool_next;  // tool after this step (written by k_finish)
   geom *g;
   dev_status *st;
 };
@@ -58,6 +61,8 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 8;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr int BLOCK = 256;
+// k_finish runs a grid-stride loop over a fixed grid of this many blocks per SM
+constexpr int FINISH_BLOCKS_PER_SM = 2;
 constexpr int PAIR_BLOCK = 128;
 constexpr unsigned long long SCAN_FLAG_AGG = 1ull << 62;
 constexpr unsigned long long SCAN_FLAG_PREFIX = 2ull << 62;
@@ -130,14 +135,8 @@ static __global__ void __launch_bounds__(BLOCK) k_bbox(int N, const double2 *__r
 
 // ---------------------------------------------------------------------------------------
 // cell hash + count (compute_hashes, grid.cu:34-51)
-static __global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A, dev_buffers D, int num_scan_tiles,
-                                                      int advance_tool, double dt) {
+static __global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A, dev_buffers D, int num_scan_tiles) {
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (advance_tool && gid == 0) {
-    mf_tool_state T = *D.tool;
-    tool_translate_rn(T, dt);
-    *D.tool = T;
-  }
   for (int t = gid; t < num_scan_tiles; t += gridDim.x * blockDim.x) D.scan_status[t] = 0ull;
   unsigned oog = 0;
   if (gid < N) {
@@ -207,32 +206,44 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int
       bmax = max(bmax, s_max[w]);
     }
     const int thread_excl = warp_excl + incl - tsum;
-    if (threadIdx.x == 0) {
-      if (bmax > 0) atomicMax(&D.st->max_cell_occupancy, bmax);
+    if (threadIdx.x < 32) {
+      // warp-wide look-back: lane l inspects tile (base - l); aggregates of the tiles up to
+      // the nearest inclusive prefix are summed in one round trip per 32 tiles
+      const unsigned lane = lane_id();
+      if (lane == 0 && bmax > 0) atomicMax(&D.st->max_cell_occupancy, bmax);
       int excl = 0;
       if (tile == 0) {
-        atomicExch(&D.scan_status[0], SCAN_FLAG_PREFIX | (unsigned long long)(unsigned)agg);
+        if (lane == 0) atomicExch(&D.scan_status[0], SCAN_FLAG_PREFIX | (unsigned long long)(unsigned)agg);
       } else {
-        atomicExch(&D.scan_status[tile], SCAN_FLAG_AGG | (unsigned long long)(unsigned)agg);
-        int t = tile - 1;
+        if (lane == 0) atomicExch(&D.scan_status[tile], SCAN_FLAG_AGG | (unsigned long long)(unsigned)agg);
+        int base = tile - 1;
         long long spins = 0;
-        while (t >= 0) {
-          unsigned long long w = *((volatile unsigned long long *)&D.scan_status[t]);
-          unsigned long long flag = w & (3ull << 62);
-          if (flag == 0ull) {
+        bool done = false;
+        while (!done) {
+          const int t = base - (int)lane;
+          unsigned long long w = 2ull << 62;  // before tile 0: an inclusive prefix of 0
+          if (t >= 0) w = *((volatile unsigned long long *)&D.scan_status[t]);
+          while (__any_sync(0xffffffffu, (w & (3ull << 62)) == 0ull)) {
             if (++spins > SCAN_SPIN_LIMIT) {
-              atomicOr(&D.st->error_flags, ERR_SCAN_WAIT);
+              if (lane == 0) atomicOr(&D.st->error_flags, ERR_SCAN_WAIT);
+              w = 2ull << 62;  // give up: the offsets of this step are wrong, flagged
               break;
             }
-            continue;
+            if ((w & (3ull << 62)) == 0ull) w = *((volatile unsigned long long *)&D.scan_status[t]);
           }
-          excl += (int)(unsigned)(w & 0xffffffffull);
-          if (flag == SCAN_FLAG_PREFIX) break;
-          --t;
+          const unsigned pre = __ballot_sync(0xffffffffu, (w & (3ull << 62)) == SCAN_FLAG_PREFIX);
+          const int last = pre ? __ffs(pre) - 1 : 31;  // nearest prefix (or the whole window)
+          int v = (int)lane <= last ? (int)(unsigned)(w & 0xffffffffull) : 0;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          excl += v;
+          done = pre != 0u;
+          base -= 32;
         }
-        atomicExch(&D.scan_status[tile], SCAN_FLAG_PREFIX | (unsigned long long)(unsigned)(excl + agg));
+        if (lane == 0)
+          atomicExch(&D.scan_status[tile], SCAN_FLAG_PREFIX | (unsigned long long)(unsigned)(excl + agg));
       }
-      s_excl = excl;
+      if (lane == 0) s_excl = excl;
     }
     __syncthreads();
     const int excl = s_excl + thread_excl;
@@ -334,11 +345,15 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
     rho = rho + 0.5 * dt * rho_t;
     T = T + 0.5 * dt * T_t;
   }
-  B.pos[q] = pos;
+  // the predicted velocity and stress are read by the pair kernels; position, density and
+  // temperature live in the pair records (the full predicted state is kept when staged)
   B.vel[q] = vel;
   B.S[q] = S;
-  B.rho[q] = rho;
-  B.T[q] = T;
+  if (!PREDICT || P.staged) {
+    B.pos[q] = pos;
+    B.rho[q] = rho;
+    B.T[q] = T;
+  }
   B.flags[q] = f;
   if (!PREDICT) return;
 
@@ -362,9 +377,12 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
   for (int k = 0; k < R_FLAGS; ++k) finite = finite && isfinite(r[k]);
   if (!finite) rf |= FLAG_NONFINITE;
   r[R_FLAGS] = __longlong_as_double((long long)rf);
-  double2 *dst = reinterpret_cast<double2 *>(D.rec + (size_t)q * R_WIDTH);
+  // the FP64 record feeds the FP64 pair kernel and the PSE pass (and R / p read-back)
+  if (!MIXED || P.staged || P.thermal_solver == MF_THERMAL_PSE) {
+    double2 *dst = reinterpret_cast<double2 *>(D.rec + (size_t)q * R_WIDTH);
 #pragma unroll
-  for (int k = 0; k < R_WIDTH / 2; ++k) dst[k] = make_double2(r[2 * k], r[2 * k + 1]);
+    for (int k = 0; k < R_WIDTH / 2; ++k) dst[k] = make_double2(r[2 * k], r[2 * k + 1]);
+  }
 
   if (MIXED) {
     // FP32 record: position relative to the origin of the particle's own cell, temperature
@@ -372,10 +390,9 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
     const geom g = *D.g;
     const int ci = hsh / g.ny, cj = hsh - ci * g.ny;
     const double ox = g.bbmin_x + ci * g.dx, oy = g.bbmin_y + cj * g.dx;
-    float fr[F_WIDTH] = {(float)(pos.x - ox), (float)(pos.y - oy), (float)vel.x, (float)vel.y, (float)sxx,
-                         (float)sxy, (float)syy, (float)Rxx, (float)Rxy, (float)Ryy, (float)h, (float)rho,
-                         (float)c, (float)vol, (float)(T - P.trml_wp.T_init),
-                         __int_as_float((int)(rf | ((unsigned)cj << 8)))};
+    float fr[F_WIDTH] = {(float)(pos.x - ox), (float)(pos.y - oy), __int_as_float((int)(rf | ((unsigned)cj << 8))),
+                         (float)vel.x, (float)vel.y, (float)sxx, (float)sxy, (float)syy, (float)Rxx, (float)Rxy,
+                         (float)Ryy, (float)h, (float)rho, (float)c, (float)vol, (float)(T - P.trml_wp.T_init)};
     float4 *fd = reinterpret_cast<float4 *>(D.recf + (size_t)q * F_WIDTH);
 #pragma unroll
     for (int k = 0; k < F_WIDTH / 4; ++k) fd[k] = make_float4(fr[4 * k], fr[4 * k + 1], fr[4 * k + 2], fr[4 * k + 3]);
@@ -398,7 +415,7 @@ __device__ __forceinline__ void load_rec(const double *__restrict__ rec, int j, 
   }
 }
 
-static __global__ void __launch_bounds__(PAIR_BLOCK) k_pair_fp64(params P, dev_buffers D) {
+static __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_pair_fp64(params P, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const double *__restrict__ rec = D.rec;
@@ -440,71 +457,82 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pair_fp64(params P, dev_b
   double vtx = 0., vty = 0., xtx = 0., xty = 0.;   // vel_t (AV), pos_t (XSPH)
   double T_lapl = 0.;
 
+  const double m_eps = -eps * mass;
   for (int ii = low_i; ii < high_i; ++ii) {
     const int j0 = __ldg(D.off + ii * g.ny + low_j);
     const int j1 = __ldg(D.off + ii * g.ny + high_j);
-    for (int j = j0; j < j1; ++j) {
-      const double2 *sj = reinterpret_cast<const double2 *>(rec + (size_t)j * R_WIDTH);
-      const double2 fx = __ldg(sj + 7);  // T, flags (R_T, R_FLAGS)
-      const unsigned fj = (unsigned)__double_as_longlong(fx.y);
-      if (fj & FLAG_BLANKED) continue;
-      const double2 xy = __ldg(sj + 0);
-      const double xij = xi - xy.x;
-      const double yij = yi - xy.y;
-      const double rr2 = xij * xij + yij * yij;
-      const bool in_support = !(rr2 >= fourh2 || rr2 < 1e-8);
-      // Outside the support the reference adds terms multiplied by W = 0: they change no
-      // finite sum, but a NaN/Inf operand turns the sum into NaN. Skip only when finite.
-      if (!in_support && !(nonfinite_i || (fj & FLAG_NONFINITE))) continue;
-      double w = 0., w_x = 0., w_y = 0.;
-      if (in_support) cubic_spline_fp64(xij, yij, rr2, h1, w, w_x, w_y);
-      const double Tj = thermal ? fx.x : 0.;
-      const double2 v = __ldg(sj + 1);
-      const double2 s01 = __ldg(sj + 2);  // sxx, sxy
-      const double2 s2r0 = __ldg(sj + 3); // syy, Rxx
-      const double2 r12 = __ldg(sj + 4);  // Rxy, Ryy
-      const double2 hrho = __ldg(sj + 5); // h, rho
-      const double2 cvol = __ldg(sj + 6); // c, vol
-      const double rhoj = hrho.y, volj = cvol.y;
-      const bool tool_j = fj & FLAG_TOOL;
-      if (!tool_i && !tool_j) {
-        vdx += (v.x - vxi) * w_x * volj;
-        vdy += (v.x - vxi) * w_y * volj;
-        vdz += (v.y - vyi) * w_x * volj;
-        vdw += (v.y - vyi) * w_y * volj;
-        double fab = w / wdeltap;
-        fab *= fab;
-        fab *= fab;
-        const double Rx = fab * (Rxxi + s2r0.y);
-        const double Ry = fab * (Rxyi + r12.x);
-        const double Rz = fab * (Ryyi + r12.y);
-        sdx += mass * (sxxi + s01.x + Rx) * w_x;
-        sdy += mass * (sxyi + s01.y + Ry) * w_y;
-        sdz += mass * (sxyi + s01.y + Ry) * w_x;
-        sdw += mass * (syyi + s2r0.x + Rz) * w_y;
-        const double vijx = vxi - v.x;
-        const double vijy = vyi - v.y;
-        const double vijposij = vijx * xij + vijy * yij;
-        const double rhoij = 0.5 * (rhoi + rhoj);
-        if (vijposij < 0.) {
-          const double cij = 0.5 * (ci + cvol.x);
-          const double hij = 0.5 * (hi + hrho.x);
-          const double muij = (hij * vijposij) / (rr2 + eta * eta * hij * hij);
-          const double piij = (-alpha * cij * muij + beta * muij * muij) / rhoij;
-          vtx += -mass * piij * w_x;
-          vty += -mass * piij * w_y;
-        }
-        xtx += -eps * w * mass / rhoij * vijx;
-        xty += -eps * w * mass / rhoij * vijy;
+    // Candidates are taken in chunks of up to 32: a cheap pass marks the ones that
+    // contribute, then the expensive body visits the marked ones in array order. Outside
+    // the support the reference adds terms multiplied by W = 0: they change no finite sum,
+    // but a NaN/Inf operand turns the sum into NaN, so those candidates are marked too.
+    for (int jb = j0; jb < j1; jb += 32) {
+      const int jn = min(32, j1 - jb);
+      unsigned mask = 0u;
+      for (int k = 0; k < jn; ++k) {
+        const double2 *sj = reinterpret_cast<const double2 *>(rec + (size_t)(jb + k) * R_WIDTH);
+        const unsigned fj = (unsigned)__double_as_longlong(__ldg(sj + 7).y);
+        const double2 xy = __ldg(sj + 0);
+        const double xij = xi - xy.x;
+        const double yij = yi - xy.y;
+        const double rr2 = xij * xij + yij * yij;
+        const bool in_support = !(rr2 >= fourh2 || rr2 < 1e-8);
+        const bool take = !(fj & FLAG_BLANKED) && (in_support || nonfinite_i || (fj & FLAG_NONFINITE));
+        mask |= (take ? 1u : 0u) << k;
       }
-      if (thermal) {
-        const double rij = sqrt(rr2);
-        if (rij > 1e-8) {
-          const double eijx = xij / rij;
-          const double eijy = yij / rij;
-          const double rij1 = 1. / rij;
-          T_lapl += 2.0 * volj * (Ti - Tj) * rij1 * (eijx * w_x + eijy * w_y);
+      while (mask) {
+        const int k = __ffs(mask) - 1;
+        mask &= mask - 1u;
+        const double2 *sj = reinterpret_cast<const double2 *>(rec + (size_t)(jb + k) * R_WIDTH);
+        const double2 fx = __ldg(sj + 7);  // T, flags
+        const unsigned fj = (unsigned)__double_as_longlong(fx.y);
+        const double2 xy = __ldg(sj + 0);
+        const double xij = xi - xy.x;
+        const double yij = yi - xy.y;
+        const double rr2 = xij * xij + yij * yij;
+        const bool in_support = !(rr2 >= fourh2 || rr2 < 1e-8);
+        double w = 0., w_x = 0., w_y = 0., dwr = 0.;
+        if (in_support) cubic_spline_fp64(xij, yij, rr2, h1, w, w_x, w_y, dwr);
+        const double2 cvol = __ldg(sj + 6);  // c, vol
+        const double volj = cvol.y;
+        const bool tool_j = fj & FLAG_TOOL;
+        if (!tool_i && !tool_j) {
+          const double2 v = __ldg(sj + 1);
+          const double2 s01 = __ldg(sj + 2);   // sxx, sxy
+          const double2 s2r0 = __ldg(sj + 3);  // syy, Rxx
+          const double2 r12 = __ldg(sj + 4);   // Rxy, Ryy
+          const double2 hrho = __ldg(sj + 5);  // h, rho
+          vdx += (v.x - vxi) * w_x * volj;
+          vdy += (v.x - vxi) * w_y * volj;
+          vdz += (v.y - vyi) * w_x * volj;
+          vdw += (v.y - vyi) * w_y * volj;
+          double fab = w / wdeltap;
+          fab *= fab;
+          fab *= fab;
+          const double Rx = fab * (Rxxi + s2r0.y);
+          const double Ry = fab * (Rxyi + r12.x);
+          const double Rz = fab * (Ryyi + r12.y);
+          sdx += mass * (sxxi + s01.x + Rx) * w_x;
+          sdy += mass * (sxyi + s01.y + Ry) * w_y;
+          sdz += mass * (sxyi + s01.y + Ry) * w_x;
+          sdw += mass * (syyi + s2r0.x + Rz) * w_y;
+          const double vijx = vxi - v.x;
+          const double vijy = vyi - v.y;
+          const double vijposij = vijx * xij + vijy * yij;
+          const double irhoij = 1. / (0.5 * (rhoi + hrho.y));
+          if (vijposij < 0.) {
+            const double cij = 0.5 * (ci + cvol.x);
+            const double hij = 0.5 * (hi + hrho.x);
+            const double muij = (hij * vijposij) / (rr2 + eta * eta * hij * hij);
+            const double piij = (-alpha * cij * muij + beta * muij * muij) * irhoij;
+            vtx += -mass * piij * w_x;
+            vty += -mass * piij * w_y;
+          }
+          const double xs = m_eps * w * irhoij;
+          xtx += xs * vijx;
+          xty += xs * vijy;
         }
+        // Brookshaw: 2 (m/rho_j)(Ti - Tj)(e_ij . grad W)/r, and (e_ij . grad W)/r = der*fac
+        if (thermal && rr2 > 1e-16) T_lapl += 2.0 * volj * (Ti - fx.x) * dwr;
       }
     }
   }
@@ -575,168 +603,232 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers
 }
 
 // ---------------------------------------------------------------------------------------
-// corrector .. invalidate, per particle, plus the tool force (leap_frog.cu:68-92,
-// actions_gpu.cu:135-162,226-349, tool_gpu.cu:151-221, output.cu:31-39)
-static __global__ void __launch_bounds__(BLOCK) k_finish(params P, dev_buffers D) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  ksum fcx{0., 0.}, fcy{0., 0.}, ftx{0., 0.}, fty{0., 0.};
-  unsigned newly_blanked = 0, capped = 0, blanked_now = 0;
-  if (q < P.N) {
-    const state_set &A = D.A;
-    const state_set &B = D.B;
-    const double dt = P.dt;
-    unsigned f = B.flags[q];
-    const bool blanked = f & FLAG_BLANKED;
-    const bool tool = f & FLAG_TOOL;
-    const bool fixed = f & FLAG_FIXED;
-    double2 pos = B.pos[q], vel = B.vel[q];
-    double4 S = B.S[q];
-    double rho = B.rho[q], T = B.T[q];
-    double2 pos_t = B.pos_t[q], vel_t = B.vel_t[q];
-    const double4 S_t = B.S_t[q];
-    const double rho_t = B.rho_t[q], T_t = B.T_t[q];
-    if (!blanked) {  // correct (leap_frog.cu:68-92) from the state at the start of the step
-      const int p = D.perm[q];
-      const double2 pos0 = A.pos[p], vel0 = A.vel[p];
-      const double4 S0 = A.S[p];
-      const double rho0 = A.rho[p], T0 = A.T[p];
-      pos.x = pos0.x + dt * pos_t.x;
-      pos.y = pos0.y + dt * pos_t.y;
-      vel.x = vel0.x + dt * vel_t.x;
-      vel.y = vel0.y + dt * vel_t.y;
-      S.x = S0.x + dt * S_t.x;
-      S.y = S0.y + dt * S_t.y;
-      S.z = S0.z + dt * S_t.z;
-      S.w = S0.w + dt * S_t.w;
-      rho = rho0 + dt * rho_t;
-      T = T0 + dt * T_t;
+// the rigid tool of this step, advanced in shared memory: tool::update_tool (tool.cpp:211-221)
+// with IEEE-rounded operations (bitwise equal to the host's double arithmetic), one lane per
+// segment and one for the fillet; block 0 stores it for the next step
+__device__ __forceinline__ void tool_advance_shared(mf_tool_state &T, const dev_buffers &D, double dt) {
+  if (threadIdx.x == 0) T = *D.tool_prev;
+  __syncthreads();
+  const double sx = __dmul_rn(dt, T.vel[0]), sy = __dmul_rn(dt, T.vel[1]);
+  const int t = threadIdx.x;
+  if (t < T.num_seg) {
+    mf_segment &s = T.seg[t];
+    s.left[0] = __dadd_rn(s.left[0], sx);
+    s.left[1] = __dadd_rn(s.left[1], sy);
+    s.right[0] = __dadd_rn(s.right[0], sx);
+    s.right[1] = __dadd_rn(s.right[1], sy);
+    line_through_rn(s.left[0], s.left[1], s.right[0], s.right[1], s.a, s.b, s.vertical);
+  } else if (t == 5 && T.has_fillet) {
+    T.fillet.p[0] = __dadd_rn(T.fillet.p[0], sx);
+    T.fillet.p[1] = __dadd_rn(T.fillet.p[1], sy);
+  }
+  __syncthreads();
+  if (blockIdx.x == 0 && threadIdx.x == 0) *D.tool_next = T;
+}
+
+// corrector .. invalidate for one particle (leap_frog.cu:68-92, actions_gpu.cu:135-162,
+// 226-349, tool_gpu.cu:151-221); returns the final position and flags
+__device__ __forceinline__ void finish_particle(const params &P, const dev_buffers &D, const mf_tool_state &TL, int q,
+                                               double2 &pos_out, unsigned &f_out, double2 &fc_out, double2 &ft_out,
+                                               unsigned &newly_blanked, unsigned &capped) {
+  const state_set &A = D.A;
+  const state_set &B = D.B;
+  const double dt = P.dt;
+  unsigned f = B.flags[q];
+  const bool blanked = f & FLAG_BLANKED;
+  const bool tool = f & FLAG_TOOL;
+  const bool fixed = f & FLAG_FIXED;
+  // the state at the start of the step, in the new order (predict/correct skip blanked
+  // particles, so for them it is also the state at the end of the step)
+  const int p = D.perm[q];
+  double2 pos = A.pos[p], vel = A.vel[p];
+  double4 S = A.S[p];
+  double rho = A.rho[p], T = A.T[p];
+  double2 pos_t = B.pos_t[q], vel_t = B.vel_t[q];
+  const double4 S_t = B.S_t[q];
+  const double rho_t = B.rho_t[q], T_t = B.T_t[q];
+  if (!blanked) {  // correct (leap_frog.cu:68-92)
+    pos.x = pos.x + dt * pos_t.x;
+    pos.y = pos.y + dt * pos_t.y;
+    vel.x = vel.x + dt * vel_t.x;
+    vel.y = vel.y + dt * vel_t.y;
+    S.x = S.x + dt * S_t.x;
+    S.y = S.y + dt * S_t.y;
+    S.z = S.z + dt * S_t.z;
+    S.w = S.w + dt * S_t.w;
+    rho = rho + dt * rho_t;
+    T = T + dt * T_t;
+  }
+  double eps_pl = B.eps_pl[q], eps_pl_dot = B.eps_pl_dot[q];
+  double2 fc = B.fc[q], ft = B.ft[q];
+  // friction heat (actions_gpu.cu:135-162), previous step's ft and n
+  if (P.has_tool && P.fric_heat && !tool) {
+    const double f_fric_mag = (double)sqrtf((float)(ft.x * ft.x + ft.y * ft.y));
+    if (f_fric_mag != 0.) {
+      const double2 normal = D.n[q];
+      const double vdx = vel.x - TL.vel[0], vdy = vel.y - TL.vel[1];
+      const double vdn = vdx * normal.x + vdy * normal.y;
+      const double vrx = vdx - vdn, vry = vdy - vdn;
+      const double v_rel_mag = (double)sqrtf((float)(vrx * vrx + vry * vry));
+      T += P.trml_wp.eta * dt * f_fric_mag * v_rel_mag / (P.trml_wp.cp * P.phys.mass);
     }
-    double eps_pl = B.eps_pl[q], eps_pl_dot = B.eps_pl_dot[q];
-    double2 fc = B.fc[q], ft = B.ft[q];
-    const mf_tool_state &TL = *D.tool;
-    // friction heat (actions_gpu.cu:135-162), previous step's ft and n
-    if (P.has_tool && P.fric_heat && !tool) {
-      const double f_fric_mag = (double)sqrtf((float)(ft.x * ft.x + ft.y * ft.y));
-      if (f_fric_mag != 0.) {
-        const double2 normal = D.n[q];
-        const double vdx = vel.x - TL.vel[0], vdy = vel.y - TL.vel[1];
-        const double vdn = vdx * normal.x + vdy * normal.y;
-        const double vrx = vdx - vdn, vry = vdy - vdn;
-        const double v_rel_mag = (double)sqrtf((float)(vrx * vrx + vry * vry));
-        T += P.trml_wp.eta * dt * f_fric_mag * v_rel_mag / (P.trml_wp.cp * P.phys.mass);
+  }
+  // JC plasticity, radial return (actions_gpu.cu:226-285)
+  if (P.plastic && !tool) {
+    const double mu = P.phys.G;
+    const double Sxx = S.x, Syy = S.z, Szz = S.w, Sxy = S.y;
+    const double norm_Strial = (double)sqrtf((float)(Sxx * Sxx + Syy * Syy + Szz * Szz + Sxy * Sxy));
+    const double pr = D.pp[q];
+    const double cxx = Sxx - pr, cyy = Syy - pr, czz = Szz - pr, cxy = Sxy;
+    const double svm = (double)sqrtf(
+        (float)((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy));
+    const double sigma_Y = sigma_yield(P.joco, eps_pl, eps_pl_dot, T);
+    if (svm < sigma_Y) {
+      eps_pl_dot = 0.;
+    } else {
+      bool cap = false;
+      const double delta_lambda = solve_secant(P.joco, P.jc_model, fmax(eps_pl_dot * dt * sqrt(2. / 3.), 1e-8),
+                                               1e-6, norm_Strial, eps_pl, T, dt, P.phys.G, cap);
+      capped += cap ? 1u : 0u;
+      const float s23f = sqrtf((float)(2.0 / 3.0));
+      const double eps_pl_new = eps_pl + (double)(s23f * fmaxf((float)delta_lambda, 0.f));
+      const double eps_pl_dot_new = (double)(s23f * fmaxf((float)delta_lambda, 0.f)) / dt;
+      S.x = Sxx - Sxx / norm_Strial * delta_lambda * 2. * mu;
+      S.z = Syy - Syy / norm_Strial * delta_lambda * 2. * mu;
+      S.w = Szz - Szz / norm_Strial * delta_lambda * 2. * mu;
+      S.y = Sxy - Sxy / norm_Strial * delta_lambda * 2. * mu;
+      if (P.trml_wp.tq != 0.) {
+        const double delta_eps_pl = eps_pl_new - eps_pl;
+        const double sY = sigma_yield(P.joco, eps_pl_new, eps_pl_dot_new, T);
+        T += P.trml_wp.tq / (P.trml_wp.cp * rho) * delta_eps_pl * sY;
       }
+      eps_pl = eps_pl_new;
+      eps_pl_dot = eps_pl_dot_new;
     }
-    // JC plasticity, radial return (actions_gpu.cu:226-285)
-    if (P.plastic && !tool) {
-      const double mu = P.phys.G;
-      const double Sxx = S.x, Syy = S.z, Szz = S.w, Sxy = S.y;
-      const double norm_Strial = (double)sqrtf((float)(Sxx * Sxx + Syy * Syy + Szz * Szz + Sxy * Sxy));
-      const double pr = D.pp[q];
-      const double cxx = Sxx - pr, cyy = Syy - pr, czz = Szz - pr, cxy = Sxy;
-      const double svm = (double)sqrtf(
-          (float)((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy));
-      const double sigma_Y = sigma_yield(P.joco, eps_pl, eps_pl_dot, T);
-      if (svm < sigma_Y) {
-        eps_pl_dot = 0.;
+  }
+  // tool particles move with the tool (tool_gpu.cu:210-221); contact (:151-207)
+  if (P.has_tool) {
+    if (tool) {
+      pos.x += dt * TL.vel[0];
+      pos.y += dt * TL.vel[1];
+    } else {
+      double cpx = 0., cpy = 0., nx = 0., ny = 0.;
+      const bool inside = establish_contact(TL, pos.x, pos.y, cpx, cpy, nx, ny);
+      if (!inside) {
+        fc = make_double2(0., 0.);
+        ft = make_double2(0., 0.);
+        D.n[q] = make_double2(0., 0.);
       } else {
-        bool cap = false;
-        const double delta_lambda = solve_secant(P.joco, P.jc_model, fmax(eps_pl_dot * dt * sqrt(2. / 3.), 1e-8),
-                                                 1e-6, norm_Strial, eps_pl, T, dt, P.phys.G, cap);
-        capped = cap ? 1u : 0u;
-        const float s23f = sqrtf((float)(2.0 / 3.0));
-        const double eps_pl_new = eps_pl + (double)(s23f * fmaxf((float)delta_lambda, 0.f));
-        const double eps_pl_dot_new = (double)(s23f * fmaxf((float)delta_lambda, 0.f)) / dt;
-        S.x = Sxx - Sxx / norm_Strial * delta_lambda * 2. * mu;
-        S.z = Syy - Syy / norm_Strial * delta_lambda * 2. * mu;
-        S.w = Szz - Szz / norm_Strial * delta_lambda * 2. * mu;
-        S.y = Sxy - Sxy / norm_Strial * delta_lambda * 2. * mu;
-        if (P.trml_wp.tq != 0.) {
-          const double delta_eps_pl = eps_pl_new - eps_pl;
-          const double sY = sigma_yield(P.joco, eps_pl_new, eps_pl_dot_new, T);
-          T += P.trml_wp.tq / (P.trml_wp.cp * rho) * delta_eps_pl * sY;
-        }
-        eps_pl = eps_pl_new;
-        eps_pl_dot = eps_pl_dot_new;
-      }
-    }
-    // tool particles move with the tool (tool_gpu.cu:210-221); contact (:151-207)
-    if (P.has_tool) {
-      if (tool) {
-        pos.x += dt * TL.vel[0];
-        pos.y += dt * TL.vel[1];
-      } else {
-        double cpx = 0., cpy = 0., nx = 0., ny = 0.;
-        const bool inside = establish_contact(TL, pos.x, pos.y, cpx, cpy, nx, ny);
-        if (!inside) {
-          fc = make_double2(0., 0.);
-          ft = make_double2(0., 0.);
-          D.n[q] = make_double2(0., 0.);
-        } else {
-          const double dt2 = dt * dt;
-          const double gN = (pos.x - cpx) * nx + (pos.y - cpy) * ny;
-          const double sc = -TL.slave_mass * gN;
-          double2 fN = make_double2(sc * nx, sc * ny);
-          fN.x = fN.x / dt2 * TL.contact_alpha;
-          fN.y = fN.y / dt2 * TL.contact_alpha;
-          double2 fT = make_double2(0., 0.);
-          if (TL.mu != 0.) {
-            const double vx = vel.x - TL.vel[0], vy = vel.y - TL.vel[1];
-            const double vrx = vx - vx * nx, vry = vy - vy * ny;
-            const double ks = TL.contact_alpha * TL.slave_mass;
-            const double kx = ks * vrx / dt, ky = ks * vry / dt;
-            const double fy = TL.mu * sqrt(fN.x * fN.x + fN.y * fN.y);
-            const double fsx = ft.x - kx, fsy = ft.y - ky;
-            const double lfs = sqrt(fsx * fsx + fsy * fsy);
-            if (lfs > fy) {
-              fT.x = fy * fsx / lfs;
-              fT.y = fy * fsy / lfs;
-            } else {
-              fT = make_double2(fsx, fsy);
-            }
+        const double dt2 = dt * dt;
+        const double gN = (pos.x - cpx) * nx + (pos.y - cpy) * ny;
+        const double sc = -TL.slave_mass * gN;
+        double2 fN = make_double2(sc * nx, sc * ny);
+        fN.x = fN.x / dt2 * TL.contact_alpha;
+        fN.y = fN.y / dt2 * TL.contact_alpha;
+        double2 fT = make_double2(0., 0.);
+        if (TL.mu != 0.) {
+          const double vx = vel.x - TL.vel[0], vy = vel.y - TL.vel[1];
+          const double vrx = vx - vx * nx, vry = vy - vy * ny;
+          const double ks = TL.contact_alpha * TL.slave_mass;
+          const double kx = ks * vrx / dt, ky = ks * vry / dt;
+          const double fy = TL.mu * sqrt(fN.x * fN.x + fN.y * fN.y);
+          const double fsx = ft.x - kx, fsy = ft.y - ky;
+          const double lfs = sqrt(fsx * fsx + fsy * fsy);
+          if (lfs > fy) {
+            fT.x = fy * fsx / lfs;
+            fT.y = fy * fsy / lfs;
+          } else {
+            fT = make_double2(fsx, fsy);
           }
-          fc = fN;
-          ft = fT;
-          D.n[q] = make_double2(nx, ny);
         }
+        fc = fN;
+        ft = fT;
+        D.n[q] = make_double2(nx, ny);
       }
     }
-    // boundary conditions (actions_gpu.cu:287-311)
-    if (!tool && fixed) {
-      vel = make_double2(0., 0.);
-      fc = make_double2(0., 0.);
-      pos_t = make_double2(0., 0.);
-      vel_t = make_double2(0., 0.);
-      B.pos_t[q] = pos_t;
-      B.vel_t[q] = vel_t;
+  }
+  // boundary conditions (actions_gpu.cu:287-311)
+  if (!tool && fixed) {
+    vel = make_double2(0., 0.);
+    fc = make_double2(0., 0.);
+    pos_t = make_double2(0., 0.);
+    vel_t = make_double2(0., 0.);
+    B.pos_t[q] = pos_t;
+    B.vel_t[q] = vel_t;
+  }
+  if (P.thermal_bc && fixed) T = P.trml_wp.T_init;
+  // invalidate (actions_gpu.cu:317-349)
+  if (!blanked) {
+    bool invalid = isnaninf(pos_t.x) || isnaninf(pos_t.y) || isnaninf(vel_t.x) || isnaninf(vel_t.y) ||
+                   isnaninf(S_t.x) || isnaninf(S_t.y) || isnaninf(S_t.z) || isnaninf(S_t.w) ||
+                   isnaninf(rho_t) || isnaninf(T_t);
+    if (invalid) {
+      f |= FLAG_BLANKED;
+      newly_blanked += 1u;
+      B.flags[q] = f;
     }
-    if (P.thermal_bc && fixed) T = P.trml_wp.T_init;
-    // invalidate (actions_gpu.cu:317-349)
-    if (!blanked) {
-      bool invalid = isnaninf(pos_t.x) || isnaninf(pos_t.y) || isnaninf(vel_t.x) || isnaninf(vel_t.y) ||
-                     isnaninf(S_t.x) || isnaninf(S_t.y) || isnaninf(S_t.z) || isnaninf(S_t.w) ||
-                     isnaninf(rho_t) || isnaninf(T_t);
-      if (invalid) {
-        f |= FLAG_BLANKED;
-        newly_blanked = 1;
-        B.flags[q] = f;
+  }
+  B.pos[q] = pos;
+  B.vel[q] = vel;
+  B.S[q] = S;
+  B.rho[q] = rho;
+  B.T[q] = T;
+  B.eps_pl[q] = eps_pl;
+  B.eps_pl_dot[q] = eps_pl_dot;
+  B.fc[q] = fc;
+  B.ft[q] = ft;
+  pos_out = pos;
+  f_out = f;
+  fc_out = fc;
+  ft_out = ft;
+}
+
+// Corrector .. invalidate for all particles plus the tool force (output.cu:31-39), on a
+// fixed grid of blocks that loops over the particles. With FUSE_HASH (locked grid) it also
+// computes the next step's cell hash and per-cell count from the final positions (the work
+// of k_hash_count) and re-arms the scan for the next step.
+template <bool FUSE_HASH>
+__global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P, dev_buffers D, int num_scan_tiles) {
+  __shared__ mf_tool_state s_tool;
+  __shared__ ksum sm[BLOCK / 32][4];
+  __shared__ unsigned smc[BLOCK / 32][4];
+  __shared__ bool last;
+  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt);
+  const int stride = gridDim.x * blockDim.x;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  ksum fcx{0., 0.}, fcy{0., 0.}, ftx{0., 0.}, fty{0., 0.};
+  unsigned newly_blanked = 0, capped = 0, blanked_now = 0, oog = 0;
+  geom g{};
+  if (FUSE_HASH) {
+    g = *D.g;
+    for (int t = gid; t < num_scan_tiles; t += stride) D.scan_status[t] = 0ull;
+  }
+  for (int q = gid; q < P.N; q += stride) {
+    double2 pos, fc, ft;
+    unsigned f;
+    finish_particle(P, D, s_tool, q, pos, f, fc, ft, newly_blanked, capped);
+    blanked_now += (f & FLAG_BLANKED) ? 1u : 0u;
+    ksum_add(fcx, fc.x);
+    ksum_add(fcy, fc.y);
+    ksum_add(ftx, ft.x);
+    ksum_add(fty, ft.y);
+    if (FUSE_HASH) {  // compute_hashes of the next step (grid.cu:34-51)
+      long long hh;
+      if (f & FLAG_BLANKED) {
+        hh = D.hash_cur[q];
+      } else {
+        const int ix = __double2int_rz((pos.x - g.bbmin_x) / g.dx);
+        const int iy = __double2int_rz((pos.y - g.bbmin_y) / g.dx);
+        hh = (long long)ix * (long long)g.ny + (long long)iy;
       }
+      if (hh < 0) { hh = 0; ++oog; }
+      else if (hh >= g.num_cell) { hh = g.num_cell - 1; ++oog; }
+      const int hsh = (int)hh;
+      D.hash_new[q] = hsh;
+      D.slot[q] = atomicAdd(&D.count[hsh], 1);
     }
-    blanked_now = (f & FLAG_BLANKED) ? 1u : 0u;
-    B.pos[q] = pos;
-    B.vel[q] = vel;
-    B.S[q] = S;
-    B.rho[q] = rho;
-    B.T[q] = T;
-    B.eps_pl[q] = eps_pl;
-    B.eps_pl_dot[q] = eps_pl_dot;
-    B.fc[q] = fc;
-    B.ft[q] = ft;
-    fcx.s = fc.x; fcy.s = fc.y; ftx.s = ft.x; fty.s = ft.y;
   }
   // block reduction of the force (compensated) and of the counters
-  __shared__ ksum sm[BLOCK / 32][4];
-  __shared__ unsigned smc[BLOCK / 32][3];
-  __shared__ bool last;
   for (int o = 16; o > 0; o >>= 1) {
     ksum a{__shfl_down_sync(0xffffffffu, fcx.s, o), __shfl_down_sync(0xffffffffu, fcx.c, o)};
     ksum b{__shfl_down_sync(0xffffffffu, fcy.s, o), __shfl_down_sync(0xffffffffu, fcy.c, o)};
@@ -744,21 +836,23 @@ static __global__ void __launch_bounds__(BLOCK) k_finish(params P, dev_buffers D
     ksum d{__shfl_down_sync(0xffffffffu, fty.s, o), __shfl_down_sync(0xffffffffu, fty.c, o)};
     ksum_merge(fcx, a); ksum_merge(fcy, b); ksum_merge(ftx, c); ksum_merge(fty, d);
   }
-  const unsigned nb = __popc(__ballot_sync(0xffffffffu, newly_blanked));
-  const unsigned nc = __popc(__ballot_sync(0xffffffffu, capped));
-  const unsigned nbl = __popc(__ballot_sync(0xffffffffu, blanked_now));
+  const unsigned nb = __reduce_add_sync(0xffffffffu, newly_blanked);
+  const unsigned nc = __reduce_add_sync(0xffffffffu, capped);
+  const unsigned nbl = __reduce_add_sync(0xffffffffu, blanked_now);
+  const unsigned noog = __reduce_add_sync(0xffffffffu, oog);
   if (lane_id() == 0) {
     sm[threadIdx.x >> 5][0] = fcx; sm[threadIdx.x >> 5][1] = fcy;
     sm[threadIdx.x >> 5][2] = ftx; sm[threadIdx.x >> 5][3] = fty;
     smc[threadIdx.x >> 5][0] = nb; smc[threadIdx.x >> 5][1] = nc; smc[threadIdx.x >> 5][2] = nbl;
+    smc[threadIdx.x >> 5][3] = noog;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     ksum r[4] = {sm[0][0], sm[0][1], sm[0][2], sm[0][3]};
-    unsigned cnt[3] = {smc[0][0], smc[0][1], smc[0][2]};
+    unsigned cnt[4] = {smc[0][0], smc[0][1], smc[0][2], smc[0][3]};
     for (int w = 1; w < BLOCK / 32; ++w) {
       for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
-      for (int k = 0; k < 3; ++k) cnt[k] += smc[w][k];
+      for (int k = 0; k < 4; ++k) cnt[k] += smc[w][k];
     }
     for (int k = 0; k < 4; ++k) {
       D.partials[blockIdx.x * 8 + 2 * k] = r[k].s;
@@ -767,6 +861,7 @@ static __global__ void __launch_bounds__(BLOCK) k_finish(params P, dev_buffers D
     if (cnt[0]) atomicAdd(&D.st->newly_blanked, (unsigned long long)cnt[0]);
     if (cnt[1]) atomicAdd(&D.st->secant_cap_hits, (unsigned long long)cnt[1]);
     if (cnt[2]) atomicAdd(&D.st->blanked, (unsigned long long)cnt[2]);
+    if (cnt[3]) atomicAdd(&D.st->out_of_grid, (unsigned long long)cnt[3]);
     __threadfence();
     const unsigned t = atomicAdd(&D.ticket[0], 1u);
     last = (t == gridDim.x - 1);

@@ -6,46 +6,48 @@
 // differences are the arithmetic type and these exact rewrites:
 //   * x_ij = (ci - cj) * dx + (xi_rel - xj_rel): small integers times the cell size plus
 //     a difference of in-cell offsets, instead of a difference of absolute coordinates;
-//   * e_ij . grad W / r = (x_ij w_x + y_ij w_y) / r^2 (Brookshaw);
-//   * divisions by r use one rsqrt per pair;
+//   * (e_ij . grad W) / r = der * fac (Brookshaw), one rsqrt per pair for 1/r;
 //   * temperatures are stored relative to the initial temperature, so Ti - Tj keeps its
 //     digits near it.
-// Its error against the FP64 oracle is measured and reported, not assumed.
+// Its error against the FP64 form is measured and reported, not assumed.
 #pragma once
 
 #include "mf_kernels.cuh"
 
 namespace mf {
 
-static __global__ void __launch_bounds__(PAIR_BLOCK) k_pair_mixed(params P, dev_buffers D) {
+static __global__ void __launch_bounds__(PAIR_BLOCK, 8) k_pair_mixed(params P, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
-  const float *__restrict__ rec = D.recf;
-  const float4 *si = reinterpret_cast<const float4 *>(rec + (size_t)q * F_WIDTH);
-  const float4 a0 = __ldg(si + 0), a1 = __ldg(si + 1), a2 = __ldg(si + 2), a3 = __ldg(si + 3);
-  const unsigned fi = (unsigned)__float_as_int(a3.w);
+  const float4 *__restrict__ rec = reinterpret_cast<const float4 *>(D.recf);
+  const float4 a0 = __ldg(rec + 4 * q + 0);  // x, y, flags|cy, vx
+  const unsigned fi = (unsigned)__float_as_int(a0.z) & 0xffu;
   if (fi & FLAG_BLANKED) return;
   const bool tool_i = fi & FLAG_TOOL;
   const bool brookshaw = P.thermal_solver == MF_THERMAL_BROOKSHAW;
   if (!brookshaw && tool_i) return;
+  const float4 a1 = __ldg(rec + 4 * q + 1);  // vy, sxx, sxy, syy
+  const float4 a2 = __ldg(rec + 4 * q + 2);  // Rxx, Rxy, Ryy, h
+  const float4 a3 = __ldg(rec + 4 * q + 3);  // rho, c, vol, T - T_init
 
   const float mass = (float)P.phys.mass;
   const float inv_wdeltap = (float)(1. / P.corr.wdeltap);
   const float alpha = (float)P.corr.alpha, beta = (float)P.corr.beta, eta = (float)P.corr.eta;
-  const float eps = (float)P.corr.xspheps;
   double thermal_alpha = 0.;
   if (brookshaw) thermal_alpha = !tool_i ? P.trml_wp.alpha : (P.thermal_tool_on ? P.trml_tool.alpha : 0.);
   const bool thermal = thermal_alpha != 0.;
   const bool nonfinite_i = fi & FLAG_NONFINITE;
+  const bool mech_i = !tool_i;
 
-  const float xi = a0.x, yi = a0.y, vxi = a0.z, vyi = a0.w;
-  const float sxxi = a1.x, sxyi = a1.y, syyi = a1.z, Rxxi = a1.w;
-  const float Rxyi = a2.x, Ryyi = a2.y, hi = a2.z, rhoi = a2.w;
-  const float ci = a3.x, Ti = thermal ? a3.z : 0.f;
+  const float xi = a0.x, yi = a0.y, vxi = a0.w, vyi = a1.x;
+  const float sxxi = a1.y, sxyi = a1.z, syyi = a1.w;
+  const float Rxxi = a2.x, Rxyi = a2.y, Ryyi = a2.z, hi = a2.w;
+  const float rhoi = a3.x, ci = a3.y, Ti = thermal ? a3.w : 0.f;
   const float h1 = 1.f / hi;
   const float fourh2 = 4.f * hi * hi;
   const float fac = 0.454728408833987f * h1 * h1;
   const float eta2 = eta * eta;
+  const float m_eps = (float)P.corr.xspheps * mass;
 
   const geom g = *D.g;
   const float dxc = (float)g.dx;
@@ -56,6 +58,8 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pair_mixed(params P, dev_
   const int low_j = gj - 2 < 0 ? 0 : gj - 2;
   const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
   const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
+  // y offset between cell rows: (gj - r) * dx = oy0 - r * dx
+  const float oy0 = (float)gj * dxc;
 
   float vdx = 0.f, vdy = 0.f, vdz = 0.f, vdw = 0.f;
   float sdx = 0.f, sdy = 0.f, sdz = 0.f, sdw = 0.f;
@@ -66,78 +70,86 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pair_mixed(params P, dev_
     const int col = ii * g.ny;
     const int j0 = __ldg(D.off + col + low_j);
     const int j1 = __ldg(D.off + col + high_j);
-    const float ox = (float)(gi - ii) * dxc;
-    for (int j = j0; j < j1; ++j) {
-      const float4 *sj = reinterpret_cast<const float4 *>(rec + (size_t)j * F_WIDTH);
-      const float4 b3 = __ldg(sj + 3);  // c, vol, T, flags|cell_y
-      const unsigned fjw = (unsigned)__float_as_int(b3.w);
-      const unsigned fj = fjw & 0xffu;
-      if (fj & FLAG_BLANKED) continue;
-      const int cyj = (int)(fjw >> 8);
-      const float4 b0 = __ldg(sj + 0);  // x_rel, y_rel, vx, vy
-      const float xij = ox + (xi - b0.x);
-      const float yij = (float)(gj - cyj) * dxc + (yi - b0.y);
-      const float rr2 = xij * xij + yij * yij;
-      const bool in_support = !(rr2 >= fourh2 || rr2 < 1e-8f);
-      if (!in_support && !(nonfinite_i || (fj & FLAG_NONFINITE))) continue;
-      float w = 0.f, w_x = 0.f, w_y = 0.f, rinv = 0.f;
-      if (in_support) {
-        rinv = rsqrtf(rr2);
-        const float rad = rr2 * rinv;
-        const float qq = rad * h1;
-        float val, der;
-        if (qq > 1.f) {
-          const float t = 2.f - qq;
-          const float t2 = t * t;
-          val = 0.25f * t2 * t2 * t2;
-          der = -0.75f * t2 * h1 * rinv;
-        } else {
-          val = 1.f - 1.5f * qq * qq * (1.f - 0.5f * qq);
-          der = -3.0f * qq * (1.f - 0.75f * qq) * h1 * rinv;
-        }
-        w = val * fac;
-        w_x = der * xij * fac;
-        w_y = der * yij * fac;
+    const float ox = (float)(gi - ii) * dxc + xi;
+    // chunks of up to 32 candidates: mark the contributing ones, then visit them in order
+    for (int jb = j0; jb < j1; jb += 32) {
+      const int jn = min(32, j1 - jb);
+      unsigned mask = 0u;
+#pragma unroll 4
+      for (int k = 0; k < jn; ++k) {
+        const float4 b0 = __ldg(rec + 4 * (jb + k));
+        const unsigned fjw = (unsigned)__float_as_int(b0.z);
+        const float xij = ox - b0.x;
+        const float yij = (oy0 - (float)(int)(fjw >> 8) * dxc) + (yi - b0.y);
+        const float rr2 = xij * xij + yij * yij;
+        const bool in_support = !(rr2 >= fourh2 || rr2 < 1e-8f);
+        const bool take = !(fjw & FLAG_BLANKED) && (in_support || nonfinite_i || (fjw & FLAG_NONFINITE));
+        mask |= (take ? 1u : 0u) << k;
       }
-      const float volj = b3.y;
-      const bool tool_j = fj & FLAG_TOOL;
-      if (!tool_i && !tool_j) {
-        const float4 b1 = __ldg(sj + 1);  // sxx, sxy, syy, Rxx
-        const float4 b2 = __ldg(sj + 2);  // Rxy, Ryy, h, rho
-        const float dvx = b0.z - vxi, dvy = b0.w - vyi;
-        vdx += dvx * w_x * volj;
-        vdy += dvx * w_y * volj;
-        vdz += dvy * w_x * volj;
-        vdw += dvy * w_y * volj;
-        float fab = w * inv_wdeltap;
-        fab *= fab;
-        fab *= fab;
-        const float Rx = fab * (Rxxi + b1.w);
-        const float Ry = fab * (Rxyi + b2.x);
-        const float Rz = fab * (Ryyi + b2.y);
-        const float sxy = sxyi + b1.y + Ry;
-        sdx += mass * (sxxi + b1.x + Rx) * w_x;
-        sdy += mass * sxy * w_y;
-        sdz += mass * sxy * w_x;
-        sdw += mass * (syyi + b1.z + Rz) * w_y;
-        const float vijposij = -(dvx * xij + dvy * yij);
-        const float rhoij = 0.5f * (rhoi + b2.w);
-        const float irhoij = __frcp_rn(rhoij);
-        if (vijposij < 0.f) {
-          const float cij = 0.5f * (ci + b3.x);
-          const float hij = 0.5f * (hi + b2.z);
-          const float muij = hij * vijposij * __frcp_rn(rr2 + eta2 * hij * hij);
-          const float piij = (-alpha * cij * muij + beta * muij * muij) * irhoij;
-          vtx -= mass * piij * w_x;
-          vty -= mass * piij * w_y;
+      while (mask) {
+        const int k = __ffs(mask) - 1;
+        mask &= mask - 1u;
+        const float4 *sj = rec + 4 * (jb + k);
+        const float4 b0 = __ldg(sj + 0);  // x, y, flags|cy, vx
+        const float4 b3 = __ldg(sj + 3);  // rho, c, vol, T - T_init
+        const unsigned fjw = (unsigned)__float_as_int(b0.z);
+        const float xij = ox - b0.x;
+        const float yij = (oy0 - (float)(int)(fjw >> 8) * dxc) + (yi - b0.y);
+        const float rr2 = xij * xij + yij * yij;
+        const bool in_support = !(rr2 >= fourh2 || rr2 < 1e-8f);
+        float w = 0.f, w_x = 0.f, w_y = 0.f, dwr = 0.f;
+        if (in_support) {
+          const float rinv = rsqrtf(rr2);
+          const float qq = rr2 * rinv * h1;
+          float val, der;
+          if (qq > 1.f) {
+            const float t = 2.f - qq;
+            const float t2 = t * t;
+            val = 0.25f * t2 * t2 * t2;
+            der = -0.75f * t2 * h1 * rinv;
+          } else {
+            val = 1.f - 1.5f * qq * qq * (1.f - 0.5f * qq);
+            der = -3.0f * qq * (1.f - 0.75f * qq) * h1 * rinv;
+          }
+          w = val * fac;
+          dwr = der * fac;
+          w_x = dwr * xij;
+          w_y = dwr * yij;
         }
-        const float xs = eps * w * mass * irhoij;
-        xtx += xs * dvx;
-        xty += xs * dvy;
-      }
-      if (thermal && rr2 > 1e-16f) {
-        // 2 (m/rho_j) (Ti - Tj) (e_ij . grad W) / r
-        T_lapl += 2.0f * volj * (Ti - b3.z) * (xij * w_x + yij * w_y) * (rinv * rinv);
+        const float volj = b3.z;
+        if (mech_i && !(fjw & FLAG_TOOL)) {
+          const float4 b1 = __ldg(sj + 1);  // vy, sxx, sxy, syy
+          const float4 b2 = __ldg(sj + 2);  // Rxx, Rxy, Ryy, h
+          const float dvx = b0.w - vxi, dvy = b1.x - vyi;
+          const float ax = dvx * volj, ay = dvy * volj;
+          vdx += ax * w_x;
+          vdy += ax * w_y;
+          vdz += ay * w_x;
+          vdw += ay * w_y;
+          float fab = w * inv_wdeltap;
+          fab *= fab;
+          fab *= fab;
+          const float sxy = mass * (sxyi + b1.z + fab * (Rxyi + b2.y));
+          sdx += mass * (sxxi + b1.y + fab * (Rxxi + b2.x)) * w_x;
+          sdy += sxy * w_y;
+          sdz += sxy * w_x;
+          sdw += mass * (syyi + b1.w + fab * (Ryyi + b2.z)) * w_y;
+          const float vijposij = -(dvx * xij + dvy * yij);
+          const float irhoij = __frcp_rn(0.5f * (rhoi + b3.x));
+          if (vijposij < 0.f) {
+            const float cij = 0.5f * (ci + b3.y);
+            const float hij = 0.5f * (hi + b2.w);
+            const float muij = hij * vijposij * __frcp_rn(rr2 + eta2 * hij * hij);
+            const float piij = (-alpha * cij * muij + beta * muij * muij) * irhoij;
+            vtx -= mass * piij * w_x;
+            vty -= mass * piij * w_y;
+          }
+          const float xs = m_eps * w * irhoij;
+          xtx += xs * dvx;
+          xty += xs * dvy;
+        }
+        // Brookshaw: 2 (m/rho_j)(Ti - Tj)(e_ij . grad W)/r with (e_ij . grad W)/r = der*fac
+        if (thermal && rr2 > 1e-16f) T_lapl += 2.0f * volj * (Ti - b3.w) * dwr;
       }
     }
   }
@@ -147,7 +159,7 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pair_mixed(params P, dev_
     D.S_der[q] = make_double4(sdx, sdy, sdz, sdw);
     D.v_der[q] = make_double4(vdx, vdy, vdz, vdw);
   }
-  if (!tool_i) {
+  if (mech_i) {
     const double4 S = B.S[q];
     const float G = (float)P.phys.G;
     const float e01 = 0.5f * (vdy + vdz);
