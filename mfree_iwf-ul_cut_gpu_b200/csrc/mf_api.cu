@@ -471,9 +471,10 @@ int mf_get_field(mf_ctx *ctx, int field, void *host) {
       std::vector<float> rec(N * F_WIDTH);
       CK(cudaMemcpy(rec.data(), ctx->D.recf, sizeof(float) * N * F_WIDTH, cudaMemcpyDeviceToHost));
       for (size_t i = 0; i < N; ++i) {
-        o[4 * i] = rec[i * F_WIDTH + F_RXX];
-        o[4 * i + 1] = rec[i * F_WIDTH + F_RXY];
-        o[4 * i + 2] = rec[i * F_WIDTH + F_RYY];
+        auto at = [&](int f) { return rec[(size_t)(f / 4) * N * 4 + (size_t)i * 4 + f % 4]; };
+        o[4 * i] = at(F_RXX);
+        o[4 * i + 1] = at(F_RXY);
+        o[4 * i + 2] = at(F_RYY);
         o[4 * i + 3] = 0.;
       }
       return MF_OK;

@@ -38,11 +38,12 @@ struct dev_buffers {
   state_set A, B;       // A: state at the start of the step (previous order), B: new order
   double2 *n;           // contact normal, indexed by array position (never permuted)
   double *rec;          // FP64 pair records, R_WIDTH doubles per particle
-  float *recf;          // FP32 pair records (mixed form), F_WIDTH floats per particle
+  float *recf;          // FP32 pair records (mixed form): F_WIDTH / 4 planes of N float4
   double *pp;           // predictor pressure (the reference's particles->p)
   double4 *S_der, *v_der;
   int *hash_cur;        // cell hash per array position (sorted order)
-  int *hash_new, *slot, *perm_u, *perm;
+  int *hash_new, *slot, *perm;
+  int4 *perm_u;         // per sorted slot: {particle, cell, cell start, cell end} (unranked)
   int *count;           // per-cell counts (max_cell)
   int *off;             // cell offsets (max_cell + 1)
   unsigned long long *scan_status;
@@ -177,12 +178,22 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int
   const int tile = s_tile;
   if (tile < num_tiles) {
     const int base = tile * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    static_assert(SCAN_ITEMS == 8, "two int4 per thread");
+    const bool full = base + SCAN_ITEMS <= num_cell;  // base is a multiple of 8: 32-byte aligned
     int v[SCAN_ITEMS];
+    if (full) {
+      const int4 c0 = reinterpret_cast<const int4 *>(D.count + base)[0];
+      const int4 c1 = reinterpret_cast<const int4 *>(D.count + base)[1];
+      v[0] = c0.x; v[1] = c0.y; v[2] = c0.z; v[3] = c0.w;
+      v[4] = c1.x; v[5] = c1.y; v[6] = c1.z; v[7] = c1.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < SCAN_ITEMS; ++k) v[k] = base + k < num_cell ? D.count[base + k] : 0;
+    }
     int tsum = 0, tmax = 0;
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS; ++k) {
-      int c = base + k;
-      int x = c < num_cell ? D.count[c] : 0;
+      const int x = v[k];
       v[k] = tsum;
       tsum += x;
       tmax = max(tmax, x);
@@ -247,12 +258,21 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int
     }
     __syncthreads();
     const int excl = s_excl + thread_excl;
+    if (full) {
+      int4 *o = reinterpret_cast<int4 *>(D.off + base);
+      o[0] = make_int4(excl + v[0], excl + v[1], excl + v[2], excl + v[3]);
+      o[1] = make_int4(excl + v[4], excl + v[5], excl + v[6], excl + v[7]);
+      int4 *z = reinterpret_cast<int4 *>(D.count + base);  // ready for the next step
+      z[0] = make_int4(0, 0, 0, 0);
+      z[1] = make_int4(0, 0, 0, 0);
+    } else {
 #pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; ++k) {
-      int c = base + k;
-      if (c < num_cell) {
-        D.off[c] = excl + v[k];
-        D.count[c] = 0;  // ready for the next step
+      for (int k = 0; k < SCAN_ITEMS; ++k) {
+        const int c = base + k;
+        if (c < num_cell) {
+          D.off[c] = excl + v[k];
+          D.count[c] = 0;
+        }
       }
     }
     if (tile == num_tiles - 1 && threadIdx.x == 0) D.off[num_cell] = s_excl + agg;
@@ -273,26 +293,27 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int
 static __global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= N) return;
-  D.perm_u[D.off[D.hash_new[q]] + D.slot[q]] = q;
+  const int c = D.hash_new[q];
+  const int s = D.off[c];
+  // the cell and its bounds travel with the particle, so the reorder needs one load
+  D.perm_u[s + D.slot[q]] = make_int4(q, c, s, D.off[c + 1]);
 }
 
 // ---------------------------------------------------------------------------------------
 // stable rank fix-up: inside a cell, the atomics gave the members in arbitrary order; the
 // stable sort wants them by previous array position. Position q of the sorted order holds
 // the member with exactly (q - cell_start) smaller previous positions.
-__device__ __forceinline__ int stable_member(const dev_buffers &D, int q) {
-  const int pu = D.perm_u[q];
-  const int c = D.hash_new[pu];
-  const int s = D.off[c], e = D.off[c + 1];
-  if (e - s == 1) return pu;
-  const int k = q - s;
-  for (int m = s; m < e; ++m) {
-    const int v = D.perm_u[m];
+__device__ __forceinline__ int2 stable_member(const dev_buffers &D, int q) {
+  const int4 u = D.perm_u[q];  // particle, cell, cell start, cell end
+  if (u.w - u.z == 1) return make_int2(u.x, u.y);
+  const int k = q - u.z;
+  for (int m = u.z; m < u.w; ++m) {
+    const int v = D.perm_u[m].x;
     int less = 0;
-    for (int m2 = s; m2 < e; ++m2) less += D.perm_u[m2] < v;
-    if (less == k) return v;
+    for (int m2 = u.z; m2 < u.w; ++m2) less += D.perm_u[m2].x < v;
+    if (less == k) return make_int2(v, u.y);
   }
-  return pu;  // unreachable for a consistent cell list
+  return make_int2(u.x, u.y);  // unreachable for a consistent cell list
 }
 
 // gather into the new order (grid_gpu_green.cu:22-116) and, if PREDICT, the predictor
@@ -302,12 +323,12 @@ template <bool PREDICT, bool MIXED>
 static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
-  const int p = stable_member(D, q);
+  const int2 pc = stable_member(D, q);
+  const int p = pc.x, hsh = pc.y;
   const state_set &A = D.A;
   const state_set &B = D.B;
   D.perm[q] = p;
   B.idx[q] = P.grid_kind == MF_GRID_GREEN ? p : A.idx[p];
-  const int hsh = D.hash_new[p];
   D.hash_cur[q] = hsh;
 
   double2 pos = A.pos[p], vel = A.vel[p];
@@ -393,9 +414,11 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
     float fr[F_WIDTH] = {(float)(pos.x - ox), (float)(pos.y - oy), __int_as_float((int)(rf | ((unsigned)cj << 8))),
                          (float)vel.x, (float)vel.y, (float)sxx, (float)sxy, (float)syy, (float)Rxx, (float)Rxy,
                          (float)Ryy, (float)h, (float)rho, (float)c, (float)vol, (float)(T - P.trml_wp.T_init)};
-    float4 *fd = reinterpret_cast<float4 *>(D.recf + (size_t)q * F_WIDTH);
+    // four planes of float4 (structure of arrays): plane k of particle q at [k * N + q]
+    float4 *fd = reinterpret_cast<float4 *>(D.recf);
 #pragma unroll
-    for (int k = 0; k < F_WIDTH / 4; ++k) fd[k] = make_float4(fr[4 * k], fr[4 * k + 1], fr[4 * k + 2], fr[4 * k + 3]);
+    for (int k = 0; k < F_WIDTH / 4; ++k)
+      fd[(size_t)k * P.N + q] = make_float4(fr[4 * k], fr[4 * k + 1], fr[4 * k + 2], fr[4 * k + 3]);
   }
 }
 
@@ -607,7 +630,11 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers
 // with IEEE-rounded operations (bitwise equal to the host's double arithmetic), one lane per
 // segment and one for the fillet; block 0 stores it for the next step
 __device__ __forceinline__ void tool_advance_shared(mf_tool_state &T, const dev_buffers &D, double dt) {
-  if (threadIdx.x == 0) T = *D.tool_prev;
+  // copied word by word by the block's threads
+  static_assert(sizeof(mf_tool_state) % sizeof(double) == 0, "tool state is a whole number of doubles");
+  constexpr int WORDS = (int)(sizeof(mf_tool_state) / sizeof(double));
+  for (int w = threadIdx.x; w < WORDS; w += blockDim.x)
+    reinterpret_cast<double *>(&T)[w] = reinterpret_cast<const double *>(D.tool_prev)[w];
   __syncthreads();
   const double sx = __dmul_rn(dt, T.vel[0]), sy = __dmul_rn(dt, T.vel[1]);
   const int t = threadIdx.x;
@@ -640,13 +667,18 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
   const bool fixed = f & FLAG_FIXED;
   // the state at the start of the step, in the new order (predict/correct skip blanked
   // particles, so for them it is also the state at the end of the step)
+  // every load is issued here, before any store, so that they are all in flight together
   const int p = D.perm[q];
-  double2 pos = A.pos[p], vel = A.vel[p];
-  double4 S = A.S[p];
-  double rho = A.rho[p], T = A.T[p];
   double2 pos_t = B.pos_t[q], vel_t = B.vel_t[q];
   const double4 S_t = B.S_t[q];
   const double rho_t = B.rho_t[q], T_t = B.T_t[q];
+  double eps_pl = B.eps_pl[q], eps_pl_dot = B.eps_pl_dot[q];
+  double2 fc = B.fc[q], ft = B.ft[q];
+  const double2 normal = D.n[q];
+  const double pr = D.pp[q];
+  double2 pos = A.pos[p], vel = A.vel[p];
+  double4 S = A.S[p];
+  double rho = A.rho[p], T = A.T[p];
   if (!blanked) {  // correct (leap_frog.cu:68-92)
     pos.x = pos.x + dt * pos_t.x;
     pos.y = pos.y + dt * pos_t.y;
@@ -659,13 +691,10 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
     rho = rho + dt * rho_t;
     T = T + dt * T_t;
   }
-  double eps_pl = B.eps_pl[q], eps_pl_dot = B.eps_pl_dot[q];
-  double2 fc = B.fc[q], ft = B.ft[q];
   // friction heat (actions_gpu.cu:135-162), previous step's ft and n
   if (P.has_tool && P.fric_heat && !tool) {
     const double f_fric_mag = (double)sqrtf((float)(ft.x * ft.x + ft.y * ft.y));
     if (f_fric_mag != 0.) {
-      const double2 normal = D.n[q];
       const double vdx = vel.x - TL.vel[0], vdy = vel.y - TL.vel[1];
       const double vdn = vdx * normal.x + vdy * normal.y;
       const double vrx = vdx - vdn, vry = vdy - vdn;
@@ -678,7 +707,6 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
     const double mu = P.phys.G;
     const double Sxx = S.x, Syy = S.z, Szz = S.w, Sxy = S.y;
     const double norm_Strial = (double)sqrtf((float)(Sxx * Sxx + Syy * Syy + Szz * Szz + Sxy * Sxy));
-    const double pr = D.pp[q];
     const double cxx = Sxx - pr, cyy = Syy - pr, czz = Szz - pr, cxy = Sxy;
     const double svm = (double)sqrtf(
         (float)((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy));

@@ -16,38 +16,120 @@
 
 namespace mf {
 
-static __global__ void __launch_bounds__(PAIR_BLOCK, 8) k_pair_mixed(params P, dev_buffers D) {
+// the i particle's values and the pair sums of one thread
+struct mixed_i {
+  float x, y, vx, vy, sxx, sxy, syy, Rxx, Rxy, Ryy, h, rho, c, T;
+  float h1, fourh2, fac;
+  bool mech, thermal, nonfinite;
+};
+struct mixed_acc {
+  float vdx, vdy, vdz, vdw, sdx, sdy, sdz, sdw, vtx, vty, xtx, xty, T_lapl;
+};
+struct mixed_const {
+  float mass, inv_wdeltap, alpha, beta, eta2, m_eps;
+};
+
+// one neighbour j (records b0..b3) of particle i at offset (xij, yij)
+__device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_const &K, mixed_acc &a, float xij,
+                                               float yij, const float4 &b0, const float4 &b1, const float4 &b2,
+                                               const float4 &b3) {
+  const unsigned fjw = (unsigned)__float_as_int(b0.z);
+  const float rr2 = xij * xij + yij * yij;
+  const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
+  float w = 0.f, w_x = 0.f, w_y = 0.f, dwr = 0.f;
+  if (in_support) {
+    const float rinv = rsqrtf(rr2);
+    const float qq = rr2 * rinv * I.h1;
+    float val, der;
+    if (qq > 1.f) {
+      const float t = 2.f - qq;
+      const float t2 = t * t;
+      val = 0.25f * t2 * t2 * t2;
+      der = -0.75f * t2 * I.h1 * rinv;
+    } else {
+      val = 1.f - 1.5f * qq * qq * (1.f - 0.5f * qq);
+      der = -3.0f * qq * (1.f - 0.75f * qq) * I.h1 * rinv;
+    }
+    w = val * I.fac;
+    dwr = der * I.fac;
+    w_x = dwr * xij;
+    w_y = dwr * yij;
+  }
+  const float volj = b3.z;
+  if (I.mech && !(fjw & FLAG_TOOL)) {
+    const float dvx = b0.w - I.vx, dvy = b1.x - I.vy;
+    const float ax = dvx * volj, ay = dvy * volj;
+    a.vdx += ax * w_x;
+    a.vdy += ax * w_y;
+    a.vdz += ay * w_x;
+    a.vdw += ay * w_y;
+    float fab = w * K.inv_wdeltap;
+    fab *= fab;
+    fab *= fab;
+    const float sxy = K.mass * (I.sxy + b1.z + fab * (I.Rxy + b2.y));
+    a.sdx += K.mass * (I.sxx + b1.y + fab * (I.Rxx + b2.x)) * w_x;
+    a.sdy += sxy * w_y;
+    a.sdz += sxy * w_x;
+    a.sdw += K.mass * (I.syy + b1.w + fab * (I.Ryy + b2.z)) * w_y;
+    const float vijposij = -(dvx * xij + dvy * yij);
+    const float irhoij = __frcp_rn(0.5f * (I.rho + b3.x));
+    if (vijposij < 0.f) {
+      const float cij = 0.5f * (I.c + b3.y);
+      const float hij = 0.5f * (I.h + b2.w);
+      const float muij = hij * vijposij * __frcp_rn(rr2 + K.eta2 * hij * hij);
+      const float piij = (-K.alpha * cij * muij + K.beta * muij * muij) * irhoij;
+      a.vtx -= K.mass * piij * w_x;
+      a.vty -= K.mass * piij * w_y;
+    }
+    const float xs = K.m_eps * w * irhoij;
+    a.xtx += xs * dvx;
+    a.xty += xs * dvy;
+  }
+  // Brookshaw: 2 (m/rho_j)(Ti - Tj)(e_ij . grad W)/r with (e_ij . grad W)/r = der*fac
+  if (I.thermal && rr2 > 1e-16f) a.T_lapl += 2.0f * volj * (I.T - b3.w) * dwr;
+}
+
+// 80 registers (6 blocks of 128 per SM) keep the kernel free of spills
+static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
-  const float4 *__restrict__ rec = reinterpret_cast<const float4 *>(D.recf);
-  const float4 a0 = __ldg(rec + 4 * q + 0);  // x, y, flags|cy, vx
+  // record planes (structure of arrays): plane k of particle j at [k * N + j]
+  const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
+  const float4 *__restrict__ r1 = r0 + P.N;
+  const float4 *__restrict__ r2 = r1 + P.N;
+  const float4 *__restrict__ r3 = r2 + P.N;
+  const float4 a0 = __ldg(r0 + q);  // x, y, flags|cy, vx
   const unsigned fi = (unsigned)__float_as_int(a0.z) & 0xffu;
   if (fi & FLAG_BLANKED) return;
   const bool tool_i = fi & FLAG_TOOL;
   const bool brookshaw = P.thermal_solver == MF_THERMAL_BROOKSHAW;
   if (!brookshaw && tool_i) return;
-  const float4 a1 = __ldg(rec + 4 * q + 1);  // vy, sxx, sxy, syy
-  const float4 a2 = __ldg(rec + 4 * q + 2);  // Rxx, Rxy, Ryy, h
-  const float4 a3 = __ldg(rec + 4 * q + 3);  // rho, c, vol, T - T_init
+  const float4 a1 = __ldg(r1 + q);  // vy, sxx, sxy, syy
+  const float4 a2 = __ldg(r2 + q);  // Rxx, Rxy, Ryy, h
+  const float4 a3 = __ldg(r3 + q);  // rho, c, vol, T - T_init
 
-  const float mass = (float)P.phys.mass;
-  const float inv_wdeltap = (float)(1. / P.corr.wdeltap);
-  const float alpha = (float)P.corr.alpha, beta = (float)P.corr.beta, eta = (float)P.corr.eta;
+  mixed_const K;
+  K.mass = (float)P.phys.mass;
+  K.inv_wdeltap = (float)(1. / P.corr.wdeltap);
+  K.alpha = (float)P.corr.alpha;
+  K.beta = (float)P.corr.beta;
+  const float eta = (float)P.corr.eta;
+  K.eta2 = eta * eta;
+  K.m_eps = (float)P.corr.xspheps * K.mass;
   double thermal_alpha = 0.;
   if (brookshaw) thermal_alpha = !tool_i ? P.trml_wp.alpha : (P.thermal_tool_on ? P.trml_tool.alpha : 0.);
-  const bool thermal = thermal_alpha != 0.;
-  const bool nonfinite_i = fi & FLAG_NONFINITE;
-  const bool mech_i = !tool_i;
 
-  const float xi = a0.x, yi = a0.y, vxi = a0.w, vyi = a1.x;
-  const float sxxi = a1.y, sxyi = a1.z, syyi = a1.w;
-  const float Rxxi = a2.x, Rxyi = a2.y, Ryyi = a2.z, hi = a2.w;
-  const float rhoi = a3.x, ci = a3.y, Ti = thermal ? a3.w : 0.f;
-  const float h1 = 1.f / hi;
-  const float fourh2 = 4.f * hi * hi;
-  const float fac = 0.454728408833987f * h1 * h1;
-  const float eta2 = eta * eta;
-  const float m_eps = (float)P.corr.xspheps * mass;
+  mixed_i I;
+  I.thermal = thermal_alpha != 0.;
+  I.nonfinite = fi & FLAG_NONFINITE;
+  I.mech = !tool_i;
+  I.x = a0.x; I.y = a0.y; I.vx = a0.w; I.vy = a1.x;
+  I.sxx = a1.y; I.sxy = a1.z; I.syy = a1.w;
+  I.Rxx = a2.x; I.Rxy = a2.y; I.Ryy = a2.z; I.h = a2.w;
+  I.rho = a3.x; I.c = a3.y; I.T = I.thermal ? a3.w : 0.f;
+  I.h1 = 1.f / I.h;
+  I.fourh2 = 4.f * I.h * I.h;
+  I.fac = 0.454728408833987f * I.h1 * I.h1;
 
   const geom g = *D.g;
   const float dxc = (float)g.dx;
@@ -61,98 +143,44 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 8) k_pair_mixed(params P, d
   // y offset between cell rows: (gj - r) * dx = oy0 - r * dx
   const float oy0 = (float)gj * dxc;
 
-  float vdx = 0.f, vdy = 0.f, vdz = 0.f, vdw = 0.f;
-  float sdx = 0.f, sdy = 0.f, sdz = 0.f, sdw = 0.f;
-  float vtx = 0.f, vty = 0.f, xtx = 0.f, xty = 0.f;
-  float T_lapl = 0.f;
+  mixed_acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
   for (int ii = low_i; ii < high_i; ++ii) {
     const int col = ii * g.ny;
     const int j0 = __ldg(D.off + col + low_j);
     const int j1 = __ldg(D.off + col + high_j);
-    const float ox = (float)(gi - ii) * dxc + xi;
+    const float ox = (float)(gi - ii) * dxc + I.x;
     // chunks of up to 32 candidates: mark the contributing ones, then visit them in order
     for (int jb = j0; jb < j1; jb += 32) {
       const int jn = min(32, j1 - jb);
       unsigned mask = 0u;
 #pragma unroll 4
       for (int k = 0; k < jn; ++k) {
-        const float4 b0 = __ldg(rec + 4 * (jb + k));
+        const float4 b0 = __ldg(r0 + jb + k);
         const unsigned fjw = (unsigned)__float_as_int(b0.z);
         const float xij = ox - b0.x;
-        const float yij = (oy0 - (float)(int)(fjw >> 8) * dxc) + (yi - b0.y);
+        const float yij = (oy0 - (float)(int)(fjw >> 8) * dxc) + (I.y - b0.y);
         const float rr2 = xij * xij + yij * yij;
-        const bool in_support = !(rr2 >= fourh2 || rr2 < 1e-8f);
-        const bool take = !(fjw & FLAG_BLANKED) && (in_support || nonfinite_i || (fjw & FLAG_NONFINITE));
+        const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
+        const bool take = !(fjw & FLAG_BLANKED) && (in_support || I.nonfinite || (fjw & FLAG_NONFINITE));
         mask |= (take ? 1u : 0u) << k;
       }
       while (mask) {
         const int k = __ffs(mask) - 1;
         mask &= mask - 1u;
-        const float4 *sj = rec + 4 * (jb + k);
-        const float4 b0 = __ldg(sj + 0);  // x, y, flags|cy, vx
-        const float4 b3 = __ldg(sj + 3);  // rho, c, vol, T - T_init
-        const unsigned fjw = (unsigned)__float_as_int(b0.z);
-        const float xij = ox - b0.x;
-        const float yij = (oy0 - (float)(int)(fjw >> 8) * dxc) + (yi - b0.y);
-        const float rr2 = xij * xij + yij * yij;
-        const bool in_support = !(rr2 >= fourh2 || rr2 < 1e-8f);
-        float w = 0.f, w_x = 0.f, w_y = 0.f, dwr = 0.f;
-        if (in_support) {
-          const float rinv = rsqrtf(rr2);
-          const float qq = rr2 * rinv * h1;
-          float val, der;
-          if (qq > 1.f) {
-            const float t = 2.f - qq;
-            const float t2 = t * t;
-            val = 0.25f * t2 * t2 * t2;
-            der = -0.75f * t2 * h1 * rinv;
-          } else {
-            val = 1.f - 1.5f * qq * qq * (1.f - 0.5f * qq);
-            der = -3.0f * qq * (1.f - 0.75f * qq) * h1 * rinv;
-          }
-          w = val * fac;
-          dwr = der * fac;
-          w_x = dwr * xij;
-          w_y = dwr * yij;
-        }
-        const float volj = b3.z;
-        if (mech_i && !(fjw & FLAG_TOOL)) {
-          const float4 b1 = __ldg(sj + 1);  // vy, sxx, sxy, syy
-          const float4 b2 = __ldg(sj + 2);  // Rxx, Rxy, Ryy, h
-          const float dvx = b0.w - vxi, dvy = b1.x - vyi;
-          const float ax = dvx * volj, ay = dvy * volj;
-          vdx += ax * w_x;
-          vdy += ax * w_y;
-          vdz += ay * w_x;
-          vdw += ay * w_y;
-          float fab = w * inv_wdeltap;
-          fab *= fab;
-          fab *= fab;
-          const float sxy = mass * (sxyi + b1.z + fab * (Rxyi + b2.y));
-          sdx += mass * (sxxi + b1.y + fab * (Rxxi + b2.x)) * w_x;
-          sdy += sxy * w_y;
-          sdz += sxy * w_x;
-          sdw += mass * (syyi + b1.w + fab * (Ryyi + b2.z)) * w_y;
-          const float vijposij = -(dvx * xij + dvy * yij);
-          const float irhoij = __frcp_rn(0.5f * (rhoi + b3.x));
-          if (vijposij < 0.f) {
-            const float cij = 0.5f * (ci + b3.y);
-            const float hij = 0.5f * (hi + b2.w);
-            const float muij = hij * vijposij * __frcp_rn(rr2 + eta2 * hij * hij);
-            const float piij = (-alpha * cij * muij + beta * muij * muij) * irhoij;
-            vtx -= mass * piij * w_x;
-            vty -= mass * piij * w_y;
-          }
-          const float xs = m_eps * w * irhoij;
-          xtx += xs * dvx;
-          xty += xs * dvy;
-        }
-        // Brookshaw: 2 (m/rho_j)(Ti - Tj)(e_ij . grad W)/r with (e_ij . grad W)/r = der*fac
-        if (thermal && rr2 > 1e-16f) T_lapl += 2.0f * volj * (Ti - b3.w) * dwr;
+        const int j = jb + k;
+        // all four planes at once: one load latency per neighbour
+        const float4 b0 = __ldg(r0 + j), b1 = __ldg(r1 + j), b2 = __ldg(r2 + j), b3 = __ldg(r3 + j);
+        const float yij = (oy0 - (float)(int)((unsigned)__float_as_int(b0.z) >> 8) * dxc) + (I.y - b0.y);
+        mixed_interact(I, K, acc, ox - b0.x, yij, b0, b1, b2, b3);
       }
     }
   }
+  const float vdx = acc.vdx, vdy = acc.vdy, vdz = acc.vdz, vdw = acc.vdw;
+  const float sdx = acc.sdx, sdy = acc.sdy, sdz = acc.sdz, sdw = acc.sdw;
+  const float vtx = acc.vtx, vty = acc.vty, xtx = acc.xtx, xty = acc.xty, T_lapl = acc.T_lapl;
+  const bool mech_i = I.mech, thermal = I.thermal;
+  const float rhoi = I.rho;
 
   const state_set &B = D.B;
   if (P.keep_derivs) {

@@ -32,11 +32,11 @@ constexpr int NA_MAX_CELLS = MF_NOALLOC_MAX_CELLS;
 constexpr int NA_SCAN_TILES = (NA_MAX_CELLS + SCAN_TILE - 1) / SCAN_TILE + 1;
 
 struct noalloc_scratch {
+  int4 perm_u[NA_MAX_PARTICLES];
   int count[NA_MAX_CELLS];
   int off[NA_MAX_CELLS + 1];
   int hash_new[NA_MAX_PARTICLES];
   int slot[NA_MAX_PARTICLES];
-  int perm_u[NA_MAX_PARTICLES];
   unsigned long long scan_status[NA_SCAN_TILES];
   geom g;
   dev_status st;
@@ -102,9 +102,9 @@ __global__ void k_na_output(int N, dev_buffers D, int *__restrict__ hash_sorted,
   const int stride = gridDim.x * blockDim.x;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   for (int q = gid; q < N; q += stride) {
-    const int p = stable_member(D, q);
-    idx[q] = p;
-    hash_sorted[q] = D.hash_new[p];
+    const int2 pc = stable_member(D, q);
+    idx[q] = pc.x;
+    hash_sorted[q] = pc.y;
   }
   for (int c = gid; c < num_cell; c += stride) {
     const int s = D.off[c], e = D.off[c + 1];
