@@ -138,7 +138,6 @@ int alloc_particles(mf_ctx *ctx, int N) {
   TRY(dalloc(ctx, L, &D.v_der, N));
   TRY(dalloc(ctx, L, &D.hash_cur, N));
   TRY(dalloc(ctx, L, &D.hash_new, N));
-  TRY(dalloc(ctx, L, &D.slot, N));
   TRY(dalloc(ctx, L, &D.perm_u, N));
   TRY(dalloc(ctx, L, &D.perm, N));
   ctx->finish_blocks = std::min((N + BLOCK - 1) / BLOCK, ctx->sm_count * FINISH_BLOCKS_PER_SM);

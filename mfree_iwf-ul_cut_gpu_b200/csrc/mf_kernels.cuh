@@ -7,7 +7,7 @@
 //                 the previous step has done it
 //   k_scan        single-pass decoupled look-back exclusive scan of the
 //                 counts -> cell offsets (the cell_start/cell_end lists)
-//   k_scatter     particle -> slot inside its cell
+//   k_scatter     particle -> slot inside its cell (atomic cursor per cell)
 //   k_reorder     stable rank fix-up inside each cell (equal to thrust's stable sort_by_key),
 //                 gather of the persistent state into the other buffer, and - in a step - the
 //                 predictor, EOS, artificial stress and the neighbour pair records
@@ -42,7 +42,7 @@ struct dev_buffers {
   double *pp;           // predictor pressure (the reference's particles->p)
   double4 *S_der, *v_der;
   int *hash_cur;        // cell hash per array position (sorted order)
-  int *hash_new, *slot, *perm;
+  int *hash_new, *perm;
   int4 *perm_u;         // per sorted slot: {particle, cell, cell start, cell end} (unranked)
   int *count;           // per-cell counts (max_cell)
   int *off;             // cell offsets (max_cell + 1)
@@ -156,7 +156,7 @@ static __global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A,
     else if (hh >= g.num_cell) { hh = g.num_cell - 1; oog = 1; }
     const int hsh = (int)hh;
     D.hash_new[gid] = hsh;
-    D.slot[gid] = atomicAdd(&D.count[hsh], 1);
+    atomicAdd(&D.count[hsh], 1);  // no return value: a fire-and-forget reduction
   }
   unsigned any = __ballot_sync(0xffffffffu, oog);
   if (any && lane_id() == 0) atomicAdd(&D.st->out_of_grid, (unsigned long long)__popc(any));
@@ -295,25 +295,28 @@ static __global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D) 
   if (q >= N) return;
   const int c = D.hash_new[q];
   const int s = D.off[c];
-  // the cell and its bounds travel with the particle, so the reorder needs one load
-  D.perm_u[s + D.slot[q]] = make_int4(q, c, s, D.off[c + 1]);
+  // the scan left the counts at zero: they serve as per-cell cursors here (the reorder
+  // zeroes them again). The cell and its bounds travel with the particle, so the reorder
+  // needs one load.
+  const int slot = atomicAdd(&D.count[c], 1);
+  D.perm_u[s + slot] = make_int4(q, c, s, D.off[c + 1]);
 }
 
 // ---------------------------------------------------------------------------------------
 // stable rank fix-up: inside a cell, the atomics gave the members in arbitrary order; the
 // stable sort wants them by previous array position. Position q of the sorted order holds
 // the member with exactly (q - cell_start) smaller previous positions.
-__device__ __forceinline__ int2 stable_member(const dev_buffers &D, int q) {
-  const int4 u = D.perm_u[q];  // particle, cell, cell start, cell end
-  if (u.w - u.z == 1) return make_int2(u.x, u.y);
+// u = perm_u[q]: particle, cell, cell start, cell end
+__device__ __forceinline__ int stable_member(const dev_buffers &D, int q, const int4 u) {
+  if (u.w - u.z == 1) return u.x;
   const int k = q - u.z;
   for (int m = u.z; m < u.w; ++m) {
     const int v = D.perm_u[m].x;
     int less = 0;
     for (int m2 = u.z; m2 < u.w; ++m2) less += D.perm_u[m2].x < v;
-    if (less == k) return make_int2(v, u.y);
+    if (less == k) return v;
   }
-  return make_int2(u.x, u.y);  // unreachable for a consistent cell list
+  return u.x;  // unreachable for a consistent cell list
 }
 
 // gather into the new order (grid_gpu_green.cu:22-116) and, if PREDICT, the predictor
@@ -323,8 +326,9 @@ template <bool PREDICT, bool MIXED>
 static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
-  const int2 pc = stable_member(D, q);
-  const int p = pc.x, hsh = pc.y;
+  const int4 u = D.perm_u[q];
+  const int p = stable_member(D, q, u), hsh = u.y;
+  if (q == u.z) D.count[hsh] = 0;  // the scatter's cursor, back to zero for the next counts
   const state_set &A = D.A;
   const state_set &B = D.B;
   D.perm[q] = p;
@@ -655,7 +659,8 @@ __device__ __forceinline__ void tool_advance_shared(mf_tool_state &T, const dev_
 
 // corrector .. invalidate for one particle (leap_frog.cu:68-92, actions_gpu.cu:135-162,
 // 226-349, tool_gpu.cu:151-221); returns the final position and flags
-__device__ __forceinline__ void finish_particle(const params &P, const dev_buffers &D, const mf_tool_state &TL, int q,
+__device__ __forceinline__ void finish_particle(const params &P, const dev_buffers &D, const mf_tool_state &TL,
+                                               const mf_joco_constants &JC, int q,
                                                double2 &pos_out, unsigned &f_out, double2 &fc_out, double2 &ft_out,
                                                unsigned &newly_blanked, unsigned &capped) {
   const state_set &A = D.A;
@@ -710,12 +715,12 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
     const double cxx = Sxx - pr, cyy = Syy - pr, czz = Szz - pr, cxy = Sxy;
     const double svm = (double)sqrtf(
         (float)((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy));
-    const double sigma_Y = sigma_yield(P.joco, eps_pl, eps_pl_dot, T);
+    const double sigma_Y = sigma_yield(JC, eps_pl, eps_pl_dot, T);
     if (svm < sigma_Y) {
       eps_pl_dot = 0.;
     } else {
       bool cap = false;
-      const double delta_lambda = solve_secant(P.joco, P.jc_model, fmax(eps_pl_dot * dt * sqrt(2. / 3.), 1e-8),
+      const double delta_lambda = solve_secant(JC, P.jc_model, fmax(eps_pl_dot * dt * sqrt(2. / 3.), 1e-8),
                                                1e-6, norm_Strial, eps_pl, T, dt, P.phys.G, cap);
       capped += cap ? 1u : 0u;
       const float s23f = sqrtf((float)(2.0 / 3.0));
@@ -727,7 +732,7 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
       S.y = Sxy - Sxy / norm_Strial * delta_lambda * 2. * mu;
       if (P.trml_wp.tq != 0.) {
         const double delta_eps_pl = eps_pl_new - eps_pl;
-        const double sY = sigma_yield(P.joco, eps_pl_new, eps_pl_dot_new, T);
+        const double sY = sigma_yield(JC, eps_pl_new, eps_pl_dot_new, T);
         T += P.trml_wp.tq / (P.trml_wp.cp * rho) * delta_eps_pl * sY;
       }
       eps_pl = eps_pl_new;
@@ -818,10 +823,15 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
 template <bool FUSE_HASH>
 __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P, dev_buffers D, int num_scan_tiles) {
   __shared__ mf_tool_state s_tool;
+  // the JC constants in shared memory: the out-of-line yield functions take them by
+  // reference, which for a kernel parameter would mean a copy on every thread's stack
+  __shared__ mf_joco_constants s_jc;
   __shared__ ksum sm[BLOCK / 32][4];
   __shared__ unsigned smc[BLOCK / 32][4];
   __shared__ bool last;
-  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt);
+  if (threadIdx.x == 0) s_jc = P.joco;
+  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt);  // (its first barrier also covers s_jc)
+  else __syncthreads();
   const int stride = gridDim.x * blockDim.x;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   ksum fcx{0., 0.}, fcy{0., 0.}, ftx{0., 0.}, fty{0., 0.};
@@ -834,7 +844,7 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
   for (int q = gid; q < P.N; q += stride) {
     double2 pos, fc, ft;
     unsigned f;
-    finish_particle(P, D, s_tool, q, pos, f, fc, ft, newly_blanked, capped);
+    finish_particle(P, D, s_tool, s_jc, q, pos, f, fc, ft, newly_blanked, capped);
     blanked_now += (f & FLAG_BLANKED) ? 1u : 0u;
     ksum_add(fcx, fc.x);
     ksum_add(fcy, fc.y);
@@ -853,7 +863,7 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
       else if (hh >= g.num_cell) { hh = g.num_cell - 1; ++oog; }
       const int hsh = (int)hh;
       D.hash_new[q] = hsh;
-      D.slot[q] = atomicAdd(&D.count[hsh], 1);
+      atomicAdd(&D.count[hsh], 1);
     }
   }
   // block reduction of the force (compensated) and of the counters

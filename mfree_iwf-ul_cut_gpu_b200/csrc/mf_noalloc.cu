@@ -36,7 +36,6 @@ struct noalloc_scratch {
   int count[NA_MAX_CELLS];
   int off[NA_MAX_CELLS + 1];
   int hash_new[NA_MAX_PARTICLES];
-  int slot[NA_MAX_PARTICLES];
   unsigned long long scan_status[NA_SCAN_TILES];
   geom g;
   dev_status st;
@@ -78,7 +77,7 @@ __global__ void k_na_clear(noalloc_scratch *S, geom g) {
     S->scan_done = 0u;
   }
 }
-
+// cell hash (compute_hashes, grid.cu:34-51), clamped into the grid, and per-cell count
 // cell hash (compute_hashes, grid.cu:34-51), clamped into the grid, and per-cell slot
 __global__ void k_na_hash(const double2 *__restrict__ pos, int N, noalloc_scratch *S) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -92,7 +91,7 @@ __global__ void k_na_hash(const double2 *__restrict__ pos, int N, noalloc_scratc
   else if (hh >= g.num_cell) hh = g.num_cell - 1;
   const int h = (int)hh;
   S->hash_new[i] = h;
-  S->slot[i] = atomicAdd(&S->count[h], 1);
+  atomicAdd(&S->count[h], 1);
 }
 
 // sorted outputs: permutation and hash per sorted position; cell bounds in the
@@ -102,9 +101,9 @@ __global__ void k_na_output(int N, dev_buffers D, int *__restrict__ hash_sorted,
   const int stride = gridDim.x * blockDim.x;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   for (int q = gid; q < N; q += stride) {
-    const int2 pc = stable_member(D, q);
-    idx[q] = pc.x;
-    hash_sorted[q] = pc.y;
+    const int4 u = D.perm_u[q];
+    idx[q] = stable_member(D, q, u);
+    hash_sorted[q] = u.y;
   }
   for (int c = gid; c < num_cell; c += stride) {
     const int s = D.off[c], e = D.off[c + 1];
@@ -139,7 +138,6 @@ extern "C" int mf_cells_build_noalloc(const double *d_pos, int N, double bbmin_x
   D.count = S->count;
   D.off = S->off;
   D.hash_new = S->hash_new;
-  D.slot = S->slot;
   D.perm_u = S->perm_u;
   D.scan_status = S->scan_status;
   D.scan_done = &S->scan_done;
