@@ -31,7 +31,12 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 PKG_DIR = ROOT / "mfree_iwf-ul_cut_gpu_b200"
 METRIC = "particle-steps/s at ~150k particles w/ thermal contact: mixed vs FP64, same B200"
-ALGO_BYTES_PER_PARTICLE_STEP = 480.0  # canonical FP64 bytes per particle-step
+# canonical algorithmic bytes per particle-step: one read and one write of the 224 B of mutable
+# FP64 state plus a 32 B read of the per-particle constants
+ALGO_BYTES_PER_PARTICLE_STEP = 480.0
+# ncu summary of the pair kernel on this workload; its "dram bytes per launch" line is the
+# roofline's measured traffic
+PAIR_PROFILE = "profiles/k_pair_mixed_cut714x214.txt"
 FLUSH_BYTES = 256 << 20
 
 
@@ -327,6 +332,20 @@ def run_reference(args):
     return 0
 
 
+def profiled_traffic(path, n_particles):
+    """DRAM bytes (read + write) per pair-kernel launch from the committed ncu summary of the
+    same workload, or None when there is none for this particle count."""
+    if not path.exists():
+        return None
+    text = path.read_text()
+    if f"{n_particles} particles" not in text:
+        return None
+    for line in text.splitlines():
+        if line.startswith("dram bytes per launch (read + write):"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -386,13 +405,7 @@ def main():
     head = results["mixed"]
     achieved = ALGO_BYTES_PER_PARTICLE_STEP * N / (head["pair_kernel_ms"] * 1e-3) / 1e9
     step_achieved = ALGO_BYTES_PER_PARTICLE_STEP * N / (head["ms_per_step"] * 1e-3) / 1e9
-    traffic = None
-    prof = ROOT / "profiles" / "pair_kernel_traffic.json"
-    if prof.exists():
-        try:
-            traffic = json.loads(prof.read_text()).get("mixed_bytes_per_launch")
-        except Exception:
-            traffic = None
+    traffic = profiled_traffic(ROOT / PAIR_PROFILE, N) if args.lattice_scale == 1.0 else None
 
     e2e = None
     if rank == 0:
