@@ -240,6 +240,96 @@ def e2e_form(mf, torch, scene, precision, steps, device):
     return (t1 - t0), h2d, d2h, finite
 
 
+def run_form(mf, scene, precision, steps, device, torch=None):
+    """`steps` steps of one form from the scene's initial state. Returns the per-step tool
+    force (steps x 2), the end state ordered by particle number, and the device time (s)."""
+    ctx = mf.Context(device)
+    ctx.upload_scene(scene, mf.GRID_GREEN)
+    ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
+    forces, left, secs = [], steps, 0.0
+    chunk = 50_000  # below the device force log's 65,536 entries
+    while left > 0:
+        n = min(left, chunk)
+        if torch is not None:
+            stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ctx.step(n)
+            b.record(stream)
+            torch.cuda.synchronize(device)
+            secs += a.elapsed_time(b) * 1e-3
+        else:
+            ctx.step(n)
+        forces.append(ctx.force_log())
+        left -= n
+    order = np.argsort(ctx.get("id"))
+    state = {k: ctx.get(k)[order] for k in ("S", "p", "eps_pl", "T", "tool_p", "blanked")}
+    status = ctx.status()
+    ctx.close()
+    return np.concatenate(forces), state, secs, status
+
+
+def von_mises(S, p):
+    """The return map's von Mises stress of (S - p I) (actions_gpu.cu:240-251)."""
+    cxx, cxy, cyy, czz = S[:, 0] - p, S[:, 1], S[:, 2] - p, S[:, 3] - p
+    return np.sqrt(np.maximum(cxx * cxx + cyy * cyy + czz * czz - cxx * cyy - cxx * czz - cyy * czz
+                              + 3.0 * cxy * cxy, 0.0))
+
+
+def form_errors(scene, ref, test):
+    """Mixed (test) against FP64 (ref): relative error of the mean tool force over the run and
+    relative L2 errors of the end fields over the workpiece particles blanked in neither."""
+    (f64, s64), (fm, sm) = ref, test
+    mask = (s64["tool_p"] == 0.0) & (s64["blanked"] == 0.0) & (sm["blanked"] == 0.0)
+
+    def rel_l2(a, b):
+        den = float(np.linalg.norm(b))
+        return float(np.linalg.norm(a - b)) / den if den > 0 else float(np.linalg.norm(a - b))
+
+    T0 = scene.s.trml_wp.T_init
+    mean64, meanm = f64.mean(axis=0), fm.mean(axis=0)
+    return {
+        "mean_fc": [float(meanm[0]), float(mean64[0])],
+        "mean_fc_rel_err": abs(float(meanm[0] - mean64[0])) / abs(float(mean64[0])) if mean64[0] else None,
+        "mean_ff_rel_err": abs(float(meanm[1] - mean64[1])) / abs(float(mean64[1])) if mean64[1] else None,
+        "von_mises_rel_l2": rel_l2(von_mises(sm["S"], sm["p"])[mask], von_mises(s64["S"], s64["p"])[mask]),
+        "eps_pl_rel_l2": rel_l2(sm["eps_pl"][mask], s64["eps_pl"][mask]),
+        "T_rise_rel_l2": rel_l2(sm["T"][mask] - T0, s64["T"][mask] - T0),
+        "blanked": [int((sm["blanked"] != 0).sum()), int((s64["blanked"] != 0).sum())],
+    }
+
+
+def steps_per_mm(scene, params):
+    """Leap-frog steps for 1 mm of tool travel (speed in cm/us, dt in us)."""
+    return 0.1 / (params.speed * scene.s.dt)
+
+
+def accuracy(mf, scene, params, steps, device):
+    """Mixed against FP64 over the first `steps` steps of the cut, both from the same state."""
+    f64, s64, _, _ = run_form(mf, scene, mf.PRECISION_FP64, steps, device)
+    fm, sm, _, _ = run_form(mf, scene, mf.PRECISION_MIXED, steps, device)
+    out = {"steps": steps, "tool_travel_um": steps * scene.s.dt * params.speed * 1e4,
+           "against": "the FP64 form (single steps equal to the oracle to 1e-12) from the same initial state"}
+    out.update(form_errors(scene, (f64, s64), (fm, sm)))
+    return out
+
+
+def cut_run(mf, torch, scene, params, mm, device):
+    """`mm` millimetres of cut in each form: device wall time per mm and the mixed form's errors."""
+    steps = int(round(mm * steps_per_mm(scene, params)))
+    f64, s64, t64, st64 = run_form(mf, scene, mf.PRECISION_FP64, steps, device, torch)
+    fm, sm, tm, stm = run_form(mf, scene, mf.PRECISION_MIXED, steps, device, torch)
+    out = {"mode": "cut", "mm": mm, "steps": steps, "n_particles": scene.N,
+           "wall_s_per_mm": {"fp64": t64 / mm, "mixed": tm / mm},
+           "particle_steps_per_s": {"fp64": scene.N * steps / t64, "mixed": scene.N * steps / tm},
+           "status": {"fp64": st64, "mixed": stm}}
+    out.update(form_errors(scene, (f64, s64), (fm, sm)))
+    # time-averaged force over the second half of the run (past the entry transient)
+    h = steps // 2
+    out["mean_force_second_half"] = {"fp64": f64[h:].mean(axis=0).tolist(), "mixed": fm[h:].mean(axis=0).tolist()}
+    return out
+
+
 def cpu_baseline(mf, scene, seconds=12.0, max_steps=5000):
     """The oracle port (C, OpenMP, all host threads) on the same scene: bounded sample."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -285,9 +375,9 @@ def scene_state(mf, scene):
 
 
 def kernels_per_step(mf, precision):
-    # locked grid, Brookshaw: scan, scatter, reorder/predict, pair, finish (the finish kernel
-    # also hashes and counts the particles for the next step)
-    return 5
+    # locked grid, Brookshaw, JC plasticity: scan, scatter, reorder/predict, pair, finish (which
+    # also hashes and counts the particles for the next step), return map of the plastic list
+    return 6
 
 
 def run_reference(args):
@@ -354,6 +444,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=500)
+    ap.add_argument("--accuracy-steps", type=int, default=20_000,
+                    help="steps of the mixed-against-FP64 error report (0: off)")
+    ap.add_argument("--cut-mm", type=float, default=0.0,
+                    help="instead of the benchmark: run this many mm of cut in both forms and report "
+                         "wall time per mm and the mixed form's errors")
     ap.add_argument("--lattice-scale", type=float, default=1.0,
                     help="lattice points per dimension relative to 714 x 214 (same 2.0 x 0.6 mm body); "
                          "values below 1 give the smaller profiling case")
@@ -376,8 +471,16 @@ def main():
                                 device_id=torch.device("cuda", device))
     mf = load_package()
     sc = args.lattice_scale
-    scene = mf.Scene.from_params(cut_params(mf, nx=int(round(714 * sc)), ny=int(round(214 * sc)), dx=2.8e-4 / sc))
+    params = cut_params(mf, nx=int(round(714 * sc)), ny=int(round(214 * sc)), dx=2.8e-4 / sc)
+    scene = mf.Scene.from_params(params)
     N = scene.N
+    if args.cut_mm > 0:
+        if rank == 0:
+            print(json.dumps(cut_run(mf, torch, scene, params, args.cut_mm, device)), flush=True)
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return 0
 
     results = {}
     clocks = None
@@ -417,6 +520,11 @@ def main():
                "steps": args.e2e_steps,
                "what": "state in from pinned host memory, per step mf_step(1) + tool force to pinned host "
                        "memory, final state out; wall clock"}
+    fp64_probe = mf.probe_fp64(device) if rank == 0 else None
+    acc = None
+    if rank == 0 and args.accuracy_steps > 0:
+        acc = accuracy(mf, scene, params, args.accuracy_steps, device)
+    spm = steps_per_mm(scene, params)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(mf, scene)
@@ -435,7 +543,11 @@ def main():
                                "pair_kernel_ms": results["fp64"]["pair_kernel_ms"]},
                       "mixed": {"value": results["mixed"]["value"], "ms_per_step": results["mixed"]["ms_per_step"],
                                 "pair_kernel_ms": results["mixed"]["pair_kernel_ms"]},
-                      "mixed_over_fp64": results["mixed"]["value"] / results["fp64"]["value"]},
+                      "mixed_over_fp64": results["mixed"]["value"] / results["fp64"]["value"],
+                      "wall_s_per_mm_cut": {f: results[f]["ms_per_step"] * 1e-3 * spm for f in ("fp64", "mixed")},
+                      "steps_per_mm_cut": spm},
+            "mixed_error": acc,
+            "fp64_probe": fp64_probe,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "kernel": "k_pair_mixed", "algorithmic_bytes_per_particle": ALGO_BYTES_PER_PARTICLE_STEP,

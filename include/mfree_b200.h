@@ -56,7 +56,9 @@ extern "C" {
 #define MF_FIELD_V_DER 22     /* 4: only with MF_OPT_KEEP_DERIVATIVES */
 #define MF_FIELD_IDX 23       /* 1 int: Green = sort permutation, Rothlin = persistent id */
 #define MF_FIELD_HASH 24      /* 1 int: cell hash of the last sort, in array order */
-#define MF_NUM_FIELDS 25
+#define MF_FIELD_ID 25        /* 1 int: particle number at creation, carried through every sort
+                                 (no counterpart in the reference: its Green grid keeps none) */
+#define MF_NUM_FIELDS 26
 
 /* ---- enums ---- */
 #define MF_GRID_GREEN 0        /* grid_gpu_green.h:38-91 */
@@ -108,6 +110,7 @@ typedef struct {
   long long secant_cap_hits;  /* JC secant solves that hit the iteration cap */
   int max_cell_occupancy;     /* largest particles-per-cell seen in the last sort */
   int error_flags;            /* bit 0: a bounded wait in the cell scan expired */
+  long long secant_iterations; /* JC secant iterations since creation (cost diagnostic) */
 } mf_status;
 
 typedef struct mf_ctx mf_ctx;
@@ -251,6 +254,12 @@ int mf_tool_translate(mf_tool_state *tool, double dt); /* tool::update_tool with
 /* ---- output: vtk_writer_write (vtk_writer.cpp:20-178, 185-264), legacy ASCII ---- */
 int mf_vtk_write_particles(mf_ctx *ctx, const char *path);
 int mf_vtk_write_tool(const mf_tool_state *tool, const char *path);
+
+/* ---- measurement aid (no counterpart in the reference): FP64 FMA throughput of the device
+   (TFLOP/s, 2 flops per FMA) and the latency in SM clock cycles of one dependent double
+   pow, log and division; allocates and frees 32 bytes of device memory ---- */
+int mf_probe_fp64(int device, double *fma_tflops, double *pow_cycles, double *log_cycles, double *div_cycles,
+                  double *sm_clock_mhz);
 
 #ifdef __cplusplus
 }

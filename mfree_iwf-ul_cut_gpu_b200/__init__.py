@@ -31,7 +31,7 @@ FIELDS = {
     "fixed": (10, 1, False), "blanked": (11, 1, False), "tool_p": (12, 1, False), "eps_pl": (13, 1, False),
     "eps_pl_dot": (14, 1, False), "T": (15, 1, False), "pos_t": (16, 2, False), "vel_t": (17, 2, False),
     "rho_t": (18, 1, False), "S_t": (19, 4, False), "T_t": (20, 1, False), "S_der": (21, 4, False),
-    "v_der": (22, 4, False), "idx": (23, 1, True), "hash": (24, 1, True),
+    "v_der": (22, 4, False), "idx": (23, 1, True), "hash": (24, 1, True), "id": (25, 1, True),
 }
 
 
@@ -84,7 +84,7 @@ class ToolState(C.Structure):
 class Status(C.Structure):
     _fields_ = [("steps", C.c_longlong), ("blanked", C.c_longlong), ("newly_blanked", C.c_longlong),
                 ("out_of_grid", C.c_longlong), ("secant_cap_hits", C.c_longlong),
-                ("max_cell_occupancy", C.c_int), ("error_flags", C.c_int)]
+                ("max_cell_occupancy", C.c_int), ("error_flags", C.c_int), ("secant_iterations", C.c_longlong)]
 
 
 _dp = C.POINTER(C.c_double)
@@ -136,6 +136,7 @@ def lib():
         "mf_set_options": ([vp, i, i, i], i), "mf_set_dt": ([vp, d], i),
         "mf_tool_set": ([vp, C.POINTER(ToolState)], i), "mf_tool_get": ([vp, C.POINTER(ToolState)], i),
         "mf_step": ([vp, i], i), "mf_step_stage": ([vp, i], i), "mf_report_force": ([vp, vp], i),
+        "mf_probe_fp64": ([i, vp, vp, vp, vp, vp], i),
         "mf_force_log": ([vp, vp, i, ip], i), "mf_force_last_async": ([vp, vp], i), "mf_status_get": ([vp, C.POINTER(Status)], i),
         "mf_cut_params_reference": ([C.POINTER(CutParams), i, d, d, d, d, d], i),
         "mf_scene_cut": ([C.POINTER(CutParams), C.POINTER(C.POINTER(SceneStruct))], i),
@@ -360,6 +361,17 @@ class Context:
 
     def vtk_write(self, path):
         self._check(self.L.mf_vtk_write_particles(self.h, str(path).encode()), "mf_vtk_write_particles")
+
+
+def probe_fp64(device=0) -> dict:
+    """FP64 FMA throughput (TFLOP/s) and the latency (SM cycles) of a dependent double pow,
+    log and division on `device` (mf_probe_fp64)."""
+    v = [C.c_double() for _ in range(5)]
+    rc = lib().mf_probe_fp64(device, *[C.byref(x) for x in v])
+    if rc != MF_OK:
+        raise MfError(rc, "mf_probe_fp64")
+    return {"fma_tflops": v[0].value, "pow_cycles": v[1].value, "log_cycles": v[2].value,
+            "div_cycles": v[3].value, "sm_clock_mhz": v[4].value}
 
 
 def tool_construct(tl, length, height, rake, clear, r, mu) -> ToolState:

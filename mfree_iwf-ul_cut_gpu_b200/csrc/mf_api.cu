@@ -110,7 +110,7 @@ int alloc_set(mf_ctx *ctx, state_set &s, int N) {
   TRY(dalloc(ctx, L, &s.rho, N)); TRY(dalloc(ctx, L, &s.T, N)); TRY(dalloc(ctx, L, &s.eps_pl, N));
   TRY(dalloc(ctx, L, &s.eps_pl_dot, N)); TRY(dalloc(ctx, L, &s.h, N)); TRY(dalloc(ctx, L, &s.rho_t, N));
   TRY(dalloc(ctx, L, &s.T_t, N)); TRY(dalloc(ctx, L, &s.S, N)); TRY(dalloc(ctx, L, &s.S_t, N));
-  TRY(dalloc(ctx, L, &s.flags, N)); TRY(dalloc(ctx, L, &s.idx, N));
+  TRY(dalloc(ctx, L, &s.flags, N)); TRY(dalloc(ctx, L, &s.idx, N)); TRY(dalloc(ctx, L, &s.id, N));
   return MF_OK;
 }
 
@@ -140,9 +140,12 @@ int alloc_particles(mf_ctx *ctx, int N) {
   TRY(dalloc(ctx, L, &D.hash_new, N));
   TRY(dalloc(ctx, L, &D.perm_u, N));
   TRY(dalloc(ctx, L, &D.perm, N));
+  TRY(dalloc(ctx, L, &D.plastic_list, N));
   ctx->finish_blocks = std::min((N + BLOCK - 1) / BLOCK, ctx->sm_count * FINISH_BLOCKS_PER_SM);
   ctx->bbox_blocks = std::min((N + BLOCK - 1) / BLOCK, ctx->sm_count * 4);
-  TRY(dalloc(ctx, L, &D.partials, (size_t)std::max(std::max(ctx->finish_blocks, ctx->bbox_blocks), 1) * 8));
+  // per-chunk force partials of the finish kernel (or per-block partials of the bbox pass)
+  const int finish_chunks = (N + BLOCK - 1) / BLOCK;
+  TRY(dalloc(ctx, L, &D.partials, (size_t)std::max(std::max(finish_chunks, ctx->bbox_blocks), 1) * 8));
   TRY(invalidate_counts(ctx));
   ctx->N = N;
   return MF_OK;
@@ -219,6 +222,12 @@ int launch_stage(mf_ctx *ctx, int stage) {
     case 3:
       if (fused_step(ctx)) k_finish<true><<<ctx->finish_blocks, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D, ctx->scan_tiles);
       else k_finish<false><<<ctx->finish_blocks, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D, ctx->scan_tiles);
+      if (ctx->P.plastic) {
+        if (ctx->P.jc_model == MF_JC_TANH)
+          k_plastic<false><<<ctx->sm_count * PLASTIC_BLOCKS_PER_SM, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+        else
+          k_plastic<true><<<ctx->sm_count * PLASTIC_BLOCKS_PER_SM, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      }
       break;
     default:
       return MF_ERR_INVALID;
@@ -278,7 +287,7 @@ field_desc describe(int f) {
       return {2, false};
     case MF_FIELD_S: case MF_FIELD_R: case MF_FIELD_S_T: case MF_FIELD_S_DER: case MF_FIELD_V_DER:
       return {4, false};
-    case MF_FIELD_IDX: case MF_FIELD_HASH:
+    case MF_FIELD_IDX: case MF_FIELD_HASH: case MF_FIELD_ID:
       return {1, true};
     default:
       return {1, false};
@@ -311,6 +320,7 @@ void *field_ptr(mf_ctx *ctx, int f) {
     case MF_FIELD_V_DER: return ctx->D.v_der;
     case MF_FIELD_IDX: return s.idx;
     case MF_FIELD_HASH: return ctx->D.hash_cur;
+    case MF_FIELD_ID: return s.id;
     default: return nullptr;
   }
 }
@@ -357,6 +367,8 @@ int mf_ctx_create(int device, mf_ctx **out) {
   }
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.g, 1);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.st, 1);
+  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.plastic_count, 1);
+  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.finish_chunk, 1);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->tool_buf[0], 1);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->tool_buf[1], 1);
   if (rc == MF_OK) {
@@ -438,6 +450,7 @@ int mf_particles_create(mf_ctx *ctx, int N, const double *pos, const double *vel
   }
   CK(cudaMemcpy(s.flags, fl.data(), sizeof(unsigned) * (size_t)N, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(s.idx, idx.data(), sizeof(int) * (size_t)N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s.id, idx.data(), sizeof(int) * (size_t)N, cudaMemcpyHostToDevice));
   ctx->has_particles = true;
   ctx->P.N = N;
   return MF_OK;
@@ -634,6 +647,7 @@ int mf_set_constants(mf_ctx *ctx, const mf_phys_constants *phys, const mf_corr_c
   P.plastic = joco ? 1 : 0;
   if (joco) P.joco = *joco;
   else std::memset(&P.joco, 0, sizeof(P.joco));
+  P.jc_lower_bound = joco && joco->A > 0. && joco->B >= 0. && joco->C >= 0. ? 1 : 0;
   std::memset(&P.trml_wp, 0, sizeof(P.trml_wp));
   std::memset(&P.trml_tool, 0, sizeof(P.trml_tool));
   if (trml_wp) P.trml_wp = *trml_wp;
@@ -804,6 +818,7 @@ int mf_status_get(mf_ctx *ctx, mf_status *out) {
   out->secant_cap_hits = (long long)st.secant_cap_hits;
   out->max_cell_occupancy = st.max_cell_occupancy;
   out->error_flags = st.error_flags;
+  out->secant_iterations = (long long)st.secant_iterations;
   return MF_OK;
 }
 

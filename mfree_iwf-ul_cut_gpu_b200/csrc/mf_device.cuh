@@ -42,6 +42,7 @@ struct params {
   int precision;
   int plastic, fric_heat, thermal_bc, thermal_wp, thermal_tool_on, has_tool, keep_derivs;
   int staged;  // step run stage by stage (mf_step_stage): keep every intermediate array
+  int jc_lower_bound;  // A > 0, B >= 0, C >= 0: the yield stress is bounded below by A (1 - theta^m)
   double dt;
   mf_phys_constants phys;
   mf_corr_constants corr;
@@ -68,6 +69,7 @@ struct dev_status {
   unsigned int force_ticket;
   unsigned int scan_tile_counter;
   unsigned long long force_log_head;
+  unsigned long long secant_iterations;
 };
 
 constexpr int FORCE_LOG_CAP = 1 << 16;
@@ -164,58 +166,76 @@ __device__ __forceinline__ void jaumann(double G, double vx_x, double vx_y, doub
 // Johnson-Cook flow stress (plasticity.cuh:30-46) and the tanh variant (:48-70). Kept out of
 // line: each call holds several pow/log expansions, and one copy keeps the instruction cache
 // and the caller's register budget small.
+// The yield stress (plasticity.cuh:30-46, 48-70). The factors that depend on the temperature
+// alone are computed once per particle (jc_temperature_terms) and passed in: the return map
+// evaluates the yield stress many times at one temperature. Every factor is the value the
+// reference computes, combined in the reference's order, so the result is the same double.
+struct jc_temp_terms {
+  double term_c;  // 1 - theta^m
+  double tanh_d;  // tanh model: 1 - (T/Tm)^d
+  double tanh_s;  // tanh model: (T/Tm)^b
+};
+
+__device__ __forceinline__ jc_temp_terms jc_temperature_terms(const mf_joco_constants &jc, int model, double t) {
+  jc_temp_terms r;
+  const double theta = (t - jc.Tref) / (jc.Tmelt - jc.Tref);
+  r.term_c = 1.0 - pow(theta, jc.m);
+  r.tanh_d = 0.;
+  r.tanh_s = 0.;
+  if (model == MF_JC_TANH) {
+    r.tanh_d = 1.0 - pow((t / jc.Tmelt), jc.tanh_d);
+    r.tanh_s = pow(t / jc.Tmelt, jc.tanh_b);
+  }
+  return r;
+}
+
 static __device__ __noinline__ double sigma_yield(const mf_joco_constants &jc, double eps_pl, double eps_pl_dot,
-                                              double t) {
-  double theta = (t - jc.Tref) / (jc.Tmelt - jc.Tref);
+                                              const jc_temp_terms &tt) {
   double Term_A = jc.A + jc.B * pow(eps_pl, jc.n);
   double Term_B = 1.0;
   double eps_dot = eps_pl_dot / jc.eps_dot_ref;
   if (eps_dot > 1.0) Term_B = 1.0 + jc.C * log(eps_dot);
   else Term_B = pow((1.0 + eps_dot), jc.C);
-  double Term_C = 1.0 - pow(theta, jc.m);
-  return Term_A * Term_B * Term_C;
+  return Term_A * Term_B * tt.term_c;
 }
 
 static __device__ __noinline__ double sigma_yield_tanh(const mf_joco_constants &jc, double eps_pl, double eps_dot_pl,
-                                                   double t) {
-  double theta = (t - jc.Tref) / (jc.Tmelt - jc.Tref);
+                                                   const jc_temp_terms &tt) {
   double Term_A = jc.A + jc.B * pow(eps_pl, jc.n) * 1.0 / exp(pow(eps_pl, jc.tanh_a));
   double Term_B = 1.0;
   double eps_dot = eps_dot_pl / jc.eps_dot_ref;
   if (eps_dot > 1.0) Term_B = 1.0 + jc.C * log(eps_dot);
   else Term_B = pow((1.0 + eps_dot), jc.C);
-  double Term_C = 1.0 - pow(theta, jc.m);
-  double tanh_D = 1.0 - pow((t / jc.Tmelt), jc.tanh_d);
-  double tanh_S = pow(t / jc.Tmelt, jc.tanh_b);
-  double Term_D = tanh_D + (1.0 - tanh_D) * tanh(1.0 / (pow(eps_pl + tanh_S, jc.tanh_c)));
-  return Term_A * Term_B * Term_C * Term_D;
+  double Term_D = tt.tanh_d + (1.0 - tt.tanh_d) * tanh(1.0 / (pow(eps_pl + tt.tanh_s, jc.tanh_c)));
+  return Term_A * Term_B * tt.term_c * Term_D;
 }
 
 // consistency function of the radial return (plasticity.cuh:74-83)
 __device__ __forceinline__ double opt_fun(const mf_joco_constants &jc, int model, double delta_lambda,
-                                          double norm_Strial, double eps_pl_init, double t, double delta_t,
-                                          double mu) {
+                                          double norm_Strial, double eps_pl_init, const jc_temp_terms &tt,
+                                          double delta_t, double mu) {
   const double s23 = sqrt(2.0 / 3.0);
   double eps_pl_equiv = eps_pl_init + s23 * fmax(delta_lambda, 0.);
   double eps_pl_equiv_dot = s23 * fmax(delta_lambda, 0.) / delta_t;
-  double sigmaY = model == MF_JC_TANH ? sigma_yield_tanh(jc, eps_pl_equiv, eps_pl_equiv_dot, t)
-                                      : sigma_yield(jc, eps_pl_equiv, eps_pl_equiv_dot, t);
+  double sigmaY = model == MF_JC_TANH ? sigma_yield_tanh(jc, eps_pl_equiv, eps_pl_equiv_dot, tt)
+                                      : sigma_yield(jc, eps_pl_equiv, eps_pl_equiv_dot, tt);
   return norm_Strial - 2 * mu * delta_lambda - s23 * sigmaY;
 }
 
 // secant iteration (plasticity.cuh:85-119): at most 102 evaluation pairs; capped -> flag
 static __device__ __noinline__ double solve_secant(const mf_joco_constants &jc, int model, double init, double tol,
-                                               double norm_Strial, double eps_pl_init, double t, double delta_t,
-                                               double mu, bool &capped) {
+                                               double norm_Strial, double eps_pl_init, const jc_temp_terms &tt,
+                                               double delta_t, double mu, bool &capped, int &iterations) {
   double delta_lambda = init;
   double delta_lambda_old = delta_lambda;
   int iter = 0;
   const int max_iter = 100;
   capped = false;
   while (true) {
-    double g = opt_fun(jc, model, delta_lambda, norm_Strial, eps_pl_init, t, delta_t, mu);
+    ++iterations;
+    double g = opt_fun(jc, model, delta_lambda, norm_Strial, eps_pl_init, tt, delta_t, mu);
     double delta_lambda_1 = delta_lambda * 1.01;
-    double g_1 = opt_fun(jc, model, delta_lambda_1, norm_Strial, eps_pl_init, t, delta_t, mu);
+    double g_1 = opt_fun(jc, model, delta_lambda_1, norm_Strial, eps_pl_init, tt, delta_t, mu);
     double slope = (g - g_1) / (delta_lambda - delta_lambda_1);
     delta_lambda_old = delta_lambda;
     delta_lambda = delta_lambda - g / slope;

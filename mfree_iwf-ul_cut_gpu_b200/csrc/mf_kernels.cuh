@@ -32,6 +32,16 @@ struct state_set {
   double4 *S, *S_t;
   unsigned *flags;
   int *idx;
+  int *id;  // particle number at creation, gathered by every sort
+};
+
+// a particle that failed the elastic test of the finish kernel, with the temperature its
+// return map starts from (after friction heat, before the thermal boundary condition)
+struct plastic_item {
+  double T;
+  double term_c;  // 1 - theta^m at T, as the elastic test computed it
+  int q;
+  int pad;
 };
 
 struct dev_buffers {
@@ -52,6 +62,9 @@ struct dev_buffers {
   unsigned *ticket;     // last-block tickets: [0] force, [1] bbox
   double *force_log;    // FORCE_LOG_CAP x 2
   double *force_last;   // 2
+  plastic_item *plastic_list;  // particles whose return map k_plastic runs (this step)
+  unsigned *plastic_count;
+  unsigned *finish_chunk;     // next chunk of the finish kernel (zeroed by the reorder)
   mf_tool_state *tool_prev;  // tool after the previous step (read)
   mf_tool_state *tool_next;  // tool after this step (written by k_finish)
   geom *g;
@@ -64,6 +77,8 @@ constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr int BLOCK = 256;
 // k_finish runs a grid-stride loop over a fixed grid of this many blocks per SM
 constexpr int FINISH_BLOCKS_PER_SM = 2;
+// k_plastic: fixed grid of this many 256-thread blocks per SM over the plastic list
+constexpr int PLASTIC_BLOCKS_PER_SM = 4;
 constexpr int PAIR_BLOCK = 128;
 constexpr unsigned long long SCAN_FLAG_AGG = 1ull << 62;
 constexpr unsigned long long SCAN_FLAG_PREFIX = 2ull << 62;
@@ -326,6 +341,10 @@ template <bool PREDICT, bool MIXED>
 static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers D) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
+  if (q == 0) {  // re-armed for the finish kernel of this step
+    *D.plastic_count = 0u;
+    *D.finish_chunk = 0u;
+  }
   const int4 u = D.perm_u[q];
   const int p = stable_member(D, q, u), hsh = u.y;
   if (q == u.z) D.count[hsh] = 0;  // the scatter's cursor, back to zero for the next counts
@@ -333,6 +352,7 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
   const state_set &B = D.B;
   D.perm[q] = p;
   B.idx[q] = P.grid_kind == MF_GRID_GREEN ? p : A.idx[p];
+  B.id[q] = A.id[p];
   D.hash_cur[q] = hsh;
 
   double2 pos = A.pos[p], vel = A.vel[p];
@@ -662,7 +682,7 @@ __device__ __forceinline__ void tool_advance_shared(mf_tool_state &T, const dev_
 __device__ __forceinline__ void finish_particle(const params &P, const dev_buffers &D, const mf_tool_state &TL,
                                                const mf_joco_constants &JC, int q,
                                                double2 &pos_out, unsigned &f_out, double2 &fc_out, double2 &ft_out,
-                                               unsigned &newly_blanked, unsigned &capped) {
+                                               unsigned &newly_blanked) {
   const state_set &A = D.A;
   const state_set &B = D.B;
   const double dt = P.dt;
@@ -709,34 +729,40 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
   }
   // JC plasticity, radial return (actions_gpu.cu:226-285)
   if (P.plastic && !tool) {
-    const double mu = P.phys.G;
     const double Sxx = S.x, Syy = S.z, Szz = S.w, Sxy = S.y;
-    const double norm_Strial = (double)sqrtf((float)(Sxx * Sxx + Syy * Syy + Szz * Szz + Sxy * Sxy));
     const double cxx = Sxx - pr, cyy = Syy - pr, czz = Szz - pr, cxy = Sxy;
     const double svm = (double)sqrtf(
         (float)((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy));
-    const double sigma_Y = sigma_yield(JC, eps_pl, eps_pl_dot, T);
-    if (svm < sigma_Y) {
+    // With A > 0 and B, C >= 0 the yield stress is at least A * (1 - theta^m): (A + B eps^n)
+    // >= A and the rate factor >= 1. A von Mises stress clearly below that bound is elastic
+    // without any FP64 pow: theta^m comes from powf, whose error (a few float ulps, plus the
+    // float rounding of theta and m) the factor 1.00001 covers, and the 0.1 % margin covers
+    // the rounding of the full yield stress. The decision is the reference's: when the bound
+    // does not settle it (or is NaN, as below Tref), the full test below runs.
+    bool elastic = false;
+    if (P.jc_lower_bound) {
+      const float theta_f = (float)((T - JC.Tref) / (JC.Tmelt - JC.Tref));
+      const double pow_hi = 1.00001 * (double)powf(theta_f, (float)JC.m);
+      elastic = svm < 0.999 * JC.A * (1.0 - pow_hi);
+    }
+    // one temperature for the whole return map: its temperature-only factors once
+    jc_temp_terms tt;
+    if (!elastic) {
+      tt = jc_temperature_terms(JC, P.jc_model, T);
+      elastic = svm < sigma_yield(JC, eps_pl, eps_pl_dot, tt);
+    }
+    if (elastic) {
       eps_pl_dot = 0.;
     } else {
-      bool cap = false;
-      const double delta_lambda = solve_secant(JC, P.jc_model, fmax(eps_pl_dot * dt * sqrt(2. / 3.), 1e-8),
-                                               1e-6, norm_Strial, eps_pl, T, dt, P.phys.G, cap);
-      capped += cap ? 1u : 0u;
-      const float s23f = sqrtf((float)(2.0 / 3.0));
-      const double eps_pl_new = eps_pl + (double)(s23f * fmaxf((float)delta_lambda, 0.f));
-      const double eps_pl_dot_new = (double)(s23f * fmaxf((float)delta_lambda, 0.f)) / dt;
-      S.x = Sxx - Sxx / norm_Strial * delta_lambda * 2. * mu;
-      S.z = Syy - Syy / norm_Strial * delta_lambda * 2. * mu;
-      S.w = Szz - Szz / norm_Strial * delta_lambda * 2. * mu;
-      S.y = Sxy - Sxy / norm_Strial * delta_lambda * 2. * mu;
-      if (P.trml_wp.tq != 0.) {
-        const double delta_eps_pl = eps_pl_new - eps_pl;
-        const double sY = sigma_yield(JC, eps_pl_new, eps_pl_dot_new, T);
-        T += P.trml_wp.tq / (P.trml_wp.cp * rho) * delta_eps_pl * sY;
-      }
-      eps_pl = eps_pl_new;
-      eps_pl_dot = eps_pl_dot_new;
+      // the return map runs in k_plastic over a compacted list with every lane busy; the
+      // trial stress, eps_pl, eps_pl_dot and rho written below are its inputs
+      const unsigned am = __activemask();
+      const int leader = __ffs(am) - 1;
+      unsigned base = 0u;
+      if ((int)lane_id() == leader) base = atomicAdd(D.plastic_count, (unsigned)__popc(am));
+      base = __shfl_sync(am, base, leader);
+      const unsigned rank = __popc(am & ((1u << lane_id()) - 1u));
+      D.plastic_list[base + rank] = plastic_item{T, tt.term_c, q, 0};
     }
   }
   // tool particles move with the tool (tool_gpu.cu:210-221); contact (:151-207)
@@ -816,10 +842,13 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
   ft_out = ft;
 }
 
-// Corrector .. invalidate for all particles plus the tool force (output.cu:31-39), on a
-// fixed grid of blocks that loops over the particles. With FUSE_HASH (locked grid) it also
-// computes the next step's cell hash and per-cell count from the final positions (the work
-// of k_hash_count) and re-arms the scan for the next step.
+// Corrector .. invalidate for all particles plus the tool force (output.cu:31-39). A fixed
+// grid of blocks takes chunks of BLOCK consecutive particles from an atomic counter, so the
+// blocks that meet the costly particles (yield tests, contact) do not set the kernel's length.
+// Each chunk's force sum goes to its own partial, and the last block to finish adds the
+// partials in chunk order: the result does not depend on which block took which chunk. With
+// FUSE_HASH (locked grid) the kernel also computes the next step's cell hash and per-cell
+// count from the final positions (the work of k_hash_count) and re-arms the scan.
 template <bool FUSE_HASH>
 __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P, dev_buffers D, int num_scan_tiles) {
   __shared__ mf_tool_state s_tool;
@@ -827,89 +856,102 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
   // reference, which for a kernel parameter would mean a copy on every thread's stack
   __shared__ mf_joco_constants s_jc;
   __shared__ ksum sm[BLOCK / 32][4];
-  __shared__ unsigned smc[BLOCK / 32][4];
+  __shared__ unsigned smc[BLOCK / 32][3];
+  __shared__ int s_chunk;
   __shared__ bool last;
   if (threadIdx.x == 0) s_jc = P.joco;
   if (P.has_tool) tool_advance_shared(s_tool, D, P.dt);  // (its first barrier also covers s_jc)
   else __syncthreads();
   const int stride = gridDim.x * blockDim.x;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  ksum fcx{0., 0.}, fcy{0., 0.}, ftx{0., 0.}, fty{0., 0.};
-  unsigned newly_blanked = 0, capped = 0, blanked_now = 0, oog = 0;
+  const int n_chunks = (P.N + BLOCK - 1) / BLOCK;
+  unsigned newly_blanked = 0, blanked_now = 0, oog = 0;
   geom g{};
   if (FUSE_HASH) {
     g = *D.g;
     for (int t = gid; t < num_scan_tiles; t += stride) D.scan_status[t] = 0ull;
   }
-  for (int q = gid; q < P.N; q += stride) {
-    double2 pos, fc, ft;
-    unsigned f;
-    finish_particle(P, D, s_tool, s_jc, q, pos, f, fc, ft, newly_blanked, capped);
-    blanked_now += (f & FLAG_BLANKED) ? 1u : 0u;
-    ksum_add(fcx, fc.x);
-    ksum_add(fcy, fc.y);
-    ksum_add(ftx, ft.x);
-    ksum_add(fty, ft.y);
-    if (FUSE_HASH) {  // compute_hashes of the next step (grid.cu:34-51)
-      long long hh;
-      if (f & FLAG_BLANKED) {
-        hh = D.hash_cur[q];
-      } else {
-        const int ix = __double2int_rz((pos.x - g.bbmin_x) / g.dx);
-        const int iy = __double2int_rz((pos.y - g.bbmin_y) / g.dx);
-        hh = (long long)ix * (long long)g.ny + (long long)iy;
+  while (true) {
+    if (threadIdx.x == 0) s_chunk = (int)atomicAdd(D.finish_chunk, 1u);
+    __syncthreads();
+    const int chunk = s_chunk;
+    if (chunk >= n_chunks) break;
+    const int q = chunk * BLOCK + threadIdx.x;
+    ksum fcx{0., 0.}, fcy{0., 0.}, ftx{0., 0.}, fty{0., 0.};
+    if (q < P.N) {
+      double2 pos, fc, ft;
+      unsigned f;
+      finish_particle(P, D, s_tool, s_jc, q, pos, f, fc, ft, newly_blanked);
+      blanked_now += (f & FLAG_BLANKED) ? 1u : 0u;
+      ksum_add(fcx, fc.x);
+      ksum_add(fcy, fc.y);
+      ksum_add(ftx, ft.x);
+      ksum_add(fty, ft.y);
+      if (FUSE_HASH) {  // compute_hashes of the next step (grid.cu:34-51)
+        long long hh;
+        if (f & FLAG_BLANKED) {
+          hh = D.hash_cur[q];
+        } else {
+          const int ix = __double2int_rz((pos.x - g.bbmin_x) / g.dx);
+          const int iy = __double2int_rz((pos.y - g.bbmin_y) / g.dx);
+          hh = (long long)ix * (long long)g.ny + (long long)iy;
+        }
+        if (hh < 0) { hh = 0; ++oog; }
+        else if (hh >= g.num_cell) { hh = g.num_cell - 1; ++oog; }
+        const int hsh = (int)hh;
+        D.hash_new[q] = hsh;
+        atomicAdd(&D.count[hsh], 1);
       }
-      if (hh < 0) { hh = 0; ++oog; }
-      else if (hh >= g.num_cell) { hh = g.num_cell - 1; ++oog; }
-      const int hsh = (int)hh;
-      D.hash_new[q] = hsh;
-      atomicAdd(&D.count[hsh], 1);
     }
+    // the chunk's force sums (compensated), in a fixed tree: warps, then warps in order
+    for (int o = 16; o > 0; o >>= 1) {
+      ksum a{__shfl_down_sync(0xffffffffu, fcx.s, o), __shfl_down_sync(0xffffffffu, fcx.c, o)};
+      ksum b{__shfl_down_sync(0xffffffffu, fcy.s, o), __shfl_down_sync(0xffffffffu, fcy.c, o)};
+      ksum c{__shfl_down_sync(0xffffffffu, ftx.s, o), __shfl_down_sync(0xffffffffu, ftx.c, o)};
+      ksum d{__shfl_down_sync(0xffffffffu, fty.s, o), __shfl_down_sync(0xffffffffu, fty.c, o)};
+      ksum_merge(fcx, a); ksum_merge(fcy, b); ksum_merge(ftx, c); ksum_merge(fty, d);
+    }
+    if (lane_id() == 0) {
+      sm[threadIdx.x >> 5][0] = fcx; sm[threadIdx.x >> 5][1] = fcy;
+      sm[threadIdx.x >> 5][2] = ftx; sm[threadIdx.x >> 5][3] = fty;
+    }
+    __syncthreads();  // sm complete; every thread has read s_chunk
+    if (threadIdx.x == 0) {
+      ksum r[4] = {sm[0][0], sm[0][1], sm[0][2], sm[0][3]};
+      for (int w = 1; w < BLOCK / 32; ++w)
+        for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
+      for (int k = 0; k < 4; ++k) {
+        D.partials[(size_t)chunk * 8 + 2 * k] = r[k].s;
+        D.partials[(size_t)chunk * 8 + 2 * k + 1] = r[k].c;
+      }
+    }
+    __syncthreads();  // sm and s_chunk are reused by the next chunk
   }
-  // block reduction of the force (compensated) and of the counters
-  for (int o = 16; o > 0; o >>= 1) {
-    ksum a{__shfl_down_sync(0xffffffffu, fcx.s, o), __shfl_down_sync(0xffffffffu, fcx.c, o)};
-    ksum b{__shfl_down_sync(0xffffffffu, fcy.s, o), __shfl_down_sync(0xffffffffu, fcy.c, o)};
-    ksum c{__shfl_down_sync(0xffffffffu, ftx.s, o), __shfl_down_sync(0xffffffffu, ftx.c, o)};
-    ksum d{__shfl_down_sync(0xffffffffu, fty.s, o), __shfl_down_sync(0xffffffffu, fty.c, o)};
-    ksum_merge(fcx, a); ksum_merge(fcy, b); ksum_merge(ftx, c); ksum_merge(fty, d);
-  }
+  // the block's counters
   const unsigned nb = __reduce_add_sync(0xffffffffu, newly_blanked);
-  const unsigned nc = __reduce_add_sync(0xffffffffu, capped);
   const unsigned nbl = __reduce_add_sync(0xffffffffu, blanked_now);
   const unsigned noog = __reduce_add_sync(0xffffffffu, oog);
   if (lane_id() == 0) {
-    sm[threadIdx.x >> 5][0] = fcx; sm[threadIdx.x >> 5][1] = fcy;
-    sm[threadIdx.x >> 5][2] = ftx; sm[threadIdx.x >> 5][3] = fty;
-    smc[threadIdx.x >> 5][0] = nb; smc[threadIdx.x >> 5][1] = nc; smc[threadIdx.x >> 5][2] = nbl;
-    smc[threadIdx.x >> 5][3] = noog;
+    smc[threadIdx.x >> 5][0] = nb; smc[threadIdx.x >> 5][1] = nbl; smc[threadIdx.x >> 5][2] = noog;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    ksum r[4] = {sm[0][0], sm[0][1], sm[0][2], sm[0][3]};
-    unsigned cnt[4] = {smc[0][0], smc[0][1], smc[0][2], smc[0][3]};
-    for (int w = 1; w < BLOCK / 32; ++w) {
-      for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
-      for (int k = 0; k < 4; ++k) cnt[k] += smc[w][k];
-    }
-    for (int k = 0; k < 4; ++k) {
-      D.partials[blockIdx.x * 8 + 2 * k] = r[k].s;
-      D.partials[blockIdx.x * 8 + 2 * k + 1] = r[k].c;
-    }
-    if (cnt[0]) atomicAdd(&D.st->newly_blanked, (unsigned long long)cnt[0]);
-    if (cnt[1]) atomicAdd(&D.st->secant_cap_hits, (unsigned long long)cnt[1]);
-    if (cnt[2]) atomicAdd(&D.st->blanked, (unsigned long long)cnt[2]);
-    if (cnt[3]) atomicAdd(&D.st->out_of_grid, (unsigned long long)cnt[3]);
+    unsigned long long cnt[3] = {smc[0][0], smc[0][1], smc[0][2]};
+    for (int w = 1; w < BLOCK / 32; ++w)
+      for (int k = 0; k < 3; ++k) cnt[k] += smc[w][k];
+    if (cnt[0]) atomicAdd(&D.st->newly_blanked, cnt[0]);
+    if (cnt[1]) atomicAdd(&D.st->blanked, cnt[1]);
+    if (cnt[2]) atomicAdd(&D.st->out_of_grid, cnt[2]);
     __threadfence();
     const unsigned t = atomicAdd(&D.ticket[0], 1u);
     last = (t == gridDim.x - 1);
   }
   __syncthreads();
   if (!last) return;
-  // last block: fixed-order reduction of all block partials
+  // last block: fixed-order reduction of all chunk partials
   __threadfence();
   ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
-  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+  for (int b = threadIdx.x; b < n_chunks; b += blockDim.x) {
     const volatile double *pr = D.partials + (size_t)b * 8;
     for (int k = 0; k < 4; ++k) {
       ksum x{pr[2 * k], pr[2 * k + 1]};
@@ -939,6 +981,150 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
     D.st->force_log_head = hd + 1;
     D.st->steps += 1;
     D.ticket[0] = 0u;
+  }
+}
+
+// JC radial return (actions_gpu.cu:226-285) for the particles the finish kernel listed: the
+// secant solve (plasticity.cuh:85-119), the stress scaled back to the yield surface, the
+// plastic work to heat, then the thermal boundary condition the finish kernel applied before
+// the return map had run (actions_gpu.cu:300-311).
+//
+// The list is short and its time is set by the particles whose secant needs the most
+// iterations, so the length of one iteration matters. With the Johnson-Cook law (PAIRED) two
+// lanes share one particle: a secant iteration needs the yield stress at delta_lambda (lane 0)
+// and at 1.01 delta_lambda (lane 1), each pow(eps, n) times a rate factor (log or pow); both
+// lanes run the same calls on their own operands at once, and shuffles exchange the results.
+// Both lanes then evaluate the reference's expressions on the same operands, so the iterates
+// are those of the one-lane solve. The tanh law takes the one-lane path.
+struct secant_in {
+  double norm_Strial, eps_pl, eps_pl_dot, term_c;
+};
+
+// yield stress from its two transcendental factors (sigma_yield's own expression order)
+__device__ __forceinline__ double jc_yield_from(const mf_joco_constants &jc, double pow_eps_n, double term_b,
+                                                double term_c) {
+  double Term_A = jc.A + jc.B * pow_eps_n;
+  return Term_A * term_b * term_c;
+}
+
+// the rate factor of sigma_yield (plasticity.cuh:35-39)
+__device__ __forceinline__ double jc_rate_factor(const mf_joco_constants &jc, double eps_pl_dot) {
+  double eps_dot = eps_pl_dot / jc.eps_dot_ref;
+  if (eps_dot > 1.0) return 1.0 + jc.C * log(eps_dot);
+  return pow((1.0 + eps_dot), jc.C);
+}
+
+// one lane pair's secant solve; sub = lane within the pair, pmask = the pair's lanes
+__device__ __forceinline__ double solve_secant_pair(const mf_joco_constants &jc, const secant_in &in, double dt,
+                                                    double mu, int sub, unsigned pmask, bool &capped,
+                                                    int &iterations) {
+  const double tol = 1e-6;
+  const double s23 = sqrt(2.0 / 3.0);
+  double delta_lambda = fmax(in.eps_pl_dot * dt * sqrt(2. / 3.), 1e-8);
+  double delta_lambda_old = delta_lambda;
+  int iter = 0;
+  const int max_iter = 100;
+  capped = false;
+  while (true) {
+    ++iterations;
+    const double delta_lambda_1 = delta_lambda * 1.01;
+    // opt_fun (plasticity.cuh:74-83) at delta_lambda on lane 0, at delta_lambda_1 on lane 1
+    const double dl = sub == 0 ? delta_lambda : delta_lambda_1;
+    const double e = in.eps_pl + s23 * fmax(dl, 0.);
+    const double ed = s23 * fmax(dl, 0.) / dt;
+    const double sY = jc_yield_from(jc, pow(e, jc.n), jc_rate_factor(jc, ed), in.term_c);
+    const double g_own = in.norm_Strial - 2 * mu * dl - s23 * sY;
+    const double g = __shfl_sync(pmask, g_own, 0, 2);
+    const double g_1 = __shfl_sync(pmask, g_own, 1, 2);
+    const double slope = (g - g_1) / (delta_lambda - delta_lambda_1);
+    delta_lambda_old = delta_lambda;
+    delta_lambda = delta_lambda - g / slope;
+    if (delta_lambda < 0.) delta_lambda = -0.1 * delta_lambda;
+    if (fabs(delta_lambda - delta_lambda_old) < tol) return delta_lambda;
+    if (iter > max_iter) { capped = true; return delta_lambda; }
+    iter++;
+  }
+}
+
+template <bool PAIRED>
+static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic(params P, dev_buffers D) {
+  __shared__ mf_joco_constants s_jc;  // by reference into the out-of-line functions
+  __shared__ unsigned long long s_cnt[BLOCK / 32][2];
+  if (threadIdx.x == 0) s_jc = P.joco;
+  __syncthreads();
+  const mf_joco_constants &JC = s_jc;
+  const unsigned n = *D.plastic_count;
+  const state_set &B = D.B;
+  const double dt = P.dt, mu = P.phys.G;
+  constexpr unsigned LANES = PAIRED ? 2u : 1u;
+  const unsigned sub = PAIRED ? (lane_id() & 1u) : 0u;
+  const unsigned pmask = PAIRED ? (0x3u << (lane_id() & ~1u)) : 0xffffffffu;
+  unsigned capped = 0u, iters_sum = 0u;
+  const unsigned stride = gridDim.x * blockDim.x / LANES;
+  for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) / LANES; i < n; i += stride) {
+    const plastic_item it = D.plastic_list[i];
+    const int q = it.q;
+    double T = it.T;
+    const double4 S = B.S[q];
+    const double eps_pl = B.eps_pl[q], eps_pl_dot = B.eps_pl_dot[q], rho = B.rho[q];
+    const unsigned f = B.flags[q];
+    const double Sxx = S.x, Syy = S.z, Szz = S.w, Sxy = S.y;
+    const double norm_Strial = (double)sqrtf((float)(Sxx * Sxx + Syy * Syy + Szz * Szz + Sxy * Sxy));
+    bool cap = false;
+    int iters = 0;
+    double delta_lambda;
+    jc_temp_terms tt;
+    if (PAIRED) {
+      const secant_in in{norm_Strial, eps_pl, eps_pl_dot, it.term_c};
+      delta_lambda = solve_secant_pair(JC, in, dt, mu, (int)sub, pmask, cap, iters);
+    } else {
+      tt = jc_temperature_terms(JC, P.jc_model, T);
+      delta_lambda = solve_secant(JC, P.jc_model, fmax(eps_pl_dot * dt * sqrt(2. / 3.), 1e-8), 1e-6, norm_Strial,
+                                  eps_pl, tt, dt, mu, cap, iters);
+    }
+    const float s23f = sqrtf((float)(2.0 / 3.0));
+    const double eps_pl_new = eps_pl + (double)(s23f * fmaxf((float)delta_lambda, 0.f));
+    const double eps_pl_dot_new = (double)(s23f * fmaxf((float)delta_lambda, 0.f)) / dt;
+    if (P.trml_wp.tq != 0.) {
+      double sY;
+      if (PAIRED) {  // sigma_yield(eps_pl_new, eps_pl_dot_new), on both lanes
+        sY = jc_yield_from(JC, pow(eps_pl_new, JC.n), jc_rate_factor(JC, eps_pl_dot_new), it.term_c);
+      } else {
+        sY = sigma_yield(JC, eps_pl_new, eps_pl_dot_new, tt);
+      }
+      const double delta_eps_pl = eps_pl_new - eps_pl;
+      T += P.trml_wp.tq / (P.trml_wp.cp * rho) * delta_eps_pl * sY;
+    }
+    if (P.thermal_bc && (f & FLAG_FIXED)) T = P.trml_wp.T_init;
+    if (sub == 0) {
+      double4 Sn;
+      Sn.x = Sxx - Sxx / norm_Strial * delta_lambda * 2. * mu;
+      Sn.z = Syy - Syy / norm_Strial * delta_lambda * 2. * mu;
+      Sn.w = Szz - Szz / norm_Strial * delta_lambda * 2. * mu;
+      Sn.y = Sxy - Sxy / norm_Strial * delta_lambda * 2. * mu;
+      B.S[q] = Sn;
+      B.eps_pl[q] = eps_pl_new;
+      B.eps_pl_dot[q] = eps_pl_dot_new;
+      B.T[q] = T;
+      capped += cap ? 1u : 0u;
+      iters_sum += (unsigned)iters;
+    }
+  }
+  const unsigned nc = __reduce_add_sync(0xffffffffu, capped);
+  const unsigned ni = __reduce_add_sync(0xffffffffu, iters_sum);
+  if (lane_id() == 0) {
+    s_cnt[threadIdx.x >> 5][0] = nc;
+    s_cnt[threadIdx.x >> 5][1] = ni;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long c = 0, itn = 0;
+    for (int w = 0; w < BLOCK / 32; ++w) {
+      c += s_cnt[w][0];
+      itn += s_cnt[w][1];
+    }
+    if (c) atomicAdd(&D.st->secant_cap_hits, c);
+    if (itn) atomicAdd(&D.st->secant_iterations, itn);
   }
 }
 

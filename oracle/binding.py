@@ -98,6 +98,7 @@ def lib():
         for f in ("orc_stage_predict", "orc_stage_interact", "orc_stage_rates", "orc_stage_finish"):
             getattr(L, f).argtypes = [C.c_void_p]
         L.orc_steps.argtypes = [C.c_void_p, C.c_int]
+        L.orc_steps_force_log.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.orc_report_force.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_out_of_grid.restype = C.c_longlong
         L.orc_out_of_grid.argtypes = [C.c_void_p]
@@ -202,6 +203,13 @@ class Oracle:
     def report_force(self):
         out = np.zeros(2)
         self.L.orc_report_force(self.s, _ptr(out))
+        return out
+
+    def steps_force_log(self, n: int):
+        """n steps; the (Fc, Ff) of report_force after each one, shape (n, 2)."""
+        out = np.zeros((n, 2))
+        if self.L.orc_steps_force_log(self.s, n, _ptr(out)) != 0:
+            raise RuntimeError("oracle step failed")
         return out
 
     def get_tool(self) -> OrcTool:

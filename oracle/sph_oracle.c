@@ -1234,3 +1234,12 @@ int orc_steps(orc_state *s, int n) {
     if (orc_step(s) != 0) return -1;
   return 0;
 }
+
+/* n steps, with report_force (output.cu:31-39) after each one into out[2k], out[2k+1] */
+int orc_steps_force_log(orc_state *s, int n, double *out) {
+  for (int k = 0; k < n; ++k) {
+    if (orc_step(s) != 0) return -1;
+    orc_report_force(s, out + 2 * k);
+  }
+  return 0;
+}

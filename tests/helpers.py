@@ -124,3 +124,27 @@ def load_oracle(orc, st, grid_kind=0, thermal_solver=0, jc_model=0):
 
 def product_tool_array(mf, t):
     return mf.tool_to_array(t)
+
+
+def scene_state(mf, sc):
+    """The state dict of an unperturbed scene (everything that is not set up starts at zero)."""
+    s = sc.s
+    N = sc.N
+    st = {"N": N}
+    for k in ("pos", "rho", "T", "h", "fixed", "tool_p"):
+        st[k] = sc.array(k).copy()
+    st["vel"] = np.zeros((N, 2))
+    for k in ("eps_pl", "eps_pl_dot", "rho_t", "T_t", "blanked"):
+        st[k] = np.zeros(N)
+    for k in ("fc", "ft", "n", "pos_t", "vel_t"):
+        st[k] = np.zeros((N, 2))
+    for k in ("S", "S_t"):
+        st[k] = np.zeros((N, 4))
+    st["phys"], st["corr"], st["joco"] = s.phys, s.corr, s.joco
+    st["trml_wp"], st["trml_tool"], st["dt"] = s.trml_wp, s.trml_tool, s.dt
+    st["grid"] = (tuple(s.grid_bbmin), tuple(s.grid_bbmax), s.grid_h)
+    tool = mf.ToolState()
+    C.memmove(C.byref(tool), C.byref(s.tool), C.sizeof(mf.ToolState))
+    st["tool"] = tool
+    st["scene"] = sc
+    return st

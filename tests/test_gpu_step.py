@@ -109,6 +109,11 @@ def test_full_steps_compressive(mf, orc, grid_kind):
         check(ctx, o, STATE + RATES, tol)
         assert np.array_equal(ctx.get("blanked"), o.get("blanked"))
     assert tool_bits(mf, orc, ctx, o)
+    # the persistent particle number: a permutation, equal to the Rothlin grid's own id
+    pid = ctx.get("id")
+    assert np.array_equal(np.sort(pid), np.arange(st["N"]))
+    if grid_kind == 1:
+        assert np.array_equal(pid, ctx.get("idx"))
     # per-particle forces matched above; the net force cancels, so check the reduction
     # itself: the compensated device sum against the exact sum of the device's own forces
     f1 = ctx.report_force()
@@ -157,11 +162,14 @@ def test_blanked_particles_and_nan_cascade(mf, orc):
     check(ctx, o, ("pos", "vel", "rho"), 1e-9, mask=nb)
 
 
-def test_tanh_yield_model(mf, orc):
+@pytest.mark.parametrize("jc_model", [0, 1])
+def test_return_map_over_the_yield_surface(mf, orc, jc_model):
+    """Many particles over the yield surface, Johnson-Cook (the four-lane solve) and the tanh
+    law (the one-lane solve): one finish stage against the oracle."""
     st = perturbed_scene(mf, ny=10, seed=16, tensile=True)
     st["S"] *= 3.0  # push particles over the yield surface
-    ctx = load_product(mf, st, jc_model=1)
-    o = load_oracle(orc, st, jc_model=1)
+    ctx = load_product(mf, st, jc_model=jc_model)
+    o = load_oracle(orc, st, jc_model=jc_model)
     ctx.stage(0)
     ctx.stage(1)
     o.L.orc_grid_update(o.s)
