@@ -160,12 +160,15 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def time_form(mf, torch, scene, precision, steps, warmup, device):
+def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None):
     """Per-step CUDA-event times (ms) of mf_step(1) with the L2 flushed between steps, plus the
-    pair kernel's own duration (mf_step_stage(2) bracketed by events)."""
+    pair kernel's own duration (mf_step_stage(2) bracketed by events). With state_in the steps
+    start from a saved state of the same scene instead of its initial state."""
     ctx = mf.Context(device)
     ctx.upload_scene(scene, mf.GRID_GREEN)
     ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
+    if state_in:
+        load_state(mf, ctx, state_in)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=device)
     ctx.step(warmup)
@@ -240,7 +243,35 @@ def e2e_form(mf, torch, scene, precision, steps, device):
     return (t1 - t0), h2d, d2h, finite
 
 
-def run_form(mf, scene, precision, steps, device, torch=None):
+STATE_FIELDS = ("pos", "vel", "h", "rho", "T", "S", "fc", "ft", "n", "fixed", "blanked", "tool_p", "eps_pl",
+                "eps_pl_dot", "pos_t", "vel_t", "rho_t", "S_t", "T_t", "id")
+
+
+def save_state(mf, ctx, path, steps):
+    """The whole particle state (array order of the last sort) and the tool, to an .npz."""
+    import ctypes as C
+
+    d = {k: ctx.get(k) for k in STATE_FIELDS}
+    t = ctx.tool_get()
+    d["tool_bytes"] = np.frombuffer(C.string_at(C.byref(t), C.sizeof(t)), dtype=np.uint8).copy()
+    d["steps"] = np.array([steps])
+    np.savez(path, **d)
+
+
+def load_state(mf, ctx, path):
+    """Overwrite a context's particle state and tool with a saved one (same scene)."""
+    import ctypes as C
+
+    d = np.load(path)
+    for k in STATE_FIELDS:
+        ctx.set(k, d[k])
+    t = mf.ToolState()
+    C.memmove(C.byref(t), d["tool_bytes"].tobytes(), C.sizeof(t))
+    ctx.tool_set(t)
+    return int(d["steps"][0])
+
+
+def run_form(mf, scene, precision, steps, device, torch=None, state_out=None):
     """`steps` steps of one form from the scene's initial state. Returns the per-step tool
     force (steps x 2), the end state ordered by particle number, and the device time (s)."""
     ctx = mf.Context(device)
@@ -265,6 +296,8 @@ def run_form(mf, scene, precision, steps, device, torch=None):
     order = np.argsort(ctx.get("id"))
     state = {k: ctx.get(k)[order] for k in ("S", "p", "eps_pl", "T", "tool_p", "blanked")}
     status = ctx.status()
+    if state_out:
+        save_state(mf, ctx, state_out, steps)
     ctx.close()
     return np.concatenate(forces), state, secs, status
 
@@ -314,10 +347,11 @@ def accuracy(mf, scene, params, steps, device):
     return out
 
 
-def cut_run(mf, torch, scene, params, mm, device):
-    """`mm` millimetres of cut in each form: device wall time per mm and the mixed form's errors."""
+def cut_run(mf, torch, scene, params, mm, device, state_out=None):
+    """`mm` millimetres of cut in each form: device wall time per mm and the mixed form's errors
+    (and, with state_out, the FP64 form's end state saved for --state-in)."""
     steps = int(round(mm * steps_per_mm(scene, params)))
-    f64, s64, t64, st64 = run_form(mf, scene, mf.PRECISION_FP64, steps, device, torch)
+    f64, s64, t64, st64 = run_form(mf, scene, mf.PRECISION_FP64, steps, device, torch, state_out=state_out)
     fm, sm, tm, stm = run_form(mf, scene, mf.PRECISION_MIXED, steps, device, torch)
     out = {"mode": "cut", "mm": mm, "steps": steps, "n_particles": scene.N,
            "wall_s_per_mm": {"fp64": t64 / mm, "mixed": tm / mm},
@@ -449,6 +483,11 @@ def main():
     ap.add_argument("--cut-mm", type=float, default=0.0,
                     help="instead of the benchmark: run this many mm of cut in both forms and report "
                          "wall time per mm and the mixed form's errors")
+    ap.add_argument("--state-out", default=None,
+                    help="with --cut-mm: save the FP64 form's end state (.npz) for --state-in")
+    ap.add_argument("--state-in", default=None,
+                    help="time both forms from this saved state of the same scene (e.g. mid-cut) "
+                         "instead of the initial state")
     ap.add_argument("--lattice-scale", type=float, default=1.0,
                     help="lattice points per dimension relative to 714 x 214 (same 2.0 x 0.6 mm body); "
                          "values below 1 give the smaller profiling case")
@@ -476,7 +515,7 @@ def main():
     N = scene.N
     if args.cut_mm > 0:
         if rank == 0:
-            print(json.dumps(cut_run(mf, torch, scene, params, args.cut_mm, device)), flush=True)
+            print(json.dumps(cut_run(mf, torch, scene, params, args.cut_mm, device, args.state_out)), flush=True)
         if world > 1:
             torch.distributed.barrier()
             torch.distributed.destroy_process_group()
@@ -489,7 +528,8 @@ def main():
             torch.distributed.barrier()
         torch.cuda.synchronize(device)
         with ClockSampler(device) as cs:
-            step_ms, pair_ms, st = time_form(mf, torch, scene, prec, args.steps, args.warmup, device)
+            step_ms, pair_ms, st = time_form(mf, torch, scene, prec, args.steps, args.warmup, device,
+                                             args.state_in)
         if name == "mixed":
             clocks = cs.summary()
         total_ms = max_over_ranks(float(step_ms.sum()), world, device=f"cuda:{device}")
@@ -537,6 +577,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed",
             "data": "synthetic",
             "config": dict(WORKLOAD, n_particles=N, n_workpiece=scene.s.n_workpiece, n_tool=scene.s.n_tool,
+                           start_state=(f"saved state {args.state_in}" if args.state_in else "initial scene"),
                            parallelism=f"replicas x{world}", l2="flushed between timed steps (256 MiB write)",
                            global_particles=N * world),
             "forms": {"fp64": {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
