@@ -155,6 +155,9 @@ int mf_grid_get_cells(mf_ctx *ctx, int *start, int *end);
 int mf_set_constants(mf_ctx *ctx, const mf_phys_constants *phys, const mf_corr_constants *corr,
                      const mf_joco_constants *joco, const mf_trml_constants *trml_wp,
                      const mf_trml_constants *trml_tool);
+/* the constants last set (has_joco: 0 when the material is not plastic) */
+int mf_get_constants(const mf_ctx *ctx, mf_phys_constants *phys, mf_corr_constants *corr, mf_joco_constants *joco,
+                     mf_trml_constants *trml_wp, mf_trml_constants *trml_tool, int *has_joco);
 int mf_set_options(mf_ctx *ctx, int thermal_solver, int jc_model, int precision);
 int mf_set_dt(mf_ctx *ctx, double dt); /* global_dt (benchmarks.cpp:20) */
 
@@ -254,6 +257,16 @@ int mf_tool_translate(mf_tool_state *tool, double dt); /* tool::update_tool with
 /* ---- output: vtk_writer_write (vtk_writer.cpp:20-178, 185-264), legacy ASCII ---- */
 int mf_vtk_write_particles(mf_ctx *ctx, const char *path);
 int mf_vtk_write_tool(const mf_tool_state *tool, const char *path);
+
+/* ---- differentiable form (no counterpart in the reference): from the context's current
+   state, runs skip_steps + window_steps FP64 steps on dual numbers and returns the mean over
+   the window of the tool force (report_force, output.cu:31-39: [0] cutting Fc, [1] feed Ff)
+   and, for param 0..5 = Johnson-Cook A, B, n, C, m or the friction coefficient mu, its
+   derivative with respect to that parameter (forward-mode tangents through every step; param
+   -1: the mean only). The context's state is not changed. Locked Green grid, Brookshaw or no
+   conduction, Johnson-Cook law only (MF_ERR_INVALID otherwise). ---- */
+int mf_tangent_mean_force(mf_ctx *ctx, int skip_steps, int window_steps, int param, double out_mean[2],
+                          double out_dmean[2]);
 
 /* ---- measurement aid (no counterpart in the reference): FP64 FMA throughput of the device
    (TFLOP/s, 2 flops per FMA) and the latency in SM clock cycles of one dependent double

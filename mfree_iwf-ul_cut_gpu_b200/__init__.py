@@ -137,6 +137,9 @@ def lib():
         "mf_tool_set": ([vp, C.POINTER(ToolState)], i), "mf_tool_get": ([vp, C.POINTER(ToolState)], i),
         "mf_step": ([vp, i], i), "mf_step_stage": ([vp, i], i), "mf_report_force": ([vp, vp], i),
         "mf_probe_fp64": ([i, vp, vp, vp, vp, vp], i),
+        "mf_tangent_mean_force": ([vp, i, i, i, vp, vp], i),
+        "mf_get_constants": ([vp, C.POINTER(Phys), C.POINTER(Corr), C.POINTER(Joco), C.POINTER(Trml),
+                              C.POINTER(Trml), ip], i),
         "mf_force_log": ([vp, vp, i, ip], i), "mf_force_last_async": ([vp, vp], i), "mf_status_get": ([vp, C.POINTER(Status)], i),
         "mf_cut_params_reference": ([C.POINTER(CutParams), i, d, d, d, d, d], i),
         "mf_scene_cut": ([C.POINTER(CutParams), C.POINTER(C.POINTER(SceneStruct))], i),
@@ -302,6 +305,23 @@ class Context:
         ref = lambda s: C.byref(s) if s is not None else None  # noqa: E731
         self._check(self.L.mf_set_constants(self.h, C.byref(phys), C.byref(corr), ref(joco), ref(trml_wp),
                                             ref(trml_tool)), "mf_set_constants")
+
+    def get_constants(self):
+        """(phys, corr, joco or None, trml_wp, trml_tool) as last set."""
+        phys, corr, joco, tw, tt, hj = Phys(), Corr(), Joco(), Trml(), Trml(), C.c_int()
+        self._check(self.L.mf_get_constants(self.h, C.byref(phys), C.byref(corr), C.byref(joco), C.byref(tw),
+                                            C.byref(tt), C.byref(hj)), "mf_get_constants")
+        return phys, corr, (joco if hj.value else None), tw, tt
+
+    def tangent_mean_force(self, skip_steps, window_steps, param=-1):
+        """Mean (Fc, Ff) over `window_steps` steps after `skip_steps`, from the current state, and
+        its derivative with respect to parameter `param` (0..5: JC A, B, n, C, m, friction mu;
+        -1: none). The state of the context is not changed (mf_tangent_mean_force)."""
+        mean = np.zeros(2)
+        dmean = np.zeros(2)
+        self._check(self.L.mf_tangent_mean_force(self.h, int(skip_steps), int(window_steps), int(param), _ptr(mean),
+                                                 _ptr(dmean)), "mf_tangent_mean_force")
+        return mean, dmean
 
     def set_options(self, thermal_solver=THERMAL_BROOKSHAW, jc_model=JC_JOHNSON_COOK, precision=PRECISION_FP64):
         self._check(self.L.mf_set_options(self.h, thermal_solver, jc_model, precision), "mf_set_options")

@@ -15,6 +15,14 @@
 
 using namespace mf;
 
+namespace mf {
+namespace tg {
+// the differentiable step (csrc/mf_tangent.cu)
+int run_mean_force(mf_ctx *ctx, int device, params P, const dev_buffers &Dctx, int skip_steps, int window_steps,
+                   int param, double out_mean[2], double out_dmean[2]);
+}  // namespace tg
+}  // namespace mf
+
 struct mf_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -661,6 +669,20 @@ int mf_set_constants(mf_ctx *ctx, const mf_phys_constants *phys, const mf_corr_c
   return MF_OK;
 }
 
+int mf_get_constants(const mf_ctx *ctx, mf_phys_constants *phys, mf_corr_constants *corr, mf_joco_constants *joco,
+                     mf_trml_constants *trml_wp, mf_trml_constants *trml_tool, int *has_joco) {
+  if (!ctx) return MF_ERR_INVALID;
+  if (!ctx->has_constants) return MF_ERR_STATE;
+  const params &P = ctx->P;
+  if (phys) *phys = P.phys;
+  if (corr) *corr = P.corr;
+  if (joco) *joco = P.joco;
+  if (trml_wp) *trml_wp = P.trml_wp;
+  if (trml_tool) *trml_tool = P.trml_tool;
+  if (has_joco) *has_joco = P.plastic;
+  return MF_OK;
+}
+
 int mf_set_options(mf_ctx *ctx, int thermal_solver, int jc_model, int precision) {
   if (!ctx) return MF_ERR_INVALID;
   if (thermal_solver != MF_THERMAL_BROOKSHAW && thermal_solver != MF_THERMAL_PSE) return MF_ERR_INVALID;
@@ -887,3 +909,21 @@ int mf_vtk_write_particles(mf_ctx *ctx, const char *path) {
 }
 
 }  // extern "C"
+
+int mf_tangent_mean_force(mf_ctx *ctx, int skip_steps, int window_steps, int param, double out_mean[2],
+                          double out_dmean[2]) {
+  if (!ctx || !out_mean || skip_steps < 0 || window_steps < 1 || param < -1 || param > 5) return MF_ERR_INVALID;
+  if (!ready(ctx) || ctx->mid_step) return MF_ERR_STATE;
+  if (!(ctx->P.dt > 0.)) return MF_ERR_STATE;
+  // the differentiable step covers the locked Green grid, Brookshaw or no conduction, and
+  // the Johnson-Cook law
+  if (!ctx->G.locked || ctx->grid_kind != MF_GRID_GREEN || ctx->P.thermal_solver == MF_THERMAL_PSE ||
+      ctx->P.jc_model != MF_JC_JOHNSON_COOK || !ctx->P.plastic)
+    return MF_ERR_INVALID;
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  params P = ctx->P;
+  P.N = ctx->N;
+  P.staged = 0;
+  return mf::tg::run_mean_force(ctx, ctx->device, P, ctx->D, skip_steps, window_steps, param, out_mean, out_dmean);
+}
