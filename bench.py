@@ -364,6 +364,88 @@ def cut_run(mf, torch, scene, params, mm, device, state_out=None):
     return out
 
 
+def sweep_params(mf, n_instances, seed=4):
+    """The batched sweep: instances of the cut with N ~ U[3k, 40k] workpiece particles (dx
+    scaled on the same 2.0 x 0.6 mm body), speed ~ U[30, 200] m/min, rake ~ U[-10, 15] deg,
+    depth of cut ~ U[20, 100] um, JC A and B ~ U[0.9, 1.1] x the Ti6Al4V values."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_instances):
+        n_wp = rng.uniform(3e3, 4e4)
+        ny = max(8, int(round(np.sqrt(n_wp / (714.0 / 214.0)))))
+        nx = int(round(ny * 714.0 / 214.0))
+        p = cut_params(mf, nx=nx, ny=ny, dx=0.06 / ny)
+        p.speed = rng.uniform(30.0, 200.0) * 100.0 / 60.0e6
+        p.rake = rng.uniform(-10.0, 15.0)
+        p.feed = rng.uniform(20e-4, 100e-4)
+        p.joco.A *= rng.uniform(0.9, 1.1)
+        p.joco.B *= rng.uniform(0.9, 1.1)
+        out.append(p)
+    return out
+
+
+def batch_run(mf, torch, n_instances, steps, device):
+    """The sweep stepped one instance at a time, all instances queued on their own streams,
+    and as one batch (wall clock, host launch cost included)."""
+    scenes = [mf.Scene.from_params(p) for p in sweep_params(mf, n_instances)]
+    n_total = sum(sc.N for sc in scenes)
+
+    def contexts():
+        cs = []
+        for sc in scenes:
+            c = mf.Context(device)
+            c.upload_scene(sc, mf.GRID_GREEN)
+            c.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, mf.PRECISION_MIXED)
+            cs.append(c)
+        return cs
+
+    cs = contexts()
+    for c in cs:
+        c.step(4)  # graphs built, counts primed
+    torch.cuda.synchronize(device)
+    # one instance at a time, as a driver that owns one instance would run them
+    t0 = time.perf_counter()
+    for c in cs:
+        c.step(steps)
+        c.synchronize()
+    one_s = time.perf_counter() - t0
+    # all instances queued at once, each on its own stream (the GPU overlaps them)
+    t0 = time.perf_counter()
+    for c in cs:
+        c.step(steps)
+    for c in cs:
+        c.synchronize()
+    seq_s = time.perf_counter() - t0
+    for c in cs:
+        c.close()
+    cs = contexts()
+    b = mf.Batch(cs, steps_per_launch=0)
+    k = b.steps_per_launch
+    launches = max(1, steps // k)
+    b.step(1)
+    for c in cs:
+        c.synchronize()
+    t0 = time.perf_counter()
+    b.step(launches)
+    for c in cs:
+        c.synchronize()
+    bat_s = time.perf_counter() - t0
+    st = [c.status() for c in cs]
+    b.close()
+    for c in cs:
+        c.close()
+    return {"mode": "batch", "instances": n_instances, "particles_total": n_total,
+            "particles_min_max": [min(sc.N for sc in scenes), max(sc.N for sc in scenes)],
+            "precision": "mixed", "steps_per_launch": k,
+            "one_at_a_time": {"steps": steps, "wall_s": one_s, "particle_steps_per_s": n_total * steps / one_s},
+            "streams": {"steps": steps, "wall_s": seq_s, "particle_steps_per_s": n_total * steps / seq_s},
+            "batched": {"steps": launches * k, "wall_s": bat_s,
+                        "particle_steps_per_s": n_total * launches * k / bat_s},
+            "batched_over_one_at_a_time": (launches * k / bat_s) / (steps / one_s),
+            "batched_over_streams": (launches * k / bat_s) / (steps / seq_s),
+            "blanked": sum(x["blanked"] for x in st), "error_flags": max(x["error_flags"] for x in st)}
+
+
 def cpu_baseline(mf, scene, seconds=12.0, max_steps=5000):
     """The oracle port (C, OpenMP, all host threads) on the same scene: bounded sample."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -483,6 +565,9 @@ def main():
     ap.add_argument("--cut-mm", type=float, default=0.0,
                     help="instead of the benchmark: run this many mm of cut in both forms and report "
                          "wall time per mm and the mixed form's errors")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="instead of the benchmark: the batched sweep of this many instances (mixed), "
+                         "stepped one by one and as one batch")
     ap.add_argument("--state-out", default=None,
                     help="with --cut-mm: save the FP64 form's end state (.npz) for --state-in")
     ap.add_argument("--state-in", default=None,
@@ -513,6 +598,13 @@ def main():
     params = cut_params(mf, nx=int(round(714 * sc)), ny=int(round(214 * sc)), dx=2.8e-4 / sc)
     scene = mf.Scene.from_params(params)
     N = scene.N
+    if args.batch > 0:
+        if rank == 0:
+            print(json.dumps(batch_run(mf, torch, args.batch, args.steps, device)), flush=True)
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return 0
     if args.cut_mm > 0:
         if rank == 0:
             print(json.dumps(cut_run(mf, torch, scene, params, args.cut_mm, device, args.state_out)), flush=True)

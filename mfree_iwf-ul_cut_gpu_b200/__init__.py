@@ -138,6 +138,9 @@ def lib():
         "mf_step": ([vp, i], i), "mf_step_stage": ([vp, i], i), "mf_report_force": ([vp, vp], i),
         "mf_probe_fp64": ([i, vp, vp, vp, vp, vp], i),
         "mf_tangent_mean_force": ([vp, i, i, i, vp, vp], i),
+        "mf_graph_capture": ([vp, i, C.POINTER(vp)], i), "mf_graph_destroy": ([vp], i),
+        "mf_batch_create": ([C.POINTER(vp), i, i, C.POINTER(vp)], i), "mf_batch_steps_per_launch": ([vp, ip], i),
+        "mf_batch_step": ([vp, i], i), "mf_batch_destroy": ([vp], i),
         "mf_get_constants": ([vp, C.POINTER(Phys), C.POINTER(Corr), C.POINTER(Joco), C.POINTER(Trml),
                               C.POINTER(Trml), ip], i),
         "mf_force_log": ([vp, vp, i, ip], i), "mf_force_last_async": ([vp, vp], i), "mf_status_get": ([vp, C.POINTER(Status)], i),
@@ -381,6 +384,39 @@ class Context:
 
     def vtk_write(self, path):
         self._check(self.L.mf_vtk_write_particles(self.h, str(path).encode()), "mf_vtk_write_particles")
+
+
+class Batch:
+    """Several contexts on one device advanced together by one graph launch (mf_batch_*).
+    steps_per_launch = 0 lets the batch pick it by measuring a few launches."""
+
+    def __init__(self, contexts, steps_per_launch=0):
+        self.L = lib()
+        self.contexts = list(contexts)
+        arr = (C.c_void_p * len(self.contexts))(*[c.h for c in self.contexts])
+        self.h = C.c_void_p()
+        rc = self.L.mf_batch_create(arr, len(self.contexts), int(steps_per_launch), C.byref(self.h))
+        if rc != MF_OK:
+            raise MfError(rc, "mf_batch_create")
+        k = C.c_int()
+        self.L.mf_batch_steps_per_launch(self.h, C.byref(k))
+        self.steps_per_launch = k.value
+
+    def step(self, n_launches=1):
+        rc = self.L.mf_batch_step(self.h, int(n_launches))
+        if rc != MF_OK:
+            raise MfError(rc, "mf_batch_step")
+
+    def close(self):
+        if self.h:
+            self.L.mf_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def probe_fp64(device=0) -> dict:

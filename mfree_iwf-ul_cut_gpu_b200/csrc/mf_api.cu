@@ -57,6 +57,8 @@ struct mf_ctx {
   // graphs: one per parity of the double buffer
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   bool graph_valid = false;
+  // bumped whenever captured work goes stale (buffers, constants, options, dt, flags)
+  unsigned long long gen = 0;
   long long steps = 0;
   unsigned long long force_read_head = 0;
   unsigned long long status_newly_blanked_seen = 0;
@@ -100,6 +102,7 @@ void free_list(std::vector<void *> &list) {
 }
 
 void drop_graphs(mf_ctx *ctx) {
+  ctx->gen++;
   for (int k = 0; k < 2; ++k)
     if (ctx->graph[k]) { cudaGraphExecDestroy(ctx->graph[k]); ctx->graph[k] = nullptr; }
   ctx->graph_valid = false;
@@ -749,6 +752,215 @@ int mf_step(mf_ctx *ctx, int n_steps) {
     ctx->cur ^= 1;
     ctx->steps++;
   }
+  return MF_OK;
+}
+
+namespace {
+
+// K steps of the context captured into a graph (the cell counts must be primed); the
+// context's parity is restored afterwards, so K even gives a replayable graph
+int capture_steps(mf_ctx *ctx, int K, cudaGraph_t *out) {
+  const int saved = ctx->cur;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = MF_OK;
+  for (int k = 0; k < K && rc == MF_OK; ++k) {
+    rc = launch_step(ctx);
+    ctx->cur ^= 1;
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  ctx->cur = saved;
+  if (rc != MF_OK || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) ctx->last_cuda_err = (int)e;
+    return rc != MF_OK ? rc : MF_ERR_CUDA;
+  }
+  *out = g;
+  return MF_OK;
+}
+
+int step_checks(mf_ctx *ctx) {
+  if (!ready(ctx)) return MF_ERR_STATE;
+  if (!(ctx->P.dt > 0.) || ctx->mid_step) return MF_ERR_STATE;
+  return MF_OK;
+}
+
+}  // namespace
+
+int mf_graph_capture(mf_ctx *ctx, int n_steps, void **graph) {
+  if (!ctx || !graph || n_steps < 2 || (n_steps & 1)) return MF_ERR_INVALID;
+  TRY(step_checks(ctx));
+  TRY(set_device(ctx));
+  ctx->P.N = ctx->N;
+  ctx->last_staged = false;
+  TRY(prime_counts(ctx));
+  cudaGraph_t g = nullptr;
+  TRY(capture_steps(ctx, n_steps, &g));
+  *graph = (void *)g;
+  return MF_OK;
+}
+
+int mf_graph_destroy(void *graph) {
+  if (!graph) return MF_ERR_INVALID;
+  return cudaGraphDestroy((cudaGraph_t)graph) == cudaSuccess ? MF_OK : MF_ERR_CUDA;
+}
+
+// ---- batched form: many contexts advanced by one graph launch ----
+struct mf_batch {
+  int device = 0;
+  std::vector<mf_ctx *> ctx;
+  std::vector<unsigned long long> gen;
+  std::vector<cudaEvent_t> ev;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int K = 0;
+};
+
+namespace {
+
+void batch_release(mf_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  b->exec = nullptr;
+}
+
+// one parent graph: a child graph of K steps per context, no edges between them
+int batch_build(mf_batch *b, int K) {
+  batch_release(b);
+  cudaGraph_t parent = nullptr;
+  cudaError_t e = cudaGraphCreate(&parent, 0);
+  if (e != cudaSuccess) return MF_ERR_CUDA;
+  int rc = MF_OK;
+  for (size_t i = 0; i < b->ctx.size() && rc == MF_OK; ++i) {
+    mf_ctx *c = b->ctx[i];
+    c->P.N = c->N;
+    c->last_staged = false;
+    rc = prime_counts(c);
+    cudaGraph_t child = nullptr;
+    if (rc == MF_OK) rc = capture_steps(c, K, &child);
+    if (rc == MF_OK) {
+      cudaGraphNode_t node;
+      if (cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child) != cudaSuccess) rc = MF_ERR_CUDA;
+      cudaGraphDestroy(child);
+    }
+    b->gen[i] = c->gen;
+  }
+  if (rc == MF_OK && cudaGraphInstantiate(&b->exec, parent, 0) != cudaSuccess) rc = MF_ERR_CUDA;
+  cudaGraphDestroy(parent);
+  if (rc == MF_OK) b->K = K;
+  return rc;
+}
+
+// the batch stream waits for every context's stream, or every context's stream for the batch
+int batch_order(mf_batch *b, bool into_batch) {
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    mf_ctx *c = b->ctx[i];
+    cudaStream_t from = into_batch ? c->stream : b->stream, to = into_batch ? b->stream : c->stream;
+    if (cudaEventRecord(b->ev[i], from) != cudaSuccess || cudaStreamWaitEvent(to, b->ev[i], 0) != cudaSuccess)
+      return MF_ERR_CUDA;
+  }
+  return MF_OK;
+}
+
+int batch_launch(mf_batch *b, int n) {
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    mf_ctx *c = b->ctx[i];
+    if (c->gen != b->gen[i] || step_checks(c) != MF_OK) return MF_ERR_STATE;  // rebuild the batch
+    c->P.N = c->N;
+    TRY(prime_counts(c));  // counts discarded by a host write since the last launch
+  }
+  TRY(batch_order(b, true));
+  for (int k = 0; k < n; ++k)
+    if (cudaGraphLaunch(b->exec, b->stream) != cudaSuccess) return MF_ERR_CUDA;
+  TRY(batch_order(b, false));
+  for (mf_ctx *c : b->ctx) {
+    c->steps += (long long)b->K * n;
+    c->last_staged = false;
+  }
+  return MF_OK;
+}
+
+}  // namespace
+
+int mf_batch_create(mf_ctx **ctxs, int n, int steps_per_launch, mf_batch **out) {
+  if (!ctxs || n < 1 || !out || steps_per_launch < 0 || (steps_per_launch & 1)) return MF_ERR_INVALID;
+  mf_batch *b = new (std::nothrow) mf_batch;
+  if (!b) return MF_ERR_NOMEM;
+  b->device = ctxs[0] ? ctxs[0]->device : 0;
+  int rc = MF_OK;
+  for (int i = 0; i < n && rc == MF_OK; ++i) {
+    mf_ctx *c = ctxs[i];
+    if (!c || c->device != b->device) rc = MF_ERR_INVALID;
+    else if (step_checks(c) != MF_OK) rc = MF_ERR_STATE;
+    for (int j = 0; j < i && rc == MF_OK; ++j)
+      if (ctxs[j] == c) rc = MF_ERR_INVALID;  // one instance once
+    if (rc == MF_OK) {
+      b->ctx.push_back(c);
+      b->gen.push_back(0);
+      cudaEvent_t ev = nullptr;
+      if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) rc = MF_ERR_CUDA;
+      b->ev.push_back(ev);
+    }
+  }
+  if (rc == MF_OK && cudaSetDevice(b->device) != cudaSuccess) rc = MF_ERR_CUDA;
+  if (rc == MF_OK && cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) rc = MF_ERR_CUDA;
+  if (rc == MF_OK && steps_per_launch > 0) rc = batch_build(b, steps_per_launch);
+  if (rc == MF_OK && steps_per_launch == 0) {
+    // autotune: the steps per launch with the highest throughput over a few real launches
+    // (these launches advance the instances)
+    const int cand[4] = {2, 4, 8, 16};
+    double best = -1.;
+    int best_k = 2;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = MF_ERR_CUDA;
+    for (int ci = 0; ci < 4 && rc == MF_OK; ++ci) {
+      rc = batch_build(b, cand[ci]);
+      if (rc == MF_OK) rc = batch_launch(b, 1);  // warm-up
+      if (rc == MF_OK && cudaEventRecord(e0, b->stream) != cudaSuccess) rc = MF_ERR_CUDA;
+      if (rc == MF_OK) rc = batch_launch(b, 2);
+      if (rc == MF_OK && cudaEventRecord(e1, b->stream) != cudaSuccess) rc = MF_ERR_CUDA;
+      float ms = 0.f;
+      if (rc == MF_OK && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        rc = MF_ERR_CUDA;
+      const double steps_per_ms = 2.0 * cand[ci] / (ms > 0.f ? ms : 1e-6f);
+      if (rc == MF_OK && steps_per_ms > best) {
+        best = steps_per_ms;
+        best_k = cand[ci];
+      }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (rc == MF_OK) rc = batch_build(b, best_k);
+  }
+  if (rc != MF_OK) {
+    mf_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return MF_OK;
+}
+
+int mf_batch_steps_per_launch(const mf_batch *b, int *k) {
+  if (!b || !k) return MF_ERR_INVALID;
+  *k = b->K;
+  return MF_OK;
+}
+
+int mf_batch_step(mf_batch *b, int n_launches) {
+  if (!b || n_launches < 0) return MF_ERR_INVALID;
+  if (!b->exec) return MF_ERR_STATE;
+  if (cudaSetDevice(b->device) != cudaSuccess) return MF_ERR_CUDA;
+  return batch_launch(b, n_launches);
+}
+
+int mf_batch_destroy(mf_batch *b) {
+  if (!b) return MF_ERR_INVALID;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_release(b);
+  for (cudaEvent_t e : b->ev)
+    if (e) cudaEventDestroy(e);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
   return MF_OK;
 }
 
