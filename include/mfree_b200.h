@@ -254,8 +254,20 @@ int mf_tool_construct(double tl_x, double tl_y, double length, double height, do
 int mf_tool_sample(const mf_tool_state *tool, double dx, double *xy_out, int capacity, int *n_out);
 int mf_tool_translate(mf_tool_state *tool, double dt); /* tool::update_tool with tool->vel */
 
+/* ---- tool wear: tool_wear::eval_usui (tool_wear.cu:20-64) on the device, from the current
+   state and the tool's velocity; out3 = min, max, mean of the Usui wear rate
+   K exp(alpha/T) p |v_r| over the particles in contact. The accumulated wear of the reference
+   (m_accum_wear += dt * mean) is the caller's sum. ---- */
+int mf_tool_wear_usui(mf_ctx *ctx, double K, double alpha, double out3[3]);
+
 /* ---- output: vtk_writer_write (vtk_writer.cpp:20-178, 185-264), legacy ASCII ---- */
 int mf_vtk_write_particles(mf_ctx *ctx, const char *path);
+/* the same file, written while the steps go on (no counterpart in the reference): the fields
+   are snapshotted inside the device, stream-ordered after the last step, copied to pinned host
+   memory on a side stream and written by a host thread; mf_vtk_flush waits for every pending
+   dump and returns the first error (mf_ctx_destroy flushes too) */
+int mf_vtk_write_particles_async(mf_ctx *ctx, const char *path);
+int mf_vtk_flush(mf_ctx *ctx);
 int mf_vtk_write_tool(const mf_tool_state *tool, const char *path);
 
 /* ---- graphs and the batched form (no counterpart in the reference) ----

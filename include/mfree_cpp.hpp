@@ -245,6 +245,35 @@ inline void vtk_writer_write(const tool *t, int step) {
   mfree::check(mf_vtk_write_tool(&t->s, buf), "vtk_writer_write");
 }
 
+// the same particle file written while the steps go on; vtk_writer_flush waits for all
+inline void vtk_writer_write_async(const particle_gpu *p, int step) {
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "results/vtk_out_%06d.vtk", step);
+  mfree::check(mf_vtk_write_particles_async(p->ctx, buf), "vtk_writer_write_async");
+}
+inline void vtk_writer_flush(const particle_gpu *p) { mfree::check(mf_vtk_flush(p->ctx), "vtk_writer_flush"); }
+
+// ---- tool_wear (tool_wear.h, tool_wear.cu:20-64): Usui wear evaluated on the device ----
+class tool_wear {
+ public:
+  tool_wear(double usui_K, double usui_alpha, unsigned int /*N_part*/, mf_phys_constants /*phys*/,
+            float2_t /*tool_vel: the tool's own velocity is used*/)
+      : m_K(usui_K), m_alpha(usui_alpha) {}
+  void eval_usui(const particle_gpu *particles, double dt, double &usui_min, double &usui_max, double &usui_avg) {
+    double out[3];
+    mfree::check(mf_tool_wear_usui(particles->ctx, m_K, m_alpha, out), "tool_wear::eval_usui");
+    usui_min = out[0];
+    usui_max = out[1];
+    usui_avg = out[2];
+    m_accum_wear += dt * usui_avg;
+  }
+  double get_accum_wear() const { return m_accum_wear; }
+
+ private:
+  double m_K = 0., m_alpha = 0., m_accum_wear = 0.;
+};
+inline tool_wear *global_wear = nullptr;
+
 // ---- setup_ref_cut (benchmarks.cpp:255-537) ----
 inline particle_gpu *setup_ref_cut(int ny, grid_base **grid, double rake = 0., double clear = 0., double chamfer = 0.,
                                    double speed = 0., double feed = 0.01) {

@@ -138,6 +138,8 @@ def lib():
         "mf_step": ([vp, i], i), "mf_step_stage": ([vp, i], i), "mf_report_force": ([vp, vp], i),
         "mf_probe_fp64": ([i, vp, vp, vp, vp, vp], i),
         "mf_tangent_mean_force": ([vp, i, i, i, vp, vp], i),
+        "mf_tool_wear_usui": ([vp, d, d, vp], i), "mf_vtk_write_particles_async": ([vp, C.c_char_p], i),
+        "mf_vtk_flush": ([vp], i),
         "mf_graph_capture": ([vp, i, C.POINTER(vp)], i), "mf_graph_destroy": ([vp], i),
         "mf_batch_create": ([C.POINTER(vp), i, i, C.POINTER(vp)], i), "mf_batch_steps_per_launch": ([vp, ip], i),
         "mf_batch_step": ([vp, i], i), "mf_batch_destroy": ([vp], i),
@@ -308,6 +310,18 @@ class Context:
         ref = lambda s: C.byref(s) if s is not None else None  # noqa: E731
         self._check(self.L.mf_set_constants(self.h, C.byref(phys), C.byref(corr), ref(joco), ref(trml_wp),
                                             ref(trml_tool)), "mf_set_constants")
+
+    def tool_wear_usui(self, K, alpha):
+        """(min, max, mean) Usui wear rate over the particles in contact (mf_tool_wear_usui)."""
+        out = np.zeros(3)
+        self._check(self.L.mf_tool_wear_usui(self.h, float(K), float(alpha), _ptr(out)), "mf_tool_wear_usui")
+        return out
+
+    def vtk_write_async(self, path):
+        self._check(self.L.mf_vtk_write_particles_async(self.h, str(path).encode()), "mf_vtk_write_particles_async")
+
+    def vtk_flush(self):
+        self._check(self.L.mf_vtk_flush(self.h), "mf_vtk_flush")
 
     def get_constants(self):
         """(phys, corr, joco or None, trml_wp, trml_tool) as last set."""

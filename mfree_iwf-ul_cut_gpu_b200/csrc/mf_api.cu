@@ -6,7 +6,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <new>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "mf_kernels.cuh"
@@ -22,6 +25,19 @@ int run_mean_force(mf_ctx *ctx, int device, params P, const dev_buffers &Dctx, i
                    int param, double out_mean[2], double out_dmean[2]);
 }  // namespace tg
 }  // namespace mf
+
+// one asynchronous particle dump: a device snapshot of the fields, their copy into pinned
+// host memory on a side stream, and a host thread that writes the file once it has landed
+struct vtk_job {
+  int n = 0;
+  double *dev = nullptr;   // snapshot: pos 2n, vel 2n, rho n, p n, T n, eps n, S 4n
+  unsigned *dev_flags = nullptr;
+  double *host = nullptr;  // pinned copy of the same
+  unsigned *host_flags = nullptr;
+  cudaEvent_t snap = nullptr, landed = nullptr;
+  std::thread writer;
+  int rc = 0;
+};
 
 struct mf_ctx {
   int device = 0;
@@ -62,6 +78,8 @@ struct mf_ctx {
   long long steps = 0;
   unsigned long long force_read_head = 0;
   unsigned long long status_newly_blanked_seen = 0;
+  cudaStream_t io_stream = nullptr;  // device-to-host copies of asynchronous dumps
+  std::vector<std::unique_ptr<vtk_job>> vtk_jobs;
 };
 
 namespace {
@@ -400,6 +418,8 @@ int mf_ctx_create(int device, mf_ctx **out) {
 int mf_ctx_destroy(mf_ctx *ctx) {
   if (!ctx) return MF_OK;
   cudaSetDevice(ctx->device);
+  mf_vtk_flush(ctx);
+  if (ctx->io_stream) cudaStreamDestroy(ctx->io_stream);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   drop_graphs(ctx);
   free_list(ctx->particle_allocs);
@@ -1068,12 +1088,85 @@ int mf_scene_upload(mf_ctx *ctx, const mf_scene *s, int grid_kind) {
 }
 
 // vtk_writer_write(const particle_gpu*, int) (vtk_writer.cpp:20-178): the unblanked particles
+// tool_wear::eval_usui (tool_wear.cu:20-64) on the device
+int mf_tool_wear_usui(mf_ctx *ctx, double K, double alpha, double out3[3]) {
+  if (!ctx || !out3) return MF_ERR_INVALID;
+  if (!ctx->has_particles || ctx->mid_step) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  double *d_out = nullptr;
+  CK(cudaMalloc(&d_out, 3 * sizeof(double)));
+  const state_set &S = ctx->set[ctx->cur];
+  const int blocks = std::max(1, std::min((ctx->N + BLOCK - 1) / BLOCK, ctx->bbox_blocks));
+  k_usui<<<blocks, BLOCK, 0, ctx->stream>>>(ctx->N, S, ctx->D, ctx->tool_buf[ctx->cur], K, alpha, d_out);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out3, d_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d_out);
+  if (e != cudaSuccess) { ctx->last_cuda_err = (int)e; return MF_ERR_CUDA; }
+  return MF_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// vtk_writer_write(const particle_gpu*, int) (vtk_writer.cpp:20-178): legacy ASCII, the
+// unblanked particles, "%f" values; fields in array order
+int write_vtk_particles(const char *path, int n, const double *pos, const double *vel, const double *rho,
+                        const double *p, const double *T, const double *eps, const double *S,
+                        const unsigned *flags) {
+  FILE *fp = std::fopen(path, "w+");
+  if (!fp) return MF_ERR_INVALID;
+  auto live = [&](int i) { return !(flags[i] & FLAG_BLANKED); };
+  int m = 0;
+  for (int i = 0; i < n; ++i) m += live(i);
+  std::fprintf(fp, "# vtk DataFile Version 2.0\nmfree iwf\nASCII\n\nDATASET UNSTRUCTURED_GRID\n");
+  std::fprintf(fp, "POINTS %d float\n", m);
+  for (int i = 0; i < n; ++i) if (live(i)) std::fprintf(fp, "%f %f %f\n", pos[2 * i], pos[2 * i + 1], 0.);
+  std::fprintf(fp, "\nCELLS %d %d\n", m, 2 * m);
+  for (int i = 0; i < n; ++i) if (live(i)) std::fprintf(fp, "%d %d\n", 1, i);
+  std::fprintf(fp, "\nCELL_TYPES %d\n", m);
+  for (int i = 0; i < n; ++i) if (live(i)) std::fprintf(fp, "%d\n", 1);
+  std::fprintf(fp, "\nPOINT_DATA %d\n", m);
+  auto scalars = [&](const char *name, auto value) {
+    std::fprintf(fp, "SCALARS %s float 1\nLOOKUP_TABLE default\n", name);
+    for (int i = 0; i < n; ++i) if (live(i)) std::fprintf(fp, "%f\n", value(i));
+    std::fprintf(fp, "\n");
+  };
+  scalars("density", [&](int i) { return rho[i]; });
+  scalars("Temperature", [&](int i) { return T[i]; });
+  scalars("Fixed", [&](int i) { return (flags[i] & FLAG_FIXED) ? 1. : 0.; });
+  scalars("Tool", [&](int i) { return (flags[i] & FLAG_TOOL) ? 1. : 0.; });
+  scalars("EquivAccumPlasticStrain", [&](int i) { return eps[i]; });
+  std::fprintf(fp, "VECTORS Velocity float\n");
+  for (int i = 0; i < n; ++i) if (live(i)) std::fprintf(fp, "%f %f %f\n", vel[2 * i], vel[2 * i + 1], 0.);
+  std::fprintf(fp, "\nSCALARS SvM float 1\nLOOKUP_TABLE default\n");
+  for (int i = 0; i < n; ++i) {
+    if (!live(i)) continue;
+    double cxx = S[4 * i] - p[i], cyy = S[4 * i + 2] - p[i], czz = S[4 * i + 3] - p[i], cxy = S[4 * i + 1];
+    double svm2 = (cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy;
+    std::fprintf(fp, "%f\n", svm2 > 0 ? std::sqrt(svm2) : 0.);
+  }
+  std::fprintf(fp, "\n");
+  return std::fclose(fp) == 0 ? MF_OK : MF_ERR_INVALID;
+}
+
+// the fields of a dump, in snapshot order
+struct vtk_src {
+  const void *ptr;
+  size_t doubles;  // per particle
+};
+
+}  // namespace
+
+extern "C" {
+
 int mf_vtk_write_particles(mf_ctx *ctx, const char *path) {
   if (!ctx || !path) return MF_ERR_INVALID;
   if (!ctx->has_particles) return MF_ERR_STATE;
   const int n = ctx->N;
-  std::vector<double> pos(2 * (size_t)n), vel(2 * (size_t)n), rho(n), p(n), T(n), eps(n), S(4 * (size_t)n), fixed(n),
-      blanked(n), tool(n);
+  std::vector<double> pos(2 * (size_t)n), vel(2 * (size_t)n), rho(n), p(n), T(n), eps(n), S(4 * (size_t)n);
+  std::vector<unsigned> flags(n);
   TRY(mf_get_field(ctx, MF_FIELD_POS, pos.data()));
   TRY(mf_get_field(ctx, MF_FIELD_VEL, vel.data()));
   TRY(mf_get_field(ctx, MF_FIELD_RHO, rho.data()));
@@ -1081,42 +1174,80 @@ int mf_vtk_write_particles(mf_ctx *ctx, const char *path) {
   TRY(mf_get_field(ctx, MF_FIELD_T, T.data()));
   TRY(mf_get_field(ctx, MF_FIELD_EPS_PL, eps.data()));
   TRY(mf_get_field(ctx, MF_FIELD_S, S.data()));
-  TRY(mf_get_field(ctx, MF_FIELD_FIXED, fixed.data()));
-  TRY(mf_get_field(ctx, MF_FIELD_BLANKED, blanked.data()));
-  TRY(mf_get_field(ctx, MF_FIELD_TOOL, tool.data()));
-  FILE *fp = std::fopen(path, "w+");
-  if (!fp) return MF_ERR_INVALID;
-  int m = 0;
-  for (int i = 0; i < n; ++i) m += blanked[i] != 1.;
-  std::fprintf(fp, "# vtk DataFile Version 2.0\nmfree iwf\nASCII\n\nDATASET UNSTRUCTURED_GRID\n");
-  std::fprintf(fp, "POINTS %d float\n", m);
-  for (int i = 0; i < n; ++i) if (blanked[i] != 1.) std::fprintf(fp, "%f %f %f\n", pos[2 * i], pos[2 * i + 1], 0.);
-  std::fprintf(fp, "\nCELLS %d %d\n", m, 2 * m);
-  for (int i = 0; i < n; ++i) if (blanked[i] != 1.) std::fprintf(fp, "%d %d\n", 1, i);
-  std::fprintf(fp, "\nCELL_TYPES %d\n", m);
-  for (int i = 0; i < n; ++i) if (blanked[i] != 1.) std::fprintf(fp, "%d\n", 1);
-  std::fprintf(fp, "\nPOINT_DATA %d\n", m);
-  auto scalars = [&](const char *name, const std::vector<double> &v) {
-    std::fprintf(fp, "SCALARS %s float 1\nLOOKUP_TABLE default\n", name);
-    for (int i = 0; i < n; ++i) if (blanked[i] != 1.) std::fprintf(fp, "%f\n", v[i]);
-    std::fprintf(fp, "\n");
-  };
-  scalars("density", rho);
-  scalars("Temperature", T);
-  scalars("Fixed", fixed);
-  scalars("Tool", tool);
-  scalars("EquivAccumPlasticStrain", eps);
-  std::fprintf(fp, "VECTORS Velocity float\n");
-  for (int i = 0; i < n; ++i) if (blanked[i] != 1.) std::fprintf(fp, "%f %f %f\n", vel[2 * i], vel[2 * i + 1], 0.);
-  std::fprintf(fp, "\nSCALARS SvM float 1\nLOOKUP_TABLE default\n");
-  for (int i = 0; i < n; ++i) {
-    if (blanked[i] == 1.) continue;
-    double cxx = S[4 * i] - p[i], cyy = S[4 * i + 2] - p[i], czz = S[4 * i + 3] - p[i], cxy = S[4 * i + 1];
-    double svm2 = (cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy;
-    std::fprintf(fp, "%f\n", svm2 > 0 ? std::sqrt(svm2) : 0.);
+  CK(cudaMemcpy(flags.data(), ctx->set[view_set(ctx)].flags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost));
+  return write_vtk_particles(path, n, pos.data(), vel.data(), rho.data(), p.data(), T.data(), eps.data(), S.data(),
+                             flags.data());
+}
+
+int mf_vtk_flush(mf_ctx *ctx) {
+  if (!ctx) return MF_ERR_INVALID;
+  int rc = MF_OK;
+  for (auto &j : ctx->vtk_jobs) {
+    if (j->writer.joinable()) j->writer.join();
+    if (j->rc != MF_OK && rc == MF_OK) rc = j->rc;
+    if (j->snap) cudaEventDestroy(j->snap);
+    if (j->landed) cudaEventDestroy(j->landed);
+    if (j->dev) cudaFree(j->dev);
+    if (j->dev_flags) cudaFree(j->dev_flags);
+    if (j->host) cudaFreeHost(j->host);
+    if (j->host_flags) cudaFreeHost(j->host_flags);
   }
-  std::fprintf(fp, "\n");
-  std::fclose(fp);
+  ctx->vtk_jobs.clear();
+  return rc;
+}
+
+// the same file as mf_vtk_write_particles, written while the steps go on: the fields are
+// copied inside the device (stream-ordered after the last step), brought to pinned host
+// memory on a side stream, and written by a host thread; mf_vtk_flush waits for all dumps
+int mf_vtk_write_particles_async(mf_ctx *ctx, const char *path) {
+  if (!ctx || !path) return MF_ERR_INVALID;
+  if (!ctx->has_particles || ctx->mid_step) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  if (!ctx->io_stream) CK(cudaStreamCreateWithFlags(&ctx->io_stream, cudaStreamNonBlocking));
+  const int n = ctx->N;
+  const state_set &s = ctx->set[ctx->cur];
+  const vtk_src src[7] = {{s.pos, 2}, {s.vel, 2}, {s.rho, 1}, {ctx->D.pp, 1}, {s.T, 1}, {s.eps_pl, 1}, {s.S, 4}};
+  const size_t per = 12;  // doubles per particle in the snapshot
+  std::unique_ptr<vtk_job> j(new (std::nothrow) vtk_job);
+  if (!j) return MF_ERR_NOMEM;
+  j->n = n;
+  cudaError_t e = cudaMalloc(&j->dev, sizeof(double) * per * n);
+  if (e == cudaSuccess) e = cudaMalloc(&j->dev_flags, sizeof(unsigned) * n);
+  if (e == cudaSuccess) e = cudaMallocHost(&j->host, sizeof(double) * per * n);
+  if (e == cudaSuccess) e = cudaMallocHost(&j->host_flags, sizeof(unsigned) * n);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j->snap, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j->landed, cudaEventDisableTiming);
+  size_t off = 0;
+  for (int k = 0; k < 7 && e == cudaSuccess; ++k) {
+    e = cudaMemcpyAsync(j->dev + off * n, src[k].ptr, sizeof(double) * src[k].doubles * n, cudaMemcpyDeviceToDevice,
+                        ctx->stream);
+    off += src[k].doubles;
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(j->dev_flags, s.flags, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(j->snap, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->io_stream, j->snap, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(j->host, j->dev, sizeof(double) * per * n, cudaMemcpyDeviceToHost, ctx->io_stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(j->host_flags, j->dev_flags, sizeof(unsigned) * n, cudaMemcpyDeviceToHost, ctx->io_stream);
+  if (e == cudaSuccess) e = cudaEventRecord(j->landed, ctx->io_stream);
+  vtk_job *jp = j.get();
+  ctx->vtk_jobs.push_back(std::move(j));  // released by mf_vtk_flush, also on failure
+  if (e != cudaSuccess) {
+    ctx->last_cuda_err = (int)e;
+    return MF_ERR_CUDA;
+  }
+  const std::string file(path);
+  const int device = ctx->device;
+  jp->writer = std::thread([jp, file, device]() {
+    cudaSetDevice(device);
+    if (cudaEventSynchronize(jp->landed) != cudaSuccess) { jp->rc = MF_ERR_CUDA; return; }
+    const int n = jp->n;
+    const double *h = jp->host;
+    jp->rc = write_vtk_particles(file.c_str(), n, h, h + 2 * (size_t)n, h + 4 * (size_t)n, h + 5 * (size_t)n,
+                                 h + 6 * (size_t)n, h + 7 * (size_t)n, h + 8 * (size_t)n, jp->host_flags);
+  });
   return MF_OK;
 }
 

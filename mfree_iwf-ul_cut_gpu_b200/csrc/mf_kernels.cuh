@@ -59,7 +59,7 @@ struct dev_buffers {
   unsigned long long *scan_status;
   unsigned *scan_done;
   double *partials;     // per-block partial sums (force / bbox)
-  unsigned *ticket;     // last-block tickets: [0] force, [1] bbox
+  unsigned *ticket;     // last-block tickets: [0] force, [1] bbox, [2] tool wear
   double *force_log;    // FORCE_LOG_CAP x 2
   double *force_last;   // 2
   plastic_item *plastic_list;  // particles whose return map k_plastic runs (this step)
@@ -1126,6 +1126,84 @@ static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic
     if (c) atomicAdd(&D.st->secant_cap_hits, c);
     if (itn) atomicAdd(&D.st->secant_iterations, itn);
   }
+}
+
+// Usui tool wear rate (tool_wear.cu:20-64) on the current state, on the device instead of
+// after six device-to-host copies: for every particle in contact (fc.x, fc.y, ft.x or fc.y
+// nonzero - the reference tests fc.y twice and never ft.y), K exp(alpha/T) p |v_r| with
+// p = |fc| / (2 pi h) and v_r = v - v*n component-wise, v = vel - tool velocity. out = min,
+// max and mean over those particles (0 when none), the sum compensated.
+static __global__ void __launch_bounds__(BLOCK) k_usui(int N, state_set S, dev_buffers D, const mf_tool_state *tool,
+                                                       double K, double alpha, double *out) {
+  __shared__ double smn[BLOCK / 32], smx[BLOCK / 32];
+  __shared__ ksum ssum[BLOCK / 32];
+  __shared__ unsigned scnt[BLOCK / 32];
+  __shared__ bool last;
+  const double BIG = 3.402823466e+38;  // FLT_MAX, the reference's start value
+  const double tvx = tool->vel[0], tvy = tool->vel[1];
+  double mn = BIG, mx = 0.;
+  ksum total{0., 0.};
+  unsigned count = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const double2 fc = S.fc[i], ft = S.ft[i];
+    if (!(fabs(fc.x) > 0. || fabs(fc.y) > 0. || fabs(ft.x) > 0. || fabs(fc.y) > 0.)) continue;
+    ++count;
+    const double2 v = S.vel[i], nn = D.n[i];
+    const double vx = v.x - tvx, vy = v.y - tvy;
+    const double vrx = vx - vx * nn.x, vry = vy - vy * nn.y;
+    const double vmag = sqrt(vrx * vrx + vry * vry);
+    const double fmag = sqrt(fc.x * fc.x + fc.y * fc.y);
+    const double A = 2 * S.h[i] * 3.14159265358979323846;
+    const double pr = fmag / A;
+    const double w = K * exp(alpha / S.T[i]) * pr * vmag;
+    ksum_add(total, w);
+    mn = fmin(mn, w);
+    mx = fmax(mx, w);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    ksum b{__shfl_down_sync(0xffffffffu, total.s, o), __shfl_down_sync(0xffffffffu, total.c, o)};
+    ksum_merge(total, b);
+  }
+  count = __reduce_add_sync(0xffffffffu, count);
+  if (lane_id() == 0) {
+    smn[threadIdx.x >> 5] = mn;
+    smx[threadIdx.x >> 5] = mx;
+    ssum[threadIdx.x >> 5] = total;
+    scnt[threadIdx.x >> 5] = count;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < BLOCK / 32; ++w) {
+      mn = fmin(mn, smn[w]);
+      mx = fmax(mx, smx[w]);
+      ksum_merge(total, ssum[w]);
+      count += scnt[w];
+    }
+    double *pr = D.partials + (size_t)blockIdx.x * 8;
+    pr[0] = mn; pr[1] = mx; pr[2] = total.s; pr[3] = total.c; pr[4] = (double)count;
+    __threadfence();
+    const unsigned t = atomicAdd(&D.ticket[2], 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  double rmn = BIG, rmx = 0., rc = 0.;
+  ksum rs{0., 0.};
+  for (unsigned b = 0; b < gridDim.x; ++b) {
+    const volatile double *pr = D.partials + (size_t)b * 8;
+    rmn = fmin(rmn, pr[0]);
+    rmx = fmax(rmx, pr[1]);
+    ksum x{pr[2], pr[3]};
+    ksum_merge(rs, x);
+    rc += pr[4];
+  }
+  out[0] = rc == 0. ? 0. : rmn;
+  out[1] = rmx;
+  out[2] = rc == 0. ? 0. : (rs.s + rs.c) / rc;
+  D.ticket[2] = 0u;
 }
 
 // report_force on the current state without stepping (output.cu:31-39)

@@ -99,6 +99,7 @@ def lib():
             getattr(L, f).argtypes = [C.c_void_p]
         L.orc_steps.argtypes = [C.c_void_p, C.c_int]
         L.orc_steps_force_log.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_usui.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p]
         L.orc_report_force.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_out_of_grid.restype = C.c_longlong
         L.orc_out_of_grid.argtypes = [C.c_void_p]
@@ -125,6 +126,7 @@ def ref():
             return None
         L = C.CDLL(str(REF_SO))
         L.refh_cubic_spline.argtypes = [C.c_double] * 5 + [C.c_void_p]
+        L.refh_usui.argtypes = [C.c_int] + [C.c_void_p] * 7 + [C.c_double] * 5 + [C.c_void_p]
         L.refh_lapl_pse.restype = C.c_double
         L.refh_lapl_pse.argtypes = [C.c_double] * 5
         L.refh_sigma_yield.restype = C.c_double
@@ -203,6 +205,11 @@ class Oracle:
     def report_force(self):
         out = np.zeros(2)
         self.L.orc_report_force(self.s, _ptr(out))
+        return out
+
+    def usui(self, K, alpha, tool_vel):
+        out = np.zeros(3)
+        self.L.orc_usui(self.s, K, alpha, tool_vel[0], tool_vel[1], _ptr(out))
         return out
 
     def steps_force_log(self, n: int):

@@ -62,9 +62,11 @@ def build_ref(force: bool = False) -> Path | None:
     if not REF_SRC.is_dir():
         return REF_LIB if REF_LIB.exists() else None
     ref_files = ["benchmarks.cpp", "tool.cpp", "geometric_primitives.cpp", "constants_structs.cpp",
-                 "grid.cu", "tool_wear.cu"]
-    srcs = [HERE / "ref_host_harness.cu", HERE / "ref_host_plasticity.cpp",
-            HERE / "ref_shim" / "glm" / "glm.hpp"] + [REF_SRC / f for f in ref_files]
+                 "grid.cu"]
+    # tool_wear.cu is compiled inside ref_host_wear.cu (its copies made host copies)
+    harness = ["ref_host_harness.cu", "ref_host_wear.cu"]
+    srcs = [HERE / f for f in harness] + [HERE / "ref_host_plasticity.cpp", HERE / "ref_shim" / "glm" / "glm.hpp",
+                                          REF_SRC / "tool_wear.cu"] + [REF_SRC / f for f in ref_files]
     if not (force or _stale(REF_LIB, srcs)):
         return REF_LIB
     obj = HERE / "_ref" / "obj"
@@ -75,7 +77,7 @@ def build_ref(force: bool = False) -> Path | None:
     nv = [NVCC, "-O3", "-std=c++14", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
           "-gencode", "arch=compute_100a,code=sm_100a", "-w", "-x", "cu", "-c"]
     objs = []
-    for f in ["ref_host_harness.cu"]:
+    for f in harness:
         o = obj / (Path(f).stem + ".o")
         _run(nv + inc + ["-o", str(o), str(HERE / f)])
         objs.append(o)

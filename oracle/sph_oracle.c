@@ -1235,6 +1235,35 @@ int orc_steps(orc_state *s, int n) {
   return 0;
 }
 
+/* Usui tool wear rate (tool_wear.cu:20-64) over the particles in contact: out = min, max,
+   average of K exp(alpha/T) p |v_r|, p = |fc| / (2 pi h), v_r = v - v*n component-wise with
+   v = vel - tool velocity. "In contact" tests fc.x, fc.y, ft.x and fc.y again (ft.y is never
+   tested), as the reference does. */
+void orc_usui(orc_state *s, double K, double alpha, double tool_vx, double tool_vy, double out3[3]) {
+  double mn = 3.402823466e+38, mx = 0., total = 0.;
+  long long count = 0;
+  for (int i = 0; i < s->N; ++i) {
+    const double fcx = s->fc[i].x, fcy = s->fc[i].y, ftx = s->ft[i].x;
+    const int in_contact = fabs(fcx) > 0. || fabs(fcy) > 0. || fabs(ftx) > 0. || fabs(fcy) > 0.;
+    if (!in_contact) continue;
+    count++;
+    const double vx = s->vel[i].x - tool_vx, vy = s->vel[i].y - tool_vy;
+    const double nx = s->n[i].x, ny = s->n[i].y;
+    const double vrx = vx - vx * nx, vry = vy - vy * ny;
+    const double vmag = sqrt(vrx * vrx + vry * vry);
+    const double fmag = sqrt(fcx * fcx + fcy * fcy);
+    const double A = 2 * s->h[i] * M_PI;
+    const double p = fmag / A;
+    const double w = K * exp(alpha / s->T[i]) * p * vmag;
+    total += w;
+    mn = fmin(mn, w);
+    mx = fmax(mx, w);
+  }
+  out3[0] = count == 0 ? 0. : mn;
+  out3[1] = mx;
+  out3[2] = count == 0 ? 0. : total / count;
+}
+
 /* n steps, with report_force (output.cu:31-39) after each one into out[2k], out[2k+1] */
 int orc_steps_force_log(orc_state *s, int n, double *out) {
   for (int k = 0; k < n; ++k) {

@@ -99,6 +99,7 @@ void orc_stage_finish(orc_state *s);    /* correct .. invalidate */
 int orc_step(orc_state *s);             /* one complete step */
 int orc_steps(orc_state *s, int n);
 int orc_steps_force_log(orc_state *s, int n, double *out); /* report_force after each step */
+void orc_usui(orc_state *s, double K, double alpha, double tool_vx, double tool_vy, double out3[3]); /* tool_wear.cu:20-64 */
 void orc_report_force(orc_state *s, double out2[2]); /* output.cu:31-39 */
 long long orc_out_of_grid(const orc_state *s);       /* hashes clamped so far */
 

@@ -142,6 +142,28 @@ def tools(R):
     np.savez_compressed(HERE / "ref_tools.npz", **out)
 
 
+def usui_inputs(rng, n=600):
+    """Seeded particle arrays for the Usui wear evaluation: about half in contact."""
+    contact = rng.random(n) < 0.5
+    fc = np.where(contact[:, None], rng.normal(0, 1e-4, (n, 2)), 0.0)
+    ft = np.where(contact[:, None], rng.normal(0, 3e-5, (n, 2)), 0.0)
+    fc[::7, 0] = 0.0  # contact seen through one component only
+    ang = rng.uniform(0, 2 * np.pi, n)
+    return {"pos": rng.uniform(0, 0.2, (n, 2)), "vel": rng.normal(0, 1e-4, (n, 2)), "fc": fc, "ft": ft,
+            "h": rng.uniform(1e-4, 1e-3, n), "n": np.stack([np.cos(ang), np.sin(ang)], axis=1),
+            "T": rng.uniform(300.0, 900.0, n), "K": np.array(1e-8), "alpha": np.array(-2500.0),
+            "tool_vel": np.array([-1.16667e-4, 0.0]), "dt": np.array(0.01)}
+
+
+def usui(R, rng):
+    d = usui_inputs(rng)
+    out = np.zeros(4)
+    R.refh_usui(len(d["h"]), *[_p(np.ascontiguousarray(d[k])) for k in ("pos", "vel", "fc", "ft", "h", "n", "T")],
+                C.c_double(float(d["K"])), C.c_double(float(d["alpha"])), C.c_double(d["tool_vel"][0]),
+                C.c_double(d["tool_vel"][1]), C.c_double(float(d["dt"])), _p(out))
+    np.savez_compressed(HERE / "ref_usui.npz", usui=out, **d)
+
+
 def main():
     build_oracle.build_ref()
     R = B.ref()
@@ -153,6 +175,7 @@ def main():
     kernels(R, rng)
     plasticity(R, rng)
     tools(R)
+    usui(R, np.random.default_rng(77))
 
 
 if __name__ == "__main__":

@@ -82,3 +82,15 @@ def test_live_reference_randomised(orc):
         L.orc_cubic_spline(*args, o1.ctypes.data_as(C.c_void_p))
         R.refh_cubic_spline(*args, o2.ctypes.data_as(C.c_void_p))
         assert bits_equal(o1, o2)
+
+
+def test_usui_wear_bitwise(orc, golden):
+    """Usui wear rate (tool_wear.cu:20-64): the oracle against the reference's own eval_usui."""
+    g = golden("ref_usui")
+    n = len(g["h"])
+    o = orc.Oracle(n)
+    for k in ("pos", "vel", "fc", "ft", "h", "n", "T"):
+        o.set_field(k, g[k])
+    out = o.usui(float(g["K"]), float(g["alpha"]), g["tool_vel"])
+    assert bits_equal(out, g["usui"][:3])
+    assert bits_equal(float(g["dt"]) * out[2], g["usui"][3])  # m_accum_wear += dt * avg
