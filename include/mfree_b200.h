@@ -29,6 +29,8 @@ extern "C" {
 #define MF_ERR_NOMEM (-5)       /* device or host allocation failed */
 #define MF_ERR_NO_DEVICE (-6)   /* no CUDA device (the product has no CPU fallback) */
 #define MF_ERR_DEVICE_FAULT (-7) /* a kernel reported an internal error (bounded wait expired) */
+#define MF_ERR_IO (-8)          /* a state file could not be written or read */
+#define MF_ERR_CORRUPT (-9)     /* a state file failed its checks (format, size, checksum) */
 
 /* ---- particle fields (particle_gpu.h:33-87) ---- */
 #define MF_FIELD_POS 0        /* 2 doubles */
@@ -253,6 +255,22 @@ int mf_tool_construct(double tl_x, double tl_y, double length, double height, do
                       double r, double mu, mf_tool_state *out);
 int mf_tool_sample(const mf_tool_state *tool, double dx, double *xy_out, int capacity, int *n_out);
 int mf_tool_translate(mf_tool_state *tool, double dt); /* tool::update_tool with tool->vel */
+
+/* ---- checkpoint / resume (no counterpart in the reference, whose state lives only on the
+   device): the complete particle state in its current array order (every per-particle field,
+   the cell hash of blanked particles included), the rigid tool and the step count, in a binary
+   file with a format tag, the particle count and an FNV-1a checksum over everything before it.
+   mf_state_load needs a context set up with the same particle count (the scene's constants,
+   grid, options and dt are not part of the state) and refuses a file that fails any check
+   (MF_ERR_CORRUPT) without changing the context. ---- */
+int mf_state_save(mf_ctx *ctx, const char *path);
+int mf_state_load(mf_ctx *ctx, const char *path);
+
+/* ---- fields to and from device memory (caller's pointers, no host round trip): the copy is
+   queued on `cuda_stream` (the context's stream when null) after the context's pending work,
+   and the context's later work waits for it; layout as mf_get_field / mf_set_field ---- */
+int mf_get_field_device(mf_ctx *ctx, int field, void *device_dst, void *cuda_stream);
+int mf_set_field_device(mf_ctx *ctx, int field, const void *device_src, void *cuda_stream);
 
 /* ---- tool wear: tool_wear::eval_usui (tool_wear.cu:20-64) on the device, from the current
    state and the tool's velocity; out3 = min, max, mean of the Usui wear rate

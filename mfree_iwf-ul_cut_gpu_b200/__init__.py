@@ -17,7 +17,9 @@ LIB_PATH = PKG_DIR / "lib" / "libmfree_b200.so"
 # ---- constants mirrored from include/mfree_b200.h ----
 MF_OK = 0
 ERRORS = {-1: "invalid argument", -2: "CUDA runtime error", -3: "call out of order", -4: "size out of range",
-          -5: "out of memory", -6: "no CUDA device", -7: "a kernel reported an internal error"}
+          -5: "out of memory", -6: "no CUDA device", -7: "a kernel reported an internal error",
+          -8: "state file input/output failed", -9: "state file failed its checks"}
+MF_ERR_CORRUPT = -9
 GRID_GREEN, GRID_ROTHLIN = 0, 1
 THERMAL_BROOKSHAW, THERMAL_PSE = 0, 1
 JC_JOHNSON_COOK, JC_TANH = 0, 1
@@ -139,6 +141,8 @@ def lib():
         "mf_probe_fp64": ([i, vp, vp, vp, vp, vp], i),
         "mf_tangent_mean_force": ([vp, i, i, i, vp, vp], i),
         "mf_tool_wear_usui": ([vp, d, d, vp], i), "mf_vtk_write_particles_async": ([vp, C.c_char_p], i),
+        "mf_state_save": ([vp, C.c_char_p], i), "mf_state_load": ([vp, C.c_char_p], i),
+        "mf_get_field_device": ([vp, i, vp, vp], i), "mf_set_field_device": ([vp, i, vp, vp], i),
         "mf_vtk_flush": ([vp], i),
         "mf_graph_capture": ([vp, i, C.POINTER(vp)], i), "mf_graph_destroy": ([vp], i),
         "mf_batch_create": ([C.POINTER(vp), i, i, C.POINTER(vp)], i), "mf_batch_steps_per_launch": ([vp, ip], i),
@@ -310,6 +314,23 @@ class Context:
         ref = lambda s: C.byref(s) if s is not None else None  # noqa: E731
         self._check(self.L.mf_set_constants(self.h, C.byref(phys), C.byref(corr), ref(joco), ref(trml_wp),
                                             ref(trml_tool)), "mf_set_constants")
+
+    def state_save(self, path):
+        self._check(self.L.mf_state_save(self.h, str(path).encode()), "mf_state_save")
+
+    def state_load(self, path):
+        self._check(self.L.mf_state_load(self.h, str(path).encode()), "mf_state_load")
+
+    def get_device(self, name, device_ptr, stream=None):
+        """Copy a field into device memory at `device_ptr` (an int address), on `stream`."""
+        fid = FIELDS[name][0]
+        self._check(self.L.mf_get_field_device(self.h, fid, C.c_void_p(device_ptr), C.c_void_p(stream)),
+                    f"mf_get_field_device({name})")
+
+    def set_device(self, name, device_ptr, stream=None):
+        fid = FIELDS[name][0]
+        self._check(self.L.mf_set_field_device(self.h, fid, C.c_void_p(device_ptr), C.c_void_p(stream)),
+                    f"mf_set_field_device({name})")
 
     def tool_wear_usui(self, K, alpha):
         """(min, max, mean) Usui wear rate over the particles in contact (mf_tool_wear_usui)."""

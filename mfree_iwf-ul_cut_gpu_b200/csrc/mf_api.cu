@@ -374,6 +374,8 @@ const char *mf_error_string(int code) {
     case MF_ERR_NOMEM: return "out of memory";
     case MF_ERR_NO_DEVICE: return "no CUDA device";
     case MF_ERR_DEVICE_FAULT: return "a kernel reported an internal error";
+    case MF_ERR_IO: return "state file input/output failed";
+    case MF_ERR_CORRUPT: return "state file failed its checks";
     default: return "unknown error";
   }
 }
@@ -1088,6 +1090,211 @@ int mf_scene_upload(mf_ctx *ctx, const mf_scene *s, int grid_kind) {
 }
 
 // vtk_writer_write(const particle_gpu*, int) (vtk_writer.cpp:20-178): the unblanked particles
+}  // extern "C"
+
+namespace {
+
+// flag bit <-> 0/1 doubles, for the device-destination field access
+__global__ void k_flag_to_double(int N, const unsigned *flags, unsigned bit, double *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N) out[i] = (flags[i] & bit) ? 1. : 0.;
+}
+__global__ void k_double_to_flag(int N, const double *in, unsigned bit, unsigned *flags, unsigned *bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double v = in[i];
+  if (!(v == 0. || v == 1.)) {
+    atomicOr(bad, 1u);
+    return;
+  }
+  flags[i] = v == 1. ? (flags[i] | bit) : (flags[i] & ~bit);
+}
+
+// the caller's stream waits for the context, or the context for the caller's stream
+int order_streams(cudaStream_t from, cudaStream_t to) {
+  if (from == to) return MF_OK;
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return MF_ERR_CUDA;
+  cudaError_t r = cudaEventRecord(e, from);
+  if (r == cudaSuccess) r = cudaStreamWaitEvent(to, e, 0);
+  cudaEventDestroy(e);
+  return r == cudaSuccess ? MF_OK : MF_ERR_CUDA;
+}
+
+int field_device_copy(mf_ctx *ctx, int field, void *dst_dev, const void *src_dev, cudaStream_t st, bool to_ctx) {
+  const size_t N = (size_t)ctx->N;
+  const unsigned bit = flag_bit(field);
+  const int view = view_set(ctx);
+  TRY(order_streams(ctx->stream, st));
+  cudaError_t e = cudaSuccess;
+  if (bit) {
+    const int nb = (ctx->N + BLOCK - 1) / BLOCK;
+    if (!to_ctx) {
+      k_flag_to_double<<<nb, BLOCK, 0, st>>>(ctx->N, ctx->set[view].flags, bit, (double *)dst_dev);
+    } else {
+      unsigned *bad = nullptr;
+      e = cudaMallocAsync(&bad, sizeof(unsigned), st);
+      if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(unsigned), st);
+      if (e == cudaSuccess)
+        k_double_to_flag<<<nb, BLOCK, 0, st>>>(ctx->N, (const double *)src_dev, bit, ctx->set[view].flags, bad);
+      unsigned hbad = 0;
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&hbad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (bad) cudaFreeAsync(bad, st);
+      if (e == cudaSuccess && hbad) return MF_ERR_INVALID;  // a value other than 0 or 1 (others kept)
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+  } else {
+    const field_desc d = describe(field);
+    void *fp = field_ptr(ctx, field);
+    if (!fp) return MF_ERR_INVALID;
+    const size_t bytes = N * d.width * (d.is_int ? sizeof(int) : sizeof(double));
+    e = to_ctx ? cudaMemcpyAsync(fp, src_dev, bytes, cudaMemcpyDeviceToDevice, st)
+               : cudaMemcpyAsync(dst_dev, fp, bytes, cudaMemcpyDeviceToDevice, st);
+  }
+  if (e != cudaSuccess) {
+    ctx->last_cuda_err = (int)e;
+    return MF_ERR_CUDA;
+  }
+  return order_streams(st, ctx->stream);
+}
+
+// state file: tag, version, particle count, steps, tool, then per field (id, bytes, data),
+// then an FNV-1a checksum of all the bytes before it
+constexpr char STATE_TAG[8] = {'M', 'F', 'B', '2', 'S', 'T', 'A', 'T'};
+constexpr int STATE_VERSION = 1;
+constexpr int STATE_FIELDS[] = {MF_FIELD_POS, MF_FIELD_VEL, MF_FIELD_H, MF_FIELD_RHO, MF_FIELD_S, MF_FIELD_FC,
+                                MF_FIELD_FT, MF_FIELD_N, MF_FIELD_FIXED, MF_FIELD_BLANKED, MF_FIELD_TOOL,
+                                MF_FIELD_EPS_PL, MF_FIELD_EPS_PL_DOT, MF_FIELD_T, MF_FIELD_POS_T, MF_FIELD_VEL_T,
+                                MF_FIELD_RHO_T, MF_FIELD_S_T, MF_FIELD_T_T, MF_FIELD_IDX, MF_FIELD_HASH, MF_FIELD_ID};
+
+struct fnv1a {
+  unsigned long long h = 1469598103934665603ull;
+  void add(const void *p, size_t n) {
+    const unsigned char *b = (const unsigned char *)p;
+    for (size_t i = 0; i < n; ++i) {
+      h ^= b[i];
+      h *= 1099511628211ull;
+    }
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int mf_get_field_device(mf_ctx *ctx, int field, void *device_dst, void *cuda_stream) {
+  if (!ctx || !device_dst || field < 0 || field >= MF_NUM_FIELDS) return MF_ERR_INVALID;
+  if (!ctx->has_particles) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  return field_device_copy(ctx, field, device_dst, nullptr, cuda_stream ? (cudaStream_t)cuda_stream : ctx->stream,
+                           false);
+}
+
+int mf_set_field_device(mf_ctx *ctx, int field, const void *device_src, void *cuda_stream) {
+  if (!ctx || !device_src || field < 0 || field >= MF_NUM_FIELDS) return MF_ERR_INVALID;
+  if (!ctx->has_particles) return MF_ERR_STATE;
+  if (field == MF_FIELD_R) return MF_ERR_INVALID;  // recomputed every step
+  TRY(set_device(ctx));
+  TRY(invalidate_counts(ctx));
+  return field_device_copy(ctx, field, nullptr, device_src, cuda_stream ? (cudaStream_t)cuda_stream : ctx->stream,
+                           true);
+}
+
+int mf_state_save(mf_ctx *ctx, const char *path) {
+  if (!ctx || !path) return MF_ERR_INVALID;
+  if (!ctx->has_particles || ctx->mid_step) return MF_ERR_STATE;
+  std::vector<unsigned char> buf;
+  auto put = [&](const void *p, size_t n) {
+    const unsigned char *b = (const unsigned char *)p;
+    buf.insert(buf.end(), b, b + n);
+  };
+  const int version = STATE_VERSION, N = ctx->N, nf = (int)(sizeof(STATE_FIELDS) / sizeof(int));
+  const long long steps = ctx->steps;
+  mf_tool_state tool{};
+  TRY(mf_tool_get(ctx, &tool));
+  put(STATE_TAG, 8);
+  put(&version, sizeof(int));
+  put(&N, sizeof(int));
+  put(&nf, sizeof(int));
+  put(&steps, sizeof(long long));
+  put(&tool, sizeof(tool));
+  std::vector<unsigned char> data;
+  for (int k = 0; k < nf; ++k) {
+    const int f = STATE_FIELDS[k];
+    const field_desc d = describe(f);
+    const long long bytes = (long long)N * d.width * (d.is_int ? sizeof(int) : sizeof(double));
+    data.resize((size_t)bytes);
+    TRY(mf_get_field(ctx, f, data.data()));
+    put(&f, sizeof(int));
+    put(&bytes, sizeof(long long));
+    put(data.data(), (size_t)bytes);
+  }
+  fnv1a h;
+  h.add(buf.data(), buf.size());
+  put(&h.h, sizeof(h.h));
+  FILE *fp = std::fopen(path, "wb");
+  if (!fp) return MF_ERR_IO;
+  const bool ok = std::fwrite(buf.data(), 1, buf.size(), fp) == buf.size();
+  if (std::fclose(fp) != 0 || !ok) return MF_ERR_IO;
+  return MF_OK;
+}
+
+int mf_state_load(mf_ctx *ctx, const char *path) {
+  if (!ctx || !path) return MF_ERR_INVALID;
+  if (!ctx->has_particles || ctx->mid_step) return MF_ERR_STATE;
+  FILE *fp = std::fopen(path, "rb");
+  if (!fp) return MF_ERR_IO;
+  std::vector<unsigned char> buf;
+  unsigned char chunk[1 << 16];
+  size_t got;
+  while ((got = std::fread(chunk, 1, sizeof(chunk), fp)) > 0) buf.insert(buf.end(), chunk, chunk + got);
+  const bool read_err = std::ferror(fp) != 0;
+  std::fclose(fp);
+  if (read_err) return MF_ERR_IO;
+  // every check before any change to the context
+  const size_t head = 8 + 3 * sizeof(int) + sizeof(long long) + sizeof(mf_tool_state);
+  if (buf.size() < head + sizeof(unsigned long long)) return MF_ERR_CORRUPT;
+  fnv1a h;
+  h.add(buf.data(), buf.size() - sizeof(unsigned long long));
+  unsigned long long stored;
+  std::memcpy(&stored, buf.data() + buf.size() - sizeof(stored), sizeof(stored));
+  if (stored != h.h || std::memcmp(buf.data(), STATE_TAG, 8) != 0) return MF_ERR_CORRUPT;
+  size_t at = 8;
+  auto get = [&](void *p, size_t n) {
+    if (at + n > buf.size() - sizeof(unsigned long long)) return false;
+    std::memcpy(p, buf.data() + at, n);
+    at += n;
+    return true;
+  };
+  int version = 0, N = 0, nf = 0;
+  long long steps = 0;
+  mf_tool_state tool{};
+  if (!get(&version, sizeof(int)) || !get(&N, sizeof(int)) || !get(&nf, sizeof(int)) ||
+      !get(&steps, sizeof(long long)) || !get(&tool, sizeof(tool)))
+    return MF_ERR_CORRUPT;
+  if (version != STATE_VERSION || N != ctx->N || nf != (int)(sizeof(STATE_FIELDS) / sizeof(int)))
+    return MF_ERR_CORRUPT;
+  std::vector<std::pair<int, size_t>> where;  // field, offset of its data
+  for (int k = 0; k < nf; ++k) {
+    int f = -1;
+    long long bytes = -1;
+    if (!get(&f, sizeof(int)) || !get(&bytes, sizeof(long long))) return MF_ERR_CORRUPT;
+    if (f != STATE_FIELDS[k]) return MF_ERR_CORRUPT;
+    const field_desc d = describe(f);
+    if (bytes != (long long)N * d.width * (d.is_int ? sizeof(int) : sizeof(double))) return MF_ERR_CORRUPT;
+    where.push_back({f, at});
+    at += (size_t)bytes;
+    if (at > buf.size() - sizeof(unsigned long long)) return MF_ERR_CORRUPT;
+  }
+  if (at != buf.size() - sizeof(unsigned long long)) return MF_ERR_CORRUPT;
+  // apply
+  for (const auto &w : where) TRY(mf_set_field(ctx, w.first, buf.data() + w.second));
+  TRY(mf_tool_set(ctx, &tool));
+  ctx->steps = steps;
+  return MF_OK;
+}
+
 // tool_wear::eval_usui (tool_wear.cu:20-64) on the device
 int mf_tool_wear_usui(mf_ctx *ctx, double K, double alpha, double out3[3]) {
   if (!ctx || !out3) return MF_ERR_INVALID;

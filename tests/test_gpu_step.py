@@ -159,6 +159,8 @@ def test_blanked_particles_and_nan_cascade(mf, orc):
         assert np.array_equal(ctx.get("blanked"), o.get("blanked"))
     nb = ctx.get("blanked") == 0.0
     assert (~nb).sum() > 0.02 * st["N"] + 5
+    # the NaN stress also ran the secant solve to its cap (plasticity.cuh:112-115)
+    assert ctx.status()["secant_cap_hits"] > 0
     check(ctx, o, ("pos", "vel", "rho"), 1e-9, mask=nb)
 
 
