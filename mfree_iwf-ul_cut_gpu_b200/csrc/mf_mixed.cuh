@@ -72,11 +72,11 @@ __device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_con
     a.sdz += sxy * w_x;
     a.sdw += K.mass * (I.syy + b1.w + fab * (I.Ryy + b2.z)) * w_y;
     const float vijposij = -(dvx * xij + dvy * yij);
-    const float irhoij = __frcp_rn(0.5f * (I.rho + b3.x));
+    const float irhoij = __fdividef(1.f, 0.5f * (I.rho + b3.x));
     if (vijposij < 0.f) {
       const float cij = 0.5f * (I.c + b3.y);
       const float hij = 0.5f * (I.h + b2.w);
-      const float muij = hij * vijposij * __frcp_rn(rr2 + K.eta2 * hij * hij);
+      const float muij = hij * vijposij * __fdividef(1.f, rr2 + K.eta2 * hij * hij);
       const float piij = (-K.alpha * cij * muij + K.beta * muij * muij) * irhoij;
       a.vtx -= K.mass * piij * w_x;
       a.vty -= K.mass * piij * w_y;
