@@ -74,9 +74,34 @@ def cut_params(mf, nx=714, ny=214, dx=2.8e-4):
     return p
 
 
+# the thermal solver of the timed forms (Brookshaw; the ~500k-particle configuration uses PSE)
+SOLVER = {"thermal": 0}
+
 WORKLOAD = {"workload": "orthogonal cut, Ti6Al4V 2.0 x 0.6 mm, 714x214 lattice dx=2.8um + sampled tool "
                         "particles, Brookshaw thermal solver, thermal contact",
             "lattice": [714, 214], "dx_um": 2.8, "thermal_solver": "brookshaw", "grid": "green (locked)"}
+
+
+def config_params(mf, name, lattice_scale=1.0):
+    """The scene parameters and workload description of a named configuration:
+    c1 = 143 x 43 lattice, dx = 14 um, adiabatic, no tool particles (~6k);
+    c2 = 714 x 214, dx = 2.8 um, Brookshaw, thermal contact (~150k, the benchmark);
+    c3 = 1290 x 387, dx = 1.55 um, PSE, thermal contact (~500k)."""
+    if name == "c1":
+        p = cut_params(mf, nx=143, ny=43, dx=1.4e-3)
+        p.sample_tool, p.use_thermals = 0, 0
+        return p, mf.THERMAL_BROOKSHAW, {"workload": "orthogonal cut, Ti6Al4V 2.0 x 0.6 mm, 143x43 lattice dx=14um, "
+                                                     "adiabatic, no tool particles", "lattice": [143, 43],
+                                         "dx_um": 14.0, "thermal_solver": "none", "grid": "green (locked)"}
+    if name == "c3":
+        p = cut_params(mf, nx=1290, ny=387, dx=1.55e-4)
+        return p, mf.THERMAL_PSE, {"workload": "orthogonal cut, Ti6Al4V 2.0 x 0.6 mm, 1290x387 lattice dx=1.55um + "
+                                               "sampled tool particles, PSE thermal solver, thermal contact",
+                                   "lattice": [1290, 387], "dx_um": 1.55, "thermal_solver": "pse",
+                                   "grid": "green (locked)"}
+    sc = lattice_scale
+    p = cut_params(mf, nx=int(round(714 * sc)), ny=int(round(214 * sc)), dx=2.8e-4 / sc)
+    return p, mf.THERMAL_BROOKSHAW, dict(WORKLOAD)
 
 
 def dist_env():
@@ -166,7 +191,7 @@ def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None)
     start from a saved state of the same scene instead of its initial state."""
     ctx = mf.Context(device)
     ctx.upload_scene(scene, mf.GRID_GREEN)
-    ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
+    ctx.set_options(SOLVER["thermal"], mf.JC_JOHNSON_COOK, precision)
     if state_in:
         load_state(mf, ctx, state_in)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
@@ -213,7 +238,7 @@ def e2e_form(mf, torch, scene, precision, steps, device):
     host memory), and the final state copied back to the host."""
     ctx = mf.Context(device)
     ctx.upload_scene(scene, mf.GRID_GREEN)
-    ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
+    ctx.set_options(SOLVER["thermal"], mf.JC_JOHNSON_COOK, precision)
     ctx.step(2)  # builds the graphs
     ctx.synchronize()
     n = scene.N
@@ -276,7 +301,7 @@ def run_form(mf, scene, precision, steps, device, torch=None, state_out=None):
     force (steps x 2), the end state ordered by particle number, and the device time (s)."""
     ctx = mf.Context(device)
     ctx.upload_scene(scene, mf.GRID_GREEN)
-    ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
+    ctx.set_options(SOLVER["thermal"], mf.JC_JOHNSON_COOK, precision)
     forces, left, secs = [], steps, 0.0
     chunk = 50_000  # below the device force log's 65,536 entries
     while left > 0:
@@ -502,7 +527,8 @@ def run_reference(args):
     if rank != 0:
         return 0
     mf = load_package()
-    scene = mf.Scene.from_params(cut_params(mf))
+    params, solver, workload = config_params(mf, args.config)
+    scene = mf.Scene.from_params(params)
     sys.path.insert(0, str(ROOT / "oracle"))
     sys.path.insert(0, str(ROOT / "tests"))
     import binding as orc
@@ -510,7 +536,7 @@ def run_reference(args):
     from helpers import load_oracle
 
     build_oracle.build_oracle()
-    o = load_oracle(orc, scene_state(mf, scene))
+    o = load_oracle(orc, scene_state(mf, scene), thermal_solver=solver)
     # each "step" is one full oracle step; bound the run to a few minutes
     o.L.orc_step(o.s)
     t0 = time.perf_counter()
@@ -529,7 +555,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": steps,
             "warmup": warm, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": dict(WORKLOAD, n_particles=scene.N, n_tool=scene.s.n_tool),
+            "config": dict(workload, name=args.config, n_particles=scene.N, n_tool=scene.s.n_tool),
             "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": cores, "kind": "port",
                              "sample": f"{steps} full steps of the {scene.N}-particle scene (requested "
                                        f"{args.steps}), C restatement of the reference step, OpenMP"},
@@ -565,6 +591,9 @@ def main():
     ap.add_argument("--cut-mm", type=float, default=0.0,
                     help="instead of the benchmark: run this many mm of cut in both forms and report "
                          "wall time per mm and the mixed form's errors")
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"],
+                    help="c2 (default): the ~150k-particle cut with thermal contact, the benchmark; "
+                         "c1: the ~6k adiabatic cut; c3: the ~500k cut with the PSE solver")
     ap.add_argument("--batch", type=int, default=0,
                     help="instead of the benchmark: the batched sweep of this many instances (mixed), "
                          "stepped one by one and as one batch")
@@ -595,7 +624,7 @@ def main():
                                 device_id=torch.device("cuda", device))
     mf = load_package()
     sc = args.lattice_scale
-    params = cut_params(mf, nx=int(round(714 * sc)), ny=int(round(214 * sc)), dx=2.8e-4 / sc)
+    params, SOLVER["thermal"], workload = config_params(mf, args.config, sc)
     scene = mf.Scene.from_params(params)
     N = scene.N
     if args.batch > 0:
@@ -668,7 +697,8 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed",
             "data": "synthetic",
-            "config": dict(WORKLOAD, n_particles=N, n_workpiece=scene.s.n_workpiece, n_tool=scene.s.n_tool,
+            "config": dict(workload, name=args.config, n_particles=N, n_workpiece=scene.s.n_workpiece,
+                           n_tool=scene.s.n_tool,
                            start_state=(f"saved state {args.state_in}" if args.state_in else "initial scene"),
                            parallelism=f"replicas x{world}", l2="flushed between timed steps (256 MiB write)",
                            global_particles=N * world),

@@ -245,8 +245,10 @@ int launch_stage(mf_ctx *ctx, int stage) {
     case 2:
       if (mixed) k_pair_mixed<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
       else k_pair_fp64<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
-      if (ctx->P.thermal_solver == MF_THERMAL_PSE && ctx->P.thermal_wp)
-        k_pse<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      if (ctx->P.thermal_solver == MF_THERMAL_PSE && ctx->P.thermal_wp) {
+        if (mixed) k_pse_mixed<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+        else k_pse<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      }
       break;
     case 3:
       if (fused_step(ctx)) k_finish<true><<<ctx->finish_blocks, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D, ctx->scan_tiles);
@@ -511,7 +513,7 @@ int mf_get_field(mf_ctx *ctx, int field, void *host) {
   }
   if (field == MF_FIELD_R) {
     double *o = (double *)host;
-    if (ctx->P.precision == MF_PRECISION_MIXED && ctx->P.thermal_solver != MF_THERMAL_PSE && !ctx->last_staged) {
+    if (ctx->P.precision == MF_PRECISION_MIXED && !ctx->last_staged) {
       // mixed form: R lives only in the FP32 pair records
       std::vector<float> rec(N * F_WIDTH);
       CK(cudaMemcpy(rec.data(), ctx->D.recf, sizeof(float) * N * F_WIDTH, cudaMemcpyDeviceToHost));

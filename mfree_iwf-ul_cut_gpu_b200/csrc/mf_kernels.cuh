@@ -422,8 +422,8 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
   for (int k = 0; k < R_FLAGS; ++k) finite = finite && isfinite(r[k]);
   if (!finite) rf |= FLAG_NONFINITE;
   r[R_FLAGS] = __longlong_as_double((long long)rf);
-  // the FP64 record feeds the FP64 pair kernel and the PSE pass (and R / p read-back)
-  if (!MIXED || P.staged || P.thermal_solver == MF_THERMAL_PSE) {
+  // the FP64 record feeds the FP64 pair kernel and its PSE pass (kept when staged, for reads)
+  if (!MIXED || P.staged) {
     double2 *dst = reinterpret_cast<double2 *>(D.rec + (size_t)q * R_WIDTH);
 #pragma unroll
     for (int k = 0; k < R_WIDTH / 2; ++k) dst[k] = make_double2(r[2 * k], r[2 * k + 1]);

@@ -4,8 +4,9 @@
 //
 // Same neighbour set and order as the plain form (interactions_gpu.cu:147-345); the
 // differences are the arithmetic type and these exact rewrites:
-//   * x_ij = (ci - cj) * dx + (xi_rel - xj_rel): small integers times the cell size plus
-//     a difference of in-cell offsets, instead of a difference of absolute coordinates;
+//   * x_ij = (ci - cj) * dx + (xi_rel - xj_rel) and y_ij likewise: a small integer times the
+//     cell size plus a difference of in-cell offsets, instead of a difference of absolute
+//     coordinates;
 //   * (e_ij . grad W) / r = der * fac (Brookshaw), one rsqrt per pair for 1/r;
 //   * temperatures are stored relative to the initial temperature, so Ti - Tj keeps its
 //     digits near it.
@@ -140,8 +141,6 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
   const int low_j = gj - 2 < 0 ? 0 : gj - 2;
   const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
   const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
-  // y offset between cell rows: (gj - r) * dx = oy0 - r * dx
-  const float oy0 = (float)gj * dxc;
 
   mixed_acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
@@ -159,7 +158,7 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
         const float4 b0 = __ldg(r0 + jb + k);
         const unsigned fjw = (unsigned)__float_as_int(b0.z);
         const float xij = ox - b0.x;
-        const float yij = (oy0 - (float)(int)(fjw >> 8) * dxc) + (I.y - b0.y);
+        const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
         const float rr2 = xij * xij + yij * yij;
         const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
         const bool take = !(fjw & FLAG_BLANKED) && (in_support || I.nonfinite || (fjw & FLAG_NONFINITE));
@@ -171,7 +170,7 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
         const int j = jb + k;
         // all four planes at once: one load latency per neighbour
         const float4 b0 = __ldg(r0 + j), b1 = __ldg(r1 + j), b2 = __ldg(r2 + j), b3 = __ldg(r3 + j);
-        const float yij = (oy0 - (float)(int)((unsigned)__float_as_int(b0.z) >> 8) * dxc) + (I.y - b0.y);
+        const float yij = fmaf((float)(gj - (int)((unsigned)__float_as_int(b0.z) >> 8)), dxc, I.y - b0.y);
         mixed_interact(I, K, acc, ox - b0.x, yij, b0, b1, b2, b3);
       }
     }
@@ -213,6 +212,54 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
     B.pos_t[q] = make_double2(xtx, xty);
   }
   if (thermal) B.T_t[q] = thermal_alpha * (double)T_lapl;
+}
+
+// PSE heat Laplacian (interactions_gpu.cu:88-144, kernels.cuh:72-89) in FP32 for the mixed
+// form, on the FP32 records: the same window (every particle of the 5x5 cells, blanked ones
+// included, no support cut-off) and the same alpha through the half-length texture binding;
+// exp from the hardware approximation, temperatures relative to the initial temperature.
+static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse_mixed(params P, dev_buffers D) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= P.N) return;
+  const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
+  const float4 *__restrict__ r2 = r0 + 2 * (size_t)P.N;
+  const float4 *__restrict__ r3 = r0 + 3 * (size_t)P.N;
+  const float4 a0 = __ldg(r0 + q);  // x, y, flags|cy, vx
+  const unsigned fi = (unsigned)__float_as_int(a0.z) & 0xffu;
+  if (fi & FLAG_BLANKED) return;
+  const float hi = __ldg(r2 + q).w;
+  const float Ti = __ldg(r3 + q).w;
+  const long long tex_elems = ((long long)sizeof(int) * P.N) / 8;
+  const bool tool_i = q < tex_elems ? (fi & FLAG_TOOL) != 0 : false;
+  const double alpha = tool_i ? P.trml_tool.alpha : P.trml_wp.alpha;
+  const float h2 = hi * hi;
+  const float inv_h2 = 1.f / h2;
+  const float coef = (float)(4. / 3.14159265358979323846) / (h2 * h2);
+  const geom g = *D.g;
+  const float dxc = (float)g.dx;
+  const int hashi = D.hash_cur[q];
+  const int gi = hashi / g.ny;
+  const int gj = hashi - gi * g.ny;
+  const int low_i = gi - 2 < 0 ? 0 : gi - 2;
+  const int low_j = gj - 2 < 0 ? 0 : gj - 2;
+  const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
+  const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
+  float T_ti = 0.f;
+  for (int ii = low_i; ii < high_i; ++ii) {
+    const int j0 = __ldg(D.off + ii * g.ny + low_j);
+    const int j1 = __ldg(D.off + ii * g.ny + high_j);
+    const float ox = (float)(gi - ii) * dxc + a0.x;
+#pragma unroll 4
+    for (int j = j0; j < j1; ++j) {
+      const float4 b0 = __ldg(r0 + j);
+      const float4 b3 = __ldg(r3 + j);  // rho, c, vol, T - T_init
+      const float xij = ox - b0.x;
+      const float yij = fmaf((float)(gj - (int)((unsigned)__float_as_int(b0.z) >> 8)), dxc, a0.y - b0.y);
+      const float w2 = coef * __expf(-(xij * xij + yij * yij) * inv_h2);
+      T_ti += (b3.w - Ti) * w2 * b3.z;
+    }
+  }
+  D.B.T_t[q] = alpha * (double)T_ti;
 }
 
 }  // namespace mf

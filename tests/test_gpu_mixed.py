@@ -13,11 +13,14 @@ from helpers import load_product, perturbed_scene
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("thermal_solver", [0, 1])
 @pytest.mark.parametrize("tensile", [False, True])
-def test_mixed_rates_one_step(mf, tensile):
+def test_mixed_rates_one_step(mf, tensile, thermal_solver):
     st = perturbed_scene(mf, ny=12, seed=31, tensile=tensile)
-    a = load_product(mf, st, precision=mf.PRECISION_FP64, flags=mf.OPT_KEEP_DERIVATIVES)
-    b = load_product(mf, st, precision=mf.PRECISION_MIXED, flags=mf.OPT_KEEP_DERIVATIVES)
+    a = load_product(mf, st, precision=mf.PRECISION_FP64, flags=mf.OPT_KEEP_DERIVATIVES,
+                     thermal_solver=thermal_solver)
+    b = load_product(mf, st, precision=mf.PRECISION_MIXED, flags=mf.OPT_KEEP_DERIVATIVES,
+                     thermal_solver=thermal_solver)
     for ctx in (a, b):
         ctx.stage(0)
         ctx.stage(1)
