@@ -369,14 +369,30 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
   // the Rothlin grid does not gather ft (grid_gpu_rothlin.cu:138-250): it stays in place
   B.ft[q] = P.grid_kind == MF_GRID_GREEN ? A.ft[p] : A.ft[q];
   B.h[q] = h;
-  B.pos_t[q] = pos_t;
-  B.vel_t[q] = vel_t;
-  B.S_t[q] = S_t;
-  B.rho_t[q] = rho_t;
-  B.T_t[q] = T_t;
-
   const bool blanked = f & FLAG_BLANKED;
   const bool tool = f & FLAG_TOOL;
+  // the previous rates travel with the particle where this step's pair pass will not
+  // overwrite them (blanked particles; tool particles' stress and density rates; the
+  // kinematic rates of tool particles under PSE; the temperature rate without conduction);
+  // staged, every rate is copied so that the half-built step reads whole
+  bool keep_kin = true, keep_mech = true, keep_T = true;
+  if (PREDICT && !P.staged && !blanked) {
+    const bool brookshaw = P.thermal_solver == MF_THERMAL_BROOKSHAW;
+    keep_kin = !brookshaw && tool;
+    keep_mech = tool;
+    const double alpha_T = !tool ? P.trml_wp.alpha : (P.thermal_tool_on ? P.trml_tool.alpha : 0.);
+    keep_T = brookshaw ? alpha_T == 0. : !P.thermal_wp;
+  }
+  if (keep_kin) {
+    B.pos_t[q] = pos_t;
+    B.vel_t[q] = vel_t;
+  }
+  if (keep_mech) {
+    B.S_t[q] = S_t;
+    B.rho_t[q] = rho_t;
+  }
+  if (keep_T) B.T_t[q] = T_t;
+
   if (PREDICT && !blanked) {
     const double dt = P.dt;
     pos.x = pos.x + 0.5 * dt * pos_t.x;
