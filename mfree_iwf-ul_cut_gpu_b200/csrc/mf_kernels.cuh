@@ -193,14 +193,15 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int
   const int tile = s_tile;
   if (tile < num_tiles) {
     const int base = tile * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
-    static_assert(SCAN_ITEMS == 8, "two int4 per thread");
-    const bool full = base + SCAN_ITEMS <= num_cell;  // base is a multiple of 8: 32-byte aligned
+    static_assert(SCAN_ITEMS % 4 == 0, "whole int4 per thread");
+    const bool full = base + SCAN_ITEMS <= num_cell;  // base: a multiple of SCAN_ITEMS, 16-byte aligned
     int v[SCAN_ITEMS];
     if (full) {
-      const int4 c0 = reinterpret_cast<const int4 *>(D.count + base)[0];
-      const int4 c1 = reinterpret_cast<const int4 *>(D.count + base)[1];
-      v[0] = c0.x; v[1] = c0.y; v[2] = c0.z; v[3] = c0.w;
-      v[4] = c1.x; v[5] = c1.y; v[6] = c1.z; v[7] = c1.w;
+#pragma unroll
+      for (int k = 0; k < SCAN_ITEMS / 4; ++k) {
+        const int4 c = reinterpret_cast<const int4 *>(D.count + base)[k];
+        v[4 * k] = c.x; v[4 * k + 1] = c.y; v[4 * k + 2] = c.z; v[4 * k + 3] = c.w;
+      }
     } else {
 #pragma unroll
       for (int k = 0; k < SCAN_ITEMS; ++k) v[k] = base + k < num_cell ? D.count[base + k] : 0;
@@ -275,11 +276,12 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int
     const int excl = s_excl + thread_excl;
     if (full) {
       int4 *o = reinterpret_cast<int4 *>(D.off + base);
-      o[0] = make_int4(excl + v[0], excl + v[1], excl + v[2], excl + v[3]);
-      o[1] = make_int4(excl + v[4], excl + v[5], excl + v[6], excl + v[7]);
       int4 *z = reinterpret_cast<int4 *>(D.count + base);  // ready for the next step
-      z[0] = make_int4(0, 0, 0, 0);
-      z[1] = make_int4(0, 0, 0, 0);
+#pragma unroll
+      for (int k = 0; k < SCAN_ITEMS / 4; ++k) {
+        o[k] = make_int4(excl + v[4 * k], excl + v[4 * k + 1], excl + v[4 * k + 2], excl + v[4 * k + 3]);
+        z[k] = make_int4(0, 0, 0, 0);
+      }
     } else {
 #pragma unroll
       for (int k = 0; k < SCAN_ITEMS; ++k) {
