@@ -211,6 +211,32 @@ bool fused_step(const mf_ctx *ctx) { return ctx->G.locked && !ctx->P.staged; }
 
 bool ready(const mf_ctx *ctx) { return ctx->has_particles && ctx->has_grid && ctx->has_constants; }
 
+#ifndef MF_USE_PDL
+#define MF_USE_PDL 1
+#endif
+// a step kernel, launched so that it may be scheduled while the previous kernel on the stream
+// drains (programmatic dependent launch); the kernel waits for its predecessor before it
+// touches memory (MF_PDL_WAIT)
+template <typename... KArgs, typename... Args>
+int launch_pdl(mf_ctx *ctx, void (*kernel)(KArgs...), int grid, int block, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = MF_USE_PDL ? 1 : 0;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, args...);
+  if (e != cudaSuccess) {
+    ctx->last_cuda_err = (int)e;
+    return MF_ERR_CUDA;
+  }
+  return MF_OK;
+}
+
 // cell-list build into the other buffer (k_hash_count .. k_reorder); PREDICT adds the
 // predictor of the step
 int launch_cells(mf_ctx *ctx, bool step_mode) {
@@ -218,13 +244,13 @@ int launch_cells(mf_ctx *ctx, bool step_mode) {
   const int nb = (N + BLOCK - 1) / BLOCK;
   bind_sets(ctx);
   if (!ctx->G.locked)
-    k_bbox<<<ctx->bbox_blocks, BLOCK, 0, ctx->stream>>>(N, ctx->D.A.pos, ctx->D.A.h, ctx->D);
+    TRY(launch_pdl(ctx, k_bbox, ctx->bbox_blocks, BLOCK, N, (const double2 *)ctx->D.A.pos, (const double *)ctx->D.A.h, ctx->D));
   if (!(step_mode && fused_step(ctx))) {
     const int hash_blocks = std::max(nb, (ctx->scan_tiles + BLOCK - 1) / BLOCK);
-    k_hash_count<<<hash_blocks, BLOCK, 0, ctx->stream>>>(N, ctx->D.A, ctx->D, ctx->scan_tiles);
+    TRY(launch_pdl(ctx, k_hash_count, hash_blocks, BLOCK, N, ctx->D.A, ctx->D, ctx->scan_tiles));
   }
-  k_scan<<<ctx->scan_tiles, SCAN_THREADS, 0, ctx->stream>>>(ctx->D, N);
-  k_scatter<<<nb, BLOCK, 0, ctx->stream>>>(N, ctx->D);
+  TRY(launch_pdl(ctx, k_scan, ctx->scan_tiles, SCAN_THREADS, ctx->D, N));
+  TRY(launch_pdl(ctx, k_scatter, nb, BLOCK, N, ctx->D));
   return MF_OK;
 }
 
@@ -239,25 +265,25 @@ int launch_stage(mf_ctx *ctx, int stage) {
       TRY(launch_cells(ctx, true));
       break;
     case 1:
-      if (mixed) k_reorder<true, true><<<nb, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
-      else k_reorder<true, false><<<nb, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      if (mixed) TRY(launch_pdl(ctx, k_reorder<true, true>, nb, BLOCK, ctx->P, ctx->D));
+      else TRY(launch_pdl(ctx, k_reorder<true, false>, nb, BLOCK, ctx->P, ctx->D));
       break;
     case 2:
-      if (mixed) k_pair_mixed<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
-      else k_pair_fp64<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+      if (mixed) TRY(launch_pdl(ctx, k_pair_mixed, npb, PAIR_BLOCK, ctx->P, ctx->D));
+      else TRY(launch_pdl(ctx, k_pair_fp64, npb, PAIR_BLOCK, ctx->P, ctx->D));
       if (ctx->P.thermal_solver == MF_THERMAL_PSE && ctx->P.thermal_wp) {
-        if (mixed) k_pse_mixed<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
-        else k_pse<<<npb, PAIR_BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+        if (mixed) TRY(launch_pdl(ctx, k_pse_mixed, npb, PAIR_BLOCK, ctx->P, ctx->D));
+        else TRY(launch_pdl(ctx, k_pse, npb, PAIR_BLOCK, ctx->P, ctx->D));
       }
       break;
     case 3:
-      if (fused_step(ctx)) k_finish<true><<<ctx->finish_blocks, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D, ctx->scan_tiles);
-      else k_finish<false><<<ctx->finish_blocks, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D, ctx->scan_tiles);
+      if (fused_step(ctx)) TRY(launch_pdl(ctx, k_finish<true>, ctx->finish_blocks, BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+      else TRY(launch_pdl(ctx, k_finish<false>, ctx->finish_blocks, BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
       if (ctx->P.plastic) {
         if (ctx->P.jc_model == MF_JC_TANH)
-          k_plastic<false><<<ctx->sm_count * PLASTIC_BLOCKS_PER_SM, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+          TRY(launch_pdl(ctx, k_plastic<false>, ctx->sm_count * PLASTIC_BLOCKS_PER_SM, BLOCK, ctx->P, ctx->D));
         else
-          k_plastic<true><<<ctx->sm_count * PLASTIC_BLOCKS_PER_SM, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+          TRY(launch_pdl(ctx, k_plastic<true>, ctx->sm_count * PLASTIC_BLOCKS_PER_SM, BLOCK, ctx->P, ctx->D));
       }
       break;
     default:

@@ -71,6 +71,14 @@ struct dev_buffers {
   dev_status *st;
 };
 
+// Programmatic dependent launch: the step's kernels are launched so that each may be
+// scheduled while its predecessor drains. Every step kernel first waits until its predecessor
+// has completed and its writes are visible, then lets its own successor be scheduled (all of
+// its blocks are then placed, so the successor's waiting blocks only take slots that would
+// otherwise idle in this kernel's tail). Both are no-ops for a plain launch.
+#define MF_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
+#define MF_PDL_TRIGGER() asm volatile("griddepcontrol.launch_dependents;" ::: "memory")
+
 constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 8;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
@@ -98,6 +106,8 @@ __device__ __forceinline__ void bbox_merge(double *a, const double *b) {
 
 static __global__ void __launch_bounds__(BLOCK) k_bbox(int N, const double2 *__restrict__ pos,
                                                 const double *__restrict__ h, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
   __shared__ double sm[BLOCK / 32][5];
   __shared__ bool last;
   const double BIG = 1.7976931348623157e+308;
@@ -152,6 +162,8 @@ static __global__ void __launch_bounds__(BLOCK) k_bbox(int N, const double2 *__r
 // ---------------------------------------------------------------------------------------
 // cell hash + count (compute_hashes, grid.cu:34-51)
 static __global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A, dev_buffers D, int num_scan_tiles) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   for (int t = gid; t < num_scan_tiles; t += gridDim.x * blockDim.x) D.scan_status[t] = 0ull;
   unsigned oog = 0;
@@ -182,6 +194,8 @@ static __global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A,
 // Tile ids come from an atomic ticket, so every tile waits only on tiles that are already
 // running; the wait is bounded and reports ERR_SCAN_WAIT instead of hanging.
 static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int N) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
   __shared__ int s_tile;
   __shared__ int s_warp[SCAN_THREADS / 32];
   __shared__ int s_excl;
@@ -308,6 +322,8 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int
 }
 
 static __global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= N) return;
   const int c = D.hash_new[q];
@@ -341,6 +357,8 @@ __device__ __forceinline__ int stable_member(const dev_buffers &D, int q, const 
 // neighbour records read by the pair kernel.
 template <bool PREDICT, bool MIXED>
 static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   if (q == 0) {  // re-armed for the finish kernel of this step
@@ -481,6 +499,8 @@ __device__ __forceinline__ void load_rec(const double *__restrict__ rec, int j, 
 }
 
 static __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_pair_fp64(params P, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const double *__restrict__ rec = D.rec;
@@ -629,6 +649,8 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_pair_fp64(params P, de
 // PSE heat Laplacian (interactions_gpu.cu:88-144): every particle of the window, blanked
 // ones included; alpha taken through the reference's half-length texture binding (:405).
 static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const double *__restrict__ rec = D.rec;
@@ -869,6 +891,8 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
 // count from the final positions (the work of k_hash_count) and re-arms the scan.
 template <bool FUSE_HASH>
 __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P, dev_buffers D, int num_scan_tiles) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
   __shared__ mf_tool_state s_tool;
   // the JC constants in shared memory: the out-of-line yield functions take them by
   // reference, which for a kernel parameter would mean a copy on every thread's stack
@@ -1066,6 +1090,8 @@ __device__ __forceinline__ double solve_secant_pair(const mf_joco_constants &jc,
 
 template <bool PAIRED>
 static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic(params P, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
   __shared__ mf_joco_constants s_jc;  // by reference into the out-of-line functions
   __shared__ unsigned long long s_cnt[BLOCK / 32][2];
   if (threadIdx.x == 0) s_jc = P.joco;

@@ -92,6 +92,8 @@ __device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_con
 
 // 80 registers (6 blocks of 128 per SM) keep the kernel free of spills
 static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   // record planes (structure of arrays): plane k of particle j at [k * N + j]
@@ -219,6 +221,8 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
 // included, no support cut-off) and the same alpha through the half-length texture binding;
 // exp from the hardware approximation, temperatures relative to the initial temperature.
 static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse_mixed(params P, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
