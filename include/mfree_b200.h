@@ -280,6 +280,11 @@ int mf_tool_wear_usui(mf_ctx *ctx, double K, double alpha, double out3[3]);
 
 /* ---- output: vtk_writer_write (vtk_writer.cpp:20-178, 185-264), legacy ASCII ---- */
 int mf_vtk_write_particles(mf_ctx *ctx, const char *path);
+/* the same file from host arrays (layouts as mf_get_field; fixed, blanked, tool_p 0/1), e.g.
+   for a state read back from a checkpoint; no device needed */
+int mf_vtk_write_particle_arrays(const char *path, int n, const double *pos, const double *vel, const double *rho,
+                                 const double *p, const double *T, const double *eps_pl, const double *S,
+                                 const double *fixed, const double *blanked, const double *tool_p);
 /* the same file, written while the steps go on (no counterpart in the reference): the fields
    are snapshotted inside the device, stream-ordered after the last step, copied to pinned host
    memory on a side stream and written by a host thread; mf_vtk_flush waits for every pending

@@ -143,7 +143,7 @@ def lib():
         "mf_tool_wear_usui": ([vp, d, d, vp], i), "mf_vtk_write_particles_async": ([vp, C.c_char_p], i),
         "mf_state_save": ([vp, C.c_char_p], i), "mf_state_load": ([vp, C.c_char_p], i),
         "mf_get_field_device": ([vp, i, vp, vp], i), "mf_set_field_device": ([vp, i, vp, vp], i),
-        "mf_vtk_flush": ([vp], i),
+        "mf_vtk_flush": ([vp], i), "mf_vtk_write_particle_arrays": ([C.c_char_p, i] + [vp] * 10, i),
         "mf_graph_capture": ([vp, i, C.POINTER(vp)], i), "mf_graph_destroy": ([vp], i),
         "mf_batch_create": ([C.POINTER(vp), i, i, C.POINTER(vp)], i), "mf_batch_steps_per_launch": ([vp, ip], i),
         "mf_batch_step": ([vp, i], i), "mf_batch_destroy": ([vp], i),
@@ -481,6 +481,24 @@ def tool_sample(tool: ToolState, dx: float) -> np.ndarray:
     if rc != MF_OK:
         raise MfError(rc, "mf_tool_sample")
     return out.reshape(-1, 2)
+
+
+def vtk_write_particle_arrays(path, fields: dict) -> None:
+    """The particle VTK file from host arrays: pos, vel, rho, p, T, eps_pl, S, fixed, blanked,
+    tool_p (mf_vtk_write_particle_arrays)."""
+    keys = ("pos", "vel", "rho", "p", "T", "eps_pl", "S", "fixed", "blanked", "tool_p")
+    arrs = [np.ascontiguousarray(fields[k], dtype=np.float64) for k in keys]
+    n = len(arrs[2])
+    rc = lib().mf_vtk_write_particle_arrays(str(path).encode(), n, *[_ptr(a) for a in arrs])
+    if rc != MF_OK:
+        raise MfError(rc, "mf_vtk_write_particle_arrays")
+
+
+def vtk_write_tool(tool: ToolState, path) -> None:
+    """vtk_writer_write(const tool*, int) (mf_vtk_write_tool): the tool as triangles."""
+    rc = lib().mf_vtk_write_tool(C.byref(tool), str(path).encode())
+    if rc != MF_OK:
+        raise MfError(rc, "mf_vtk_write_tool")
 
 
 def tool_translate(tool: ToolState, dt: float) -> None:

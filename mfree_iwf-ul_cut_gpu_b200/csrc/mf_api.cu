@@ -1396,6 +1396,18 @@ struct vtk_src {
 
 extern "C" {
 
+int mf_vtk_write_particle_arrays(const char *path, int n, const double *pos, const double *vel, const double *rho,
+                                 const double *p, const double *T, const double *eps_pl, const double *S,
+                                 const double *fixed, const double *blanked, const double *tool_p) {
+  if (!path || n < 0 || !pos || !vel || !rho || !p || !T || !eps_pl || !S || !fixed || !blanked || !tool_p)
+    return MF_ERR_INVALID;
+  std::vector<unsigned> flags((size_t)n);
+  for (int i = 0; i < n; ++i)
+    flags[i] = (fixed[i] == 1. ? FLAG_FIXED : 0u) | (blanked[i] == 1. ? FLAG_BLANKED : 0u) |
+               (tool_p[i] == 1. ? FLAG_TOOL : 0u);
+  return write_vtk_particles(path, n, pos, vel, rho, p, T, eps_pl, S, flags.data());
+}
+
 int mf_vtk_write_particles(mf_ctx *ctx, const char *path) {
   if (!ctx || !path) return MF_ERR_INVALID;
   if (!ctx->has_particles) return MF_ERR_STATE;

@@ -63,10 +63,12 @@ def build_ref(force: bool = False) -> Path | None:
         return REF_LIB if REF_LIB.exists() else None
     ref_files = ["benchmarks.cpp", "tool.cpp", "geometric_primitives.cpp", "constants_structs.cpp",
                  "grid.cu"]
-    # tool_wear.cu is compiled inside ref_host_wear.cu (its copies made host copies)
-    harness = ["ref_host_harness.cu", "ref_host_wear.cu"]
+    # tool_wear.cu and vtk_writer.cpp are compiled inside ref_host_wear.cu and ref_host_vtk.cu
+    # (their device-to-host copies made host copies)
+    harness = ["ref_host_harness.cu", "ref_host_wear.cu", "ref_host_vtk.cu"]
     srcs = [HERE / f for f in harness] + [HERE / "ref_host_plasticity.cpp", HERE / "ref_shim" / "glm" / "glm.hpp",
-                                          REF_SRC / "tool_wear.cu"] + [REF_SRC / f for f in ref_files]
+                                          REF_SRC / "tool_wear.cu", REF_SRC / "vtk_writer.cpp"] + \
+        [REF_SRC / f for f in ref_files]
     if not (force or _stale(REF_LIB, srcs)):
         return REF_LIB
     obj = HERE / "_ref" / "obj"

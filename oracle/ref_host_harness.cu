@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "benchmarks.h"
+#include "vtk_writer.h"
 #include "kernels.cuh"
 
 // ---------------------------------------------------------------------------------------
@@ -179,6 +180,37 @@ static int dump_tool(tool *t, double *seg_out, double *fillet_out, double *misc_
 }
 int refh_tool_dump(double *seg_out, double *fillet_out, double *misc_out) {
   return dump_tool(g_tool, seg_out, fillet_out, misc_out);
+}
+// vtk_writer_write(const tool*, int) (vtk_writer.cpp:185-264) on the current tool: writes
+// results/vtk_tool_<step>.vtk under the working directory
+int refh_vtk_tool(int step) {
+  if (!g_tool) return -1;
+  vtk_writer_write(g_tool, step);
+  return 0;
+}
+// vtk_writer_write(const particle_gpu*, int) (vtk_writer.cpp:20-178) on host arrays: writes
+// results/vtk_out_<step>.vtk under the working directory. The reference never fills its
+// blanked array (Q12), so which particles it skips depends on uninitialised memory; callers
+// check the POINTS count.
+int refh_vtk_particles(int step, int N, const double *pos, const double *vel, const double *rho, const double *h,
+                       const double *p, const double *T, const double *eps, const double *S, const double *fixed,
+                       const double *tool_p) {
+  std::vector<int> idx((size_t)N);
+  for (int i = 0; i < N; ++i) idx[i] = i;
+  particle_gpu pg((float2_t *)pos, (float2_t *)vel, (float_t *)rho, (float_t *)h, (unsigned)N);
+  pg.idx = idx.data();
+  pg.pos = (float2_t *)pos;
+  pg.vel = (float2_t *)vel;
+  pg.rho = (float_t *)rho;
+  pg.h = (float_t *)h;
+  pg.p = (float_t *)p;
+  pg.T = (float_t *)T;
+  pg.eps_pl = (float_t *)eps;
+  pg.S = (float4_t *)S;
+  pg.fixed = (float_t *)fixed;
+  pg.tool_particle = (float_t *)tool_p;
+  vtk_writer_write(&pg, step);
+  return 0;
 }
 void refh_tool_set_vel(double vx, double vy) { if (g_tool) g_tool->set_vel(glm::dvec2(vx, vy)); }
 void refh_tool_update(double dt) { if (g_tool) g_tool->update_tool(dt); }

@@ -164,6 +164,66 @@ def usui(R, rng):
     np.savez_compressed(HERE / "ref_usui.npz", usui=out, **d)
 
 
+def vtk_tools(R):
+    """The reference's tool VTK file (vtk_writer.cpp:185-264) for each tool of TOOLS, as built
+    and after a translation (the writer writes results/vtk_tool_<step>.vtk under the working
+    directory, so it runs in a scratch directory)."""
+    import os
+    import tempfile
+
+    R.refh_tool_create.argtypes = [C.c_double] * 8
+    R.refh_tool_set_vel.argtypes = [C.c_double, C.c_double]
+    R.refh_tool_update.argtypes = [C.c_double]
+    out = {}
+    cwd = os.getcwd()
+    scratch = ROOT / "_work"
+    scratch.mkdir(exist_ok=True)
+    with tempfile.TemporaryDirectory(dir=scratch) as d:
+        os.chdir(d)
+        try:
+            os.mkdir("results")
+            for k, t in enumerate(TOOLS):
+                R.refh_tool_create(*t)
+                R.refh_vtk_tool(2 * k)
+                R.refh_tool_set_vel(-1.16667e-4, 0.0)
+                R.refh_tool_update(37.5)
+                R.refh_vtk_tool(2 * k + 1)
+                for step in (2 * k, 2 * k + 1):
+                    data = open(f"results/vtk_tool_{step:06d}.vtk", "rb").read()
+                    out[f"t{k}_{'moved' if step % 2 else 'built'}"] = np.frombuffer(data, dtype=np.uint8)
+        finally:
+            os.chdir(cwd)
+    np.savez_compressed(HERE / "ref_vtk_tool.npz", **out)
+
+
+def vtk_particles(R, rng, n=400):
+    """The reference's particle VTK file (vtk_writer.cpp:20-178) for a seeded state. The
+    reference never fills its blanked array (Q12); the fixture is kept only if it wrote every
+    particle, so that it is the writer's output for an all-unblanked state."""
+    import os
+    import tempfile
+
+    d = {"pos": rng.uniform(-0.05, 0.2, (n, 2)), "vel": rng.normal(0, 1e-4, (n, 2)),
+         "rho": rng.uniform(4.3, 4.5, n), "h": np.full(n, 4.2e-4), "p": rng.normal(0, 1e-3, n),
+         "T": rng.uniform(300, 900, n), "eps_pl": rng.uniform(0, 2, n), "S": rng.normal(0, 1e-2, (n, 4)),
+         "fixed": (rng.random(n) < 0.1).astype(float), "tool_p": (rng.random(n) < 0.2).astype(float)}
+    R.refh_vtk_particles.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 10
+    cwd = os.getcwd()
+    scratch = ROOT / "_work"
+    scratch.mkdir(exist_ok=True)
+    with tempfile.TemporaryDirectory(dir=scratch) as tdir:
+        os.chdir(tdir)
+        try:
+            os.mkdir("results")
+            R.refh_vtk_particles(3, n, *[_p(np.ascontiguousarray(d[k])) for k in
+                                         ("pos", "vel", "rho", "h", "p", "T", "eps_pl", "S", "fixed", "tool_p")])
+            data = open("results/vtk_out_000003.vtk", "rb").read()
+        finally:
+            os.chdir(cwd)
+    assert f"POINTS {n} float".encode() in data, "the reference skipped particles (uninitialised blanked array)"
+    np.savez_compressed(HERE / "ref_vtk_particles.npz", vtk=np.frombuffer(data, dtype=np.uint8), **d)
+
+
 def main():
     build_oracle.build_ref()
     R = B.ref()
@@ -176,6 +236,8 @@ def main():
     plasticity(R, rng)
     tools(R)
     usui(R, np.random.default_rng(77))
+    vtk_tools(R)
+    vtk_particles(R, np.random.default_rng(91))
 
 
 if __name__ == "__main__":

@@ -104,3 +104,38 @@ def test_generalised_scene_explicit_lattice(mf):
     # dt = cfl*hdx*dx/(sqrt(K/rho0) + sqrt(v))
     s = sc.s
     assert abs(s.dt - 0.3 * 1.5 * 1.4e-3 / (np.sqrt(s.phys.K / s.phys.rho0) + np.sqrt(s.speed))) < 1e-18
+
+
+# (tl_x, tl_y, length, height, rake, clear, r, mu), as tests/golden/make_golden.py's TOOLS
+VTK_TOOLS = [
+    (-0.046, 0.0986074, 0.0413176, 0.0431, 10.0, 8.0, 0.002, 0.35),
+    (-0.046, 0.0986074, 0.0413176, 0.0431, 0.0, 7.0, 0.0005, 0.35),
+    (-0.046, 0.0986074, 0.0413176, 0.0431, -10.0, 6.0, 0.001, 0.2),
+    (0.0, 0.01, 0.02, 0.02, 15.0, 8.0, 0.0, 0.35),
+]
+
+
+@pytest.mark.parametrize("k", range(len(VTK_TOOLS)))
+def test_tool_vtk_file_byte_equal(mf, golden, tmp_path, k):
+    """mf_vtk_write_tool against the reference's own vtk_writer_write(const tool*, int)
+    (vtk_writer.cpp:185-264), as built and after a translation."""
+    g = golden("ref_vtk_tool")
+    t = VTK_TOOLS[k]
+    tool = mf.tool_construct((t[0], t[1]), *t[2:])
+    mf.vtk_write_tool(tool, tmp_path / "built.vtk")
+    assert (tmp_path / "built.vtk").read_bytes() == bytes(g[f"t{k}_built"])
+    tool.vel[0], tool.vel[1] = -1.16667e-4, 0.0
+    mf.tool_translate(tool, 37.5)
+    mf.vtk_write_tool(tool, tmp_path / "moved.vtk")
+    assert (tmp_path / "moved.vtk").read_bytes() == bytes(g[f"t{k}_moved"])
+
+
+def test_particle_vtk_file_byte_equal(mf, golden, tmp_path):
+    """The particle VTK writer (shared by mf_vtk_write_particles and its asynchronous form)
+    against the reference's own vtk_writer_write(const particle_gpu*, int)
+    (vtk_writer.cpp:20-178) on the same host arrays, every particle unblanked."""
+    g = golden("ref_vtk_particles")
+    fields = {k: g[k] for k in ("pos", "vel", "rho", "p", "T", "eps_pl", "S", "fixed", "tool_p")}
+    fields["blanked"] = np.zeros(len(g["rho"]))
+    mf.vtk_write_particle_arrays(tmp_path / "p.vtk", fields)
+    assert (tmp_path / "p.vtk").read_bytes() == bytes(g["vtk"])
