@@ -555,9 +555,10 @@ int mf_get_field(mf_ctx *ctx, int field, void *host) {
     std::vector<double> rec(N * R_WIDTH);
     CK(cudaMemcpy(rec.data(), ctx->D.rec, sizeof(double) * N * R_WIDTH, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < N; ++i) {
-      o[4 * i] = rec[i * R_WIDTH + R_RXX];
-      o[4 * i + 1] = rec[i * R_WIDTH + R_RXY];
-      o[4 * i + 2] = rec[i * R_WIDTH + R_RYY];
+      auto at = [&](int f) { return rec[(size_t)(f / 2) * N * 2 + (size_t)i * 2 + f % 2]; };
+      o[4 * i] = at(R_RXX);
+      o[4 * i + 1] = at(R_RXY);
+      o[4 * i + 2] = at(R_RYY);
       o[4 * i + 3] = 0.;
     }
     return MF_OK;

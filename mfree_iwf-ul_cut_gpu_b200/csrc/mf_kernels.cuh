@@ -47,7 +47,7 @@ struct plastic_item {
 struct dev_buffers {
   state_set A, B;       // A: state at the start of the step (previous order), B: new order
   double2 *n;           // contact normal, indexed by array position (never permuted)
-  double *rec;          // FP64 pair records, R_WIDTH doubles per particle
+  double *rec;          // FP64 pair records: R_WIDTH / 2 planes of N double2
   float *recf;          // FP32 pair records (mixed form): F_WIDTH / 4 planes of N float4
   double *pp;           // predictor pressure (the reference's particles->p)
   double4 *S_der, *v_der;
@@ -460,9 +460,10 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
   r[R_FLAGS] = __longlong_as_double((long long)rf);
   // the FP64 record feeds the FP64 pair kernel and its PSE pass (kept when staged, for reads)
   if (!MIXED || P.staged) {
-    double2 *dst = reinterpret_cast<double2 *>(D.rec + (size_t)q * R_WIDTH);
+    // eight planes of double2 (structure of arrays): plane k of particle q at [k * N + q]
+    double2 *dst = reinterpret_cast<double2 *>(D.rec);
 #pragma unroll
-    for (int k = 0; k < R_WIDTH / 2; ++k) dst[k] = make_double2(r[2 * k], r[2 * k + 1]);
+    for (int k = 0; k < R_WIDTH / 2; ++k) dst[(size_t)k * P.N + q] = make_double2(r[2 * k], r[2 * k + 1]);
   }
 
   if (MIXED) {
@@ -488,11 +489,15 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
 // consecutive hashes, so their particles form one contiguous range of the sorted order;
 // visiting the columns in x order and each range in array order is the reference's
 // neighbour order (x-cell outer, y-cell inner, sorted order within a cell).
-__device__ __forceinline__ void load_rec(const double *__restrict__ rec, int j, double *r) {
-  const double2 *s = reinterpret_cast<const double2 *>(rec + (size_t)j * R_WIDTH);
+// plane k of the FP64 record of particle j
+__device__ __forceinline__ double2 rec_plane(const double *__restrict__ rec, int N, int k, int j) {
+  return __ldg(reinterpret_cast<const double2 *>(rec) + (size_t)k * N + j);
+}
+
+__device__ __forceinline__ void load_rec(const double *__restrict__ rec, int N, int j, double *r) {
 #pragma unroll
   for (int k = 0; k < R_WIDTH / 2; ++k) {
-    double2 v = __ldg(s + k);
+    const double2 v = rec_plane(rec, N, k, j);
     r[2 * k] = v.x;
     r[2 * k + 1] = v.y;
   }
@@ -504,8 +509,9 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_pair_fp64(params P, de
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const double *__restrict__ rec = D.rec;
+  const int N = P.N;
   double ri[R_WIDTH];
-  load_rec(rec, q, ri);
+  load_rec(rec, N, q, ri);
   const unsigned fi = (unsigned)__double_as_longlong(ri[R_FLAGS]);
   if (fi & FLAG_BLANKED) return;
   const bool tool_i = fi & FLAG_TOOL;
@@ -554,9 +560,8 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_pair_fp64(params P, de
       const int jn = min(32, j1 - jb);
       unsigned mask = 0u;
       for (int k = 0; k < jn; ++k) {
-        const double2 *sj = reinterpret_cast<const double2 *>(rec + (size_t)(jb + k) * R_WIDTH);
-        const unsigned fj = (unsigned)__double_as_longlong(__ldg(sj + 7).y);
-        const double2 xy = __ldg(sj + 0);
+        const unsigned fj = (unsigned)__double_as_longlong(rec_plane(rec, N, 7, jb + k).y);
+        const double2 xy = rec_plane(rec, N, 0, jb + k);
         const double xij = xi - xy.x;
         const double yij = yi - xy.y;
         const double rr2 = xij * xij + yij * yij;
@@ -567,25 +572,25 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_pair_fp64(params P, de
       while (mask) {
         const int k = __ffs(mask) - 1;
         mask &= mask - 1u;
-        const double2 *sj = reinterpret_cast<const double2 *>(rec + (size_t)(jb + k) * R_WIDTH);
-        const double2 fx = __ldg(sj + 7);  // T, flags
+        const int j = jb + k;
+        const double2 fx = rec_plane(rec, N, 7, j);    // T, flags
+        const double2 xy = rec_plane(rec, N, 0, j);
+        const double2 cvol = rec_plane(rec, N, 6, j);  // c, vol
         const unsigned fj = (unsigned)__double_as_longlong(fx.y);
-        const double2 xy = __ldg(sj + 0);
         const double xij = xi - xy.x;
         const double yij = yi - xy.y;
         const double rr2 = xij * xij + yij * yij;
         const bool in_support = !(rr2 >= fourh2 || rr2 < 1e-8);
         double w = 0., w_x = 0., w_y = 0., dwr = 0.;
         if (in_support) cubic_spline_fp64(xij, yij, rr2, h1, w, w_x, w_y, dwr);
-        const double2 cvol = __ldg(sj + 6);  // c, vol
         const double volj = cvol.y;
         const bool tool_j = fj & FLAG_TOOL;
         if (!tool_i && !tool_j) {
-          const double2 v = __ldg(sj + 1);
-          const double2 s01 = __ldg(sj + 2);   // sxx, sxy
-          const double2 s2r0 = __ldg(sj + 3);  // syy, Rxx
-          const double2 r12 = __ldg(sj + 4);   // Rxy, Ryy
-          const double2 hrho = __ldg(sj + 5);  // h, rho
+          const double2 v = rec_plane(rec, N, 1, j);
+          const double2 s01 = rec_plane(rec, N, 2, j);   // sxx, sxy
+          const double2 s2r0 = rec_plane(rec, N, 3, j);  // syy, Rxx
+          const double2 r12 = rec_plane(rec, N, 4, j);   // Rxy, Ryy
+          const double2 hrho = rec_plane(rec, N, 5, j);  // h, rho
           vdx += (v.x - vxi) * w_x * volj;
           vdy += (v.x - vxi) * w_y * volj;
           vdz += (v.y - vyi) * w_x * volj;
@@ -654,12 +659,12 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const double *__restrict__ rec = D.rec;
-  const double2 *si = reinterpret_cast<const double2 *>(rec + (size_t)q * R_WIDTH);
-  const double2 fx = __ldg(si + 7);
+  const int N = P.N;
+  const double2 fx = rec_plane(rec, N, 7, q);
   const unsigned fi = (unsigned)__double_as_longlong(fx.y);
   if (fi & FLAG_BLANKED) return;
-  const double2 xy = __ldg(si + 0);
-  const double hi = __ldg(si + 5).x;
+  const double2 xy = rec_plane(rec, N, 0, q);
+  const double hi = rec_plane(rec, N, 5, q).x;
   const double Ti = fx.x;
   const double mass = P.phys.mass;
   const long long tex_elems = ((long long)sizeof(int) * P.N) / 8;
@@ -678,10 +683,9 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers
     const int j0 = __ldg(D.off + ii * g.ny + low_j);
     const int j1 = __ldg(D.off + ii * g.ny + high_j);
     for (int j = j0; j < j1; ++j) {
-      const double2 *sj = reinterpret_cast<const double2 *>(rec + (size_t)j * R_WIDTH);
-      const double2 pj = __ldg(sj + 0);
-      const double Tj = __ldg(sj + 7).x;
-      const double rhoj = __ldg(sj + 5).y;
+      const double2 pj = rec_plane(rec, N, 0, j);
+      const double Tj = rec_plane(rec, N, 7, j).x;
+      const double rhoj = rec_plane(rec, N, 5, j).y;
       const double w2 = lapl_pse_fp64(xy.x - pj.x, xy.y - pj.y, hi);
       T_ti += (Tj - Ti) * w2 * mass / rhoj;
     }
