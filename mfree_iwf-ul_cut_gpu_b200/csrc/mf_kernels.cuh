@@ -38,8 +38,8 @@ struct state_set {
 // a particle that failed the elastic test of the finish kernel, with the temperature its
 // return map starts from (after friction heat, before the thermal boundary condition)
 struct plastic_item {
-  double T;
-  double term_c;  // 1 - theta^m at T, as the elastic test computed it
+  double T;    // temperature of the yield test (after friction heat)
+  double svm;  // von Mises stress of the trial state
   int q;
   int pad;
 };
@@ -781,32 +781,28 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
     // >= A and the rate factor >= 1. A von Mises stress clearly below that bound is elastic
     // without any FP64 pow: theta^m comes from powf, whose error (a few float ulps, plus the
     // float rounding of theta and m) the factor 1.00001 covers, and the 0.1 % margin covers
-    // the rounding of the full yield stress. The decision is the reference's: when the bound
-    // does not settle it (or is NaN, as below Tref), the full test below runs.
+    // the rounding of the full yield stress. Every other particle goes to k_plastic, which
+    // runs the reference's full FP64 yield test and, where it yields, the return map over a
+    // compacted list with every lane busy; the trial stress, eps_pl, eps_pl_dot and rho
+    // written below are its inputs. Keeping the FP64 pow/log of the full test out of this
+    // kernel keeps its register budget small.
     bool elastic = false;
     if (P.jc_lower_bound) {
-      const float theta_f = (float)((T - JC.Tref) / (JC.Tmelt - JC.Tref));
+      // theta in float: three float roundings (about 2e-7 relative), far inside the margin
+      const float theta_f = (float)(T - JC.Tref) * (1.f / (float)(JC.Tmelt - JC.Tref));
       const double pow_hi = 1.00001 * (double)powf(theta_f, (float)JC.m);
       elastic = svm < 0.999 * JC.A * (1.0 - pow_hi);
-    }
-    // one temperature for the whole return map: its temperature-only factors once
-    jc_temp_terms tt;
-    if (!elastic) {
-      tt = jc_temperature_terms(JC, P.jc_model, T);
-      elastic = svm < sigma_yield(JC, eps_pl, eps_pl_dot, tt);
     }
     if (elastic) {
       eps_pl_dot = 0.;
     } else {
-      // the return map runs in k_plastic over a compacted list with every lane busy; the
-      // trial stress, eps_pl, eps_pl_dot and rho written below are its inputs
       const unsigned am = __activemask();
       const int leader = __ffs(am) - 1;
       unsigned base = 0u;
       if ((int)lane_id() == leader) base = atomicAdd(D.plastic_count, (unsigned)__popc(am));
       base = __shfl_sync(am, base, leader);
       const unsigned rank = __popc(am & ((1u << lane_id()) - 1u));
-      D.plastic_list[base + rank] = plastic_item{T, tt.term_c, q, 0};
+      D.plastic_list[base + rank] = plastic_item{T, svm, q, 0};
     }
   }
   // tool particles move with the tool (tool_gpu.cu:210-221); contact (:151-207)
@@ -903,10 +899,13 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
   __shared__ mf_joco_constants s_jc;
   __shared__ ksum sm[BLOCK / 32][4];
   __shared__ unsigned smc[BLOCK / 32][3];
-  __shared__ int s_chunk;
+  __shared__ int s_chunk[2];  // this chunk and the next, taken while this one runs
   __shared__ bool last;
-  if (threadIdx.x == 0) s_jc = P.joco;
-  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt);  // (its first barrier also covers s_jc)
+  if (threadIdx.x == 0) {
+    s_jc = P.joco;
+    s_chunk[0] = (int)atomicAdd(D.finish_chunk, 1u);
+  }
+  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt);  // (its first barrier also covers s_jc, s_chunk)
   else __syncthreads();
   const int stride = gridDim.x * blockDim.x;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -917,22 +916,19 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
     g = *D.g;
     for (int t = gid; t < num_scan_tiles; t += stride) D.scan_status[t] = 0ull;
   }
-  while (true) {
-    if (threadIdx.x == 0) s_chunk = (int)atomicAdd(D.finish_chunk, 1u);
-    __syncthreads();
-    const int chunk = s_chunk;
+  for (int buf = 0;; buf ^= 1) {
+    const int chunk = s_chunk[buf];
     if (chunk >= n_chunks) break;
+    // the next chunk's index: its atomic runs while this chunk is processed (every thread
+    // read s_chunk[buf ^ 1] before the previous chunk's barriers)
+    if (threadIdx.x == 0) s_chunk[buf ^ 1] = (int)atomicAdd(D.finish_chunk, 1u);
     const int q = chunk * BLOCK + threadIdx.x;
-    ksum fcx{0., 0.}, fcy{0., 0.}, ftx{0., 0.}, fty{0., 0.};
+    double2 fc = make_double2(0., 0.), ft = make_double2(0., 0.);
     if (q < P.N) {
-      double2 pos, fc, ft;
+      double2 pos;
       unsigned f;
       finish_particle(P, D, s_tool, s_jc, q, pos, f, fc, ft, newly_blanked);
       blanked_now += (f & FLAG_BLANKED) ? 1u : 0u;
-      ksum_add(fcx, fc.x);
-      ksum_add(fcy, fc.y);
-      ksum_add(ftx, ft.x);
-      ksum_add(fty, ft.y);
       if (FUSE_HASH) {  // compute_hashes of the next step (grid.cu:34-51)
         long long hh;
         if (f & FLAG_BLANKED) {
@@ -949,29 +945,46 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
         atomicAdd(&D.count[hsh], 1);
       }
     }
-    // the chunk's force sums (compensated), in a fixed tree: warps, then warps in order
-    for (int o = 16; o > 0; o >>= 1) {
-      ksum a{__shfl_down_sync(0xffffffffu, fcx.s, o), __shfl_down_sync(0xffffffffu, fcx.c, o)};
-      ksum b{__shfl_down_sync(0xffffffffu, fcy.s, o), __shfl_down_sync(0xffffffffu, fcy.c, o)};
-      ksum c{__shfl_down_sync(0xffffffffu, ftx.s, o), __shfl_down_sync(0xffffffffu, ftx.c, o)};
-      ksum d{__shfl_down_sync(0xffffffffu, fty.s, o), __shfl_down_sync(0xffffffffu, fty.c, o)};
-      ksum_merge(fcx, a); ksum_merge(fcy, b); ksum_merge(ftx, c); ksum_merge(fty, d);
+    // the chunk's force sums (compensated), in a fixed tree: warps, then warps in order. Only
+    // particles in contact carry a force; a warp or chunk whose forces are all zero has the
+    // partial {+0, +0}, which is what the sums give for zeros, so their arithmetic is skipped.
+    const bool nz = fc.x != 0. || fc.y != 0. || ft.x != 0. || ft.y != 0.;
+    if (__any_sync(0xffffffffu, nz)) {
+      ksum fcx{0., 0.}, fcy{0., 0.}, ftx{0., 0.}, fty{0., 0.};
+      ksum_add(fcx, fc.x);
+      ksum_add(fcy, fc.y);
+      ksum_add(ftx, ft.x);
+      ksum_add(fty, ft.y);
+      for (int o = 16; o > 0; o >>= 1) {
+        ksum a{__shfl_down_sync(0xffffffffu, fcx.s, o), __shfl_down_sync(0xffffffffu, fcx.c, o)};
+        ksum b{__shfl_down_sync(0xffffffffu, fcy.s, o), __shfl_down_sync(0xffffffffu, fcy.c, o)};
+        ksum c{__shfl_down_sync(0xffffffffu, ftx.s, o), __shfl_down_sync(0xffffffffu, ftx.c, o)};
+        ksum d{__shfl_down_sync(0xffffffffu, fty.s, o), __shfl_down_sync(0xffffffffu, fty.c, o)};
+        ksum_merge(fcx, a); ksum_merge(fcy, b); ksum_merge(ftx, c); ksum_merge(fty, d);
+      }
+      if (lane_id() == 0) {
+        sm[threadIdx.x >> 5][0] = fcx; sm[threadIdx.x >> 5][1] = fcy;
+        sm[threadIdx.x >> 5][2] = ftx; sm[threadIdx.x >> 5][3] = fty;
+      }
+    } else if (lane_id() == 0) {
+      const ksum z{0., 0.};
+      sm[threadIdx.x >> 5][0] = z; sm[threadIdx.x >> 5][1] = z;
+      sm[threadIdx.x >> 5][2] = z; sm[threadIdx.x >> 5][3] = z;
     }
-    if (lane_id() == 0) {
-      sm[threadIdx.x >> 5][0] = fcx; sm[threadIdx.x >> 5][1] = fcy;
-      sm[threadIdx.x >> 5][2] = ftx; sm[threadIdx.x >> 5][3] = fty;
-    }
-    __syncthreads();  // sm complete; every thread has read s_chunk
+    const bool chunk_nz = __syncthreads_or(nz);  // sm complete
     if (threadIdx.x == 0) {
-      ksum r[4] = {sm[0][0], sm[0][1], sm[0][2], sm[0][3]};
-      for (int w = 1; w < BLOCK / 32; ++w)
-        for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
+      ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
+      if (chunk_nz) {
+        for (int k = 0; k < 4; ++k) r[k] = sm[0][k];
+        for (int w = 1; w < BLOCK / 32; ++w)
+          for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
+      }
       for (int k = 0; k < 4; ++k) {
         D.partials[(size_t)chunk * 8 + 2 * k] = r[k].s;
         D.partials[(size_t)chunk * 8 + 2 * k + 1] = r[k].c;
       }
     }
-    __syncthreads();  // sm and s_chunk are reused by the next chunk
+    __syncthreads();  // sm is reused, s_chunk[buf ^ 1] is set for the next chunk
   }
   // the block's counters
   const unsigned nb = __reduce_add_sync(0xffffffffu, newly_blanked);
@@ -1030,10 +1043,11 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
   }
 }
 
-// JC radial return (actions_gpu.cu:226-285) for the particles the finish kernel listed: the
-// secant solve (plasticity.cuh:85-119), the stress scaled back to the yield surface, the
-// plastic work to heat, then the thermal boundary condition the finish kernel applied before
-// the return map had run (actions_gpu.cu:300-311).
+// JC plasticity (actions_gpu.cu:226-285) for the particles the finish kernel listed: the
+// yield test its lower bound left open, then for those that yield the secant solve
+// (plasticity.cuh:85-119), the stress scaled back to the yield surface, the plastic work to
+// heat, then the thermal boundary condition the finish kernel applied before the return map
+// had run (actions_gpu.cu:300-311).
 //
 // The list is short and its time is set by the particles whose secant needs the most
 // iterations, so the length of one iteration matters. With the Johnson-Cook law (PAIRED) two
@@ -1113,20 +1127,25 @@ static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic
     const plastic_item it = D.plastic_list[i];
     const int q = it.q;
     double T = it.T;
+    const double eps_pl = B.eps_pl[q], eps_pl_dot = B.eps_pl_dot[q];
+    // one temperature for the whole return map: its temperature-only factors once
+    const jc_temp_terms tt = jc_temperature_terms(JC, P.jc_model, T);
+    if (it.svm < sigma_yield(JC, eps_pl, eps_pl_dot, tt)) {  // elastic after all
+      if (sub == 0) B.eps_pl_dot[q] = 0.;
+      continue;
+    }
     const double4 S = B.S[q];
-    const double eps_pl = B.eps_pl[q], eps_pl_dot = B.eps_pl_dot[q], rho = B.rho[q];
+    const double rho = B.rho[q];
     const unsigned f = B.flags[q];
     const double Sxx = S.x, Syy = S.z, Szz = S.w, Sxy = S.y;
     const double norm_Strial = (double)sqrtf((float)(Sxx * Sxx + Syy * Syy + Szz * Szz + Sxy * Sxy));
     bool cap = false;
     int iters = 0;
     double delta_lambda;
-    jc_temp_terms tt;
     if (PAIRED) {
-      const secant_in in{norm_Strial, eps_pl, eps_pl_dot, it.term_c};
+      const secant_in in{norm_Strial, eps_pl, eps_pl_dot, tt.term_c};
       delta_lambda = solve_secant_pair(JC, in, dt, mu, (int)sub, pmask, cap, iters);
     } else {
-      tt = jc_temperature_terms(JC, P.jc_model, T);
       delta_lambda = solve_secant(JC, P.jc_model, fmax(eps_pl_dot * dt * sqrt(2. / 3.), 1e-8), 1e-6, norm_Strial,
                                   eps_pl, tt, dt, mu, cap, iters);
     }
@@ -1136,7 +1155,7 @@ static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic
     if (P.trml_wp.tq != 0.) {
       double sY;
       if (PAIRED) {  // sigma_yield(eps_pl_new, eps_pl_dot_new), on both lanes
-        sY = jc_yield_from(JC, pow(eps_pl_new, JC.n), jc_rate_factor(JC, eps_pl_dot_new), it.term_c);
+        sY = jc_yield_from(JC, pow(eps_pl_new, JC.n), jc_rate_factor(JC, eps_pl_dot_new), tt.term_c);
       } else {
         sY = sigma_yield(JC, eps_pl_new, eps_pl_dot_new, tt);
       }

@@ -19,16 +19,29 @@ namespace mf {
 
 // the i particle's values and the pair sums of one thread
 struct mixed_i {
-  float x, y, vx, vy, sxx, sxy, syy, Rxx, Rxy, Ryy, h, rho, c, T;
+  float x, y, sxy, Rxy, h, rho, c, T;
+  float2 nv;      // (-vx, -vy)
+  float2 s_diag;  // (sxx, syy)
+  float2 r_diag;  // (Rxx, Ryy)
   float h1, fourh2, fac;
   bool mech, thermal, nonfinite;
 };
+// Lane pairs for the packed FP32 instructions of sm_100 (two FMAs per issue). The constant
+// factors of a sum are applied once at the end: the stress and viscosity sums without the
+// mass, XSPH without mass * eps, the Brookshaw sum without its factor 2.
 struct mixed_acc {
-  float vdx, vdy, vdz, vdw, sdx, sdy, sdz, sdw, vtx, vty, xtx, xty, T_lapl;
+  float2 vd01, vd23;  // (vdx, vdy), (vdz, vdw)
+  float2 sd_xw;       // (sdx, sdw) / mass
+  float2 sd_zy;       // (sdz, sdy) / mass
+  float2 vt;          // (vtx, vty) / mass
+  float2 xt;          // (xtx, xty) / (mass * eps)
+  float T_lapl;       // / 2
 };
 struct mixed_const {
-  float mass, inv_wdeltap, alpha, beta, eta2, m_eps;
+  float inv_wdeltap, alpha, beta, eta2;
 };
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 // one neighbour j (records b0..b3) of particle i at offset (xij, yij)
 __device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_const &K, mixed_acc &a, float xij,
@@ -37,7 +50,7 @@ __device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_con
   const unsigned fjw = (unsigned)__float_as_int(b0.z);
   const float rr2 = xij * xij + yij * yij;
   const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
-  float w = 0.f, w_x = 0.f, w_y = 0.f, dwr = 0.f;
+  float w = 0.f, dwr = 0.f;
   if (in_support) {
     const float rinv = rsqrtf(rr2);
     const float qq = rr2 * rinv * I.h1;
@@ -53,41 +66,38 @@ __device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_con
     }
     w = val * I.fac;
     dwr = der * I.fac;
-    w_x = dwr * xij;
-    w_y = dwr * yij;
   }
+  const float2 pij = f2(xij, yij);
+  const float2 w_xy = __fmul2_rn(f2(dwr, dwr), pij);
   const float volj = b3.z;
   if (I.mech && !(fjw & FLAG_TOOL)) {
-    const float dvx = b0.w - I.vx, dvy = b1.x - I.vy;
-    const float ax = dvx * volj, ay = dvy * volj;
-    a.vdx += ax * w_x;
-    a.vdy += ax * w_y;
-    a.vdz += ay * w_x;
-    a.vdw += ay * w_y;
+    const float2 dv = __fadd2_rn(f2(b0.w, b1.x), I.nv);
+    const float2 av = __fmul2_rn(dv, f2(volj, volj));
+    a.vd01 = __ffma2_rn(f2(av.x, av.x), w_xy, a.vd01);
+    a.vd23 = __ffma2_rn(f2(av.y, av.y), w_xy, a.vd23);
     float fab = w * K.inv_wdeltap;
     fab *= fab;
     fab *= fab;
-    const float sxy = K.mass * (I.sxy + b1.z + fab * (I.Rxy + b2.y));
-    a.sdx += K.mass * (I.sxx + b1.y + fab * (I.Rxx + b2.x)) * w_x;
-    a.sdy += sxy * w_y;
-    a.sdz += sxy * w_x;
-    a.sdw += K.mass * (I.syy + b1.w + fab * (I.Ryy + b2.z)) * w_y;
-    const float vijposij = -(dvx * xij + dvy * yij);
-    const float irhoij = __fdividef(1.f, 0.5f * (I.rho + b3.x));
+    const float2 sd = __ffma2_rn(f2(fab, fab), __fadd2_rn(I.r_diag, f2(b2.x, b2.z)),
+                                 __fadd2_rn(I.s_diag, f2(b1.y, b1.w)));
+    const float sxy = fmaf(fab, I.Rxy + b2.y, I.sxy + b1.z);
+    a.sd_xw = __ffma2_rn(sd, w_xy, a.sd_xw);
+    a.sd_zy = __ffma2_rn(f2(sxy, sxy), w_xy, a.sd_zy);
+    const float2 dvp = __fmul2_rn(dv, pij);
+    const float vijposij = -(dvp.x + dvp.y);
+    const float irhoij = __fdividef(2.f, I.rho + b3.x);
     if (vijposij < 0.f) {
       const float cij = 0.5f * (I.c + b3.y);
       const float hij = 0.5f * (I.h + b2.w);
       const float muij = hij * vijposij * __fdividef(1.f, rr2 + K.eta2 * hij * hij);
-      const float piij = (-K.alpha * cij * muij + K.beta * muij * muij) * irhoij;
-      a.vtx -= K.mass * piij * w_x;
-      a.vty -= K.mass * piij * w_y;
+      const float npi = (K.alpha * cij * muij - K.beta * muij * muij) * irhoij;  // -pi_ij
+      a.vt = __ffma2_rn(f2(npi, npi), w_xy, a.vt);
     }
-    const float xs = K.m_eps * w * irhoij;
-    a.xtx += xs * dvx;
-    a.xty += xs * dvy;
+    const float xs = w * irhoij;
+    a.xt = __ffma2_rn(f2(xs, xs), dv, a.xt);
   }
   // Brookshaw: 2 (m/rho_j)(Ti - Tj)(e_ij . grad W)/r with (e_ij . grad W)/r = der*fac
-  if (I.thermal && rr2 > 1e-16f) a.T_lapl += 2.0f * volj * (I.T - b3.w) * dwr;
+  if (I.thermal && rr2 > 1e-16f) a.T_lapl = fmaf(volj * (I.T - b3.w), dwr, a.T_lapl);
 }
 
 // 80 registers (6 blocks of 128 per SM) keep the kernel free of spills
@@ -112,13 +122,11 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
   const float4 a3 = __ldg(r3 + q);  // rho, c, vol, T - T_init
 
   mixed_const K;
-  K.mass = (float)P.phys.mass;
   K.inv_wdeltap = (float)(1. / P.corr.wdeltap);
   K.alpha = (float)P.corr.alpha;
   K.beta = (float)P.corr.beta;
   const float eta = (float)P.corr.eta;
   K.eta2 = eta * eta;
-  K.m_eps = (float)P.corr.xspheps * K.mass;
   double thermal_alpha = 0.;
   if (brookshaw) thermal_alpha = !tool_i ? P.trml_wp.alpha : (P.thermal_tool_on ? P.trml_tool.alpha : 0.);
 
@@ -126,9 +134,9 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
   I.thermal = thermal_alpha != 0.;
   I.nonfinite = fi & FLAG_NONFINITE;
   I.mech = !tool_i;
-  I.x = a0.x; I.y = a0.y; I.vx = a0.w; I.vy = a1.x;
-  I.sxx = a1.y; I.sxy = a1.z; I.syy = a1.w;
-  I.Rxx = a2.x; I.Rxy = a2.y; I.Ryy = a2.z; I.h = a2.w;
+  I.x = a0.x; I.y = a0.y; I.nv = f2(-a0.w, -a1.x);
+  I.s_diag = f2(a1.y, a1.w); I.sxy = a1.z;
+  I.r_diag = f2(a2.x, a2.z); I.Rxy = a2.y; I.h = a2.w;
   I.rho = a3.x; I.c = a3.y; I.T = I.thermal ? a3.w : 0.f;
   I.h1 = 1.f / I.h;
   I.fourh2 = 4.f * I.h * I.h;
@@ -144,7 +152,9 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
   const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
   const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
 
-  mixed_acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  mixed_acc acc;
+  acc.vd01 = acc.vd23 = acc.sd_xw = acc.sd_zy = acc.vt = acc.xt = f2(0.f, 0.f);
+  acc.T_lapl = 0.f;
 
   for (int ii = low_i; ii < high_i; ++ii) {
     const int col = ii * g.ny;
@@ -177,9 +187,13 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
       }
     }
   }
-  const float vdx = acc.vdx, vdy = acc.vdy, vdz = acc.vdz, vdw = acc.vdw;
-  const float sdx = acc.sdx, sdy = acc.sdy, sdz = acc.sdz, sdw = acc.sdw;
-  const float vtx = acc.vtx, vty = acc.vty, xtx = acc.xtx, xty = acc.xty, T_lapl = acc.T_lapl;
+  const float mass = (float)P.phys.mass;
+  const float m_eps = (float)P.corr.xspheps * mass;
+  const float vdx = acc.vd01.x, vdy = acc.vd01.y, vdz = acc.vd23.x, vdw = acc.vd23.y;
+  const float sdx = mass * acc.sd_xw.x, sdy = mass * acc.sd_zy.y, sdz = mass * acc.sd_zy.x,
+              sdw = mass * acc.sd_xw.y;
+  const float vtx = mass * acc.vt.x, vty = mass * acc.vt.y;
+  const float xtx = m_eps * acc.xt.x, xty = m_eps * acc.xt.y, T_lapl = 2.f * acc.T_lapl;
   const bool mech_i = I.mech, thermal = I.thermal;
   const float rhoi = I.rho;
 
