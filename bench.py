@@ -185,19 +185,24 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None):
-    """Per-step CUDA-event times (ms) of mf_step(1) with the L2 flushed between steps, plus the
-    pair kernel's own duration (mf_step_stage(2) bracketed by events). With state_in the steps
-    start from a saved state of the same scene instead of its initial state."""
+def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None, flags=0):
+    """Per-step CUDA-event times (ms) of mf_step(1) with the L2 flushed between steps, then
+    a few steps run kernel by kernel (mf_step_timed, L2 flushed) for the device time of each
+    part: cell sort, predictor, interactions + rates (the pair kernel), corrector ..
+    plasticity. With neighbour lists (the mixed form) also one step that sorts and rebuilds
+    the lists, forced by a host write. With state_in the steps start from a saved state of the
+    same scene instead of its initial state."""
     ctx = mf.Context(device)
     ctx.upload_scene(scene, mf.GRID_GREEN)
     ctx.set_options(SOLVER["thermal"], mf.JC_JOHNSON_COOK, precision)
+    ctx.set_flags(flags)
     if state_in:
         load_state(mf, ctx, state_in)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=device)
     ctx.step(warmup)
     ctx.synchronize()
+    sorts0 = ctx.status()["sorts"]
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     with torch.cuda.stream(stream):
         for k in range(steps):
@@ -207,23 +212,27 @@ def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None)
             ev[k][1].record(stream)
     torch.cuda.synchronize(device)
     step_ms = np.array([a.elapsed_time(b) for a, b in ev])
-    # pair kernel alone (stage 2), a few samples, cold L2 as above
-    pair = []
+    st = ctx.status()
+    extra = {"sorts_in_timed_steps": int(st["sorts"] - sorts0)}
+    stages = []
     with torch.cuda.stream(stream):
         for _ in range(max(5, min(20, steps // 4))):
-            ctx.stage(0)
-            ctx.stage(1)
             flush.zero_()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            ctx.stage(2)
-            b.record(stream)
-            ctx.stage(3)
             torch.cuda.synchronize(device)
-            pair.append(a.elapsed_time(b))
-    st = ctx.status()
+            stages.append(ctx.step_timed())
+    stages = np.array(stages)
+    extra["stage_ms_median"] = [float(x) for x in np.median(stages, axis=0)]
+    if precision == mf.PRECISION_MIXED and not flags & mf.OPT_SORT_EVERY_STEP:
+        sort_ms = []
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                ctx.set("T", ctx.get("T"))  # a host write: the next step sorts and rebuilds the lists
+                flush.zero_()
+                torch.cuda.synchronize(device)
+                sort_ms.append(float(ctx.step_timed().sum()))
+        extra["sort_step_ms"] = float(np.median(sort_ms))
     ctx.close()
-    return step_ms, np.array(pair), st
+    return step_ms, stages[:, 2], st, extra
 
 
 E2E_FIELDS = ("pos", "vel", "h", "rho", "T", "fixed", "blanked", "tool_p", "S", "eps_pl", "eps_pl_dot", "fc", "ft",
@@ -365,9 +374,10 @@ def steps_per_mm(scene, params):
 def accuracy(mf, scene, params, steps, device):
     """Mixed against FP64 over the first `steps` steps of the cut, both from the same state."""
     f64, s64, _, _ = run_form(mf, scene, mf.PRECISION_FP64, steps, device)
-    fm, sm, _, _ = run_form(mf, scene, mf.PRECISION_MIXED, steps, device)
+    fm, sm, _, stm = run_form(mf, scene, mf.PRECISION_MIXED, steps, device)
     out = {"steps": steps, "tool_travel_um": steps * scene.s.dt * params.speed * 1e4,
-           "against": "the FP64 form (single steps equal to the oracle to 1e-12) from the same initial state"}
+           "against": "the FP64 form (single steps equal to the oracle to 1e-12) from the same initial state",
+           "mixed_sorts": int(stm["sorts"]), "mixed_error_flags": int(stm["error_flags"])}
     out.update(form_errors(scene, (f64, s64), (fm, sm)))
     return out
 
@@ -602,6 +612,9 @@ def main():
     ap.add_argument("--state-in", default=None,
                     help="time both forms from this saved state of the same scene (e.g. mid-cut) "
                          "instead of the initial state")
+    ap.add_argument("--forms", default="fp64,mixed_sort_every_step,mixed",
+                    help="comma-separated forms to time (all three for the benchmark line; one, e.g. "
+                         "'mixed', for a profiling run)")
     ap.add_argument("--lattice-scale", type=float, default=1.0,
                     help="lattice points per dimension relative to 714 x 214 (same 2.0 x 0.6 mm body); "
                          "values below 1 give the smaller profiling case")
@@ -644,21 +657,42 @@ def main():
 
     results = {}
     clocks = None
-    for name, prec in (("fp64", mf.PRECISION_FP64), ("mixed", mf.PRECISION_MIXED)):
+    forms = [f for f in (("fp64", mf.PRECISION_FP64, 0),
+                         ("mixed_sort_every_step", mf.PRECISION_MIXED, mf.OPT_SORT_EVERY_STEP),
+                         ("mixed", mf.PRECISION_MIXED, 0)) if f[0] in args.forms.split(",")]
+    for name, prec, flags in forms:
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize(device)
         with ClockSampler(device) as cs:
-            step_ms, pair_ms, st = time_form(mf, torch, scene, prec, args.steps, args.warmup, device,
-                                             args.state_in)
+            step_ms, pair_ms, st, extra = time_form(mf, torch, scene, prec, args.steps, args.warmup, device,
+                                                    args.state_in, flags)
         if name == "mixed":
             clocks = cs.summary()
         total_ms = max_over_ranks(float(step_ms.sum()), world, device=f"cuda:{device}")
-        particles = sum_over_ranks(float(N), world, device=f"cuda:{device}")
-        value = particles * args.steps / (total_ms * 1e-3)
-        pair_mean = float(pair_ms.mean())
-        results[name] = {"value": value, "ms_per_step": total_ms / args.steps,
-                         "pair_kernel_ms": pair_mean, "status": st}
+        results[name] = {"ms_per_step": total_ms / args.steps, "pair_kernel_ms": float(np.median(pair_ms)),
+                         "status": st, **extra}
+    if set(results) != {"fp64", "mixed_sort_every_step", "mixed"}:  # a profiling run: no benchmark line
+        if rank == 0:
+            print(json.dumps({"forms": {f: {k: v for k, v in r.items() if k != "status"}
+                                        for f, r in results.items()}}), flush=True)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+    acc = None
+    if rank == 0 and args.accuracy_steps > 0:
+        acc = accuracy(mf, scene, params, args.accuracy_steps, device)
+    # neighbour lists: the timed steps may hold fewer sorts than a long run; charge each step
+    # its share of a sorting step's extra time, at the long run's steps per sort
+    mx = results["mixed"]
+    steps_per_sort = (acc["steps"] / max(acc["mixed_sorts"], 1) if acc else
+                      (args.steps + args.warmup) / max(mx["status"]["sorts"], 1))
+    mx["steps_per_sort"] = steps_per_sort
+    mx["timed_ms_per_step"] = mx["ms_per_step"]
+    mx["ms_per_step"] = mx["timed_ms_per_step"] + max(0.0, mx["sort_step_ms"] - mx["timed_ms_per_step"]) / steps_per_sort
+    particles = sum_over_ranks(float(N), world, device=f"cuda:{device}")
+    for name, r in results.items():
+        r["value"] = particles / (r["ms_per_step"] * 1e-3)
     # roofline of the dominant kernel (the pair kernel) on the canonical per-particle bytes
     peaks_file = ROOT / "MEASURED_PEAKS.json"
     if peaks_file.exists():
@@ -682,9 +716,6 @@ def main():
                "what": "state in from pinned host memory, per step mf_step(1) + tool force to pinned host "
                        "memory, final state out; wall clock"}
     fp64_probe = mf.probe_fp64(device) if rank == 0 else None
-    acc = None
-    if rank == 0 and args.accuracy_steps > 0:
-        acc = accuracy(mf, scene, params, args.accuracy_steps, device)
     spm = steps_per_mm(scene, params)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -702,13 +733,16 @@ def main():
                            start_state=(f"saved state {args.state_in}" if args.state_in else "initial scene"),
                            parallelism=f"replicas x{world}", l2="flushed between timed steps (256 MiB write)",
                            global_particles=N * world),
-            "forms": {"fp64": {"value": results["fp64"]["value"], "ms_per_step": results["fp64"]["ms_per_step"],
-                               "pair_kernel_ms": results["fp64"]["pair_kernel_ms"]},
-                      "mixed": {"value": results["mixed"]["value"], "ms_per_step": results["mixed"]["ms_per_step"],
-                                "pair_kernel_ms": results["mixed"]["pair_kernel_ms"]},
-                      "mixed_over_fp64": results["mixed"]["value"] / results["fp64"]["value"],
-                      "wall_s_per_mm_cut": {f: results[f]["ms_per_step"] * 1e-3 * spm for f in ("fp64", "mixed")},
-                      "steps_per_mm_cut": spm},
+            "forms": dict(
+                {f: {k: v for k, v in r.items() if k != "status"} for f, r in results.items()},
+                mixed_over_fp64=results["mixed"]["value"] / results["fp64"]["value"],
+                mixed_sort_every_step_over_fp64=results["mixed_sort_every_step"]["value"] / results["fp64"]["value"],
+                wall_s_per_mm_cut={f: r["ms_per_step"] * 1e-3 * spm for f, r in results.items()},
+                steps_per_mm_cut=spm,
+                note="mixed: neighbour lists between sorts (ms_per_step = timed steps + each step's share of a "
+                     "sorting step's extra time at steps_per_sort); mixed_sort_every_step: the same FP32 pair "
+                     "sums with the cell list sorted every step, as the FP64 form does; pair_kernel_ms: median "
+                     "of steps launched kernel by kernel (mf_step_timed) after an L2 flush"),
             "mixed_error": acc,
             "fp64_probe": fp64_probe,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

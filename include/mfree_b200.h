@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-#define MF_ABI_VERSION 1
+#define MF_ABI_VERSION 2
 
 /* ---- status codes ---- */
 #define MF_OK 0
@@ -75,6 +75,8 @@ extern "C" {
 /* option bits for mf_set_flags */
 #define MF_OPT_KEEP_DERIVATIVES 1 /* also store S_der / v_der (the reference's public arrays) */
 #define MF_OPT_NO_GRAPHS 2        /* launch kernels directly instead of replaying CUDA graphs */
+#define MF_OPT_SORT_EVERY_STEP 4  /* mixed form: sort the cell list every step (as the FP64 form
+                                     does) instead of keeping neighbour lists between sorts */
 
 /* ---- constants (constants_structs.h:25-82), same member order ---- */
 typedef struct { double E, nu, rho0, K, G, mass, mass_tool; } mf_phys_constants;
@@ -111,8 +113,13 @@ typedef struct {
   long long out_of_grid;      /* hashes outside [0, num_cell) clamped since creation */
   long long secant_cap_hits;  /* JC secant solves that hit the iteration cap */
   int max_cell_occupancy;     /* largest particles-per-cell seen in the last sort */
-  int error_flags;            /* bit 0: a bounded wait in the cell scan expired */
+  int error_flags;            /* bit 0: a bounded wait in the cell scan expired; bit 1: the
+                                 adaptive grid outgrew max_cell; bit 2: a neighbour list was
+                                 full (neighbours dropped); bit 3: a particle moved more than
+                                 half the neighbour-list skin between two sorts (a guard) */
   long long secant_iterations; /* JC secant iterations since creation (cost diagnostic) */
+  long long sorts;            /* cell-list sorts since creation (one per step, except for the
+                                 mixed form with neighbour lists) */
 } mf_status;
 
 typedef struct mf_ctx mf_ctx;
@@ -125,6 +132,11 @@ int mf_ctx_create(int device, mf_ctx **out);
 int mf_ctx_destroy(mf_ctx *ctx);
 int mf_ctx_stream(mf_ctx *ctx, void **cuda_stream);   /* the stream all work is queued on */
 int mf_set_flags(mf_ctx *ctx, int flags);
+/* Skin of the mixed form's neighbour lists (a length; <= 0 restores the default, a tenth of
+   the cell size): each particle lists its candidates within 2 h + skin, and the cell list is
+   sorted again on the steps where some particle would otherwise be more than 0.45 skin from
+   where its list was built. No counterpart in the reference, which sorts every step. */
+int mf_set_neighbour_skin(mf_ctx *ctx, double skin);
 int mf_synchronize(mf_ctx *ctx);
 
 /* ---- particles: particle_gpu(...) constructors (particle_gpu.h:81-86, particle_gpu.cu:97-125).
@@ -170,6 +182,11 @@ int mf_tool_get(mf_ctx *ctx, mf_tool_state *tool);
 
 /* ---- stepping: leap_frog::step (leap_frog.cu:94-155), n times, queued asynchronously ---- */
 int mf_step(mf_ctx *ctx, int n_steps);
+/* One step, launched kernel by kernel (no graph) with CUDA events between its four parts
+   (the cell sort, predictor, interactions + rates, corrector .. plasticity); their durations
+   in stage_ms[4], in milliseconds. Synchronizes the context's stream. For timing only: the
+   step is the same as one of mf_step. No counterpart in the reference. */
+int mf_step_timed(mf_ctx *ctx, float *stage_ms);
 /* parts of one step, for parity tests: 0 grid (sort), 1 predictor (init, predict, eos,
    artificial stress), 2 interactions + rates, 3 corrector .. invalidate. */
 int mf_step_stage(mf_ctx *ctx, int stage);

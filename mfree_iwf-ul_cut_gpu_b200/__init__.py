@@ -24,7 +24,7 @@ GRID_GREEN, GRID_ROTHLIN = 0, 1
 THERMAL_BROOKSHAW, THERMAL_PSE = 0, 1
 JC_JOHNSON_COOK, JC_TANH = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-OPT_KEEP_DERIVATIVES, OPT_NO_GRAPHS = 1, 2
+OPT_KEEP_DERIVATIVES, OPT_NO_GRAPHS, OPT_SORT_EVERY_STEP = 1, 2, 4
 
 # name -> (field id, doubles per particle, is_int)
 FIELDS = {
@@ -86,7 +86,8 @@ class ToolState(C.Structure):
 class Status(C.Structure):
     _fields_ = [("steps", C.c_longlong), ("blanked", C.c_longlong), ("newly_blanked", C.c_longlong),
                 ("out_of_grid", C.c_longlong), ("secant_cap_hits", C.c_longlong),
-                ("max_cell_occupancy", C.c_int), ("error_flags", C.c_int), ("secant_iterations", C.c_longlong)]
+                ("max_cell_occupancy", C.c_int), ("error_flags", C.c_int), ("secant_iterations", C.c_longlong),
+                ("sorts", C.c_longlong)]
 
 
 _dp = C.POINTER(C.c_double)
@@ -127,7 +128,7 @@ def lib():
     sig = {
         "mf_version": ([], i), "mf_error_string": ([i], C.c_char_p), "mf_last_cuda_error": ([vp], i),
         "mf_ctx_create": ([i, C.POINTER(vp)], i), "mf_ctx_destroy": ([vp], i),
-        "mf_ctx_stream": ([vp, C.POINTER(vp)], i), "mf_set_flags": ([vp, i], i), "mf_synchronize": ([vp], i),
+        "mf_ctx_stream": ([vp, C.POINTER(vp)], i), "mf_set_flags": ([vp, i], i), "mf_set_neighbour_skin": ([vp, C.c_double], i), "mf_synchronize": ([vp], i),
         "mf_particles_create": ([vp, i] + [vp] * 8, i), "mf_particles_count": ([vp, ip], i),
         "mf_get_field": ([vp, i, vp], i), "mf_set_field": ([vp, i, vp], i),
         "mf_grid_create_locked": ([vp, i, d, d, d, d, d], i), "mf_grid_create_adaptive": ([vp, i, i], i),
@@ -137,7 +138,7 @@ def lib():
                               C.POINTER(Trml)], i),
         "mf_set_options": ([vp, i, i, i], i), "mf_set_dt": ([vp, d], i),
         "mf_tool_set": ([vp, C.POINTER(ToolState)], i), "mf_tool_get": ([vp, C.POINTER(ToolState)], i),
-        "mf_step": ([vp, i], i), "mf_step_stage": ([vp, i], i), "mf_report_force": ([vp, vp], i),
+        "mf_step": ([vp, i], i), "mf_step_timed": ([vp, vp], i), "mf_step_stage": ([vp, i], i), "mf_report_force": ([vp, vp], i),
         "mf_probe_fp64": ([i, vp, vp, vp, vp, vp], i),
         "mf_tangent_mean_force": ([vp, i, i, i, vp, vp], i),
         "mf_tool_wear_usui": ([vp, d, d, vp], i), "mf_vtk_write_particles_async": ([vp, C.c_char_p], i),
@@ -367,6 +368,10 @@ class Context:
     def set_flags(self, flags):
         self._check(self.L.mf_set_flags(self.h, flags), "mf_set_flags")
 
+    def set_neighbour_skin(self, skin):
+        """Mixed form: skin of the neighbour lists (<= 0: a tenth of the cell size)."""
+        self._check(self.L.mf_set_neighbour_skin(self.h, float(skin)), "mf_set_neighbour_skin")
+
     def set_dt(self, dt):
         self._check(self.L.mf_set_dt(self.h, dt), "mf_set_dt")
 
@@ -385,6 +390,13 @@ class Context:
     # stepping ----------------------------------------------------------------------------
     def step(self, n=1):
         self._check(self.L.mf_step(self.h, n), "mf_step")
+
+    def step_timed(self):
+        """One step kernel by kernel; the device time (ms) of its four parts: cell sort,
+        predictor, interactions + rates, corrector .. plasticity."""
+        out = (C.c_float * 4)()
+        self._check(self.L.mf_step_timed(self.h, C.cast(out, C.c_void_p)), "mf_step_timed")
+        return np.array(out[:], dtype=np.float64)
 
     def stage(self, k):
         self._check(self.L.mf_step_stage(self.h, k), "mf_step_stage")

@@ -69,6 +69,7 @@ struct mf_ctx {
   // k_finish of the last step already hashed and counted the particles for the next one
   // (locked grid): the next step starts at the scan
   bool counts_ready = false;
+  double skin = 0.;  // neighbour-list skin (mixed form); <= 0: a tenth of the cell size
   std::vector<void *> particle_allocs, grid_allocs, fixed_allocs;
   // graphs: one per parity of the double buffer
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -170,6 +171,9 @@ int alloc_particles(mf_ctx *ctx, int N) {
   TRY(dalloc(ctx, L, &D.perm_u, N));
   TRY(dalloc(ctx, L, &D.perm, N));
   TRY(dalloc(ctx, L, &D.plastic_list, N));
+  TRY(dalloc(ctx, L, &D.nlist, (size_t)LIST_CAP * N));
+  TRY(dalloc(ctx, L, &D.ncount, N));
+  TRY(dalloc(ctx, L, &D.pos_build, N));
   ctx->finish_blocks = std::min((N + BLOCK - 1) / BLOCK, ctx->sm_count * FINISH_BLOCKS_PER_SM);
   ctx->bbox_blocks = std::min((N + BLOCK - 1) / BLOCK, ctx->sm_count * 4);
   // per-chunk force partials of the finish kernel (or per-block partials of the bbox pass)
@@ -211,6 +215,20 @@ bool fused_step(const mf_ctx *ctx) { return ctx->G.locked && !ctx->P.staged; }
 
 bool ready(const mf_ctx *ctx) { return ctx->has_particles && ctx->has_grid && ctx->has_constants; }
 
+// Neighbour lists for the mixed form (steps on a locked grid): its pair sums are not tied to
+// the reference's summation order, so the cell list need not be sorted every step. Not with
+// the PSE solver, whose window has no support cut-off, nor when asked to sort every step.
+bool list_mode(const mf_ctx *ctx) {
+  return ctx->P.precision == MF_PRECISION_MIXED && fused_step(ctx) && !(ctx->flags & MF_OPT_SORT_EVERY_STEP) &&
+         !(ctx->P.thermal_solver == MF_THERMAL_PSE && ctx->P.thermal_wp) &&
+         (long long)ctx->N <= (long long)LIST_INDEX_MASK + 1;
+}
+
+void set_list_mode(mf_ctx *ctx) {
+  ctx->P.verlet = list_mode(ctx) ? 1 : 0;
+  ctx->P.skin = (float)(ctx->skin > 0. ? ctx->skin : 0.1 * ctx->G.dx);
+}
+
 #ifndef MF_USE_PDL
 #define MF_USE_PDL 1
 #endif
@@ -249,8 +267,9 @@ int launch_cells(mf_ctx *ctx, bool step_mode) {
     const int hash_blocks = std::max(nb, (ctx->scan_tiles + BLOCK - 1) / BLOCK);
     TRY(launch_pdl(ctx, k_hash_count, hash_blocks, BLOCK, N, ctx->D.A, ctx->D, ctx->scan_tiles));
   }
-  TRY(launch_pdl(ctx, k_scan, ctx->scan_tiles, SCAN_THREADS, ctx->D, N));
-  TRY(launch_pdl(ctx, k_scatter, nb, BLOCK, N, ctx->D));
+  const int verlet = step_mode ? ctx->P.verlet : 0;  // a sort outside a step always sorts
+  TRY(launch_pdl(ctx, k_scan, ctx->scan_tiles, SCAN_THREADS, ctx->D, N, verlet));
+  TRY(launch_pdl(ctx, k_scatter, nb, BLOCK, N, ctx->D, verlet));
   return MF_OK;
 }
 
@@ -259,6 +278,7 @@ int launch_stage(mf_ctx *ctx, int stage) {
   const int nb = (N + BLOCK - 1) / BLOCK;
   const int npb = (N + PAIR_BLOCK - 1) / PAIR_BLOCK;
   bind_sets(ctx);
+  set_list_mode(ctx);
   const bool mixed = ctx->P.precision == MF_PRECISION_MIXED;
   switch (stage) {
     case 0:
@@ -269,7 +289,8 @@ int launch_stage(mf_ctx *ctx, int stage) {
       else TRY(launch_pdl(ctx, k_reorder<true, false>, nb, BLOCK, ctx->P, ctx->D));
       break;
     case 2:
-      if (mixed) TRY(launch_pdl(ctx, k_pair_mixed, npb, PAIR_BLOCK, ctx->P, ctx->D));
+      if (mixed && ctx->P.verlet) TRY(launch_pdl(ctx, k_pair_mixed<true>, npb, PAIR_BLOCK, ctx->P, ctx->D));
+      else if (mixed) TRY(launch_pdl(ctx, k_pair_mixed<false>, npb, PAIR_BLOCK, ctx->P, ctx->D));
       else TRY(launch_pdl(ctx, k_pair_fp64, npb, PAIR_BLOCK, ctx->P, ctx->D));
       if (ctx->P.thermal_solver == MF_THERMAL_PSE && ctx->P.thermal_wp) {
         if (mixed) TRY(launch_pdl(ctx, k_pse_mixed, npb, PAIR_BLOCK, ctx->P, ctx->D));
@@ -308,6 +329,8 @@ int prime_counts(mf_ctx *ctx) {
   k_hash_count<<<hash_blocks, BLOCK, 0, ctx->stream>>>(ctx->N, ctx->D.A, ctx->D, ctx->scan_tiles);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) { ctx->last_cuda_err = (int)e; return MF_ERR_CUDA; }
+  // with neighbour lists the next step sorts (and builds the lists): any nonzero value
+  CK(cudaMemsetAsync(&ctx->D.st->sort_now, 1, sizeof(unsigned), ctx->stream));
   ctx->counts_ready = true;
   return MF_OK;
 }
@@ -471,6 +494,13 @@ int mf_set_flags(mf_ctx *ctx, int flags) {
   ctx->flags = flags;
   ctx->P.keep_derivs = (flags & MF_OPT_KEEP_DERIVATIVES) ? 1 : 0;
   drop_graphs(ctx);
+  return MF_OK;
+}
+
+int mf_set_neighbour_skin(mf_ctx *ctx, double skin) {
+  if (!ctx || !(skin == skin)) return MF_ERR_INVALID;
+  ctx->skin = skin;
+  drop_graphs(ctx);  // the skin is a kernel parameter
   return MF_OK;
 }
 
@@ -667,7 +697,9 @@ int mf_grid_build(mf_ctx *ctx) {
   TRY(invalidate_counts(ctx));
   TRY(launch_cells(ctx, false));
   const int nb = (ctx->N + BLOCK - 1) / BLOCK;
-  k_reorder<false, false><<<nb, BLOCK, 0, ctx->stream>>>(ctx->P, ctx->D);
+  params Pg = ctx->P;
+  Pg.verlet = 0;  // a sort outside a step always sorts
+  k_reorder<false, false><<<nb, BLOCK, 0, ctx->stream>>>(Pg, ctx->D);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) { ctx->last_cuda_err = (int)e; return MF_ERR_CUDA; }
   ctx->cur ^= 1;
@@ -803,6 +835,35 @@ int mf_step(mf_ctx *ctx, int n_steps) {
     ctx->cur ^= 1;
     ctx->steps++;
   }
+  return MF_OK;
+}
+
+int mf_step_timed(mf_ctx *ctx, float *stage_ms) {
+  if (!ctx || !stage_ms) return MF_ERR_INVALID;
+  if (!ready(ctx)) return MF_ERR_STATE;
+  if (!(ctx->P.dt > 0.) || ctx->mid_step) return MF_ERR_STATE;
+  TRY(set_device(ctx));
+  ctx->P.N = ctx->N;
+  ctx->last_staged = false;
+  TRY(prime_counts(ctx));
+  cudaEvent_t ev[5] = {};
+  int rc = MF_OK;
+  for (int k = 0; k < 5 && rc == MF_OK; ++k)
+    if (cudaEventCreate(&ev[k]) != cudaSuccess) rc = MF_ERR_CUDA;
+  for (int s = 0; s < 4 && rc == MF_OK; ++s) {
+    if (cudaEventRecord(ev[s], ctx->stream) != cudaSuccess) rc = MF_ERR_CUDA;
+    if (rc == MF_OK) rc = launch_stage(ctx, s);
+  }
+  if (rc == MF_OK && cudaEventRecord(ev[4], ctx->stream) != cudaSuccess) rc = MF_ERR_CUDA;
+  if (rc == MF_OK && cudaEventSynchronize(ev[4]) != cudaSuccess) rc = MF_ERR_CUDA;
+  for (int s = 0; s < 4 && rc == MF_OK; ++s)
+    if (cudaEventElapsedTime(&stage_ms[s], ev[s], ev[s + 1]) != cudaSuccess) rc = MF_ERR_CUDA;
+  for (int k = 0; k < 5; ++k)
+    if (ev[k]) cudaEventDestroy(ev[k]);
+  if (rc == MF_ERR_CUDA) ctx->last_cuda_err = (int)cudaGetLastError();
+  if (rc != MF_OK) return rc;
+  ctx->cur ^= 1;
+  ctx->steps++;
   return MF_OK;
 }
 
@@ -1104,6 +1165,7 @@ int mf_status_get(mf_ctx *ctx, mf_status *out) {
   out->max_cell_occupancy = st.max_cell_occupancy;
   out->error_flags = st.error_flags;
   out->secant_iterations = (long long)st.secant_iterations;
+  out->sorts = (long long)st.sorts;
   return MF_OK;
 }
 

@@ -43,6 +43,11 @@ struct params {
   int plastic, fric_heat, thermal_bc, thermal_wp, thermal_tool_on, has_tool, keep_derivs;
   int staged;  // step run stage by stage (mf_step_stage): keep every intermediate array
   int jc_lower_bound;  // A > 0, B >= 0, C >= 0: the yield stress is bounded below by A (1 - theta^m)
+  // mixed form with neighbour lists: the cell list is sorted only on steps where some
+  // particle's predicted position is more than 0.45 skin from where its list was built; in
+  // between, each particle's candidates within 2 h + skin are kept in a list
+  int verlet;
+  float skin;
   double dt;
   mf_phys_constants phys;
   mf_corr_constants corr;
@@ -70,11 +75,23 @@ struct dev_status {
   unsigned int scan_tile_counter;
   unsigned long long force_log_head;
   unsigned long long secant_iterations;
+  unsigned long long sorts;  // cell-list sorts (every step, except with neighbour lists)
+  unsigned int sort_now;     // neighbour lists: this step sorts (set by the previous step)
+  unsigned int want_sort;    // neighbour lists: a particle's next predicted position is more
+                             // than 0.45 skin from where its list was built
 };
 
 constexpr int FORCE_LOG_CAP = 1 << 16;
 constexpr int ERR_SCAN_WAIT = 1;
 constexpr int ERR_GRID_BUDGET = 2;
+constexpr int ERR_LIST_OVERFLOW = 4;  // a neighbour list was full: neighbours were dropped
+constexpr int ERR_SKIN = 8;           // a particle moved more than skin / 2 on one list (guard)
+
+// neighbour list entry: particle index in the low LIST_INDEX_BITS bits, above them the
+// column offset of the pair's cells (i's column - j's column) + 3, in [0, 6]
+constexpr int LIST_CAP = 64;
+constexpr int LIST_INDEX_BITS = 26;
+constexpr unsigned LIST_INDEX_MASK = (1u << LIST_INDEX_BITS) - 1u;
 
 // ---------------------------------------------------------------------------------------
 // SPH kernel function: cubic spline (kernels.cuh:30-70). hi enters through h1 = 1/hi and

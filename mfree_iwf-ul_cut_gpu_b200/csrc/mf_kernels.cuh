@@ -65,6 +65,11 @@ struct dev_buffers {
   plastic_item *plastic_list;  // particles whose return map k_plastic runs (this step)
   unsigned *plastic_count;
   unsigned *finish_chunk;     // next chunk of the finish kernel (zeroed by the reorder)
+  // neighbour lists (mixed form): entry k of particle q at nlist[q * LIST_CAP + k], ncount[q]
+  // entries; pos_build[q] the predicted position the list was built from
+  unsigned *nlist;
+  int *ncount;
+  double2 *pos_build;
   mf_tool_state *tool_prev;  // tool after the previous step (read)
   mf_tool_state *tool_next;  // tool after this step (written by k_finish)
   geom *g;
@@ -193,9 +198,18 @@ static __global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A,
 // exclusive scan of the cell counts -> offsets, single pass with decoupled look-back.
 // Tile ids come from an atomic ticket, so every tile waits only on tiles that are already
 // running; the wait is bounded and reports ERR_SCAN_WAIT instead of hanging.
-static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int N) {
+static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int N, int verlet) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
+  if (verlet && !D.st->sort_now) {
+    // neighbour lists, no sort this step: the counts the finish kernel made go unused; back
+    // to zero for the next step's (block b clears tile b; the grid has a block per tile)
+    const int num_cell = D.g->num_cell;
+    for (int c = blockIdx.x * SCAN_TILE + threadIdx.x; c < min(num_cell, (blockIdx.x + 1) * SCAN_TILE);
+         c += SCAN_THREADS)
+      D.count[c] = 0;
+    return;
+  }
   __shared__ int s_tile;
   __shared__ int s_warp[SCAN_THREADS / 32];
   __shared__ int s_excl;
@@ -321,11 +335,12 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int
   (void)N;
 }
 
-static __global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D) {
+static __global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D, int verlet) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= N) return;
+  if (verlet && !D.st->sort_now) return;  // neighbour lists, no sort this step
   const int c = D.hash_new[q];
   const int s = D.off[c];
   // the scan left the counts at zero: they serve as per-cell cursors here (the reorder
@@ -361,19 +376,29 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
   MF_PDL_TRIGGER();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
+  // with neighbour lists, a step without a sort keeps the order and the cells of the last
+  // sort: the identity permutation
+  const bool sort = !P.verlet || D.st->sort_now;
   if (q == 0) {  // re-armed for the finish kernel of this step
     *D.plastic_count = 0u;
     *D.finish_chunk = 0u;
+    if (sort) D.st->sorts += 1ull;
   }
-  const int4 u = D.perm_u[q];
-  const int p = stable_member(D, q, u), hsh = u.y;
-  if (q == u.z) D.count[hsh] = 0;  // the scatter's cursor, back to zero for the next counts
+  int p = q, hsh;
+  if (sort) {
+    const int4 u = D.perm_u[q];
+    p = stable_member(D, q, u);
+    hsh = u.y;
+    if (q == u.z) D.count[hsh] = 0;  // the scatter's cursor, back to zero for the next counts
+    D.hash_cur[q] = hsh;
+  } else {
+    hsh = D.hash_cur[q];
+  }
   const state_set &A = D.A;
   const state_set &B = D.B;
   D.perm[q] = p;
   B.idx[q] = P.grid_kind == MF_GRID_GREEN ? p : A.idx[p];
   B.id[q] = A.id[p];
-  D.hash_cur[q] = hsh;
 
   double2 pos = A.pos[p], vel = A.vel[p];
   double4 S = A.S[p];
@@ -480,6 +505,20 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
 #pragma unroll
     for (int k = 0; k < F_WIDTH / 4; ++k)
       fd[(size_t)k * P.N + q] = make_float4(fr[4 * k], fr[4 * k + 1], fr[4 * k + 2], fr[4 * k + 3]);
+    if (P.verlet) {
+      // the lists stay valid while every particle is within skin / 2 of where it was at the
+      // last sort (then every pair closer than 2 h was closer than 2 h + skin there); the
+      // previous step's finish kernel checked this step's predicted positions against
+      // 0.45 skin and asked for a sort where needed, so the test below is a guard
+      if (sort) {
+        D.pos_build[q] = pos;
+      } else if (!blanked && !(rf & FLAG_NONFINITE)) {  // (non-finite ones are blanked this step)
+        const double2 pb = D.pos_build[q];
+        const double ddx = pos.x - pb.x, ddy = pos.y - pb.y;
+        const double half = 0.5 * (double)P.skin;
+        if (ddx * ddx + ddy * ddy > half * half) atomicOr(&D.st->error_flags, ERR_SKIN);
+      }
+    }
   }
 }
 
@@ -726,7 +765,7 @@ __device__ __forceinline__ void tool_advance_shared(mf_tool_state &T, const dev_
 __device__ __forceinline__ void finish_particle(const params &P, const dev_buffers &D, const mf_tool_state &TL,
                                                const mf_joco_constants &JC, int q,
                                                double2 &pos_out, unsigned &f_out, double2 &fc_out, double2 &ft_out,
-                                               unsigned &newly_blanked) {
+                                               unsigned &newly_blanked, bool &want_sort) {
   const state_set &A = D.A;
   const state_set &B = D.B;
   const double dt = P.dt;
@@ -867,6 +906,16 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
       B.flags[q] = f;
     }
   }
+  // neighbour lists: the next step's predictor moves the particle to pos + dt/2 pos_t
+  // (leap_frog.cu:30-66); a sort is asked for when that is more than 0.45 skin from where its
+  // list was built (the lists hold while every particle stays within skin / 2)
+  if (P.verlet && !(f & FLAG_BLANKED)) {
+    const double2 pb = D.pos_build[q];
+    const double px = pos.x + 0.5 * dt * pos_t.x, py = pos.y + 0.5 * dt * pos_t.y;
+    const double ddx = px - pb.x, ddy = py - pb.y;
+    const double lim = 0.45 * (double)P.skin;
+    if (!(ddx * ddx + ddy * ddy <= lim * lim)) want_sort = true;
+  }
   B.pos[q] = pos;
   B.vel[q] = vel;
   B.S[q] = S;
@@ -911,6 +960,7 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   const int n_chunks = (P.N + BLOCK - 1) / BLOCK;
   unsigned newly_blanked = 0, blanked_now = 0, oog = 0;
+  bool want_sort = false;
   geom g{};
   if (FUSE_HASH) {
     g = *D.g;
@@ -927,7 +977,7 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
     if (q < P.N) {
       double2 pos;
       unsigned f;
-      finish_particle(P, D, s_tool, s_jc, q, pos, f, fc, ft, newly_blanked);
+      finish_particle(P, D, s_tool, s_jc, q, pos, f, fc, ft, newly_blanked, want_sort);
       blanked_now += (f & FLAG_BLANKED) ? 1u : 0u;
       if (FUSE_HASH) {  // compute_hashes of the next step (grid.cu:34-51)
         long long hh;
@@ -993,11 +1043,14 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
   if (lane_id() == 0) {
     smc[threadIdx.x >> 5][0] = nb; smc[threadIdx.x >> 5][1] = nbl; smc[threadIdx.x >> 5][2] = noog;
   }
-  __syncthreads();
+  // with neighbour lists the hashes and counts above serve the next step only if it sorts,
+  // which is known once every particle has been checked (last block, below)
+  const bool block_wants_sort = __syncthreads_or(want_sort);
   if (threadIdx.x == 0) {
     unsigned long long cnt[3] = {smc[0][0], smc[0][1], smc[0][2]};
     for (int w = 1; w < BLOCK / 32; ++w)
       for (int k = 0; k < 3; ++k) cnt[k] += smc[w][k];
+    if (block_wants_sort) D.st->want_sort = 1u;  // (before the fence and the ticket below)
     if (cnt[0]) atomicAdd(&D.st->newly_blanked, cnt[0]);
     if (cnt[1]) atomicAdd(&D.st->blanked, cnt[1]);
     if (cnt[2]) atomicAdd(&D.st->out_of_grid, cnt[2]);
@@ -1039,6 +1092,10 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
     D.force_log[2 * (hd % FORCE_LOG_CAP) + 1] = Fy;
     D.st->force_log_head = hd + 1;
     D.st->steps += 1;
+    if (P.verlet) {  // every particle is checked: the next step sorts if one asked for it
+      D.st->sort_now = D.st->want_sort;
+      D.st->want_sort = 0u;
+    }
     D.ticket[0] = 0u;
   }
 }

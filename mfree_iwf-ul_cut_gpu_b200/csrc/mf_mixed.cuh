@@ -100,7 +100,51 @@ __device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_con
   if (I.thermal && rr2 > 1e-16f) a.T_lapl = fmaf(volj * (I.T - b3.w), dwr, a.T_lapl);
 }
 
-// 80 registers (6 blocks of 128 per SM) keep the kernel free of spills
+// Neighbour list of particle q, built on a step that sorted: the candidates within
+// 2 h_i + skin over the 7x7 cells around its own (the 5x5 window widened by one cell, which
+// covers that radius for h_i up to the cell size), blanked ones left out, non-finite ones
+// kept (their pair terms carry the NaN). Columns in x order and each column's range in array
+// order, so the in-support candidates come in the order of the 5x5 window.
+__device__ __forceinline__ int build_list(const dev_buffers &D, const float4 *__restrict__ r0, int q,
+                                          const mixed_i &I, const geom &g, int gi, int gj, float dxc,
+                                          float skin) {
+  const float R = 2.f * I.h + skin;
+  const float R2 = R * R;
+  const int low_i = gi - 3 < 0 ? 0 : gi - 3;
+  const int low_j = gj - 3 < 0 ? 0 : gj - 3;
+  const int high_i = gi + 4 > g.nx ? g.nx : gi + 4;
+  const int high_j = gj + 4 > g.ny ? g.ny : gj + 4;
+  unsigned *row = D.nlist + (size_t)q * LIST_CAP;
+  int cnt = 0;
+  for (int ii = low_i; ii < high_i; ++ii) {
+    const int col = ii * g.ny;
+    const int j0 = __ldg(D.off + col + low_j);
+    const int j1 = __ldg(D.off + col + high_j);
+    const float ox = (float)(gi - ii) * dxc + I.x;
+    const unsigned tag = (unsigned)(gi - ii + 3) << LIST_INDEX_BITS;
+    for (int j = j0; j < j1; ++j) {
+      const float4 b0 = __ldg(r0 + j);
+      const unsigned fjw = (unsigned)__float_as_int(b0.z);
+      const float xij = ox - b0.x;
+      const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
+      const float rr2 = xij * xij + yij * yij;
+      if (!(fjw & FLAG_BLANKED) && (!(rr2 >= R2) || (fjw & FLAG_NONFINITE))) {
+        if (cnt < LIST_CAP) row[cnt] = (unsigned)j | tag;
+        ++cnt;
+      }
+    }
+  }
+  if (cnt > LIST_CAP) {
+    atomicOr(&D.st->error_flags, ERR_LIST_OVERFLOW);
+    cnt = LIST_CAP;
+  }
+  D.ncount[q] = cnt;
+  return cnt;
+}
+
+// LIST: the neighbour-list form (steps with P.verlet). 80 registers (6 blocks of 128 per SM)
+// keep both forms free of spills; the list form measured slower at 7 and 8 blocks per SM
+template <bool LIST>
 static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, dev_buffers D) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
@@ -147,43 +191,71 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
   const int hashi = D.hash_cur[q];
   const int gi = hashi / g.ny;
   const int gj = hashi - gi * g.ny;
-  const int low_i = gi - 2 < 0 ? 0 : gi - 2;
-  const int low_j = gj - 2 < 0 ? 0 : gj - 2;
-  const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
-  const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
 
   mixed_acc acc;
   acc.vd01 = acc.vd23 = acc.sd_xw = acc.sd_zy = acc.vt = acc.xt = f2(0.f, 0.f);
   acc.T_lapl = 0.f;
 
-  for (int ii = low_i; ii < high_i; ++ii) {
-    const int col = ii * g.ny;
-    const int j0 = __ldg(D.off + col + low_j);
-    const int j1 = __ldg(D.off + col + high_j);
-    const float ox = (float)(gi - ii) * dxc + I.x;
-    // chunks of up to 32 candidates: mark the contributing ones, then visit them in order
-    for (int jb = j0; jb < j1; jb += 32) {
-      const int jn = min(32, j1 - jb);
-      unsigned mask = 0u;
-#pragma unroll 4
-      for (int k = 0; k < jn; ++k) {
-        const float4 b0 = __ldg(r0 + jb + k);
+  if (LIST && !I.nonfinite) {
+    // neighbour list: built on a sorting step, then read; each entry passes the same
+    // support test as a window candidate. A particle's row is contiguous: four entries per
+    // 16-byte load; an entry past the count reads the particle's own record (always valid,
+    // so the loads need no guard) and is skipped.
+    const int cnt = D.st->sort_now ? build_list(D, r0, q, I, g, gi, gj, dxc, P.skin) : D.ncount[q];
+    const uint4 *row = reinterpret_cast<const uint4 *>(D.nlist + (size_t)q * LIST_CAP);
+    for (int k0 = 0; k0 < cnt; k0 += 4) {
+      const uint4 e4 = row[k0 >> 2];
+      const unsigned ev[4] = {e4.x, e4.y, e4.z, e4.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool live = k0 + u < cnt;
+        const unsigned e = live ? ev[u] : (unsigned)q | (3u << LIST_INDEX_BITS);
+        const int j = (int)(e & LIST_INDEX_MASK);
+        const float ox = (float)((int)(e >> LIST_INDEX_BITS) - 3) * dxc + I.x;
+        const float4 b0 = __ldg(r0 + j), b1 = __ldg(r1 + j), b2 = __ldg(r2 + j), b3 = __ldg(r3 + j);
         const unsigned fjw = (unsigned)__float_as_int(b0.z);
         const float xij = ox - b0.x;
         const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
         const float rr2 = xij * xij + yij * yij;
         const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
-        const bool take = !(fjw & FLAG_BLANKED) && (in_support || I.nonfinite || (fjw & FLAG_NONFINITE));
-        mask |= (take ? 1u : 0u) << k;
+        if (live && !(fjw & FLAG_BLANKED) && (in_support || (fjw & FLAG_NONFINITE)))
+          mixed_interact(I, K, acc, xij, yij, b0, b1, b2, b3);
       }
-      while (mask) {
-        const int k = __ffs(mask) - 1;
-        mask &= mask - 1u;
-        const int j = jb + k;
-        // all four planes at once: one load latency per neighbour
-        const float4 b0 = __ldg(r0 + j), b1 = __ldg(r1 + j), b2 = __ldg(r2 + j), b3 = __ldg(r3 + j);
-        const float yij = fmaf((float)(gj - (int)((unsigned)__float_as_int(b0.z) >> 8)), dxc, I.y - b0.y);
-        mixed_interact(I, K, acc, ox - b0.x, yij, b0, b1, b2, b3);
+    }
+  } else {  // the 5x5 window (interactions_gpu.cu:147-345)
+    const int low_i = gi - 2 < 0 ? 0 : gi - 2;
+    const int low_j = gj - 2 < 0 ? 0 : gj - 2;
+    const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
+    const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
+    for (int ii = low_i; ii < high_i; ++ii) {
+      const int col = ii * g.ny;
+      const int j0 = __ldg(D.off + col + low_j);
+      const int j1 = __ldg(D.off + col + high_j);
+      const float ox = (float)(gi - ii) * dxc + I.x;
+      // chunks of up to 32 candidates: mark the contributing ones, then visit them in order
+      for (int jb = j0; jb < j1; jb += 32) {
+        const int jn = min(32, j1 - jb);
+        unsigned mask = 0u;
+#pragma unroll 4
+        for (int k = 0; k < jn; ++k) {
+          const float4 b0 = __ldg(r0 + jb + k);
+          const unsigned fjw = (unsigned)__float_as_int(b0.z);
+          const float xij = ox - b0.x;
+          const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
+          const float rr2 = xij * xij + yij * yij;
+          const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
+          const bool take = !(fjw & FLAG_BLANKED) && (in_support || I.nonfinite || (fjw & FLAG_NONFINITE));
+          mask |= (take ? 1u : 0u) << k;
+        }
+        while (mask) {
+          const int k = __ffs(mask) - 1;
+          mask &= mask - 1u;
+          const int j = jb + k;
+          // all four planes at once: one load latency per neighbour
+          const float4 b0 = __ldg(r0 + j), b1 = __ldg(r1 + j), b2 = __ldg(r2 + j), b3 = __ldg(r3 + j);
+          const float yij = fmaf((float)(gj - (int)((unsigned)__float_as_int(b0.z) >> 8)), dxc, I.y - b0.y);
+          mixed_interact(I, K, acc, ox - b0.x, yij, b0, b1, b2, b3);
+        }
       }
     }
   }

@@ -148,8 +148,8 @@ extern "C" int mf_cells_build_noalloc(const double *d_pos, int N, double bbmin_x
   const int ob = (std::max(N, g.num_cell) + BLOCK - 1) / BLOCK;
   k_na_clear<<<std::min(ob, 148 * 8), BLOCK, 0, st>>>(S, g);
   k_na_hash<<<nb, BLOCK, 0, st>>>(reinterpret_cast<const double2 *>(d_pos), N, S);
-  k_scan<<<scan_tiles, SCAN_THREADS, 0, st>>>(D, N);
-  k_scatter<<<nb, BLOCK, 0, st>>>(N, D);
+  k_scan<<<scan_tiles, SCAN_THREADS, 0, st>>>(D, N, 0);
+  k_scatter<<<nb, BLOCK, 0, st>>>(N, D, 0);
   k_na_output<<<std::min(ob, 148 * 16), BLOCK, 0, st>>>(N, D, d_hash_sorted, d_idx, d_cell_start, d_cell_end,
                                                         g.num_cell);
   return cudaGetLastError() == cudaSuccess ? MF_OK : MF_ERR_CUDA;

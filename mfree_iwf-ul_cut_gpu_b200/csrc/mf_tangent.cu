@@ -594,8 +594,8 @@ int run_mean_force(mf_ctx *ctx, int device, params P, const dev_buffers &Dctx, i
     As.flags = TB.flagsv;
     k_t_posv<<<nb, 128>>>(N, TB);
     k_hash_count<<<hb, 128>>>(N, As, D, scan_tiles);
-    k_scan<<<scan_tiles, SCAN_THREADS>>>(D, N);
-    k_scatter<<<(N + BLOCK - 1) / BLOCK, BLOCK>>>(N, D);
+    k_scan<<<scan_tiles, SCAN_THREADS>>>(D, N, 0);
+    k_scatter<<<(N + BLOCK - 1) / BLOCK, BLOCK>>>(N, D, 0);
     k_t_reorder<<<nb, 128>>>(P, D, TB);
     k_t_pair<<<nb, 128>>>(P, D, TB);
     if (P.has_tool) mf_tool_translate(&TL, P.dt);  // tool::update_tool, before contact

@@ -27,7 +27,7 @@ def test_every_declared_symbol_is_exported(mf):
 
 def test_version_and_error_strings(mf):
     L = mf.lib()
-    assert L.mf_version() == 1
+    assert L.mf_version() == 2
     for code in (0, -1, -2, -3, -4, -5, -6, -7):
         assert L.mf_error_string(code)
 

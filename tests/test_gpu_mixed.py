@@ -38,9 +38,11 @@ def test_mixed_many_steps(mf):
     b = load_product(mf, st, precision=mf.PRECISION_MIXED)
     a.step(30)
     b.step(30)
-    assert np.array_equal(a.get("blanked"), b.get("blanked"))
+    # the mixed form keeps neighbour lists and sorts less often: compare particle by particle
+    oa, ob = np.argsort(a.get("id")), np.argsort(b.get("id"))
+    assert np.array_equal(a.get("blanked")[oa], b.get("blanked")[ob])
     for f in ("pos", "vel", "rho", "S", "T"):
-        va, vb = a.get(f), b.get(f)
+        va, vb = a.get(f)[oa], b.get(f)[ob]
         assert np.isfinite(vb).all(), f
         if f == "pos":
             err = np.abs(vb - va).max() / st["grid"][2]
