@@ -120,11 +120,17 @@ void free_list(std::vector<void *> &list) {
   list.clear();
 }
 
+int invalidate_counts(mf_ctx *ctx);
+
+// Captured work is stale: buffers, constants, options, dt or flags changed. The next step also
+// starts over from a sort (its counts primed again): with neighbour lists the last step may
+// have run the next step's predictor with the old parameters.
 void drop_graphs(mf_ctx *ctx) {
   ctx->gen++;
   for (int k = 0; k < 2; ++k)
     if (ctx->graph[k]) { cudaGraphExecDestroy(ctx->graph[k]); ctx->graph[k] = nullptr; }
   ctx->graph_valid = false;
+  (void)invalidate_counts(ctx);  // (a failed memset surfaces at the next synchronizing call)
 }
 
 #define TRY(x)                 \
@@ -141,6 +147,7 @@ int alloc_set(mf_ctx *ctx, state_set &s, int N) {
   TRY(dalloc(ctx, L, &s.eps_pl_dot, N)); TRY(dalloc(ctx, L, &s.h, N)); TRY(dalloc(ctx, L, &s.rho_t, N));
   TRY(dalloc(ctx, L, &s.T_t, N)); TRY(dalloc(ctx, L, &s.S, N)); TRY(dalloc(ctx, L, &s.S_t, N));
   TRY(dalloc(ctx, L, &s.flags, N)); TRY(dalloc(ctx, L, &s.idx, N)); TRY(dalloc(ctx, L, &s.id, N));
+  TRY(dalloc(ctx, L, &s.pp, N));
   return MF_OK;
 }
 
@@ -163,7 +170,6 @@ int alloc_particles(mf_ctx *ctx, int N) {
   TRY(dalloc(ctx, L, &D.n, N));
   TRY(dalloc(ctx, L, &D.rec, (size_t)N * R_WIDTH));
   TRY(dalloc(ctx, L, &D.recf, (size_t)N * F_WIDTH));
-  TRY(dalloc(ctx, L, &D.pp, N));
   TRY(dalloc(ctx, L, &D.S_der, N));
   TRY(dalloc(ctx, L, &D.v_der, N));
   TRY(dalloc(ctx, L, &D.hash_cur, N));
@@ -225,6 +231,9 @@ bool list_mode(const mf_ctx *ctx) {
 }
 
 void set_list_mode(mf_ctx *ctx) {
+  // the EOS sound speed of every particle: the device's float rounding of the same IEEE
+  // operations, computed once
+  ctx->P.eos_c0 = (double)sqrtf((float)(ctx->P.phys.K / ctx->P.phys.rho0));
   ctx->P.verlet = list_mode(ctx) ? 1 : 0;
   ctx->P.skin = (float)(ctx->skin > 0. ? ctx->skin : 0.1 * ctx->G.dx);
 }
@@ -383,7 +392,7 @@ void *field_ptr(mf_ctx *ctx, int f) {
     case MF_FIELD_VEL: return s.vel;
     case MF_FIELD_H: return s.h;
     case MF_FIELD_RHO: return s.rho;
-    case MF_FIELD_P: return ctx->D.pp;
+    case MF_FIELD_P: return s.pp;
     case MF_FIELD_S: return s.S;
     case MF_FIELD_FC: return s.fc;
     case MF_FIELD_FT: return s.ft;
@@ -1516,7 +1525,7 @@ int mf_vtk_write_particles_async(mf_ctx *ctx, const char *path) {
   if (!ctx->io_stream) CK(cudaStreamCreateWithFlags(&ctx->io_stream, cudaStreamNonBlocking));
   const int n = ctx->N;
   const state_set &s = ctx->set[ctx->cur];
-  const vtk_src src[7] = {{s.pos, 2}, {s.vel, 2}, {s.rho, 1}, {ctx->D.pp, 1}, {s.T, 1}, {s.eps_pl, 1}, {s.S, 4}};
+  const vtk_src src[7] = {{s.pos, 2}, {s.vel, 2}, {s.rho, 1}, {s.pp, 1}, {s.T, 1}, {s.eps_pl, 1}, {s.S, 4}};
   const size_t per = 12;  // doubles per particle in the snapshot
   std::unique_ptr<vtk_job> j(new (std::nothrow) vtk_job);
   if (!j) return MF_ERR_NOMEM;

@@ -48,6 +48,7 @@ struct params {
   // between, each particle's candidates within 2 h + skin are kept in a list
   int verlet;
   float skin;
+  double eos_c0;  // (double)sqrtf((float)(K / rho0)), the EOS sound speed (actions_gpu.cu:41-51)
   double dt;
   mf_phys_constants phys;
   mf_corr_constants corr;
@@ -79,13 +80,15 @@ struct dev_status {
   unsigned int sort_now;     // neighbour lists: this step sorts (set by the previous step)
   unsigned int want_sort;    // neighbour lists: a particle's next predicted position is more
                              // than 0.45 skin from where its list was built
+  unsigned int predicted;    // neighbour lists: the last finish kernel also ran the next step's
+                             // predictor (it did not follow a sort); the next step, if it does
+                             // not sort, skips the reorder kernel
 };
 
 constexpr int FORCE_LOG_CAP = 1 << 16;
 constexpr int ERR_SCAN_WAIT = 1;
 constexpr int ERR_GRID_BUDGET = 2;
 constexpr int ERR_LIST_OVERFLOW = 4;  // a neighbour list was full: neighbours were dropped
-constexpr int ERR_SKIN = 8;           // a particle moved more than skin / 2 on one list (guard)
 
 // neighbour list entry: particle index in the low LIST_INDEX_BITS bits, above them the
 // column offset of the pair's cells (i's column - j's column) + 3, in [0, 6]
@@ -152,6 +155,24 @@ __device__ __forceinline__ void artificial_stress(double rhoi, double pi, double
   Rxx = cos_theta2 * rot_rxx + sin_theta2 * rot_ryy;
   Rxy = cos_theta * sin_theta * (rot_rxx - rot_ryy);
   Ryy = sin_theta2 * rot_rxx + cos_theta2 * rot_ryy;
+}
+
+// The same in float for the mixed form's FP32 records, from rho21 = 1 / rho^2: the angle and
+// its cosine and sine are the reference's float ones; the deviatoric parts are rounded once.
+__device__ __forceinline__ void artificial_stress_f(double rhoi21, double pi, double Sx, double Sy, double Sz,
+                                                    double eps, float &Rxx, float &Rxy, float &Ryy) {
+  const float sxx = (float)(Sx - pi), sxy = (float)Sy, syy = (float)(Sz - pi);
+  const float theta = 0.5f * atan2f(2.f * sxy, (float)((Sx - pi) - (Sz - pi)));
+  const float c = cosf(theta), s = sinf(theta);
+  const float c2 = c * c, s2 = s * s, cs = c * s;
+  const float rot_sxx = c2 * sxx + 2.f * cs * sxy + s2 * syy;
+  const float rot_syy = s2 * sxx - 2.f * cs * sxy + c2 * syy;
+  const float er = -(float)eps * (float)rhoi21;
+  const float rot_rxx = rot_sxx > 0.f ? er * rot_sxx : 0.f;
+  const float rot_ryy = rot_syy > 0.f ? er * rot_syy : 0.f;
+  Rxx = c2 * rot_rxx + s2 * rot_ryy;
+  Rxy = cs * (rot_rxx - rot_ryy);
+  Ryy = s2 * rot_rxx + c2 * rot_ryy;
 }
 
 // Jaumann stress rate (actions_gpu.cu:99-133). The reference builds 3x3 GLM matrices; the

@@ -29,6 +29,7 @@ namespace mf {
 struct state_set {
   double2 *pos, *vel, *fc, *ft, *pos_t, *vel_t;
   double *rho, *T, *eps_pl, *eps_pl_dot, *h, *rho_t, *T_t;
+  double *pp;  // predictor pressure (the reference's particles->p), of the step that wrote the set
   double4 *S, *S_t;
   unsigned *flags;
   int *idx;
@@ -49,7 +50,6 @@ struct dev_buffers {
   double2 *n;           // contact normal, indexed by array position (never permuted)
   double *rec;          // FP64 pair records: R_WIDTH / 2 planes of N double2
   float *recf;          // FP32 pair records (mixed form): F_WIDTH / 4 planes of N float4
-  double *pp;           // predictor pressure (the reference's particles->p)
   double4 *S_der, *v_der;
   int *hash_cur;        // cell hash per array position (sorted order)
   int *hash_new, *perm;
@@ -93,6 +93,11 @@ constexpr int FINISH_BLOCKS_PER_SM = 2;
 // k_plastic: fixed grid of this many 256-thread blocks per SM over the plastic list
 constexpr int PLASTIC_BLOCKS_PER_SM = 4;
 constexpr int PAIR_BLOCK = 128;
+// k_reorder: blocks per SM its register budget allows (REORDER_BLOCKS_PER_SM x 256 threads per
+// SM, so that a ~180k-particle grid runs in one wave)
+#ifndef REORDER_BLOCKS_PER_SM
+#define REORDER_BLOCKS_PER_SM 5
+#endif
 constexpr unsigned long long SCAN_FLAG_AGG = 1ull << 62;
 constexpr unsigned long long SCAN_FLAG_PREFIX = 2ull << 62;
 constexpr long long SCAN_SPIN_LIMIT = 1ll << 24;
@@ -370,8 +375,135 @@ __device__ __forceinline__ int stable_member(const dev_buffers &D, int q, const 
 // gather into the new order (grid_gpu_green.cu:22-116) and, if PREDICT, the predictor
 // (leap_frog.cu:30-66), EOS (actions_gpu.cu:41-51), artificial stress (:53-97) and the
 // neighbour records read by the pair kernel.
+// The predictor of a step for the particle at array position q (leap_frog.cu:30-66), EOS
+// (actions_gpu.cu:41-51), artificial stress (:53-97) and the neighbour pair records, from the
+// particle's state at the start of the step and its rates. Writes the predicted velocity and
+// stress, the rates the pair pass will not overwrite, the flags and the pressure into set B,
+// and the records. With neighbour lists, a sorting step (build) also keeps the predicted
+// position its lists are built from.
+template <bool MIXED>
+__device__ __forceinline__ void predict_particle(const params &P, const dev_buffers &D, const state_set &B, int q,
+                                                 int hsh, double2 pos, double2 vel, double4 S, double rho, double T,
+                                                 const double2 &pos_t, const double2 &vel_t, const double4 &S_t,
+                                                 double rho_t, double T_t, unsigned f, double h, bool build) {
+  const bool blanked = f & FLAG_BLANKED;
+  const bool tool = f & FLAG_TOOL;
+  // the previous rates travel with the particle where this step's pair pass will not
+  // overwrite them (blanked particles; tool particles' stress and density rates; the
+  // kinematic rates of tool particles under PSE; the temperature rate without conduction);
+  // staged, every rate is copied so that the half-built step reads whole
+  bool keep_kin = true, keep_mech = true, keep_T = true;
+  if (!P.staged && !blanked) {
+    const bool brookshaw = P.thermal_solver == MF_THERMAL_BROOKSHAW;
+    keep_kin = !brookshaw && tool;
+    keep_mech = tool;
+    const double alpha_T = !tool ? P.trml_wp.alpha : (P.thermal_tool_on ? P.trml_tool.alpha : 0.);
+    keep_T = brookshaw ? alpha_T == 0. : !P.thermal_wp;
+  }
+  if (keep_kin) {
+    B.pos_t[q] = pos_t;
+    B.vel_t[q] = vel_t;
+  }
+  if (keep_mech) {
+    B.S_t[q] = S_t;
+    B.rho_t[q] = rho_t;
+  }
+  if (keep_T) B.T_t[q] = T_t;
+
+  if (!blanked) {
+    const double dt = P.dt;
+    pos.x = pos.x + 0.5 * dt * pos_t.x;
+    pos.y = pos.y + 0.5 * dt * pos_t.y;
+    vel.x = vel.x + 0.5 * dt * vel_t.x;
+    vel.y = vel.y + 0.5 * dt * vel_t.y;
+    S.x = S.x + 0.5 * dt * S_t.x;
+    S.y = S.y + 0.5 * dt * S_t.y;
+    S.z = S.z + 0.5 * dt * S_t.z;
+    S.w = S.w + 0.5 * dt * S_t.w;
+    rho = rho + 0.5 * dt * rho_t;
+    T = T + 0.5 * dt * T_t;
+  }
+  // the predicted velocity and stress are read by the pair kernels; position, density and
+  // temperature live in the pair records (the full predicted state is kept when staged)
+  B.vel[q] = vel;
+  B.S[q] = S;
+  if (P.staged) {
+    B.pos[q] = pos;
+    B.rho[q] = rho;
+    B.T[q] = T;
+  }
+  B.flags[q] = f;
+
+  const double mass = P.phys.mass, K = P.phys.K;
+  double prs = 0.;
+  if (!tool) prs = P.eos_c0 * P.eos_c0 * (rho - P.phys.rho0);
+  B.pp[q] = prs;
+  unsigned rf = f & (FLAG_BLANKED | FLAG_TOOL | FLAG_FIXED);
+  float fr[F_WIDTH];
+  if (!MIXED || P.staged) {
+    double Rxx = 0., Rxy = 0., Ryy = 0.;
+    if (!tool) artificial_stress(rho, prs, S.x, S.y, S.z, P.corr.stresseps, Rxx, Rxy, Ryy);
+    const double rho21 = 1. / (rho * rho);
+    const double sxx = (S.x - prs) * rho21, sxy = S.y * rho21, syy = (S.z - prs) * rho21;
+    const double c = (double)sqrtf((float)(K / rho));
+    const double vol = mass / rho;
+    double r[R_WIDTH] = {pos.x, pos.y, vel.x, vel.y, sxx, sxy, syy, Rxx, Rxy, Ryy, h, rho, c, vol, T, 0.};
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < R_FLAGS; ++k) finite = finite && isfinite(r[k]);
+    if (!finite) rf |= FLAG_NONFINITE;
+    r[R_FLAGS] = __longlong_as_double((long long)rf);
+    // the FP64 record feeds the FP64 pair kernel and its PSE pass (kept when staged, for reads);
+    // eight planes of double2 (structure of arrays): plane k of particle q at [k * N + q]
+    double2 *dst = reinterpret_cast<double2 *>(D.rec);
+#pragma unroll
+    for (int k = 0; k < R_WIDTH / 2; ++k) dst[(size_t)k * P.N + q] = make_double2(r[2 * k], r[2 * k + 1]);
+    const float fv[12] = {(float)vel.x, (float)vel.y, (float)sxx, (float)sxy, (float)syy, (float)Rxx,
+                          (float)Rxy, (float)Ryy, (float)h, (float)rho, (float)c, (float)vol};
+#pragma unroll
+    for (int k = 0; k < 12; ++k) fr[3 + k] = fv[k];
+  } else {
+    // the mixed form's FP32 record only: one FP64 reciprocal of rho for 1 / rho^2, c and the
+    // volume, the artificial stress in float
+    const double rinv = 1. / rho, rho21 = rinv * rinv;
+    float Rxx = 0.f, Rxy = 0.f, Ryy = 0.f;
+    if (!tool) artificial_stress_f(rho21, prs, S.x, S.y, S.z, P.corr.stresseps, Rxx, Rxy, Ryy);
+    const float fv[12] = {(float)vel.x, (float)vel.y, (float)((S.x - prs) * rho21), (float)(S.y * rho21),
+                          (float)((S.z - prs) * rho21), Rxx, Rxy, Ryy, (float)h, (float)rho,
+                          sqrtf((float)(K * rinv)), (float)(mass * rinv)};
+    bool finite = isfinite(pos.x) && isfinite(pos.y) && isfinite(T);
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      fr[3 + k] = fv[k];
+      finite = finite && isfinite(fv[k]);
+    }
+    if (!finite) rf |= FLAG_NONFINITE;
+  }
+
+  if (MIXED) {
+    // FP32 record: position relative to the origin of the particle's own cell, temperature
+    // relative to the initial temperature (only differences of T enter the pair sums)
+    const geom g = *D.g;
+    const int ci = hsh / g.ny, cj = hsh - ci * g.ny;
+    const double ox = g.bbmin_x + ci * g.dx, oy = g.bbmin_y + cj * g.dx;
+    fr[0] = (float)(pos.x - ox);
+    fr[1] = (float)(pos.y - oy);
+    fr[2] = __int_as_float((int)(rf | ((unsigned)cj << 8)));
+    fr[15] = (float)(T - P.trml_wp.T_init);
+    // four planes of float4 (structure of arrays): plane k of particle q at [k * N + q]
+    float4 *fd = reinterpret_cast<float4 *>(D.recf);
+#pragma unroll
+    for (int k = 0; k < F_WIDTH / 4; ++k)
+      fd[(size_t)k * P.N + q] = make_float4(fr[4 * k], fr[4 * k + 1], fr[4 * k + 2], fr[4 * k + 3]);
+    // the lists stay valid while every particle is within skin / 2 of where it was at the
+    // last sort (then every pair closer than 2 h was closer than 2 h + skin there); each step's
+    // finish kernel checks the next step's predicted positions against 0.45 skin
+    if (P.verlet && build) D.pos_build[q] = pos;
+  }
+}
+
 template <bool PREDICT, bool MIXED>
-static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers D) {
+static __global__ void __launch_bounds__(BLOCK, REORDER_BLOCKS_PER_SM) k_reorder(params P, dev_buffers D) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -384,6 +516,9 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
     *D.finish_chunk = 0u;
     if (sort) D.st->sorts += 1ull;
   }
+  // neighbour lists, no sort, and the previous step's finish (and plastic) kernels already ran
+  // this step's predictor: nothing left to do
+  if (PREDICT && !sort && D.st->predicted) return;
   int p = q, hsh;
   if (sort) {
     const int4 u = D.perm_u[q];
@@ -414,112 +549,21 @@ static __global__ void __launch_bounds__(BLOCK) k_reorder(params P, dev_buffers 
   // the Rothlin grid does not gather ft (grid_gpu_rothlin.cu:138-250): it stays in place
   B.ft[q] = P.grid_kind == MF_GRID_GREEN ? A.ft[p] : A.ft[q];
   B.h[q] = h;
-  const bool blanked = f & FLAG_BLANKED;
-  const bool tool = f & FLAG_TOOL;
-  // the previous rates travel with the particle where this step's pair pass will not
-  // overwrite them (blanked particles; tool particles' stress and density rates; the
-  // kinematic rates of tool particles under PSE; the temperature rate without conduction);
-  // staged, every rate is copied so that the half-built step reads whole
-  bool keep_kin = true, keep_mech = true, keep_T = true;
-  if (PREDICT && !P.staged && !blanked) {
-    const bool brookshaw = P.thermal_solver == MF_THERMAL_BROOKSHAW;
-    keep_kin = !brookshaw && tool;
-    keep_mech = tool;
-    const double alpha_T = !tool ? P.trml_wp.alpha : (P.thermal_tool_on ? P.trml_tool.alpha : 0.);
-    keep_T = brookshaw ? alpha_T == 0. : !P.thermal_wp;
-  }
-  if (keep_kin) {
+  if (!PREDICT) {  // a sort outside a step: the state moves as it is
     B.pos_t[q] = pos_t;
     B.vel_t[q] = vel_t;
-  }
-  if (keep_mech) {
     B.S_t[q] = S_t;
     B.rho_t[q] = rho_t;
-  }
-  if (keep_T) B.T_t[q] = T_t;
-
-  if (PREDICT && !blanked) {
-    const double dt = P.dt;
-    pos.x = pos.x + 0.5 * dt * pos_t.x;
-    pos.y = pos.y + 0.5 * dt * pos_t.y;
-    vel.x = vel.x + 0.5 * dt * vel_t.x;
-    vel.y = vel.y + 0.5 * dt * vel_t.y;
-    S.x = S.x + 0.5 * dt * S_t.x;
-    S.y = S.y + 0.5 * dt * S_t.y;
-    S.z = S.z + 0.5 * dt * S_t.z;
-    S.w = S.w + 0.5 * dt * S_t.w;
-    rho = rho + 0.5 * dt * rho_t;
-    T = T + 0.5 * dt * T_t;
-  }
-  // the predicted velocity and stress are read by the pair kernels; position, density and
-  // temperature live in the pair records (the full predicted state is kept when staged)
-  B.vel[q] = vel;
-  B.S[q] = S;
-  if (!PREDICT || P.staged) {
+    B.T_t[q] = T_t;
+    B.vel[q] = vel;
+    B.S[q] = S;
     B.pos[q] = pos;
     B.rho[q] = rho;
     B.T[q] = T;
+    B.flags[q] = f;
+    return;
   }
-  B.flags[q] = f;
-  if (!PREDICT) return;
-
-  const double mass = P.phys.mass, K = P.phys.K;
-  double prs = 0., Rxx = 0., Rxy = 0., Ryy = 0.;
-  if (!tool) {
-    const double rho0 = P.phys.rho0;
-    const double c0 = (double)sqrtf((float)(K / rho0));
-    prs = c0 * c0 * (rho - rho0);
-    artificial_stress(rho, prs, S.x, S.y, S.z, P.corr.stresseps, Rxx, Rxy, Ryy);
-  }
-  D.pp[q] = prs;
-  const double rho21 = 1. / (rho * rho);
-  const double sxx = (S.x - prs) * rho21, sxy = S.y * rho21, syy = (S.z - prs) * rho21;
-  const double c = (double)sqrtf((float)(K / rho));
-  const double vol = mass / rho;
-  double r[R_WIDTH] = {pos.x, pos.y, vel.x, vel.y, sxx, sxy, syy, Rxx, Rxy, Ryy, h, rho, c, vol, T, 0.};
-  unsigned rf = f & (FLAG_BLANKED | FLAG_TOOL | FLAG_FIXED);
-  bool finite = true;
-#pragma unroll
-  for (int k = 0; k < R_FLAGS; ++k) finite = finite && isfinite(r[k]);
-  if (!finite) rf |= FLAG_NONFINITE;
-  r[R_FLAGS] = __longlong_as_double((long long)rf);
-  // the FP64 record feeds the FP64 pair kernel and its PSE pass (kept when staged, for reads)
-  if (!MIXED || P.staged) {
-    // eight planes of double2 (structure of arrays): plane k of particle q at [k * N + q]
-    double2 *dst = reinterpret_cast<double2 *>(D.rec);
-#pragma unroll
-    for (int k = 0; k < R_WIDTH / 2; ++k) dst[(size_t)k * P.N + q] = make_double2(r[2 * k], r[2 * k + 1]);
-  }
-
-  if (MIXED) {
-    // FP32 record: position relative to the origin of the particle's own cell, temperature
-    // relative to the initial temperature (only differences of T enter the pair sums)
-    const geom g = *D.g;
-    const int ci = hsh / g.ny, cj = hsh - ci * g.ny;
-    const double ox = g.bbmin_x + ci * g.dx, oy = g.bbmin_y + cj * g.dx;
-    float fr[F_WIDTH] = {(float)(pos.x - ox), (float)(pos.y - oy), __int_as_float((int)(rf | ((unsigned)cj << 8))),
-                         (float)vel.x, (float)vel.y, (float)sxx, (float)sxy, (float)syy, (float)Rxx, (float)Rxy,
-                         (float)Ryy, (float)h, (float)rho, (float)c, (float)vol, (float)(T - P.trml_wp.T_init)};
-    // four planes of float4 (structure of arrays): plane k of particle q at [k * N + q]
-    float4 *fd = reinterpret_cast<float4 *>(D.recf);
-#pragma unroll
-    for (int k = 0; k < F_WIDTH / 4; ++k)
-      fd[(size_t)k * P.N + q] = make_float4(fr[4 * k], fr[4 * k + 1], fr[4 * k + 2], fr[4 * k + 3]);
-    if (P.verlet) {
-      // the lists stay valid while every particle is within skin / 2 of where it was at the
-      // last sort (then every pair closer than 2 h was closer than 2 h + skin there); the
-      // previous step's finish kernel checked this step's predicted positions against
-      // 0.45 skin and asked for a sort where needed, so the test below is a guard
-      if (sort) {
-        D.pos_build[q] = pos;
-      } else if (!blanked && !(rf & FLAG_NONFINITE)) {  // (non-finite ones are blanked this step)
-        const double2 pb = D.pos_build[q];
-        const double ddx = pos.x - pb.x, ddy = pos.y - pb.y;
-        const double half = 0.5 * (double)P.skin;
-        if (ddx * ddx + ddy * ddy > half * half) atomicOr(&D.st->error_flags, ERR_SKIN);
-      }
-    }
-  }
+  predict_particle<MIXED>(P, D, B, q, hsh, pos, vel, S, rho, T, pos_t, vel_t, S_t, rho_t, T_t, f, h, sort);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -765,7 +809,7 @@ __device__ __forceinline__ void tool_advance_shared(mf_tool_state &T, const dev_
 __device__ __forceinline__ void finish_particle(const params &P, const dev_buffers &D, const mf_tool_state &TL,
                                                const mf_joco_constants &JC, int q,
                                                double2 &pos_out, unsigned &f_out, double2 &fc_out, double2 &ft_out,
-                                               unsigned &newly_blanked, bool &want_sort) {
+                                               unsigned &newly_blanked, bool &want_sort, bool identity) {
   const state_set &A = D.A;
   const state_set &B = D.B;
   const double dt = P.dt;
@@ -776,14 +820,14 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
   // the state at the start of the step, in the new order (predict/correct skip blanked
   // particles, so for them it is also the state at the end of the step)
   // every load is issued here, before any store, so that they are all in flight together
-  const int p = D.perm[q];
+  const int p = identity ? q : D.perm[q];
   double2 pos_t = B.pos_t[q], vel_t = B.vel_t[q];
   const double4 S_t = B.S_t[q];
   const double rho_t = B.rho_t[q], T_t = B.T_t[q];
   double eps_pl = B.eps_pl[q], eps_pl_dot = B.eps_pl_dot[q];
   double2 fc = B.fc[q], ft = B.ft[q];
   const double2 normal = D.n[q];
-  const double pr = D.pp[q];
+  const double pr = B.pp[q];
   double2 pos = A.pos[p], vel = A.vel[p];
   double4 S = A.S[p];
   double rho = A.rho[p], T = A.T[p];
@@ -925,6 +969,20 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
   B.eps_pl_dot[q] = eps_pl_dot;
   B.fc[q] = fc;
   B.ft[q] = ft;
+  if (identity) {
+    // neighbour lists, a step without a sort: the next step keeps this order, so its
+    // predictor runs here, on the final state still in registers, into the set the next step
+    // writes (this step's start set, read above by this thread only). If the next step sorts,
+    // its reorder kernel redoes it; k_plastic redoes it for the particles it changes.
+    const state_set &N1 = D.A;
+    N1.idx[q] = P.grid_kind == MF_GRID_GREEN ? q : B.idx[q];
+    N1.eps_pl[q] = eps_pl;
+    N1.eps_pl_dot[q] = eps_pl_dot;
+    N1.fc[q] = fc;
+    N1.ft[q] = ft;
+    predict_particle<true>(P, D, N1, q, D.hash_cur[q], pos, vel, S, rho, T, pos_t, vel_t, S_t, rho_t, T_t, f, B.h[q],
+                           false);
+  }
   pos_out = pos;
   f_out = f;
   fc_out = fc;
@@ -961,9 +1019,15 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
   const int n_chunks = (P.N + BLOCK - 1) / BLOCK;
   unsigned newly_blanked = 0, blanked_now = 0, oog = 0;
   bool want_sort = false;
+  // neighbour lists, a step without a sort: the order is the previous step's (the last block
+  // sets sort_now for the next step only after every block has read it here); such a step
+  // also runs the next step's predictor
+  const bool identity = P.verlet && !*(volatile unsigned *)&D.st->sort_now;
   geom g{};
+  double inv_dx = 0.;
   if (FUSE_HASH) {
     g = *D.g;
+    inv_dx = 1. / g.dx;
     for (int t = gid; t < num_scan_tiles; t += stride) D.scan_status[t] = 0ull;
   }
   for (int buf = 0;; buf ^= 1) {
@@ -977,15 +1041,17 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
     if (q < P.N) {
       double2 pos;
       unsigned f;
-      finish_particle(P, D, s_tool, s_jc, q, pos, f, fc, ft, newly_blanked, want_sort);
+      finish_particle(P, D, s_tool, s_jc, q, pos, f, fc, ft, newly_blanked, want_sort, identity);
       blanked_now += (f & FLAG_BLANKED) ? 1u : 0u;
       if (FUSE_HASH) {  // compute_hashes of the next step (grid.cu:34-51)
         long long hh;
         if (f & FLAG_BLANKED) {
           hh = D.hash_cur[q];
         } else {
-          const int ix = __double2int_rz((pos.x - g.bbmin_x) / g.dx);
-          const int iy = __double2int_rz((pos.y - g.bbmin_y) / g.dx);
+          // (the FP64 form divides as the reference does; the mixed form with neighbour lists,
+          // which needs no particular cell for a particle on a cell edge, multiplies)
+          const int ix = __double2int_rz(P.verlet ? (pos.x - g.bbmin_x) * inv_dx : (pos.x - g.bbmin_x) / g.dx);
+          const int iy = __double2int_rz(P.verlet ? (pos.y - g.bbmin_y) * inv_dx : (pos.y - g.bbmin_y) / g.dx);
           hh = (long long)ix * (long long)g.ny + (long long)iy;
         }
         if (hh < 0) { hh = 0; ++oog; }
@@ -1095,6 +1161,7 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
     if (P.verlet) {  // every particle is checked: the next step sorts if one asked for it
       D.st->sort_now = D.st->want_sort;
       D.st->want_sort = 0u;
+      D.st->predicted = identity ? 1u : 0u;
     }
     D.ticket[0] = 0u;
   }
@@ -1175,6 +1242,9 @@ static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic
   const unsigned n = *D.plastic_count;
   const state_set &B = D.B;
   const double dt = P.dt, mu = P.phys.G;
+  // neighbour lists: the finish kernel ran the next step's predictor; redone here where the
+  // return map changes the state
+  const bool fuse = P.verlet && D.st->predicted;
   constexpr unsigned LANES = PAIRED ? 2u : 1u;
   const unsigned sub = PAIRED ? (lane_id() & 1u) : 0u;
   const unsigned pmask = PAIRED ? (0x3u << (lane_id() & ~1u)) : 0xffffffffu;
@@ -1188,7 +1258,10 @@ static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic
     // one temperature for the whole return map: its temperature-only factors once
     const jc_temp_terms tt = jc_temperature_terms(JC, P.jc_model, T);
     if (it.svm < sigma_yield(JC, eps_pl, eps_pl_dot, tt)) {  // elastic after all
-      if (sub == 0) B.eps_pl_dot[q] = 0.;
+      if (sub == 0) {
+        B.eps_pl_dot[q] = 0.;
+        if (fuse) D.A.eps_pl_dot[q] = 0.;
+      }
       continue;
     }
     const double4 S = B.S[q];
@@ -1230,6 +1303,13 @@ static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic
       B.eps_pl[q] = eps_pl_new;
       B.eps_pl_dot[q] = eps_pl_dot_new;
       B.T[q] = T;
+      if (fuse) {
+        const state_set &N1 = D.A;
+        N1.eps_pl[q] = eps_pl_new;
+        N1.eps_pl_dot[q] = eps_pl_dot_new;
+        predict_particle<true>(P, D, N1, q, D.hash_cur[q], B.pos[q], B.vel[q], Sn, rho, T, B.pos_t[q], B.vel_t[q],
+                               B.S_t[q], B.rho_t[q], B.T_t[q], f, B.h[q], false);
+      }
       capped += cap ? 1u : 0u;
       iters_sum += (unsigned)iters;
     }

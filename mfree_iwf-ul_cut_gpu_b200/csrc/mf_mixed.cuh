@@ -203,9 +203,10 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
     // so the loads need no guard) and is skipped.
     const int cnt = D.st->sort_now ? build_list(D, r0, q, I, g, gi, gj, dxc, P.skin) : D.ncount[q];
     const uint4 *row = reinterpret_cast<const uint4 *>(D.nlist + (size_t)q * LIST_CAP);
+    uint4 e4 = row[0];  // (a row is LIST_CAP entries: the first four are always there)
     for (int k0 = 0; k0 < cnt; k0 += 4) {
-      const uint4 e4 = row[k0 >> 2];
       const unsigned ev[4] = {e4.x, e4.y, e4.z, e4.w};
+      if (k0 + 4 < cnt) e4 = row[(k0 >> 2) + 1];  // the next four, in flight during these
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         const bool live = k0 + u < cnt;
