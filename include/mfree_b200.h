@@ -115,8 +115,7 @@ typedef struct {
   int max_cell_occupancy;     /* largest particles-per-cell seen in the last sort */
   int error_flags;            /* bit 0: a bounded wait in the cell scan expired; bit 1: the
                                  adaptive grid outgrew max_cell; bit 2: a neighbour list was
-                                 full (neighbours dropped); bit 3: a particle moved more than
-                                 half the neighbour-list skin between two sorts (a guard) */
+                                 full (neighbours dropped) */
   long long secant_iterations; /* JC secant iterations since creation (cost diagnostic) */
   long long sorts;            /* cell-list sorts since creation (one per step, except for the
                                  mixed form with neighbour lists) */
