@@ -180,10 +180,10 @@ int alloc_particles(mf_ctx *ctx, int N) {
   TRY(dalloc(ctx, L, &D.nlist, (size_t)LIST_CAP * N));
   TRY(dalloc(ctx, L, &D.ncount, N));
   TRY(dalloc(ctx, L, &D.pos_build, N));
-  ctx->finish_blocks = std::min((N + BLOCK - 1) / BLOCK, ctx->sm_count * FINISH_BLOCKS_PER_SM);
+  ctx->finish_blocks = std::min((N + FINISH_BLOCK - 1) / FINISH_BLOCK, ctx->sm_count * FINISH_BLOCKS_PER_SM);
   ctx->bbox_blocks = std::min((N + BLOCK - 1) / BLOCK, ctx->sm_count * 4);
   // per-chunk force partials of the finish kernel (or per-block partials of the bbox pass)
-  const int finish_chunks = (N + BLOCK - 1) / BLOCK;
+  const int finish_chunks = (N + FINISH_BLOCK - 1) / FINISH_BLOCK;
   TRY(dalloc(ctx, L, &D.partials, (size_t)std::max(std::max(finish_chunks, ctx->bbox_blocks), 1) * 8));
   TRY(invalidate_counts(ctx));
   ctx->N = N;
@@ -307,8 +307,8 @@ int launch_stage(mf_ctx *ctx, int stage) {
       }
       break;
     case 3:
-      if (fused_step(ctx)) TRY(launch_pdl(ctx, k_finish<true>, ctx->finish_blocks, BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
-      else TRY(launch_pdl(ctx, k_finish<false>, ctx->finish_blocks, BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+      if (fused_step(ctx)) TRY(launch_pdl(ctx, k_finish<true>, ctx->finish_blocks, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+      else TRY(launch_pdl(ctx, k_finish<false>, ctx->finish_blocks, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
       if (ctx->P.plastic) {
         if (ctx->P.jc_model == MF_JC_TANH)
           TRY(launch_pdl(ctx, k_plastic<false>, ctx->sm_count * PLASTIC_BLOCKS_PER_SM, BLOCK, ctx->P, ctx->D));

@@ -88,8 +88,14 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 8;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr int BLOCK = 256;
-// k_finish runs a grid-stride loop over a fixed grid of this many blocks per SM
-constexpr int FINISH_BLOCKS_PER_SM = 2;
+// k_finish: a fixed grid of FINISH_BLOCKS_PER_SM blocks of FINISH_BLOCK threads per SM takes
+// FINISH_BLOCK-particle chunks from an atomic counter
+#ifndef FINISH_BLOCK
+#define FINISH_BLOCK 256
+#endif
+#ifndef FINISH_BLOCKS_PER_SM
+#define FINISH_BLOCKS_PER_SM 2
+#endif
 // k_plastic: fixed grid of this many 256-thread blocks per SM over the plastic list
 constexpr int PLASTIC_BLOCKS_PER_SM = 4;
 constexpr int PAIR_BLOCK = 128;
@@ -997,15 +1003,15 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
 // FUSE_HASH (locked grid) the kernel also computes the next step's cell hash and per-cell
 // count from the final positions (the work of k_hash_count) and re-arms the scan.
 template <bool FUSE_HASH>
-__global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P, dev_buffers D, int num_scan_tiles) {
+__global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P, dev_buffers D, int num_scan_tiles) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
   __shared__ mf_tool_state s_tool;
   // the JC constants in shared memory: the out-of-line yield functions take them by
   // reference, which for a kernel parameter would mean a copy on every thread's stack
   __shared__ mf_joco_constants s_jc;
-  __shared__ ksum sm[BLOCK / 32][4];
-  __shared__ unsigned smc[BLOCK / 32][3];
+  __shared__ ksum sm[FINISH_BLOCK / 32][4];
+  __shared__ unsigned smc[FINISH_BLOCK / 32][3];
   __shared__ int s_chunk[2];  // this chunk and the next, taken while this one runs
   __shared__ bool last;
   if (threadIdx.x == 0) {
@@ -1016,7 +1022,7 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
   else __syncthreads();
   const int stride = gridDim.x * blockDim.x;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n_chunks = (P.N + BLOCK - 1) / BLOCK;
+  const int n_chunks = (P.N + FINISH_BLOCK - 1) / FINISH_BLOCK;
   unsigned newly_blanked = 0, blanked_now = 0, oog = 0;
   bool want_sort = false;
   // neighbour lists, a step without a sort: the order is the previous step's (the last block
@@ -1036,7 +1042,7 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
     // the next chunk's index: its atomic runs while this chunk is processed (every thread
     // read s_chunk[buf ^ 1] before the previous chunk's barriers)
     if (threadIdx.x == 0) s_chunk[buf ^ 1] = (int)atomicAdd(D.finish_chunk, 1u);
-    const int q = chunk * BLOCK + threadIdx.x;
+    const int q = chunk * FINISH_BLOCK + threadIdx.x;
     double2 fc = make_double2(0., 0.), ft = make_double2(0., 0.);
     if (q < P.N) {
       double2 pos;
@@ -1092,7 +1098,7 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
       ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
       if (chunk_nz) {
         for (int k = 0; k < 4; ++k) r[k] = sm[0][k];
-        for (int w = 1; w < BLOCK / 32; ++w)
+        for (int w = 1; w < FINISH_BLOCK / 32; ++w)
           for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
       }
       for (int k = 0; k < 4; ++k) {
@@ -1114,7 +1120,7 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
   const bool block_wants_sort = __syncthreads_or(want_sort);
   if (threadIdx.x == 0) {
     unsigned long long cnt[3] = {smc[0][0], smc[0][1], smc[0][2]};
-    for (int w = 1; w < BLOCK / 32; ++w)
+    for (int w = 1; w < FINISH_BLOCK / 32; ++w)
       for (int k = 0; k < 3; ++k) cnt[k] += smc[w][k];
     if (block_wants_sort) D.st->want_sort = 1u;  // (before the fence and the ticket below)
     if (cnt[0]) atomicAdd(&D.st->newly_blanked, cnt[0]);
@@ -1146,7 +1152,7 @@ __global__ void __launch_bounds__(BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P
     for (int k = 0; k < 4; ++k) sm[threadIdx.x >> 5][k] = r[k];
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 1; w < BLOCK / 32; ++w)
+    for (int w = 1; w < FINISH_BLOCK / 32; ++w)
       for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
     // report_force: total contact force plus total friction force
     const double Fx = (r[0].s + r[0].c) + (r[2].s + r[2].c);
