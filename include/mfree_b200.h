@@ -132,9 +132,10 @@ int mf_ctx_destroy(mf_ctx *ctx);
 int mf_ctx_stream(mf_ctx *ctx, void **cuda_stream);   /* the stream all work is queued on */
 int mf_set_flags(mf_ctx *ctx, int flags);
 /* Skin of the mixed form's neighbour lists (a length; <= 0 restores the default, a tenth of
-   the cell size): each particle lists its candidates within 2 h + skin, and the cell list is
-   sorted again on the steps where some particle would otherwise be more than 0.45 skin from
-   where its list was built. No counterpart in the reference, which sorts every step. */
+   the cell size; larger values are limited to half the cell size): each particle lists its
+   candidates within 2 h + skin, and the cell list is sorted again on the steps where some
+   particle would otherwise be more than 0.45 skin from where its list was built. No
+   counterpart in the reference, which sorts every step. */
 int mf_set_neighbour_skin(mf_ctx *ctx, double skin);
 int mf_synchronize(mf_ctx *ctx);
 

@@ -235,7 +235,11 @@ void set_list_mode(mf_ctx *ctx) {
   // operations, computed once
   ctx->P.eos_c0 = (double)sqrtf((float)(ctx->P.phys.K / ctx->P.phys.rho0));
   ctx->P.verlet = list_mode(ctx) ? 1 : 0;
-  ctx->P.skin = (float)(ctx->skin > 0. ? ctx->skin : 0.1 * ctx->G.dx);
+  // at most half a cell: the lists are built over the 7x7 cells around a particle, which hold
+  // every candidate within 2 h + skin while h + skin / 2 is at most the cell size, and 64
+  // entries hold the candidates of a lattice with h = 1.5 spacings up to that skin
+  const double skin = ctx->skin > 0. ? ctx->skin : 0.1 * ctx->G.dx;
+  ctx->P.skin = (float)std::min(skin, 0.5 * ctx->G.dx);
 }
 
 #ifndef MF_USE_PDL

@@ -113,3 +113,20 @@ def test_sorts_every_step_outside_list_mode(mf):
         c = load_product(mf, st, **kw)
         c.step(5)
         assert c.status()["sorts"] == 5, kw
+
+
+def test_large_skin_is_limited(mf):
+    """A skin of ten cells is limited to half a cell: the lists stay complete and below their
+    64 entries (no error flag), and the run follows the form that sorts every step."""
+    st = perturbed_scene(mf, ny=12, seed=66, blank_frac=0.02)
+    a, b = pair(mf, st)
+    a.set_neighbour_skin(10.0 * st["grid"][2])
+    a.step(30)
+    b.step(30)
+    sa = a.status()
+    assert sa["error_flags"] == 0, sa["error_flags"]
+    assert sa["sorts"] < 30
+    assert np.array_equal(by_id(a, "blanked"), by_id(b, "blanked"))
+    for f in FIELDS:
+        x, y = by_id(a, f), by_id(b, f)
+        assert rel_err(x, y) < 1e-4, (f, rel_err(x, y), sa["sorts"])
