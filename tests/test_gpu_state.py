@@ -31,6 +31,29 @@ def test_resume_continues_bit_for_bit(mf, tmp_path, grid_kind):
         assert bits_equal(sa[f], sb[f]), f
 
 
+def test_mixed_resume(mf, tmp_path):
+    """The mixed form sorted every step resumes bit for bit; on neighbour lists a loaded state
+    starts with a sort (the lists are not saved), so the resumed run follows the uninterrupted
+    one to FP32 summation order."""
+    from conftest import rel_err
+    st = perturbed_scene(mf, ny=12, seed=52, blank_frac=0.01)
+    for flags, exact in ((mf.OPT_SORT_EVERY_STEP, True), (0, False)):
+        a = load_product(mf, st, precision=mf.PRECISION_MIXED, flags=flags)
+        a.step(5)
+        a.state_save(tmp_path / "m.bin")
+        a.step(5)
+        b = load_product(mf, st, precision=mf.PRECISION_MIXED, flags=flags)
+        b.state_load(tmp_path / "m.bin")
+        b.step(5)
+        oa, ob = np.argsort(a.get("id")), np.argsort(b.get("id"))
+        for f in ("pos", "vel", "S", "rho", "T", "eps_pl", "blanked"):
+            x, y = a.get(f)[oa], b.get(f)[ob]
+            if exact:
+                assert bits_equal(x, y), (f, flags)
+            else:
+                assert rel_err(x, y) < 1e-5, (f, rel_err(x, y))
+
+
 def test_corrupted_or_foreign_files_are_refused(mf, tmp_path):
     st = perturbed_scene(mf, ny=12, seed=52)
     a = load_product(mf, st)
