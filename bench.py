@@ -215,6 +215,15 @@ def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None,
     step_ms = np.array([a.elapsed_time(b) for a, b in ev])
     st = ctx.status()
     extra = {"sorts_in_timed_steps": int(st["sorts"] - sorts0)}
+    # the same number of steps back to back, one event pair, no flush (as a run executes them;
+    # a step's working set is about the L2's size, so this is reported beside, not instead)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        a.record(stream)
+        ctx.step(steps)
+        b.record(stream)
+    torch.cuda.synchronize(device)
+    extra["back_to_back_ms_per_step"] = a.elapsed_time(b) / steps
     stages = []
     with torch.cuda.stream(stream):
         for _ in range(max(5, min(20, steps // 4))):
@@ -745,12 +754,16 @@ def main():
                 {f: {k: v for k, v in r.items() if k != "status"} for f, r in results.items()},
                 mixed_over_fp64=results["mixed"]["value"] / results["fp64"]["value"],
                 mixed_sort_every_step_over_fp64=results["mixed_sort_every_step"]["value"] / results["fp64"]["value"],
+                mixed_over_fp64_back_to_back=(results["fp64"]["back_to_back_ms_per_step"]
+                                              / results["mixed"]["back_to_back_ms_per_step"]),
                 wall_s_per_mm_cut={f: r["ms_per_step"] * 1e-3 * spm for f, r in results.items()},
                 steps_per_mm_cut=spm,
                 note="mixed: neighbour lists between sorts (ms_per_step = timed steps + each step's share of a "
                      "sorting step's extra time at steps_per_sort); mixed_sort_every_step: the same FP32 pair "
                      "sums with the cell list sorted every step, as the FP64 form does; pair_kernel_ms: median "
-                     "of steps launched kernel by kernel (mf_step_timed) after an L2 flush"),
+                     "of steps launched kernel by kernel (mf_step_timed) after an L2 flush; "
+                     "back_to_back_ms_per_step: the same number of steps without flushes, one event pair "
+                     "(reported beside the flushed headline)"),
             "mixed_error": acc,
             "fp64_probe": fp64_probe,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
