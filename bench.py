@@ -36,7 +36,7 @@ METRIC = "particle-steps/s at ~150k particles w/ thermal contact: mixed vs FP64,
 ALGO_BYTES_PER_PARTICLE_STEP = 480.0
 # ncu summary of the pair kernel on this workload; its "dram bytes per launch" line is the
 # roofline's measured traffic
-PAIR_PROFILE = "profiles/k_pair_mixed_list_cut714x214.txt"
+PAIR_PROFILE = "profiles/k_pair_mixed_cut714x214.txt"
 FLUSH_BYTES = 256 << 20
 
 
@@ -189,8 +189,8 @@ def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None,
     """Per-step CUDA-event times (ms) of mf_step(1) with the L2 flushed between steps, then
     a few steps run kernel by kernel (mf_step_timed, L2 flushed) for the device time of each
     part: cell sort, predictor, interactions + rates (the pair kernel), corrector ..
-    plasticity. With neighbour lists (the mixed form) also one step that sorts and rebuilds
-    the lists, forced by a host write. With state_in the steps start from a saved state of the
+    plasticity. With neighbour lists (flags) also one step that sorts and rebuilds the lists,
+    forced by a host write. With state_in the steps start from a saved state of the
     same scene instead of its initial state."""
     ctx = mf.Context(device)
     ctx.upload_scene(scene, mf.GRID_GREEN)
@@ -214,7 +214,8 @@ def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None,
     torch.cuda.synchronize(device)
     step_ms = np.array([a.elapsed_time(b) for a, b in ev])
     st = ctx.status()
-    extra = {"sorts_in_timed_steps": int(st["sorts"] - sorts0)}
+    extra = {"sorts_in_timed_steps": int(st["sorts"] - sorts0),
+             "steps_per_sort": (warmup + steps) / max(st["sorts"], 1)}
     # the same number of steps back to back, one event pair, no flush (as a run executes them;
     # a step's working set is about the L2's size, so this is reported beside, not instead)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -232,7 +233,7 @@ def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None,
             stages.append(ctx.step_timed())
     stages = np.array(stages)
     extra["stage_ms_median"] = [float(x) for x in np.median(stages, axis=0)]
-    if precision == mf.PRECISION_MIXED and not flags & mf.OPT_SORT_EVERY_STEP:
+    if precision == mf.PRECISION_MIXED and flags & mf.OPT_NEIGHBOUR_LISTS:
         sort_ms = []
         with torch.cuda.stream(stream):
             for _ in range(3):
@@ -627,7 +628,7 @@ def main():
     ap.add_argument("--skin", type=float, default=0.0,
                     help="neighbour-list skin of the mixed form as a fraction of the cell size (0: the "
                          "library's default, a tenth)")
-    ap.add_argument("--forms", default="fp64,mixed_sort_every_step,mixed",
+    ap.add_argument("--forms", default="fp64,mixed,mixed_lists",
                     help="comma-separated forms to time (all three for the benchmark line; one, e.g. "
                          "'mixed', for a profiling run)")
     ap.add_argument("--lattice-scale", type=float, default=1.0,
@@ -673,9 +674,9 @@ def main():
 
     results = {}
     clocks = None
-    forms = [f for f in (("fp64", mf.PRECISION_FP64, 0),
-                         ("mixed_sort_every_step", mf.PRECISION_MIXED, mf.OPT_SORT_EVERY_STEP),
-                         ("mixed", mf.PRECISION_MIXED, 0)) if f[0] in args.forms.split(",")]
+    forms = [f for f in (("fp64", mf.PRECISION_FP64, 0), ("mixed", mf.PRECISION_MIXED, 0),
+                         ("mixed_lists", mf.PRECISION_MIXED, mf.OPT_NEIGHBOUR_LISTS | mf.OPT_FUSED_PREDICTOR))
+             if f[0] in args.forms.split(",")]
     for name, prec, flags in forms:
         if world > 1:
             torch.distributed.barrier()
@@ -688,7 +689,7 @@ def main():
         total_ms = max_over_ranks(float(step_ms.sum()), world, device=f"cuda:{device}")
         results[name] = {"ms_per_step": total_ms / args.steps, "pair_kernel_ms": float(np.median(pair_ms)),
                          "status": st, **extra}
-    if set(results) != {"fp64", "mixed_sort_every_step", "mixed"}:  # a profiling run: no benchmark line
+    if set(results) != {"fp64", "mixed", "mixed_lists"}:  # a profiling run: no benchmark line
         if rank == 0:
             print(json.dumps({"forms": {f: {k: v for k, v in r.items() if k != "status"}
                                         for f, r in results.items()}}), flush=True)
@@ -698,15 +699,12 @@ def main():
     acc = None
     if rank == 0 and args.accuracy_steps > 0:
         acc = accuracy(mf, scene, params, args.accuracy_steps, device)
-    # neighbour lists: the timed steps may hold fewer sorts than a long run; charge each step
-    # its share of a sorting step's extra time, at the long run's steps per sort
-    mx = results["mixed"]
-    steps_per_sort = (acc["steps"] / max(acc["mixed_sorts"], 1) if acc else
-                      (args.steps + args.warmup) / max(mx["status"]["sorts"], 1))
-    mx["steps_per_sort"] = steps_per_sort
-    mx["timed_ms_per_step"] = mx["ms_per_step"]
-    if mx["sorts_in_timed_steps"] < args.steps:  # (without lists, e.g. PSE, every timed step sorted)
-        mx["ms_per_step"] += max(0.0, mx["sort_step_ms"] - mx["timed_ms_per_step"]) / steps_per_sort
+    # neighbour lists: the timed steps may hold fewer sorts than a run; charge each step its
+    # share of a sorting step's extra time, at the context's steps per sort
+    ml = results["mixed_lists"]
+    ml["timed_ms_per_step"] = ml["ms_per_step"]
+    if ml["sorts_in_timed_steps"] < args.steps:  # (without lists, e.g. PSE, every timed step sorted)
+        ml["ms_per_step"] += max(0.0, ml["sort_step_ms"] - ml["timed_ms_per_step"]) / ml["steps_per_sort"]
     particles = sum_over_ranks(float(N), world, device=f"cuda:{device}")
     for name, r in results.items():
         r["value"] = particles / (r["ms_per_step"] * 1e-3)
@@ -753,14 +751,16 @@ def main():
             "forms": dict(
                 {f: {k: v for k, v in r.items() if k != "status"} for f, r in results.items()},
                 mixed_over_fp64=results["mixed"]["value"] / results["fp64"]["value"],
-                mixed_sort_every_step_over_fp64=results["mixed_sort_every_step"]["value"] / results["fp64"]["value"],
                 mixed_over_fp64_back_to_back=(results["fp64"]["back_to_back_ms_per_step"]
                                               / results["mixed"]["back_to_back_ms_per_step"]),
+                mixed_lists_over_fp64=results["mixed_lists"]["value"] / results["fp64"]["value"],
                 wall_s_per_mm_cut={f: r["ms_per_step"] * 1e-3 * spm for f, r in results.items()},
                 steps_per_mm_cut=spm,
-                note="mixed: neighbour lists between sorts (ms_per_step = timed steps + each step's share of a "
-                     "sorting step's extra time at steps_per_sort); mixed_sort_every_step: the same FP32 pair "
-                     "sums with the cell list sorted every step, as the FP64 form does; pair_kernel_ms: median "
+                note="mixed (the headline): FP32 pair sums, the cell list sorted every step as in the FP64 "
+                     "form; mixed_lists: the same sums on neighbour lists kept between sorts, with the fused "
+                     "predictor (experimental: it "
+                     "failed a 1 mm cut; ms_per_step = timed steps + each step's share of a sorting step's extra "
+                     "time at steps_per_sort); pair_kernel_ms: median "
                      "of steps launched kernel by kernel (mf_step_timed) after an L2 flush; "
                      "back_to_back_ms_per_step: the same number of steps without flushes, one event pair "
                      "(reported beside the flushed headline)"),

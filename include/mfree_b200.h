@@ -75,8 +75,14 @@ extern "C" {
 /* option bits for mf_set_flags */
 #define MF_OPT_KEEP_DERIVATIVES 1 /* also store S_der / v_der (the reference's public arrays) */
 #define MF_OPT_NO_GRAPHS 2        /* launch kernels directly instead of replaying CUDA graphs */
-#define MF_OPT_SORT_EVERY_STEP 4  /* mixed form: sort the cell list every step (as the FP64 form
-                                     does) instead of keeping neighbour lists between sorts */
+#define MF_OPT_SORT_EVERY_STEP 4  /* mixed form: sort the cell list every step, as the FP64 form
+                                     does (the default; overrides MF_OPT_NEIGHBOUR_LISTS) */
+#define MF_OPT_FUSED_PREDICTOR 8  /* with MF_OPT_NEIGHBOUR_LISTS: run the next step's predictor in
+                                     the finish kernel instead of the reorder kernel (faster) */
+#define MF_OPT_NEIGHBOUR_LISTS 16 /* mixed form: keep neighbour lists between cell-list sorts
+                                     (faster; experimental: over a 1 mm cut of the ~150k-particle
+                                     scene, 36 particles became non-finite after ~0.55 mm, which
+                                     the form that sorts every step does not show) */
 
 /* ---- constants (constants_structs.h:25-82), same member order ---- */
 typedef struct { double E, nu, rho0, K, G, mass, mass_tool; } mf_phys_constants;

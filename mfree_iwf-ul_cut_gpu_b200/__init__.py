@@ -24,7 +24,7 @@ GRID_GREEN, GRID_ROTHLIN = 0, 1
 THERMAL_BROOKSHAW, THERMAL_PSE = 0, 1
 JC_JOHNSON_COOK, JC_TANH = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-OPT_KEEP_DERIVATIVES, OPT_NO_GRAPHS, OPT_SORT_EVERY_STEP = 1, 2, 4
+OPT_KEEP_DERIVATIVES, OPT_NO_GRAPHS, OPT_SORT_EVERY_STEP, OPT_FUSED_PREDICTOR, OPT_NEIGHBOUR_LISTS = 1, 2, 4, 8, 16
 
 # name -> (field id, doubles per particle, is_int)
 FIELDS = {

@@ -221,11 +221,13 @@ bool fused_step(const mf_ctx *ctx) { return ctx->G.locked && !ctx->P.staged; }
 
 bool ready(const mf_ctx *ctx) { return ctx->has_particles && ctx->has_grid && ctx->has_constants; }
 
-// Neighbour lists for the mixed form (steps on a locked grid): its pair sums are not tied to
-// the reference's summation order, so the cell list need not be sorted every step. Not with
-// the PSE solver, whose window has no support cut-off, nor when asked to sort every step.
+// Neighbour lists for the mixed form (steps on a locked grid), when asked for: its pair sums
+// are not tied to the reference's summation order, so the cell list need not be sorted every
+// step. Not with the PSE solver, whose window has no support cut-off, nor when asked to sort
+// every step.
 bool list_mode(const mf_ctx *ctx) {
-  return ctx->P.precision == MF_PRECISION_MIXED && fused_step(ctx) && !(ctx->flags & MF_OPT_SORT_EVERY_STEP) &&
+  return ctx->P.precision == MF_PRECISION_MIXED && fused_step(ctx) && (ctx->flags & MF_OPT_NEIGHBOUR_LISTS) &&
+         !(ctx->flags & MF_OPT_SORT_EVERY_STEP) &&
          !(ctx->P.thermal_solver == MF_THERMAL_PSE && ctx->P.thermal_wp) &&
          (long long)ctx->N <= (long long)LIST_INDEX_MASK + 1;
 }
@@ -235,6 +237,7 @@ void set_list_mode(mf_ctx *ctx) {
   // operations, computed once
   ctx->P.eos_c0 = (double)sqrtf((float)(ctx->P.phys.K / ctx->P.phys.rho0));
   ctx->P.verlet = list_mode(ctx) ? 1 : 0;
+  ctx->P.fuse = ctx->P.verlet && (ctx->flags & MF_OPT_FUSED_PREDICTOR) ? 1 : 0;
   // at most half a cell: the lists are built over the 7x7 cells around a particle, which hold
   // every candidate within 2 h + skin while h + skin / 2 is at most the cell size, and 64
   // entries hold the candidates of a lattice with h = 1.5 spacings up to that skin

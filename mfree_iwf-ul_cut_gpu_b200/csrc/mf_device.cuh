@@ -47,6 +47,7 @@ struct params {
   // particle's predicted position is more than 0.45 skin from where its list was built; in
   // between, each particle's candidates within 2 h + skin are kept in a list
   int verlet;
+  int fuse;  // neighbour lists: the finish kernel also runs the next step's predictor
   float skin;
   double eos_c0;  // (double)sqrtf((float)(K / rho0)), the EOS sound speed (actions_gpu.cu:41-51)
   double dt;

@@ -815,7 +815,8 @@ __device__ __forceinline__ void tool_advance_shared(mf_tool_state &T, const dev_
 __device__ __forceinline__ void finish_particle(const params &P, const dev_buffers &D, const mf_tool_state &TL,
                                                const mf_joco_constants &JC, int q,
                                                double2 &pos_out, unsigned &f_out, double2 &fc_out, double2 &ft_out,
-                                               unsigned &newly_blanked, bool &want_sort, bool identity) {
+                                               unsigned &newly_blanked, bool &want_sort, bool identity,
+                                               bool fuse) {
   const state_set &A = D.A;
   const state_set &B = D.B;
   const double dt = P.dt;
@@ -975,7 +976,7 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
   B.eps_pl_dot[q] = eps_pl_dot;
   B.fc[q] = fc;
   B.ft[q] = ft;
-  if (identity) {
+  if (fuse) {
     // neighbour lists, a step without a sort: the next step keeps this order, so its
     // predictor runs here, on the final state still in registers, into the set the next step
     // writes (this step's start set, read above by this thread only). If the next step sorts,
@@ -1029,6 +1030,7 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
   // sets sort_now for the next step only after every block has read it here); such a step
   // also runs the next step's predictor
   const bool identity = P.verlet && !*(volatile unsigned *)&D.st->sort_now;
+  const bool fuse = identity && P.fuse;
   geom g{};
   double inv_dx = 0.;
   if (FUSE_HASH) {
@@ -1047,7 +1049,7 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
     if (q < P.N) {
       double2 pos;
       unsigned f;
-      finish_particle(P, D, s_tool, s_jc, q, pos, f, fc, ft, newly_blanked, want_sort, identity);
+      finish_particle(P, D, s_tool, s_jc, q, pos, f, fc, ft, newly_blanked, want_sort, identity, fuse);
       blanked_now += (f & FLAG_BLANKED) ? 1u : 0u;
       if (FUSE_HASH) {  // compute_hashes of the next step (grid.cu:34-51)
         long long hh;
@@ -1167,7 +1169,7 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
     if (P.verlet) {  // every particle is checked: the next step sorts if one asked for it
       D.st->sort_now = D.st->want_sort;
       D.st->want_sort = 0u;
-      D.st->predicted = identity ? 1u : 0u;
+      D.st->predicted = fuse ? 1u : 0u;
     }
     D.ticket[0] = 0u;
   }

@@ -38,7 +38,7 @@ def test_mixed_many_steps(mf):
     b = load_product(mf, st, precision=mf.PRECISION_MIXED)
     a.step(30)
     b.step(30)
-    # the mixed form keeps neighbour lists and sorts less often: compare particle by particle
+    # compare particle by particle (the array orders of two runs need not agree)
     oa, ob = np.argsort(a.get("id")), np.argsort(b.get("id"))
     assert np.array_equal(a.get("blanked")[oa], b.get("blanked")[ob])
     for f in ("pos", "vel", "rho", "S", "T"):

@@ -1,4 +1,5 @@
-"""Neighbour lists of the mixed form against the mixed form that sorts every step.
+"""Neighbour lists of the mixed form (opt-in, MF_OPT_NEIGHBOUR_LISTS) against the mixed form
+that sorts every step (the default).
 
 With neighbour lists the cell list is sorted only on the steps where some particle would
 otherwise be more than 0.45 skin from where its list was built; in between, each particle
@@ -24,18 +25,21 @@ def by_id(ctx, f):
 
 
 def pair(mf, st, **kw):
-    a = load_product(mf, st, precision=mf.PRECISION_MIXED, **kw)
+    a = load_product(mf, st, precision=mf.PRECISION_MIXED, flags=mf.OPT_NEIGHBOUR_LISTS, **kw)
     b = load_product(mf, st, precision=mf.PRECISION_MIXED, flags=mf.OPT_SORT_EVERY_STEP, **kw)
     return a, b
 
 
+@pytest.mark.parametrize("fused", [False, True])
 @pytest.mark.parametrize("blank_frac", [0.0, 0.05])
-def test_lists_equal_sorting_every_step(mf, blank_frac):
+def test_lists_equal_sorting_every_step(mf, blank_frac, fused):
     """A step on lists in which no particle changed cell: the same bits as sorting every step."""
     # the tool at rest and not in contact: slow particles, no sort after the first
     st = perturbed_scene(mf, ny=12, seed=61, blank_frac=blank_frac, tool_push_dx=0.0)
     st["tool"].vel[0] = st["tool"].vel[1] = 0.0
     a, b = pair(mf, st)
+    if fused:
+        a.set_flags(mf.OPT_NEIGHBOUR_LISTS | mf.OPT_FUSED_PREDICTOR)
     a.step(1)
     b.step(1)
     cells0 = by_id(b, "hash")
@@ -73,11 +77,14 @@ def test_thin_skin_sorts_every_step(mf):
     assert np.array_equal(a.force_log(), b.force_log())
 
 
-def test_lists_close_to_sorting_every_step(mf):
+@pytest.mark.parametrize("fused", [False, True])
+def test_lists_close_to_sorting_every_step(mf, fused):
     """The tool pushed into the workpiece: fast particles that cross cells and force sorts;
     only the FP32 summation order differs."""
     st = perturbed_scene(mf, ny=12, seed=65, blank_frac=0.02)
     a, b = pair(mf, st)
+    if fused:
+        a.set_flags(mf.OPT_NEIGHBOUR_LISTS | mf.OPT_FUSED_PREDICTOR)
     a.step(40)
     b.step(40)
     sa = a.status()
@@ -109,7 +116,8 @@ def test_lists_track_sorting_every_step_long(mf):
 
 def test_sorts_every_step_outside_list_mode(mf):
     st = perturbed_scene(mf, ny=10, seed=64)
-    for kw in ({"precision": mf.PRECISION_FP64}, {"precision": mf.PRECISION_MIXED, "thermal_solver": 1}):
+    for kw in ({"precision": mf.PRECISION_FP64}, {"precision": mf.PRECISION_MIXED},
+               {"precision": mf.PRECISION_MIXED, "thermal_solver": 1, "flags": mf.OPT_NEIGHBOUR_LISTS}):
         c = load_product(mf, st, **kw)
         c.step(5)
         assert c.status()["sorts"] == 5, kw

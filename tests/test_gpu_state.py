@@ -32,12 +32,12 @@ def test_resume_continues_bit_for_bit(mf, tmp_path, grid_kind):
 
 
 def test_mixed_resume(mf, tmp_path):
-    """The mixed form sorted every step resumes bit for bit; on neighbour lists a loaded state
-    starts with a sort (the lists are not saved), so the resumed run follows the uninterrupted
-    one to FP32 summation order."""
+    """The mixed form (sorted every step) resumes bit for bit; on neighbour lists a loaded
+    state starts with a sort (the lists are not saved), so the resumed run follows the
+    uninterrupted one to FP32 summation order."""
     from conftest import rel_err
     st = perturbed_scene(mf, ny=12, seed=52, blank_frac=0.01)
-    for flags, exact in ((mf.OPT_SORT_EVERY_STEP, True), (0, False)):
+    for flags, exact in ((0, True), (mf.OPT_NEIGHBOUR_LISTS, False)):
         a = load_product(mf, st, precision=mf.PRECISION_MIXED, flags=flags)
         a.step(5)
         a.state_save(tmp_path / "m.bin")
