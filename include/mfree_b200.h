@@ -235,6 +235,9 @@ typedef struct {
   double grid_bbmin[2], grid_bbmax[2], grid_h;
   double dt, t_final;
   double feed, speed;
+  int grid_max_cell; /* > 0: an adaptive grid of at most this many cells, its box taken from the
+                        particles at every sort (grid_gpu_green(max_cell, N), grid.cu:139-158);
+                        0: the locked box grid_bbmin .. grid_bbmax with cells of grid_h */
 } mf_scene;
 
 typedef struct {
@@ -268,8 +271,18 @@ int mf_cut_params_reference(mf_cut_params *p, int ny, double rake, double clear,
 int mf_scene_cut(const mf_cut_params *p, mf_scene **out);
 int mf_scene_setup_ref_cut(int ny, double rake, double clear, double chamfer, double speed, double feed,
                            mf_scene **out);
+/* the reference's two validation scenes, SI units, no tool (num_seg 0), no thermal constants:
+   setup_rings(nbox) (benchmarks.cpp:161-253): two rubber-like rings (inner radius 0.03, outer
+   0.04) moving at +-200 toward each other, locked box (-0.2, -0.08) .. (0.2, 0.08), no
+   plasticity; setup_impact(nbox) (benchmarks.cpp:23-159): a steel disc (radius 0.2) at 1000
+   against a wall of nbox/2 columns fixed at top and bottom, Johnson-Cook plasticity, an
+   adaptive Green grid of at most 10 N cells. nbox >= 2 lattice points across the outer
+   diameter. */
+int mf_scene_setup_rings(int nbox, mf_scene **out);
+int mf_scene_setup_impact(int nbox, mf_scene **out);
 int mf_scene_free(mf_scene *scene);
-/* particles + locked Green/Rothlin grid + constants + tool + dt from a scene */
+/* particles + grid (locked box, or adaptive when grid_max_cell > 0) + constants + tool + dt
+   from a scene */
 int mf_scene_upload(mf_ctx *ctx, const mf_scene *scene, int grid_kind);
 
 /* ---- host tool geometry (tool.cpp): the (tl, length, height, rake, clear, r, mu) constructor,

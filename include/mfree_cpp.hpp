@@ -8,7 +8,8 @@
 //   leap_frog                      leap_frog.h:36-50
 //   tool, tool_gpu_*               tool.h:36-144, tool_gpu.h:29-35
 //   actions_setup_* / interactions_setup_*   actions_gpu.h:59-63, interactions_gpu.h:36-51
-//   setup_ref_cut                  benchmarks.h:48
+//   setup_ref_cut, setup_rings,    benchmarks.h:48, benchmarks.cpp:23-253
+//   setup_impact
 //   report_force                   output.h:26
 //   vtk_writer_write               vtk_writer.h:28-29
 //   global_dt, global_t_final, global_tool, global_step   benchmarks.cpp:20-21, mfree_gpu.cpp:46-48
@@ -274,19 +275,21 @@ class tool_wear {
 };
 inline tool_wear *global_wear = nullptr;
 
-// ---- setup_ref_cut (benchmarks.cpp:255-537) ----
-inline particle_gpu *setup_ref_cut(int ny, grid_base **grid, double rake = 0., double clear = 0., double chamfer = 0.,
-                                   double speed = 0., double feed = 0.01) {
-  mf_scene *sc = nullptr;
-  mfree::check(mf_scene_setup_ref_cut(ny, rake, clear, chamfer, speed, feed, &sc), "setup_ref_cut");
+// ---- the scenes of benchmarks.cpp: a host scene made into particles, a grid and constants ----
+// (the grid is the scene's locked box, or adaptive when the scene asks for one; a scene
+// with a tool also becomes global_tool)
+inline particle_gpu *particles_from_scene(mf_scene *sc, grid_base **grid) {
   std::vector<float2_t> pos((size_t)sc->N), vel((size_t)sc->N);
   for (int i = 0; i < sc->N; ++i) {
     pos[i] = {sc->pos[2 * i], sc->pos[2 * i + 1]};
     vel[i] = {sc->vel[2 * i], sc->vel[2 * i + 1]};
   }
   particle_gpu *p = new particle_gpu(pos.data(), vel.data(), sc->rho, sc->T, sc->h, sc->fixed, sc->tool_p, sc->N);
-  *grid = new grid_gpu_green(sc->N, float2_t{sc->grid_bbmin[0], sc->grid_bbmin[1]},
-                             float2_t{sc->grid_bbmax[0], sc->grid_bbmax[1]}, sc->grid_h);
+  if (sc->grid_max_cell > 0)
+    *grid = new grid_gpu_green((unsigned)sc->grid_max_cell, (unsigned)sc->N);
+  else
+    *grid = new grid_gpu_green(sc->N, float2_t{sc->grid_bbmin[0], sc->grid_bbmin[1]},
+                               float2_t{sc->grid_bbmax[0], sc->grid_bbmax[1]}, sc->grid_h);
   auto &C = mfree_constants();
   C.phys = sc->phys;
   C.corr = sc->corr;
@@ -295,11 +298,33 @@ inline particle_gpu *setup_ref_cut(int ny, grid_base **grid, double rake = 0., d
   C.trml_wp = sc->trml_wp;
   C.trml_tool = sc->trml_tool;
   C.apply();
-  global_tool = new tool();
-  global_tool->s = sc->tool;
-  mfree::check(mf_tool_set(p->ctx, &global_tool->s), "tool_gpu_set_up_tool");
+  if (sc->tool.num_seg > 0) {
+    global_tool = new tool();
+    global_tool->s = sc->tool;
+    mfree::check(mf_tool_set(p->ctx, &global_tool->s), "tool_gpu_set_up_tool");
+  }
   global_dt = sc->dt;
   global_t_final = sc->t_final;
   mf_scene_free(sc);
   return p;
+}
+
+// setup_ref_cut (benchmarks.cpp:255-537)
+inline particle_gpu *setup_ref_cut(int ny, grid_base **grid, double rake = 0., double clear = 0., double chamfer = 0.,
+                                   double speed = 0., double feed = 0.01) {
+  mf_scene *sc = nullptr;
+  mfree::check(mf_scene_setup_ref_cut(ny, rake, clear, chamfer, speed, feed, &sc), "setup_ref_cut");
+  return particles_from_scene(sc, grid);
+}
+
+// setup_rings (benchmarks.cpp:161-253) and setup_impact (benchmarks.cpp:23-159): no tool
+inline particle_gpu *setup_rings(int nbox, grid_base **grid) {
+  mf_scene *sc = nullptr;
+  mfree::check(mf_scene_setup_rings(nbox, &sc), "setup_rings");
+  return particles_from_scene(sc, grid);
+}
+inline particle_gpu *setup_impact(int nbox, grid_base **grid) {
+  mf_scene *sc = nullptr;
+  mfree::check(mf_scene_setup_impact(nbox, &sc), "setup_impact");
+  return particles_from_scene(sc, grid);
 }

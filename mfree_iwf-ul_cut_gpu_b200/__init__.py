@@ -99,7 +99,7 @@ class SceneStruct(C.Structure):
                 ("phys", Phys), ("corr", Corr), ("joco", Joco), ("trml_wp", Trml), ("trml_tool", Trml),
                 ("has_joco", C.c_int), ("tool", ToolState), ("grid_bbmin", C.c_double * 2),
                 ("grid_bbmax", C.c_double * 2), ("grid_h", C.c_double), ("dt", C.c_double), ("t_final", C.c_double),
-                ("feed", C.c_double), ("speed", C.c_double)]
+                ("feed", C.c_double), ("speed", C.c_double), ("grid_max_cell", C.c_int)]
 
 
 class CutParams(C.Structure):
@@ -154,6 +154,8 @@ def lib():
         "mf_cut_params_reference": ([C.POINTER(CutParams), i, d, d, d, d, d], i),
         "mf_scene_cut": ([C.POINTER(CutParams), C.POINTER(C.POINTER(SceneStruct))], i),
         "mf_scene_setup_ref_cut": ([i, d, d, d, d, d, C.POINTER(C.POINTER(SceneStruct))], i),
+        "mf_scene_setup_rings": ([i, C.POINTER(C.POINTER(SceneStruct))], i),
+        "mf_scene_setup_impact": ([i, C.POINTER(C.POINTER(SceneStruct))], i),
         "mf_scene_free": ([C.POINTER(SceneStruct)], i),
         "mf_scene_upload": ([vp, C.POINTER(SceneStruct), i], i),
         "mf_tool_construct": ([d] * 8 + [C.POINTER(ToolState)], i),
@@ -196,6 +198,24 @@ class Scene:
         rc = lib().mf_scene_setup_ref_cut(ny, rake, clear, chamfer, speed, feed, C.byref(out))
         if rc != MF_OK:
             raise MfError(rc, "mf_scene_setup_ref_cut")
+        return cls(out)
+
+    @classmethod
+    def rings(cls, nbox):
+        """setup_rings(nbox) (benchmarks.cpp:161-253): two colliding rubber-like rings."""
+        out = C.POINTER(SceneStruct)()
+        rc = lib().mf_scene_setup_rings(int(nbox), C.byref(out))
+        if rc != MF_OK:
+            raise MfError(rc, "mf_scene_setup_rings")
+        return cls(out)
+
+    @classmethod
+    def impact(cls, nbox):
+        """setup_impact(nbox) (benchmarks.cpp:23-159): a steel disc against a fixed wall."""
+        out = C.POINTER(SceneStruct)()
+        rc = lib().mf_scene_setup_impact(int(nbox), C.byref(out))
+        if rc != MF_OK:
+            raise MfError(rc, "mf_scene_setup_impact")
         return cls(out)
 
     @classmethod

@@ -1188,8 +1188,11 @@ int mf_status_get(mf_ctx *ctx, mf_status *out) {
 int mf_scene_upload(mf_ctx *ctx, const mf_scene *s, int grid_kind) {
   if (!ctx || !s) return MF_ERR_INVALID;
   TRY(mf_particles_create(ctx, s->N, s->pos, s->vel, s->rho, s->T, s->h, s->fixed, s->tool_p, nullptr));
-  TRY(mf_grid_create_locked(ctx, grid_kind, s->grid_bbmin[0], s->grid_bbmin[1], s->grid_bbmax[0], s->grid_bbmax[1],
-                            s->grid_h));
+  if (s->grid_max_cell > 0)
+    TRY(mf_grid_create_adaptive(ctx, grid_kind, s->grid_max_cell));
+  else
+    TRY(mf_grid_create_locked(ctx, grid_kind, s->grid_bbmin[0], s->grid_bbmin[1], s->grid_bbmax[0],
+                              s->grid_bbmax[1], s->grid_h));
   TRY(mf_set_constants(ctx, &s->phys, &s->corr, s->has_joco ? &s->joco : nullptr, &s->trml_wp, &s->trml_tool));
   TRY(mf_tool_set(ctx, &s->tool));
   TRY(mf_set_dt(ctx, s->dt));

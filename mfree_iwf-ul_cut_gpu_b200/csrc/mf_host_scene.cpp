@@ -519,6 +519,168 @@ int mf_scene_setup_ref_cut(int ny, double rake, double clear, double chamfer, do
   return mf_scene_cut(&p, out);
 }
 
+namespace {
+
+// a scene of N particles with every array allocated (velocities zero) and no tool
+mf_scene *scene_alloc(int N) {
+  mf_scene *S = new (std::nothrow) mf_scene;
+  if (!S) return nullptr;
+  std::memset(S, 0, sizeof(*S));
+  S->N = N;
+  S->n_workpiece = N;
+  S->pos = (double *)std::malloc(sizeof(double) * 2 * (size_t)N);
+  S->vel = (double *)std::calloc(2 * (size_t)N, sizeof(double));
+  S->rho = (double *)std::calloc((size_t)N, sizeof(double));
+  S->T = (double *)std::calloc((size_t)N, sizeof(double));
+  S->h = (double *)std::calloc((size_t)N, sizeof(double));
+  S->fixed = (double *)std::calloc((size_t)N, sizeof(double));
+  S->tool_p = (double *)std::calloc((size_t)N, sizeof(double));
+  if (!S->pos || !S->vel || !S->rho || !S->T || !S->h || !S->fixed || !S->tool_p) {
+    mf_scene_free(S);
+    return nullptr;
+  }
+  return S;
+}
+
+// elastic constants from E, nu and rho0, with the particle mass of a dx x dx cell
+void set_elastic(mf_phys_constants &phys, double E, double nu, double rho0, double dx) {
+  std::memset(&phys, 0, sizeof(phys));
+  phys.E = E;
+  phys.nu = nu;
+  phys.rho0 = rho0;
+  phys.G = phys.E / (2. * (1. + phys.nu));
+  phys.K = 2.0 * phys.G * (1 + phys.nu) / (3 * (1 - 2 * phys.nu));
+  phys.mass = dx * dx * phys.rho0;
+}
+
+// the correction constants both validation scenes use, with W(dx) at h = hdx dx
+void set_validation_corr(mf_corr_constants &corr, double dx, double hdx) {
+  std::memset(&corr, 0, sizeof(corr));
+  corr.alpha = 1.;
+  corr.beta = 1.;
+  corr.eta = 0.1;
+  corr.xspheps = 0.5;
+  corr.stresseps = 0.3;
+  double h1 = 1. / (hdx * dx);
+  double q = dx * h1;
+  double fac = 10 * (M_1_PI) / 7.0 * h1 * h1;
+  corr.wdeltap = fac * (1 - 1.5 * q * q * (1 - 0.5 * q));
+}
+
+}  // namespace
+
+// setup_rings (benchmarks.cpp:161-253): a lattice of nbox x nbox points over the square
+// [-ro, ro]^2 keeps the annulus ri <= r < ro, once shifted left and once right by ro + 0.001,
+// the two copies interleaved point by point; the left ring moves at +200, the right at -200
+// (the 170 of the time-step formula is not the velocity given)
+int mf_scene_setup_rings(int nbox, mf_scene **out) {
+  if (!out) return MF_ERR_INVALID;
+  *out = nullptr;
+  if (nbox < 2 || nbox > 46340) return MF_ERR_INVALID;
+  const double ri = 0.03, ro = 0.04;
+  const double spacing = ro + 0.001;
+  const double dx = 2 * ro / (nbox - 1);
+  const double hdx = 1.7;
+
+  std::vector<v2> pos;
+  for (int i = 0; i < nbox; i++) {
+    for (int j = 0; j < nbox; j++) {
+      double px = -ro + i * dx, py = -ro + j * dx;
+      double dist = std::sqrt(px * px + py * py);
+      if (dist < ro && dist >= ri) {
+        pos.push_back(mk(px - spacing, py));
+        pos.push_back(mk(px + spacing, py));
+      }
+    }
+  }
+  // the reference holds the points in an array of nbox^2 and asserts that fewer were made
+  if (pos.empty() || pos.size() >= (size_t)nbox * (size_t)nbox) return MF_ERR_INVALID;
+  const int n = (int)pos.size();
+
+  mf_scene *S = scene_alloc(n);
+  if (!S) return MF_ERR_NOMEM;
+  set_elastic(S->phys, 1e7, 0.4, 1., dx);
+  set_validation_corr(S->corr, dx, hdx);
+  const double vel_ring = 170.;
+  S->t_final = 2.5 * ro / vel_ring;
+  S->dt = 0.5 * hdx * dx / (std::sqrt(S->phys.K / S->phys.rho0) + std::sqrt(vel_ring));
+  for (int i = 0; i < n; i++) {
+    S->pos[2 * i] = pos[i].x;
+    S->pos[2 * i + 1] = pos[i].y;
+    S->rho[i] = S->phys.rho0;
+    S->h[i] = hdx * dx;
+    S->vel[2 * i] = (pos[i].x < 0) ? 200 : -200;
+  }
+  S->grid_bbmin[0] = -5 * ro; S->grid_bbmin[1] = -2 * ro;
+  S->grid_bbmax[0] = 5 * ro; S->grid_bbmax[1] = 2 * ro;
+  S->grid_h = hdx * dx;
+  *out = S;
+  return MF_OK;
+}
+
+// setup_impact (benchmarks.cpp:23-159): the flyer is the disc r < ro of an nbox x nbox lattice
+// over [-ro, ro]^2 shifted left by ro + 0.05, at +1000; the wall is nbox/2 columns from x = 0
+// and the rows y = j dx - 1 <= 1, its top and bottom rows fixed; T = Tref everywhere
+int mf_scene_setup_impact(int nbox, mf_scene **out) {
+  if (!out) return MF_ERR_INVALID;
+  *out = nullptr;
+  if (nbox < 2 || nbox > 4096) return MF_ERR_INVALID;
+  const double ro = 0.2;
+  const double dx = 2 * ro / (nbox - 1);
+  const double hdx = 1.7;
+  const double spacing = ro + 0.05;
+
+  std::vector<v2> pos;
+  for (int i = 0; i < nbox; i++) {
+    for (int j = 0; j < nbox; j++) {
+      double px = -ro + i * dx, py = -ro + j * dx;
+      double dist = std::sqrt(px * px + py * py);
+      if (dist < ro) pos.push_back(mk(px - spacing, py));
+    }
+  }
+  const int n_flyer = (int)pos.size();
+  for (int i = 0; i < nbox / 2; i++) {
+    for (int j = 0; j < 10 * nbox; j++) {
+      if (j * dx - 1. > 1.) continue;
+      pos.push_back(mk(i * dx, j * dx - 1.));
+    }
+  }
+  const int n = (int)pos.size();
+  if (n == 0) return MF_ERR_INVALID;
+
+  mf_scene *S = scene_alloc(n);
+  if (!S) return MF_ERR_NOMEM;
+  set_elastic(S->phys, 200e9, 0.29, 7830.0, dx);
+  set_validation_corr(S->corr, dx, hdx);
+  mf_joco_constants &joco = S->joco;
+  std::memset(&joco, 0, sizeof(joco));
+  joco.A = 792.0e6;
+  joco.B = 510.0e6;
+  joco.C = 0.014;
+  joco.m = 1.03;
+  joco.n = 0.26;
+  joco.Tref = 273.0;
+  joco.Tmelt = 1793.0;
+  joco.eps_dot_ref = 1;
+  S->has_joco = 1;
+  const double vel_flyer = 1e3;
+  S->dt = 0.3 * hdx * dx / (std::sqrt(S->phys.K / S->phys.rho0) + std::sqrt(vel_flyer));
+  S->t_final = 2 * ro / vel_flyer;
+  for (int i = 0; i < n; i++) {
+    S->pos[2 * i] = pos[i].x;
+    S->pos[2 * i + 1] = pos[i].y;
+    S->rho[i] = S->phys.rho0;
+    S->h[i] = hdx * dx;
+    if (i < n_flyer) S->vel[2 * i] = 1e3;
+    S->fixed[i] = (pos[i].y < -1 + dx / 2 || pos[i].y > 1 - dx / 2) ? 1. : 0.;
+    S->T[i] = joco.Tref;
+  }
+  S->grid_max_cell = 10 * n;
+  S->grid_h = hdx * dx;
+  *out = S;
+  return MF_OK;
+}
+
 // tool triangles for VTK (vtk_writer.cpp:185-264)
 int mf_vtk_write_tool(const mf_tool_state *ts, const char *path) {
   if (!ts || !path) return MF_ERR_INVALID;

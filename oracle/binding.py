@@ -150,6 +150,7 @@ def ref():
         L.refh_get_constants.argtypes = [C.c_void_p]
         L.refh_get_grid.argtypes = [C.c_void_p]
         L.refh_get_scene_tool.argtypes = [C.c_void_p] * 4
+        L.refh_get_grid_max_cell.restype = C.c_int
         _ref = L
     return _ref
 

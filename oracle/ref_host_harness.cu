@@ -44,6 +44,7 @@ struct recorded {
   phys_constants contact_phys;
   tool *contact_tool = 0;
   grid_base *grid = 0;
+  unsigned int grid_max_cell = 0;  // max_cell of an adaptive grid_gpu_green, 0 for a locked one
 };
 recorded g_rec;
 
@@ -121,9 +122,13 @@ particle_gpu::particle_gpu(float2_t *pos, float2_t *vel_init, float_t *rho, floa
 }
 
 // grid_gpu_green: geometry only (the buffers are device memory; not needed here)
-grid_gpu_green::grid_gpu_green(unsigned int max_cell, unsigned int N) : grid_base(max_cell, N) {}
+grid_gpu_green::grid_gpu_green(unsigned int max_cell, unsigned int N) : grid_base(max_cell, N) {
+  g_rec.grid_max_cell = max_cell;
+}
 grid_gpu_green::grid_gpu_green(int num_part, float2_t bbmin, float2_t bbmax, float_t h)
-    : grid_base(num_part, bbmin, bbmax, h) {}
+    : grid_base(num_part, bbmin, bbmax, h) {
+  g_rec.grid_max_cell = 0;
+}
 void grid_gpu_green::sort(particle_gpu *, tool *) const {}
 void grid_gpu_green::get_cells(particle_gpu *, int *, int *) {}
 
@@ -240,14 +245,20 @@ int refh_setup_ref_cut(int ny, double rake, double clear, double chamfer, double
   (void)p;
   return (int)g_rec.N;
 }
+// (each setup starts from an empty record and no tool: the rings and impact scenes set
+// neither Johnson-Cook nor thermal constants nor a tool)
 int refh_setup_rings(int nbox) {
   grid_base *grid = 0;
+  g_rec = recorded();
+  global_tool = 0;
   setup_rings(nbox, &grid);
   g_rec.grid = grid;
   return (int)g_rec.N;
 }
 int refh_setup_impact(int nbox) {
   grid_base *grid = 0;
+  g_rec = recorded();
+  global_tool = 0;
   setup_impact(nbox, &grid);
   g_rec.grid = grid;
   return (int)g_rec.N;
@@ -302,6 +313,8 @@ int refh_get_grid(double *out) {
   out[8] = g->is_locked() ? 1. : 0.;
   return 9;
 }
+// max_cell of the last scene's grid when it is an adaptive grid_gpu_green, else 0
+int refh_get_grid_max_cell() { return (int)g_rec.grid_max_cell; }
 // the scene's tool (after positioning) and its velocity
 int refh_get_scene_tool(double *seg_out, double *fillet_out, double *misc_out, double *vel_out) {
   if (!global_tool) return -1;

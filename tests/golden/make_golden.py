@@ -6,7 +6,8 @@ geometric_primitives.cpp, kernels.cuh, plasticity.cuh), compiled where they lie 
 oracle/build_oracle.py into oracle/_ref/libref_host.so, on seeded inputs. They pin the
 oracle and the product's host code on machines where the reference tree is absent.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py              # every fixture
+    python tests/golden/make_golden.py validation   # the rings and impact scenes only
 """
 from __future__ import annotations
 
@@ -29,6 +30,13 @@ SCENES = {
     "ref_cut_default": (30, 10.0, 8.0, 0.002, SPEED_70, 0.01),
     "ref_cut_ny12_rake0": (12, 0.0, 7.0, 0.0005, 1.16667e-4, 0.005),
     "ref_cut_sharp": (16, 5.0, 8.0, 0.0, SPEED_70, 0.01),
+}
+VALIDATION = {
+    # name: (setup function, nbox)
+    "ref_rings_nbox40": ("rings", 40),
+    "ref_rings_nbox21": ("rings", 21),
+    "ref_impact_nbox30": ("impact", 30),
+    "ref_impact_nbox17": ("impact", 17),
 }
 JC_REF = [0.00862, 0.00331, 0.01, 0.34, 0.8, 1836.0, 300.0, 1e-6, 1.1, 0.4, 12.0, 1.0]
 TOOLS = [
@@ -224,11 +232,35 @@ def vtk_particles(R, rng, n=400):
     np.savez_compressed(HERE / "ref_vtk_particles.npz", vtk=np.frombuffer(data, dtype=np.uint8), **d)
 
 
+def validation_scene(R, name, kind, nbox):
+    """setup_rings / setup_impact (benchmarks.cpp:161-253, 23-159): arrays, constants, grid."""
+    n = (R.refh_setup_rings if kind == "rings" else R.refh_setup_impact)(nbox)
+    out = {"kind": np.array(kind), "nbox": np.array(nbox), "N": np.array(n)}
+    for k, f in enumerate(["pos", "vel", "rho", "T", "h", "fixed", "tool_p"]):
+        w = 2 if f in ("pos", "vel") else 1
+        a = np.zeros(n * w)
+        R.refh_get_array(k, _p(a))
+        out[f] = a
+    c = np.zeros(64)
+    k = R.refh_get_constants(_p(c))
+    out["constants"] = c[:k]
+    g = np.zeros(9)
+    R.refh_get_grid(_p(g))
+    out["grid"] = g
+    out["grid_max_cell"] = np.array(R.refh_get_grid_max_cell())
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    return n
+
+
 def main():
     build_oracle.build_ref()
     R = B.ref()
     if R is None:
         raise SystemExit("the reference tree is not available; fixtures cannot be regenerated here")
+    for name, (kind, nbox) in VALIDATION.items():
+        print(name, validation_scene(R, name, kind, nbox))
+    if sys.argv[1:] == ["validation"]:
+        return
     rng = np.random.default_rng(20261203)
     for name, args in SCENES.items():
         print(name, scene(R, name, args))

@@ -139,3 +139,46 @@ def test_particle_vtk_file_byte_equal(mf, golden, tmp_path):
     fields["blanked"] = np.zeros(len(g["rho"]))
     mf.vtk_write_particle_arrays(tmp_path / "p.vtk", fields)
     assert (tmp_path / "p.vtk").read_bytes() == bytes(g["vtk"])
+
+
+VALIDATION = ("ref_rings_nbox40", "ref_rings_nbox21", "ref_impact_nbox30", "ref_impact_nbox17")
+
+
+@pytest.mark.parametrize("name", VALIDATION)
+def test_validation_scenes_bitwise(mf, orc, golden, name):
+    """mf_scene_setup_rings / mf_scene_setup_impact against the reference's own setup_rings /
+    setup_impact (benchmarks.cpp:161-253, 23-159): arrays, constants, time step and grid."""
+    g = golden(name)
+    kind, nbox = str(g["kind"]), int(g["nbox"])
+    sc = (mf.Scene.rings if kind == "rings" else mf.Scene.impact)(nbox)
+    s = sc.s
+    assert sc.N == int(g["N"]) and s.n_workpiece == sc.N and s.n_tool == 0
+    for k in ARRAYS:
+        assert bits_equal(sc.array(k).reshape(-1), g[k]), k
+    c = scene_constants(mf, s)
+    c[-1] = float(s.has_joco)  # rings set no Johnson-Cook constants (no plasticity)
+    assert bits_equal(c, g["constants"])
+    assert s.has_joco == (1 if kind == "impact" else 0)
+    assert s.tool.num_seg == 0 and s.tool.has_fillet == 0
+    locked = bool(g["grid"][8])
+    assert s.grid_max_cell == int(g["grid_max_cell"])
+    assert locked == (s.grid_max_cell == 0) == (kind == "rings")
+    if locked:  # the box through grid_base::set_geometry gives the reference's grid
+        o = orc.Oracle(sc.N)
+        o.L.orc_set_grid_locked(o.s, 0, s.grid_bbmin[0], s.grid_bbmin[1], s.grid_bbmax[0], s.grid_bbmax[1],
+                                s.grid_h)
+        geo = o.geometry()
+        nx, ny, bx0, by0, bx1, by1, dx, nc, _ = g["grid"]
+        assert (geo["nx"], geo["ny"], geo["num_cell"]) == (int(nx), int(ny), int(nc))
+        assert bits_equal([geo["bbmin_x"], geo["bbmin_y"], geo["bbmax_x"], geo["bbmax_y"], geo["dx"]],
+                          [bx0, by0, bx1, by1, dx])
+    else:
+        assert s.grid_max_cell == 10 * sc.N
+
+
+@pytest.mark.parametrize("nbox", [-3, 0, 1])
+def test_validation_scenes_refuse_degenerate_lattices(mf, nbox):
+    for make in (mf.Scene.rings, mf.Scene.impact):
+        with pytest.raises(mf.MfError) as e:
+            make(nbox)
+        assert e.value.code == -1  # MF_ERR_INVALID
