@@ -360,6 +360,11 @@ int mf_batch_destroy(mf_batch *batch);
    conduction, Johnson-Cook law only (MF_ERR_INVALID otherwise). ---- */
 int mf_tangent_mean_force(mf_ctx *ctx, int skip_steps, int window_steps, int param, double out_mean[2],
                           double out_dmean[2]);
+/* the same for all six parameters in one pass (six tangent directions carried together):
+   out_dmean[2k], out_dmean[2k + 1] = d(mean Fc), d(mean Ff) with respect to parameter k =
+   A, B, n, C, m, mu; each equals what mf_tangent_mean_force returns for param k. */
+int mf_tangent_mean_force_all(mf_ctx *ctx, int skip_steps, int window_steps, double out_mean[2],
+                              double out_dmean[12]);
 
 /* ---- measurement aid (no counterpart in the reference): FP64 FMA throughput of the device
    (TFLOP/s, 2 flops per FMA) and the latency in SM clock cycles of one dependent double

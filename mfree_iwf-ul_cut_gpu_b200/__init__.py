@@ -141,6 +141,7 @@ def lib():
         "mf_step": ([vp, i], i), "mf_step_timed": ([vp, vp], i), "mf_step_stage": ([vp, i], i), "mf_report_force": ([vp, vp], i),
         "mf_probe_fp64": ([i, vp, vp, vp, vp, vp], i),
         "mf_tangent_mean_force": ([vp, i, i, i, vp, vp], i),
+        "mf_tangent_mean_force_all": ([vp, i, i, vp, vp], i),
         "mf_tool_wear_usui": ([vp, d, d, vp], i), "mf_vtk_write_particles_async": ([vp, C.c_char_p], i),
         "mf_state_save": ([vp, C.c_char_p], i), "mf_state_load": ([vp, C.c_char_p], i),
         "mf_get_field_device": ([vp, i, vp, vp], i), "mf_set_field_device": ([vp, i, vp, vp], i),
@@ -381,6 +382,16 @@ class Context:
         self._check(self.L.mf_tangent_mean_force(self.h, int(skip_steps), int(window_steps), int(param), _ptr(mean),
                                                  _ptr(dmean)), "mf_tangent_mean_force")
         return mean, dmean
+
+    def tangent_mean_force_all(self, skip_steps, window_steps):
+        """Mean (Fc, Ff) as tangent_mean_force, with its derivatives with respect to all six
+        parameters from one pass: row k of the (6, 2) array is d(mean Fc, mean Ff) / d(A, B, n,
+        C, m, mu)[k] (mf_tangent_mean_force_all)."""
+        mean = np.zeros(2)
+        dmean = np.zeros(12)
+        self._check(self.L.mf_tangent_mean_force_all(self.h, int(skip_steps), int(window_steps), _ptr(mean),
+                                                     _ptr(dmean)), "mf_tangent_mean_force_all")
+        return mean, dmean.reshape(6, 2)
 
     def set_options(self, thermal_solver=THERMAL_BROOKSHAW, jc_model=JC_JOHNSON_COOK, precision=PRECISION_FP64):
         self._check(self.L.mf_set_options(self.h, thermal_solver, jc_model, precision), "mf_set_options")

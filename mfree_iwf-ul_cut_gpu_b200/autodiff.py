@@ -6,8 +6,8 @@
 
 `ctx` is a product Context holding the scene's state (it is not advanced). The forward pass
 runs the FP64 step on dual numbers with no derivative direction; the backward pass runs it once
-per parameter with that parameter's derivative carried forward through every step, and
-returns grad_output times those six derivatives. This module is the only PyTorch in the
+more with all six parameters' derivatives carried forward together through every step
+(mf_tangent_mean_force_all), and returns grad_output times those six derivatives. This module is the only PyTorch in the
 package; it imports torch on use.
 """
 from __future__ import annotations
@@ -52,11 +52,8 @@ def _function_class():
         def backward(fctx, grad_out):
             (theta,) = fctx.saved_tensors
             apply_parameters(fctx.ctx, theta.detach().cpu().tolist())
-            grads = []
-            for k in range(len(PARAMS)):
-                _, dmean = fctx.ctx.tangent_mean_force(fctx.skip, fctx.window, k)
-                grads.append(dmean[0])
-            g = torch.tensor(grads, dtype=torch.float64) * grad_out
+            _, dmean = fctx.ctx.tangent_mean_force_all(fctx.skip, fctx.window)
+            g = torch.tensor(dmean[:, 0].copy(), dtype=torch.float64) * grad_out
             return g, None, None, None
 
     return MeanCuttingForce

@@ -19,11 +19,16 @@
 using namespace mf;
 
 namespace mf {
+// the differentiable step (csrc/mf_tangent.cu): one derivative direction (tg), all six (tg6);
+// out_dmean holds d(mean Fc), d(mean Ff) per direction
 namespace tg {
-// the differentiable step (csrc/mf_tangent.cu)
 int run_mean_force(mf_ctx *ctx, int device, params P, const dev_buffers &Dctx, int skip_steps, int window_steps,
-                   int param, double out_mean[2], double out_dmean[2]);
+                   int param, double out_mean[2], double out_dmean[]);
 }  // namespace tg
+namespace tg6 {
+int run_mean_force(mf_ctx *ctx, int device, params P, const dev_buffers &Dctx, int skip_steps, int window_steps,
+                   int param, double out_mean[2], double out_dmean[]);
+}  // namespace tg6
 }  // namespace mf
 
 // one asynchronous particle dump: a device snapshot of the fields, their copy into pinned
@@ -1582,16 +1587,35 @@ int mf_vtk_write_particles_async(mf_ctx *ctx, const char *path) {
 
 }  // extern "C"
 
-int mf_tangent_mean_force(mf_ctx *ctx, int skip_steps, int window_steps, int param, double out_mean[2],
-                          double out_dmean[2]) {
-  if (!ctx || !out_mean || skip_steps < 0 || window_steps < 1 || param < -1 || param > 5) return MF_ERR_INVALID;
+namespace {
+// the contexts the differentiable step covers: a locked Green grid, Brookshaw or no
+// conduction, and the Johnson-Cook law
+int tangent_check(mf_ctx *ctx) {
   if (!ready(ctx) || ctx->mid_step) return MF_ERR_STATE;
   if (!(ctx->P.dt > 0.)) return MF_ERR_STATE;
-  // the differentiable step covers the locked Green grid, Brookshaw or no conduction, and
-  // the Johnson-Cook law
   if (!ctx->G.locked || ctx->grid_kind != MF_GRID_GREEN || ctx->P.thermal_solver == MF_THERMAL_PSE ||
       ctx->P.jc_model != MF_JC_JOHNSON_COOK || !ctx->P.plastic)
     return MF_ERR_INVALID;
+  return MF_OK;
+}
+}  // namespace
+
+int mf_tangent_mean_force_all(mf_ctx *ctx, int skip_steps, int window_steps, double out_mean[2],
+                              double out_dmean[12]) {
+  if (!ctx || !out_mean || !out_dmean || skip_steps < 0 || window_steps < 1) return MF_ERR_INVALID;
+  TRY(tangent_check(ctx));
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  params P = ctx->P;
+  P.N = ctx->N;
+  P.staged = 0;
+  return mf::tg6::run_mean_force(ctx, ctx->device, P, ctx->D, skip_steps, window_steps, -1, out_mean, out_dmean);
+}
+
+int mf_tangent_mean_force(mf_ctx *ctx, int skip_steps, int window_steps, int param, double out_mean[2],
+                          double out_dmean[2]) {
+  if (!ctx || !out_mean || skip_steps < 0 || window_steps < 1 || param < -1 || param > 5) return MF_ERR_INVALID;
+  TRY(tangent_check(ctx));
   TRY(set_device(ctx));
   CK(cudaStreamSynchronize(ctx->stream));
   params P = ctx->P;

@@ -84,9 +84,25 @@ def test_autograd_function(mf):
     mean, _ = ctx.tangent_mean_force(0, WINDOW, -1)
     assert math.isclose(float(fc.detach()), mean[0], rel_tol=0, abs_tol=0)
     (2.0 * fc).backward()
+    _, d6 = ctx.tangent_mean_force_all(0, WINDOW)
+    for k in range(6):
+        assert float(theta.grad[k]) == 2.0 * d6[k, 0], ad.PARAMS[k]
+
+
+def test_all_six_directions_in_one_pass(mf):
+    """Six tangent directions carried together: the value and each direction's derivatives are
+    those of the single-direction pass. Each direction's arithmetic is the same expression,
+    independent of the others, so they are expected bit for bit; the derivative tolerance 1e-9
+    leaves room only for a different fused multiply-add contraction grown over the window."""
+    st, ctx = loaded_scene(mf)
+    mean6, d6 = ctx.tangent_mean_force_all(0, WINDOW)
+    mean1, _ = ctx.tangent_mean_force(0, WINDOW, -1)
+    np.testing.assert_allclose(mean6, mean1, rtol=1e-13, atol=0.0)
+    assert d6.shape == (6, 2)
     for k in range(6):
         _, d = ctx.tangent_mean_force(0, WINDOW, k)
-        assert float(theta.grad[k]) == 2.0 * d[0], ad.PARAMS[k]
+        np.testing.assert_allclose(d6[k], d, rtol=1e-9, atol=1e-9 * np.abs(d).max())
+        assert np.abs(d6[k, 0]) > 0.0, k
 
 
 def test_unsupported_settings_are_rejected(mf):
@@ -94,6 +110,8 @@ def test_unsupported_settings_are_rejected(mf):
     ctx.set_options(mf.THERMAL_PSE, mf.JC_JOHNSON_COOK, mf.PRECISION_FP64)
     with pytest.raises(mf.MfError):
         ctx.tangent_mean_force(0, 5, 0)
+    with pytest.raises(mf.MfError):
+        ctx.tangent_mean_force_all(0, 5)
     ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_TANH, mf.PRECISION_FP64)
     with pytest.raises(mf.MfError):
         ctx.tangent_mean_force(0, 5, 0)
