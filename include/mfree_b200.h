@@ -143,6 +143,13 @@ int mf_set_flags(mf_ctx *ctx, int flags);
    particle would otherwise be more than 0.45 skin from where its list was built. No
    counterpart in the reference, which sorts every step. */
 int mf_set_neighbour_skin(mf_ctx *ctx, double skin);
+/* Diagnostic of the neighbour lists (no counterpart in the reference), O(N^2): after a step on
+   lists, counts the pairs of unblanked, finite particles closer than 2 h_i in the current pair
+   records (*pairs) and those of them missing from the lists (*missing, 0 when the lists hold
+   what they promise). *stale = 1 when the records are already the next step's (fused predictor)
+   and that step sorts, so that the lists need not hold for them. MF_ERR_STATE unless the last
+   step ran on neighbour lists. */
+int mf_list_check(mf_ctx *ctx, long long *pairs, long long *missing, int *stale);
 int mf_synchronize(mf_ctx *ctx);
 
 /* ---- particles: particle_gpu(...) constructors (particle_gpu.h:81-86, particle_gpu.cu:97-125).

@@ -128,7 +128,8 @@ def lib():
     sig = {
         "mf_version": ([], i), "mf_error_string": ([i], C.c_char_p), "mf_last_cuda_error": ([vp], i),
         "mf_ctx_create": ([i, C.POINTER(vp)], i), "mf_ctx_destroy": ([vp], i),
-        "mf_ctx_stream": ([vp, C.POINTER(vp)], i), "mf_set_flags": ([vp, i], i), "mf_set_neighbour_skin": ([vp, C.c_double], i), "mf_synchronize": ([vp], i),
+        "mf_ctx_stream": ([vp, C.POINTER(vp)], i), "mf_set_flags": ([vp, i], i), "mf_set_neighbour_skin": ([vp, C.c_double], i),
+        "mf_list_check": ([vp, vp, vp, vp], i), "mf_synchronize": ([vp], i),
         "mf_particles_create": ([vp, i] + [vp] * 8, i), "mf_particles_count": ([vp, ip], i),
         "mf_get_field": ([vp, i, vp], i), "mf_set_field": ([vp, i, vp], i),
         "mf_grid_create_locked": ([vp, i, d, d, d, d, d], i), "mf_grid_create_adaptive": ([vp, i, i], i),
@@ -402,6 +403,15 @@ class Context:
     def set_neighbour_skin(self, skin):
         """Mixed form: skin of the neighbour lists (<= 0: a tenth of the cell size)."""
         self._check(self.L.mf_set_neighbour_skin(self.h, float(skin)), "mf_set_neighbour_skin")
+
+    def list_check(self):
+        """After a step on neighbour lists: the in-support pairs of the current pair records, how
+        many of them the lists miss, and whether the records are already those of a next step
+        that sorts (then the lists need not hold for them) (mf_list_check; O(N^2))."""
+        pairs, missing, stale = C.c_longlong(), C.c_longlong(), C.c_int()
+        self._check(self.L.mf_list_check(self.h, C.byref(pairs), C.byref(missing), C.byref(stale)),
+                    "mf_list_check")
+        return {"pairs": pairs.value, "missing": missing.value, "stale": bool(stale.value)}
 
     def set_dt(self, dt):
         self._check(self.L.mf_set_dt(self.h, dt), "mf_set_dt")

@@ -525,6 +525,45 @@ int mf_set_neighbour_skin(mf_ctx *ctx, double skin) {
   return MF_OK;
 }
 
+int mf_list_check(mf_ctx *ctx, long long *pairs, long long *missing, int *stale) {
+  if (!ctx || !pairs || !missing) return MF_ERR_INVALID;
+  if (!ready(ctx) || ctx->mid_step) return MF_ERR_STATE;
+  if (!ctx->P.verlet) return MF_ERR_STATE;  // the last step did not run on neighbour lists
+  TRY(set_device(ctx));
+  CK(cudaStreamSynchronize(ctx->stream));
+  dev_status st;
+  CK(cudaMemcpy(&st, ctx->D.st, sizeof(st), cudaMemcpyDeviceToHost));
+  const int N = ctx->N;
+  const int nb = (N + BLOCK - 1) / BLOCK;
+  double2 *abs = nullptr;
+  unsigned long long *out = nullptr;
+  unsigned long long h[2] = {0ull, 0ull};
+  cudaError_t e = cudaMalloc(&abs, sizeof(double2) * (size_t)N);
+  if (e == cudaSuccess) e = cudaMalloc(&out, sizeof(h));
+  if (e == cudaSuccess) e = cudaMemsetAsync(out, 0, sizeof(h), ctx->stream);
+  if (e == cudaSuccess) {
+    params P = ctx->P;
+    P.N = N;
+    k_list_abs<<<nb, BLOCK, 0, ctx->stream>>>(N, ctx->D, abs);
+    k_list_check<<<nb, BLOCK, 0, ctx->stream>>>(P, ctx->D, abs, out);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (abs) cudaFree(abs);
+  if (out) cudaFree(out);
+  if (e != cudaSuccess) {
+    ctx->last_cuda_err = (int)e;
+    return e == cudaErrorMemoryAllocation ? MF_ERR_NOMEM : MF_ERR_CUDA;
+  }
+  *pairs = (long long)h[0];
+  *missing = (long long)h[1];
+  // with the fused predictor the records may already be the next step's; the lists hold for
+  // them only if that step does not sort
+  if (stale) *stale = (st.predicted && st.sort_now) ? 1 : 0;
+  return MF_OK;
+}
+
 int mf_synchronize(mf_ctx *ctx) {
   if (!ctx) return MF_ERR_INVALID;
   TRY(set_device(ctx));

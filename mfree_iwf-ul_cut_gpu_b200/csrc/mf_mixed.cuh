@@ -142,6 +142,54 @@ __device__ __forceinline__ int build_list(const dev_buffers &D, const float4 *__
   return cnt;
 }
 
+// The neighbour-list invariant by brute force (a diagnostic: all N^2 pairs). k_list_abs puts
+// every particle's position in FP64 from its pair record (origin of the cell of the last sort
+// plus the FP32 offset); k_list_check then requires of every particle i that has a list (not
+// blanked, finite, not a tool particle without heat conduction) that each unblanked, finite j
+// closer than 2 h_i (h_i of the record, less a 1e-5 relative margin; the pair kernel's
+// zero-distance cut-off 1e-8 left out) is among the ncount[i] entries of its row.
+// out[0] += such pairs, out[1] += those missing from the lists.
+static __global__ void k_list_abs(int N, dev_buffers D, double2 *abs) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  const float4 b0 = reinterpret_cast<const float4 *>(D.recf)[j];
+  const geom g = *D.g;
+  const int hj = D.hash_cur[j];
+  const int cx = hj / g.ny, cy = hj - cx * g.ny;
+  abs[j] = make_double2(g.bbmin_x + cx * g.dx + (double)b0.x, g.bbmin_y + cy * g.dx + (double)b0.y);
+}
+
+static __global__ void k_list_check(params P, dev_buffers D, const double2 *__restrict__ abs,
+                                    unsigned long long *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.N) return;
+  const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
+  const unsigned fi = (unsigned)__float_as_int(r0[i].z) & 0xffu;
+  if (fi & (FLAG_BLANKED | FLAG_NONFINITE)) return;
+  if ((fi & FLAG_TOOL) && P.thermal_solver != MF_THERMAL_BROOKSHAW) return;  // no pair sums
+  const double h = (double)r0[2 * (size_t)P.N + i].w;
+  const double lim = 4. * h * h * (1. - 1e-5);
+  const double2 xi = abs[i];
+  const unsigned *row = D.nlist + (size_t)i * LIST_CAP;
+  const int cnt = min(D.ncount[i], LIST_CAP);
+  unsigned long long pairs = 0, missing = 0;
+  for (int j = 0; j < P.N; ++j) {
+    if (j == i) continue;
+    const unsigned fj = (unsigned)__float_as_int(r0[j].z);
+    if (fj & (FLAG_BLANKED | FLAG_NONFINITE)) continue;
+    const double2 xj = abs[j];
+    const double dx = xi.x - xj.x, dy = xi.y - xj.y;
+    const double rr2 = dx * dx + dy * dy;
+    if (!(rr2 < lim) || rr2 < 1e-8) continue;
+    ++pairs;
+    bool found = false;
+    for (int k = 0; k < cnt && !found; ++k) found = (row[k] & LIST_INDEX_MASK) == (unsigned)j;
+    if (!found) ++missing;
+  }
+  if (pairs) atomicAdd(out, pairs);
+  if (missing) atomicAdd(out + 1, missing);
+}
+
 // LIST: the neighbour-list form (steps with P.verlet). 80 registers (6 blocks of 128 per SM)
 // keep both forms free of spills; the list form measured slower at 7 and 8 blocks per SM
 template <bool LIST>

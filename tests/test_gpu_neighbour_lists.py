@@ -138,3 +138,36 @@ def test_large_skin_is_limited(mf):
     for f in FIELDS:
         x, y = by_id(a, f), by_id(b, f)
         assert rel_err(x, y) < 1e-4, (f, rel_err(x, y), sa["sorts"])
+
+
+@pytest.mark.parametrize("fused", [False, True])
+def test_lists_hold_every_in_support_pair(mf, fused):
+    """The list invariant checked by brute force after every step (mf_list_check): with the
+    scene's random velocities 30 times faster (the fastest particles reach 0.45 skin in a few
+    steps) and the tool cutting, the lists are reused up to their limit and rebuilt many times;
+    every unblanked pair closer than 2 h_i in the pair records must be in the lists."""
+    st = perturbed_scene(mf, ny=12, seed=68, blank_frac=0.02)
+    st["vel"] = st["vel"] * 30.0
+    flags = mf.OPT_NEIGHBOUR_LISTS | (mf.OPT_FUSED_PREDICTOR if fused else 0)
+    ctx = load_product(mf, st, precision=mf.PRECISION_MIXED, flags=flags)
+    checked = 0
+    for k in range(80):
+        ctx.step(1)
+        r = ctx.list_check()
+        live = int((ctx.get("blanked") == 0.0).sum())
+        assert r["pairs"] > 10 * live, (k, r, live)  # ~24 in-support neighbours per particle
+        if not r["stale"]:
+            assert r["missing"] == 0, (k, r)
+            checked += 1
+    s = ctx.status()
+    assert s["error_flags"] == 0
+    assert 2 <= s["sorts"] < 80, s["sorts"]
+    assert checked >= (80 if not fused else 40), checked
+
+
+def test_list_check_needs_a_list_step(mf):
+    st = perturbed_scene(mf, ny=8, seed=69)
+    ctx = load_product(mf, st, precision=mf.PRECISION_MIXED)  # sorts every step: no lists
+    ctx.step(2)
+    with pytest.raises(mf.MfError):
+        ctx.list_check()
