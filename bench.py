@@ -715,6 +715,10 @@ def main():
         peak_src = "measured"
     else:
         peak, peak_src = 6650.0, "fallback"
+    for r in results.values():  # every form on the same canonical bytes: whole step, pair kernel
+        r["roofline_frac_step"] = ALGO_BYTES_PER_PARTICLE_STEP * N / (r["ms_per_step"] * 1e-3) / 1e9 / peak
+        r["roofline_frac_pair_kernel"] = (ALGO_BYTES_PER_PARTICLE_STEP * N / (r["pair_kernel_ms"] * 1e-3) / 1e9
+                                          / peak)
     head = results["mixed"]
     achieved = ALGO_BYTES_PER_PARTICLE_STEP * N / (head["pair_kernel_ms"] * 1e-3) / 1e9
     step_achieved = ALGO_BYTES_PER_PARTICLE_STEP * N / (head["ms_per_step"] * 1e-3) / 1e9
