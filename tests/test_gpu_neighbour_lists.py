@@ -146,7 +146,10 @@ def test_lists_hold_every_in_support_pair(mf, fused):
     scene's random velocities 30 times faster (the fastest particles reach 0.45 skin in a few
     steps) and the tool cutting, the lists are reused up to their limit and rebuilt many times;
     every unblanked pair closer than 2 h_i in the pair records must be in the lists."""
-    st = perturbed_scene(mf, ny=12, seed=68, blank_frac=0.02)
+    # (the tool one cell into the workpiece: where tool and workpiece particles overlap the
+    # candidates within 2h + skin double, and three cells of overlap would bring them near the
+    # 64 entries of a row)
+    st = perturbed_scene(mf, ny=12, seed=68, blank_frac=0.02, tool_push_dx=1.0)
     st["vel"] = st["vel"] * 30.0
     flags = mf.OPT_NEIGHBOUR_LISTS | (mf.OPT_FUSED_PREDICTOR if fused else 0)
     ctx = load_product(mf, st, precision=mf.PRECISION_MIXED, flags=flags)
