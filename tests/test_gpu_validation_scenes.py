@@ -25,8 +25,9 @@ from conftest import bits_equal, rel_err
 
 pytestmark = pytest.mark.gpu
 
+# (idx too: the Rothlin grid carries it through every sort as the particle's number)
 LOADED = ("pos", "vel", "rho", "T", "h", "fixed", "tool_p", "S", "eps_pl", "eps_pl_dot", "fc", "ft", "n",
-          "pos_t", "vel_t", "rho_t", "S_t", "T_t", "blanked")
+          "pos_t", "vel_t", "rho_t", "S_t", "T_t", "blanked", "idx")
 STATE = ("pos", "vel", "S", "rho", "T", "eps_pl", "eps_pl_dot")
 RATES = ("pos_t", "vel_t", "S_t", "rho_t")
 FLOAT_ROUNDED = {"eps_pl_dot": 1e-7}
