@@ -113,3 +113,29 @@ def test_validation_scene_steps_against_oracle(mf, orc, kind, nbox, grid_kind, s
         wall = ctx.get("pos")[:, 0] > -0.01
         assert np.abs(vel[wall & ~fixed]).max() > 0.0
         assert np.all(vel[fixed] == 0.0)
+
+
+@pytest.mark.parametrize("kind,nbox,grid_kind", [("rings", 21, 0), ("impact", 17, 0), ("impact", 17, 1)])
+def test_mixed_form_rates_on_validation_scenes(mf, kind, nbox, grid_kind):
+    """The mixed form (FP32 pair sums on cell-relative coordinates) on the SI-unit scenes and
+    the adaptive grid: one step's rates against the FP64 form's from the same state, after a few
+    FP64 steps so that the rings touch and the disc's support reaches the wall (norm-wise 1e-4,
+    as on the cut)."""
+    sc = getattr(mf.Scene, kind)(nbox)
+    a = mf.Context(0)
+    a.upload_scene(sc, grid_kind)
+    a.step(5)
+    b = mf.Context(0)
+    b.upload_scene(sc, grid_kind)
+    for f in LOADED:
+        b.set(f, a.get(f))
+    b.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, mf.PRECISION_MIXED)
+    for ctx in (a, b):
+        for s in range(3):  # cell list, predictor, pair sums and rates
+            ctx.stage(s)
+    nb = a.get("blanked") == 0.0
+    for f in RATES:
+        x, y = b.get(f)[nb], a.get(f)[nb]
+        assert np.isfinite(x).all(), f
+        assert np.abs(y).max() > 0.0, f
+        assert rel_err(x, y) < 1e-4, (f, rel_err(x, y))
