@@ -494,8 +494,19 @@ def batch_run(mf, torch, n_instances, steps, device):
             "blanked": sum(x["blanked"] for x in st), "error_flags": max(x["error_flags"] for x in st)}
 
 
+REF_FUNCTIONS = ("the reference's own kernels.cuh / plasticity.cuh functions (cubic_spline, lapl_pse, "
+                 "sigma_yield, solve_secant) compiled for the host, inside the C restatement's OpenMP loops over "
+                 "the same cell lists")
+
+
+def cpu_kind(orc, o):
+    """Put oracle state `o` on the reference's host-compiled per-particle functions where they
+    were built (cpu_baseline kind "reference"), else leave the restatement ("port")."""
+    return "reference" if orc.use_reference_functions(o) else "port"
+
+
 def cpu_baseline(mf, scene, seconds=12.0, max_steps=5000):
-    """The oracle port (C, OpenMP, all host threads) on the same scene: bounded sample."""
+    """The CPU path (C, OpenMP, all host threads) on the same scene: bounded sample."""
     sys.path.insert(0, str(ROOT / "oracle"))
     sys.path.insert(0, str(ROOT / "tests"))
     import binding as orc
@@ -505,6 +516,7 @@ def cpu_baseline(mf, scene, seconds=12.0, max_steps=5000):
     build_oracle.build_oracle()
     st = scene_state(mf, scene)
     o = load_oracle(orc, st)
+    kind = cpu_kind(orc, o)
     o.L.orc_step(o.s)  # warm-up (first-touch of the pages)
     t0 = time.perf_counter()
     o.L.orc_step(o.s)
@@ -513,9 +525,10 @@ def cpu_baseline(mf, scene, seconds=12.0, max_steps=5000):
     t0 = time.perf_counter()
     o.L.orc_steps(o.s, k)
     dt = time.perf_counter() - t0
+    what = REF_FUNCTIONS if kind == "reference" else "the C restatement, OpenMP"
     return {"value": scene.N * k / dt, "unit": "particle-steps/s", "cores": int(orc.lib().orc_get_threads()),
-            "kind": "port", "sample": f"{k} steps of the full {scene.N}-particle scene after 1 warm-up step "
-                                      f"(oracle C restatement, OpenMP), {dt:.1f} s"}
+            "kind": kind, "sample": f"{k} steps of the full {scene.N}-particle scene after 1 warm-up step "
+                                    f"({what}), {dt:.1f} s"}
 
 
 def scene_state(mf, scene):
@@ -560,6 +573,7 @@ def run_reference(args):
 
     build_oracle.build_oracle()
     o = load_oracle(orc, scene_state(mf, scene), thermal_solver=solver)
+    kind = cpu_kind(orc, o)
     # each "step" is one full oracle step; bound the run to a few minutes
     o.L.orc_step(o.s)
     t0 = time.perf_counter()
@@ -579,9 +593,10 @@ def run_reference(args):
             "warmup": warm, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": dict(workload, name=args.config, n_particles=scene.N, n_tool=scene.s.n_tool),
-            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": cores, "kind": kind,
                              "sample": f"{steps} full steps of the {scene.N}-particle scene (requested "
-                                       f"{args.steps}), C restatement of the reference step, OpenMP"},
+                                       f"{args.steps}), " + (REF_FUNCTIONS if kind == "reference" else
+                                                             "C restatement of the reference step, OpenMP")},
             "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0

@@ -92,6 +92,7 @@ def lib():
         L.orc_cells.argtypes = [C.c_void_p, C.c_int]
         L.orc_num_cell.argtypes = [C.c_void_p]
         L.orc_set_tool.argtypes = [C.c_void_p, C.POINTER(OrcTool)]
+        L.orc_set_reference_functions.argtypes = [C.c_void_p] * 5
         L.orc_get_tool.argtypes = [C.c_void_p, C.POINTER(OrcTool)]
         for f in ("orc_grid_update", "orc_step"):
             getattr(L, f).argtypes = [C.c_void_p]
@@ -135,6 +136,8 @@ def ref():
         L.refh_sigma_yield_tanh.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
         L.refh_solve_secant.restype = C.c_double
         L.refh_solve_secant.argtypes = [C.c_void_p, C.c_int] + [C.c_double] * 7
+        L.refh_solve_secant_jc.restype = C.c_double
+        L.refh_solve_secant_jc.argtypes = [C.c_void_p] + [C.c_double] * 7
         L.refh_tool_create.argtypes = [C.c_double] * 8
         L.refh_tool_create_points.argtypes = [C.c_void_p, C.c_double, C.c_double]
         L.refh_tool_dump.argtypes = [C.c_void_p] * 3
@@ -153,6 +156,20 @@ def ref():
         L.refh_get_grid_max_cell.restype = C.c_int
         _ref = L
     return _ref
+
+
+def use_reference_functions(o) -> bool:
+    """Run oracle state `o` on the reference's own host-compiled per-particle functions
+    (kernels.cuh cubic_spline, lapl_pse; plasticity.cuh sigma_yield, solve_secant) instead of
+    the restatements; False (nothing changed) where the reference's sources were not built."""
+    R = ref()
+    if R is None:
+        return False
+    fns = [C.cast(getattr(R, n), C.c_void_p) for n in
+           ("refh_cubic_spline", "refh_lapl_pse", "refh_sigma_yield", "refh_solve_secant_jc")]
+    o.L.orc_set_reference_functions(o.s, *fns)
+    o._ref_fns = fns
+    return True
 
 
 def joco_struct(jc12) -> OrcJoco:

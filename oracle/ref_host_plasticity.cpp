@@ -40,4 +40,11 @@ double refh_solve_secant(const double *jc12, int model, double init, double tol,
   return r;
 }
 
+// solve_secant with the reference's default yield law (m_s_yield = sigma_yield, untouched):
+// safe to call from several threads at once
+double refh_solve_secant_jc(const double *jc12, double init, double tol, double norm_Strial, double eps_pl_init,
+                            double T, double dt, double mu) {
+  return solve_secant(make_jc(jc12), init, tol, norm_Strial, eps_pl_init, T, dt, mu);
+}
+
 }  // extern "C"

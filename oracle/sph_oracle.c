@@ -59,6 +59,11 @@ struct orc_state {
   orc_tool tool;
   double dt;
   long long out_of_grid;
+  /* the reference's host-compiled functions, when set (orc_set_reference_functions) */
+  orc_ref_kernel_fn ref_kernel;
+  orc_ref_pse_fn ref_pse;
+  orc_ref_yield_fn ref_yield;
+  orc_ref_secant_fn ref_secant;
 };
 
 static int g_threads = 0;
@@ -181,6 +186,14 @@ void orc_set_constants(orc_state *s, const orc_phys *phys, const orc_corr *corr,
   s->thermal_bc = s->trml_tool.alpha != 0.;   /* actions_gpu.cu:466-468 */
   s->thermal_wp = s->trml_wp.alpha != 0.;     /* interactions_gpu.cu:443 */
   s->thermal_tool_on = s->trml_tool.alpha != 0.; /* interactions_gpu.cu:453 */
+}
+
+void orc_set_reference_functions(orc_state *s, orc_ref_kernel_fn kernel, orc_ref_pse_fn pse,
+                                 orc_ref_yield_fn yield, orc_ref_secant_fn secant) {
+  s->ref_kernel = kernel;
+  s->ref_pse = pse;
+  s->ref_yield = yield;
+  s->ref_secant = secant;
 }
 
 void orc_set_options(orc_state *s, int thermal_solver, int jc_model) {
@@ -767,13 +780,18 @@ static void plasticity_johnson_cook(orc_state *s) {
     double eps_pl = s->eps_pl[i], eps_pl_dot = s->eps_pl_dot[i], T = s->T[i];
     double svm = sqrtf((float)((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz +
                                3.0 * cxy * cxy));
-    double sigma_Y = orc_sigma_yield(jc, eps_pl, eps_pl_dot, T);
+    const int ref_jc = s->jc_model == 0;  /* the reference's functions cover its default law */
+    double sigma_Y = (s->ref_yield && ref_jc) ? s->ref_yield((const double *)jc, eps_pl, eps_pl_dot, T)
+                                               : orc_sigma_yield(jc, eps_pl, eps_pl_dot, T);
     if (svm < sigma_Y) {
       s->eps_pl_dot[i] = 0.;
       continue;
     }
-    double delta_lambda = orc_solve_secant(jc, s->jc_model, fmax(eps_pl_dot * dt * sqrt(2. / 3.), 1e-8), 1e-6,
-                                           norm_Strial, eps_pl, T, dt, s->phys.G, NULL);
+    const double init = fmax(eps_pl_dot * dt * sqrt(2. / 3.), 1e-8);
+    double delta_lambda =
+        (s->ref_secant && ref_jc)
+            ? s->ref_secant((const double *)jc, init, 1e-6, norm_Strial, eps_pl, T, dt, s->phys.G)
+            : orc_solve_secant(jc, s->jc_model, init, 1e-6, norm_Strial, eps_pl, T, dt, s->phys.G, NULL);
     double eps_pl_new = eps_pl + (double)(sqrtf((float)(2.0 / 3.0)) * fmaxf((float)delta_lambda, 0.f));
     double eps_pl_dot_new = (double)(sqrtf((float)(2.0 / 3.0)) * fmaxf((float)delta_lambda, 0.f)) / dt;
     s->eps_pl[i] = eps_pl_new;
@@ -786,7 +804,8 @@ static void plasticity_johnson_cook(orc_state *s) {
     s->S[i] = S_new;
     if (s->trml_wp.tq != 0.) {
       double delta_eps_pl = eps_pl_new - eps_pl;
-      double sY = orc_sigma_yield(jc, eps_pl_new, eps_pl_dot_new, T);
+      double sY = (s->ref_yield && ref_jc) ? s->ref_yield((const double *)jc, eps_pl_new, eps_pl_dot_new, T)
+                                           : orc_sigma_yield(jc, eps_pl_new, eps_pl_dot_new, T);
       double rho = s->rho[i];
       s->T[i] += s->trml_wp.tq / (s->trml_wp.cp * rho) * delta_eps_pl * sY;
     }
@@ -889,7 +908,14 @@ static void interactions_monaghan(orc_state *s) {
           double is_tool_particle_j = s->tool_particle[iter];
           double volj = mass / rhoj;
           double rhoj21 = 1. / (rhoj * rhoj);
-          d3 ww = cubic_spline(pi, pj, hi);
+          d3 ww;
+          if (s->ref_kernel) {
+            double o3[3];
+            s->ref_kernel(pi.x, pi.y, pj.x, pj.y, hi, o3);
+            ww.x = o3[0]; ww.y = o3[1]; ww.z = o3[2];
+          } else {
+            ww = cubic_spline(pi, pj, hi);
+          }
           double w = ww.x, w_x = ww.y, w_y = ww.z;
           if (!(is_tool_particle_i == 1.) && !(is_tool_particle_j == 1.)) {
             vi_der.x += (vj.x - vi.x) * w_x * volj;
@@ -982,7 +1008,7 @@ static void interactions_heat_pse(orc_state *s) {
         for (int iter = c_start; iter < c_end; iter++) {
           d2 pj = s->pos[iter];
           double Tj = s->T[iter], rhoj = s->rho[iter];
-          double w2_pse = lapl_pse(pi, pj, hi);
+          double w2_pse = s->ref_pse ? s->ref_pse(pi.x, pi.y, pj.x, pj.y, hi) : lapl_pse(pi, pj, hi);
           T_ti += (Tj - Ti) * w2_pse * mass / rhoj;
         }
       }

@@ -76,6 +76,19 @@ void orc_set_constants(orc_state *s, const orc_phys *phys, const orc_corr *corr,
                        const orc_trml *trml_wp, const orc_trml *trml_tool);
 /* thermal_solver: 0 Brookshaw, 1 PSE. jc_model: 0 Johnson-Cook, 1 tanh variant */
 void orc_set_options(orc_state *s, int thermal_solver, int jc_model);
+/* The reference's own per-particle functions in place of this file's restatements at their call
+   sites: kernels.cuh cubic_spline and lapl_pse, plasticity.cuh sigma_yield and solve_secant (the
+   Johnson-Cook law; the tanh law keeps the restatement), compiled for the host by
+   oracle/build_oracle.py (refh_cubic_spline, refh_lapl_pse, refh_sigma_yield,
+   refh_solve_secant_jc). The Johnson-Cook constants are passed as the 12 doubles of orc_joco.
+   NULL pointers restore the restatements. */
+typedef void (*orc_ref_kernel_fn)(double xi, double yi, double xj, double yj, double hi, double *out3);
+typedef double (*orc_ref_pse_fn)(double xi, double yi, double xj, double yj, double hi);
+typedef double (*orc_ref_yield_fn)(const double *jc12, double eps_pl, double eps_pl_dot, double T);
+typedef double (*orc_ref_secant_fn)(const double *jc12, double init, double tol, double norm_Strial,
+                                    double eps_pl_init, double T, double dt, double mu);
+void orc_set_reference_functions(orc_state *s, orc_ref_kernel_fn kernel, orc_ref_pse_fn pse,
+                                 orc_ref_yield_fn yield, orc_ref_secant_fn secant);
 void orc_set_dt(orc_state *s, double dt);
 /* grid_kind: 0 Green, 1 Rothlin. Locked bbox (grid.cu:139-158) */
 int orc_set_grid_locked(orc_state *s, int grid_kind, double bbmin_x, double bbmin_y, double bbmax_x,
