@@ -317,15 +317,23 @@ def load_state(mf, ctx, path):
     return int(d["steps"][0])
 
 
-def run_form(mf, scene, precision, steps, device, torch=None, state_out=None):
+def run_form(mf, scene, precision, steps, device, torch=None, state_out=None, flags=0, list_check_every=0):
     """`steps` steps of one form from the scene's initial state. Returns the per-step tool
-    force (steps x 2), the end state ordered by particle number, and the device time (s)."""
+    force (steps x 2), the end state ordered by particle number, the device time (s) and the
+    status. With neighbour lists (flags) and list_check_every > 0, the lists are checked by brute
+    force (mf_list_check) every that many steps, outside the timed chunks; the status then
+    carries the checks."""
     ctx = mf.Context(device)
     ctx.upload_scene(scene, mf.GRID_GREEN)
     ctx.set_options(SOLVER["thermal"], mf.JC_JOHNSON_COOK, precision)
     ctx.set_neighbour_skin(SOLVER["skin"])
+    ctx.set_flags(flags)
+    checking = list_check_every > 0 and bool(flags & mf.OPT_NEIGHBOUR_LISTS)
+    checks = []
     forces, left, secs = [], steps, 0.0
     chunk = 50_000  # below the device force log's 65,536 entries
+    if checking:
+        chunk = min(chunk, list_check_every)
     while left > 0:
         n = min(left, chunk)
         if torch is not None:
@@ -340,9 +348,20 @@ def run_form(mf, scene, precision, steps, device, torch=None, state_out=None):
             ctx.step(n)
         forces.append(ctx.force_log())
         left -= n
+        if checking:
+            c = ctx.list_check()
+            st = ctx.status()
+            checks.append({"steps": steps - left, "pairs": c["pairs"], "missing": c["missing"], "stale": c["stale"],
+                           "blanked": st["blanked"], "sorts": st["sorts"], "secant_cap_hits": st["secant_cap_hits"]})
     order = np.argsort(ctx.get("id"))
     state = {k: ctx.get(k)[order] for k in ("S", "p", "eps_pl", "T", "tool_p", "blanked")}
     status = ctx.status()
+    if checking:
+        valid = [c for c in checks if not c["stale"]]
+        bad = [c["steps"] for c in valid if c["missing"] > 0]
+        status["list_checks"] = {"every": list_check_every, "checked": len(valid),
+                                 "missing_total": int(sum(c["missing"] for c in valid)),
+                                 "first_step_missing": bad[0] if bad else None, "log": checks}
     if state_out:
         save_state(mf, ctx, state_out, steps)
     ctx.close()
@@ -395,12 +414,22 @@ def accuracy(mf, scene, params, steps, device):
     return out
 
 
-def cut_run(mf, torch, scene, params, mm, device, state_out=None):
+def cut_run(mf, torch, scene, params, mm, device, state_out=None, lists=False, list_check_every=0):
     """`mm` millimetres of cut in each form: device wall time per mm and the mixed form's errors
-    (and, with state_out, the FP64 form's end state saved for --state-in)."""
+    (and, with state_out, the FP64 form's end state saved for --state-in). With `lists` the
+    mixed form on neighbour lists (fused predictor) runs too, its lists checked every
+    list_check_every steps when that is > 0."""
     steps = int(round(mm * steps_per_mm(scene, params)))
     f64, s64, t64, st64 = run_form(mf, scene, mf.PRECISION_FP64, steps, device, torch, state_out=state_out)
     fm, sm, tm, stm = run_form(mf, scene, mf.PRECISION_MIXED, steps, device, torch)
+    lists_out = None
+    if lists:
+        fl, sl, tl, stl = run_form(mf, scene, mf.PRECISION_MIXED, steps, device, torch,
+                                   flags=mf.OPT_NEIGHBOUR_LISTS | mf.OPT_FUSED_PREDICTOR,
+                                   list_check_every=list_check_every)
+        lists_out = {"wall_s_per_mm": tl / mm, "particle_steps_per_s": scene.N * steps / tl, "status": stl,
+                     "errors": form_errors(scene, (f64, s64), (fl, sl)),
+                     "mean_force_second_half": fl[steps // 2:].mean(axis=0).tolist()}
     out = {"mode": "cut", "mm": mm, "steps": steps, "n_particles": scene.N,
            "wall_s_per_mm": {"fp64": t64 / mm, "mixed": tm / mm},
            "particle_steps_per_s": {"fp64": scene.N * steps / t64, "mixed": scene.N * steps / tm},
@@ -409,6 +438,8 @@ def cut_run(mf, torch, scene, params, mm, device, state_out=None):
     # time-averaged force over the second half of the run (past the entry transient)
     h = steps // 2
     out["mean_force_second_half"] = {"fp64": f64[h:].mean(axis=0).tolist(), "mixed": fm[h:].mean(axis=0).tolist()}
+    if lists_out is not None:
+        out["mixed_lists"] = lists_out
     return out
 
 
@@ -629,6 +660,11 @@ def main():
     ap.add_argument("--cut-mm", type=float, default=0.0,
                     help="instead of the benchmark: run this many mm of cut in both forms and report "
                          "wall time per mm and the mixed form's errors")
+    ap.add_argument("--cut-lists", action="store_true",
+                    help="with --cut-mm: also run the mixed form on neighbour lists (fused predictor)")
+    ap.add_argument("--list-check-every", type=int, default=0,
+                    help="with --cut-lists: check the neighbour lists by brute force (mf_list_check) every "
+                         "this many steps (0: never)")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"],
                     help="c2 (default): the ~150k-particle cut with thermal contact, the benchmark; "
                          "c1: the ~6k adiabatic cut; c3: the ~500k cut with the PSE solver")
@@ -681,7 +717,8 @@ def main():
         return 0
     if args.cut_mm > 0:
         if rank == 0:
-            print(json.dumps(cut_run(mf, torch, scene, params, args.cut_mm, device, args.state_out)), flush=True)
+            print(json.dumps(cut_run(mf, torch, scene, params, args.cut_mm, device, args.state_out,
+                                     lists=args.cut_lists, list_check_every=args.list_check_every)), flush=True)
         if world > 1:
             torch.distributed.barrier()
             torch.distributed.destroy_process_group()
