@@ -284,7 +284,7 @@ int mf_scene_setup_ref_cut(int ny, double rake, double clear, double chamfer, do
    plasticity; setup_impact(nbox) (benchmarks.cpp:23-159): a steel disc (radius 0.2) at 1000
    against a wall of nbox/2 columns fixed at top and bottom, Johnson-Cook plasticity, an
    adaptive Green grid of at most 10 N cells. nbox >= 2 lattice points across the outer
-   diameter. */
+   diameter; a lattice that puts no particle in the body is refused (MF_ERR_INVALID). */
 int mf_scene_setup_rings(int nbox, mf_scene **out);
 int mf_scene_setup_impact(int nbox, mf_scene **out);
 int mf_scene_free(mf_scene *scene);

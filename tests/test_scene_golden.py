@@ -2,6 +2,8 @@
 
 All of it runs on the CPU through the C ABI (no device needed for the host scene code).
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -182,3 +184,32 @@ def test_validation_scenes_refuse_degenerate_lattices(mf, nbox):
         with pytest.raises(mf.MfError) as e:
             make(nbox)
         assert e.value.code == -1  # MF_ERR_INVALID
+
+
+@pytest.mark.parametrize("kind", ["rings", "impact"])
+def test_validation_scenes_live_against_the_reference(mf, orc, kind):
+    """The same comparison live, against the reference's own setup compiled on this host, over a
+    range of lattice sizes (odd and even nbox, coarse to fine)."""
+    R = orc.ref()
+    if R is None:
+        pytest.skip("the reference's sources were not built here")
+    setup = R.refh_setup_rings if kind == "rings" else R.refh_setup_impact
+    make = mf.Scene.rings if kind == "rings" else mf.Scene.impact
+    for nbox in (5, 8, 13, 24, 37, 50, 64):
+        n = setup(nbox)
+        if n == 0:  # (nbox 5: no lattice point in the rings) an empty scene is refused
+            with pytest.raises(mf.MfError):
+                make(nbox)
+            continue
+        sc = make(nbox)
+        assert sc.N == n, nbox
+        for k, f in enumerate(ARRAYS):
+            ref = np.zeros(n * (2 if f in ("pos", "vel") else 1))
+            R.refh_get_array(k, ref.ctypes.data_as(C.c_void_p))
+            assert bits_equal(sc.array(f).reshape(-1), ref), (nbox, f)
+        c = np.zeros(64)
+        m = R.refh_get_constants(c.ctypes.data_as(C.c_void_p))
+        mine = scene_constants(mf, sc.s)
+        mine[-1] = float(sc.s.has_joco)
+        assert bits_equal(mine, c[:m]), nbox
+        assert sc.s.grid_max_cell == R.refh_get_grid_max_cell(), nbox
