@@ -96,18 +96,19 @@ def test_usui_wear_bitwise(orc, golden):
     assert bits_equal(float(g["dt"]) * out[2], g["usui"][3])  # m_accum_wear += dt * avg
 
 
-@pytest.mark.parametrize("thermal_solver", [0, 1])
-def test_oracle_on_the_reference_functions_is_the_same_bit_for_bit(mf, orc, thermal_solver):
+@pytest.mark.parametrize("thermal_solver,jc_model", [(0, 0), (1, 0), (0, 1)])
+def test_oracle_on_the_reference_functions_is_the_same_bit_for_bit(mf, orc, thermal_solver, jc_model):
     """The oracle stepping with the reference's own host-compiled kernels.cuh / plasticity.cuh
     functions at their call sites (the CPU baseline's reference form) equals the restatement
-    bit for bit: three steps of a cut with contact, yielding and heat conduction."""
+    bit for bit: three steps of a cut with contact, yielding and heat conduction (with the tanh
+    yield law the return map keeps the restatement; the kernels are still the reference's)."""
     if orc.ref() is None:
         pytest.skip("the reference's sources were not built here")
     from helpers import load_oracle, perturbed_scene
     st = perturbed_scene(mf, ny=10, seed=71, tensile=True)
     st["S"] *= 3.0  # particles over the yield surface
-    a = load_oracle(orc, st, thermal_solver=thermal_solver)
-    b = load_oracle(orc, st, thermal_solver=thermal_solver)
+    a = load_oracle(orc, st, thermal_solver=thermal_solver, jc_model=jc_model)
+    b = load_oracle(orc, st, thermal_solver=thermal_solver, jc_model=jc_model)
     assert orc.use_reference_functions(b)
     for _ in range(3):
         assert a.L.orc_step(a.s) == 0 and b.L.orc_step(b.s) == 0
