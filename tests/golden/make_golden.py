@@ -8,6 +8,7 @@ oracle and the product's host code on machines where the reference tree is absen
 
     python tests/golden/make_golden.py              # every fixture
     python tests/golden/make_golden.py validation   # the rings and impact scenes only
+    python tests/golden/make_golden.py oracle       # the oracle's own step (oracle_steps.npz)
 """
 from __future__ import annotations
 
@@ -252,7 +253,26 @@ def validation_scene(R, name, kind, nbox):
     return n
 
 
+def oracle_fixture():
+    """The oracle's own step on the benchmark configurations (tests/golden/oracle_steps.py);
+    needs the product's host scene code and the oracle, not the reference."""
+    import importlib.util
+
+    import oracle_steps
+
+    build_oracle.build_oracle()
+    spec = importlib.util.spec_from_file_location("mfree_b200", ROOT / "mfree_iwf-ul_cut_gpu_b200" / "__init__.py",
+                                                  submodule_search_locations=[str(ROOT / "mfree_iwf-ul_cut_gpu_b200")])
+    mf = importlib.util.module_from_spec(spec)
+    sys.modules["mfree_b200"] = mf
+    spec.loader.exec_module(mf)
+    np.savez_compressed(HERE / "oracle_steps.npz", **oracle_steps.compute(mf, B))
+
+
 def main():
+    if sys.argv[1:] == ["oracle"]:
+        oracle_fixture()
+        return
     build_oracle.build_ref()
     R = B.ref()
     if R is None:

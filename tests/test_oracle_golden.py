@@ -116,3 +116,21 @@ def test_oracle_on_the_reference_functions_is_the_same_bit_for_bit(mf, orc, ther
               "T_t", "blanked"):
         assert bits_equal(a.get(f), b.get(f)), f
     assert (a.get("eps_pl") > 0.0).sum() > 10  # the return map ran
+
+
+def test_oracle_step_fixtures(mf, orc, golden):
+    """The oracle's own step on the benchmark configurations against its fixtures: c1 after one
+    step (arrays, bit for bit) and 1,000 steps, c2 after one step (digests of every per-particle
+    field). A regression pin of the checker itself (tests/golden/oracle_steps.py)."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    import oracle_steps
+
+    g = golden("oracle_steps")
+    o = oracle_steps.run(mf, orc, "c1", 1)
+    for f in oracle_steps.ARRAY_FIELDS:
+        assert bits_equal(o.get(f), g["c1_step1_" + f]), f
+    assert oracle_steps.digest(o) == str(g["c1_step1_sha256"])
+    assert oracle_steps.digest(oracle_steps.run(mf, orc, "c1", 1000)) == str(g["c1_step1000_sha256"])
+    assert oracle_steps.digest(oracle_steps.run(mf, orc, "c2", 1)) == str(g["c2_step1_sha256"])
