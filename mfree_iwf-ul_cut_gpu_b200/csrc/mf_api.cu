@@ -1,6 +1,7 @@
 // C ABI of the B200 SPH step (include/mfree_b200.h): context, device buffers, launches and
 // CUDA-graph replay of leap_frog::step (leap_frog.cu:94-155).
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cmath>
 #include <cstdio>
@@ -17,6 +18,17 @@
 #include "mfree_b200.h"
 
 using namespace mf;
+
+namespace {
+// a named NVTX range for profilers (Nsight Compute --nvtx filters, timelines) over one entry
+// point or stage; header-only NVTX, a no-op unless a tool is attached
+struct nvtx_range {
+  explicit nvtx_range(const char *name) { nvtxRangePushA(name); }
+  ~nvtx_range() { nvtxRangePop(); }
+  nvtx_range(const nvtx_range &) = delete;
+  nvtx_range &operator=(const nvtx_range &) = delete;
+};
+}  // namespace
 
 namespace mf {
 // the differentiable step (csrc/mf_tangent.cu): one derivative direction (tg), all six (tg6);
@@ -295,6 +307,9 @@ int launch_cells(mf_ctx *ctx, bool step_mode) {
 }
 
 int launch_stage(mf_ctx *ctx, int stage) {
+  static const char *const names[4] = {"mf stage 0: cell list", "mf stage 1: predictor",
+                                       "mf stage 2: pair sums", "mf stage 3: finish + return map"};
+  nvtx_range range(stage >= 0 && stage < 4 ? names[stage] : "mf stage");
   const int N = ctx->N;
   const int nb = (N + BLOCK - 1) / BLOCK;
   const int npb = (N + PAIR_BLOCK - 1) / PAIR_BLOCK;
@@ -750,6 +765,7 @@ int mf_grid_geometry(mf_ctx *ctx, int *nx, int *ny, int *num_cell, double *out5)
 }
 
 int mf_grid_build(mf_ctx *ctx) {
+  nvtx_range range("mf_grid_build");
   if (!ctx) return MF_ERR_INVALID;
   if (!ctx->has_particles || !ctx->has_grid || ctx->mid_step) return MF_ERR_STATE;
   TRY(set_device(ctx));
@@ -877,6 +893,7 @@ int mf_tool_get(mf_ctx *ctx, mf_tool_state *tool) {
 }
 
 int mf_step(mf_ctx *ctx, int n_steps) {
+  nvtx_range range("mf_step");
   if (!ctx || n_steps < 0) return MF_ERR_INVALID;
   if (!ready(ctx)) return MF_ERR_STATE;
   if (!(ctx->P.dt > 0.) || ctx->mid_step) return MF_ERR_STATE;
@@ -1118,6 +1135,7 @@ int mf_batch_steps_per_launch(const mf_batch *b, int *k) {
 }
 
 int mf_batch_step(mf_batch *b, int n_launches) {
+  nvtx_range range("mf_batch_step");
   if (!b || n_launches < 0) return MF_ERR_INVALID;
   if (!b->exec) return MF_ERR_STATE;
   if (cudaSetDevice(b->device) != cudaSuccess) return MF_ERR_CUDA;
@@ -1641,6 +1659,7 @@ int tangent_check(mf_ctx *ctx) {
 
 int mf_tangent_mean_force_all(mf_ctx *ctx, int skip_steps, int window_steps, double out_mean[2],
                               double out_dmean[12]) {
+  nvtx_range range("mf_tangent_mean_force_all");
   if (!ctx || !out_mean || !out_dmean || skip_steps < 0 || window_steps < 1) return MF_ERR_INVALID;
   TRY(tangent_check(ctx));
   TRY(set_device(ctx));
@@ -1653,6 +1672,7 @@ int mf_tangent_mean_force_all(mf_ctx *ctx, int skip_steps, int window_steps, dou
 
 int mf_tangent_mean_force(mf_ctx *ctx, int skip_steps, int window_steps, int param, double out_mean[2],
                           double out_dmean[2]) {
+  nvtx_range range("mf_tangent_mean_force");
   if (!ctx || !out_mean || skip_steps < 0 || window_steps < 1 || param < -1 || param > 5) return MF_ERR_INVALID;
   TRY(tangent_check(ctx));
   TRY(set_device(ctx));
