@@ -241,6 +241,7 @@ inline void vtk_writer_write(const particle_gpu *p, int step) {
   mfree::check(mf_vtk_write_particles(p->ctx, buf), "vtk_writer_write");
 }
 inline void vtk_writer_write(const tool *t, int step) {
+  if (!t) return;  // a scene without a tool (setup_rings, setup_impact) leaves global_tool null
   char buf[256];
   std::snprintf(buf, sizeof(buf), "results/vtk_tool_%06d.vtk", step);
   mfree::check(mf_vtk_write_tool(&t->s, buf), "vtk_writer_write");

@@ -23,6 +23,7 @@ int main(int argc, char **) {
     particles = setup_impact(30, &grid);
   else
     particles = setup_ref_cut(30, &grid, 10., 8., 0.002, 83.333328e-5 / 500. * 70., 0.01);
+  if (global_tool == 0) global_tool = new tool();  // as the reference's main does
   leap_frog *stepper = new leap_frog(particles->N, grid->num_cell());
   int last_step = (int)(global_t_final / global_dt), freq = last_step / 135;
   for (int step = 0; step < last_step + 1; step++) {
