@@ -25,3 +25,20 @@ def test_reference_arm_prints_one_contract_line(mf, orc):
     assert cb["kind"] == ("reference" if orc.ref() is not None else "port")
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_benchmark_workloads_are_the_configurations(mf):
+    """The scenes bench.py times: particle counts (workpiece + sampled tool particles), heat
+    solver and time step of c1, c2 (the headline) and c3, as the measurements quote them."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("mfree_bench_workloads", ROOT / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    expected = {"c1": (6149, 0, mf.THERMAL_BROOKSHAW, 1.1752e-3), "c2": (152796, 23899, mf.THERMAL_BROOKSHAW, 2.3505e-4),
+                "c3": (499230, 78325, mf.THERMAL_PSE, 1.3012e-4)}
+    for name, (n_wp, n_tool, solver, dt) in expected.items():
+        p, s, _ = bench.config_params(mf, name)
+        sc = mf.Scene.from_params(p)
+        assert (sc.s.n_workpiece, sc.s.n_tool, s) == (n_wp, n_tool, solver), name
+        assert abs(sc.s.dt - dt) < 1e-4 * dt, name
