@@ -83,6 +83,14 @@ extern "C" {
                                      (faster; experimental: over a 1 mm cut of the ~150k-particle
                                      scene, 36 particles became non-finite after ~0.55 mm, which
                                      the form that sorts every step does not show) */
+#define MF_OPT_SMOOTH_MODEL 32     /* differentiable form only (mf_tangent_mean_force*): a smooth
+                                     model, no counterpart in the reference: FP64 roots, angles
+                                     and plastic increment where the reference rounds to float
+                                     (actions_gpu.cu:47,76-77,145,159,239,252,264-265;
+                                     kernels.cuh:50; interactions_gpu.cu:293-294) and the return
+                                     map converged to 1e-13 relative instead of the reference's
+                                     1e-6 absolute (plasticity.cuh:108), so that the objective
+                                     is differentiable and finite differences converge */
 
 /* ---- constants (constants_structs.h:25-82), same member order ---- */
 typedef struct { double E, nu, rho0, K, G, mass, mass_tool; } mf_phys_constants;
@@ -220,14 +228,30 @@ int mf_status_get(mf_ctx *ctx, mf_status *status);
    caller-owned device buffers only (d_pos: 2N doubles; d_hash_sorted, d_idx: N ints;
    d_cell_start, d_cell_end: nx*ny ints, -1 on empty cells), queued on `stream`. The grid is
    given directly (origin bbmin, cell size dx, nx x ny cells, as mf_grid_geometry reports).
-   Scratch is one fixed device array inside the library, so N is limited to
-   MF_NOALLOC_MAX_PARTICLES and nx*ny to MF_NOALLOC_MAX_CELLS (MF_ERR_RANGE beyond). The first
-   call on a device looks up that array's address; make it before any stream capture. Calls
-   share the array: calls that overlap on the GPU race. No cudaMalloc/cudaFree is made. */
+   d_pos must be 16-byte aligned, the int buffers 4-byte aligned (MF_ERR_INVALID otherwise,
+   before anything is launched). Scratch is one fixed device array of 26 MiB inside the
+   library, so N is limited to MF_NOALLOC_MAX_PARTICLES and nx*ny to MF_NOALLOC_MAX_CELLS
+   (MF_ERR_RANGE beyond). A particle outside the grid is put into the nearest cell and counted;
+   a cell of m particles costs O(m^2) in all. d_status (optional, caller-owned device memory,
+   8-byte aligned; NULL: not written) receives, after every other kernel of the call, the
+   number of such clamped particles, the error flags (1: the scan's bounded wait expired, the
+   output is wrong) and the largest cell occupancy; a nonzero out_of_grid or error_flags means
+   the cell list is not the reference's. The return code covers the launches only (each
+   launch's own error; an earlier error of the caller's work is neither read nor cleared). The
+   first call on a device looks up the scratch array's address and caches it; make it before
+   any stream capture. After a cudaDeviceReset the cached address is stale: do not call this
+   again on a device that was reset. Calls share the array: calls that overlap on the GPU race.
+   No cudaMalloc/cudaFree is made. */
 #define MF_NOALLOC_MAX_PARTICLES (1 << 19)
 #define MF_NOALLOC_MAX_CELLS (1 << 21)
+typedef struct {
+  unsigned long long out_of_grid;        /* particles clamped into the grid */
+  unsigned long long error_flags;        /* 1: the scan's bounded wait expired */
+  unsigned long long max_cell_occupancy; /* largest number of particles in one cell */
+} mf_noalloc_status;
 int mf_cells_build_noalloc(const double *d_pos, int N, double bbmin_x, double bbmin_y, double dx, int nx, int ny,
-                           int *d_hash_sorted, int *d_idx, int *d_cell_start, int *d_cell_end, void *stream);
+                           int *d_hash_sorted, int *d_idx, int *d_cell_start, int *d_cell_end,
+                           mf_noalloc_status *d_status, void *stream);
 
 /* ---- host scene setup: setup_ref_cut (benchmarks.cpp:255-537) and its generalisation ---- */
 typedef struct {
@@ -372,12 +396,6 @@ int mf_tangent_mean_force(mf_ctx *ctx, int skip_steps, int window_steps, int par
    A, B, n, C, m, mu; each equals what mf_tangent_mean_force returns for param k. */
 int mf_tangent_mean_force_all(mf_ctx *ctx, int skip_steps, int window_steps, double out_mean[2],
                               double out_dmean[12]);
-
-/* ---- measurement aid (no counterpart in the reference): FP64 FMA throughput of the device
-   (TFLOP/s, 2 flops per FMA) and the latency in SM clock cycles of one dependent double
-   pow, log and division; allocates and frees 32 bytes of device memory ---- */
-int mf_probe_fp64(int device, double *fma_tflops, double *pow_cycles, double *log_cycles, double *div_cycles,
-                  double *sm_clock_mhz);
 
 #ifdef __cplusplus
 }
