@@ -25,6 +25,7 @@ THERMAL_BROOKSHAW, THERMAL_PSE = 0, 1
 JC_JOHNSON_COOK, JC_TANH = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 OPT_KEEP_DERIVATIVES, OPT_NO_GRAPHS, OPT_SORT_EVERY_STEP, OPT_FUSED_PREDICTOR, OPT_NEIGHBOUR_LISTS = 1, 2, 4, 8, 16
+OPT_SMOOTH_MODEL = 32  # differentiable form: the smooth model (FP64 roots, converged return map)
 
 # name -> (field id, doubles per particle, is_int)
 FIELDS = {
@@ -140,7 +141,6 @@ def lib():
         "mf_set_options": ([vp, i, i, i], i), "mf_set_dt": ([vp, d], i),
         "mf_tool_set": ([vp, C.POINTER(ToolState)], i), "mf_tool_get": ([vp, C.POINTER(ToolState)], i),
         "mf_step": ([vp, i], i), "mf_step_timed": ([vp, vp], i), "mf_step_stage": ([vp, i], i), "mf_report_force": ([vp, vp], i),
-        "mf_probe_fp64": ([i, vp, vp, vp, vp, vp], i),
         "mf_tangent_mean_force": ([vp, i, i, i, vp, vp], i),
         "mf_tangent_mean_force_all": ([vp, i, i, vp, vp], i),
         "mf_tool_wear_usui": ([vp, d, d, vp], i), "mf_vtk_write_particles_async": ([vp, C.c_char_p], i),
@@ -509,9 +509,15 @@ class Batch:
 
 def probe_fp64(device=0) -> dict:
     """FP64 FMA throughput (TFLOP/s) and the latency (SM cycles) of a dependent double pow,
-    log and division on `device` (mf_probe_fp64)."""
+    log and division on `device` (mf_probe_fp64 of the benchmark-only lib/libmf_probe.so)."""
+    path = LIB_PATH.parent / "libmf_probe.so"
+    if not path.exists():
+        raise RuntimeError(f"probe library missing: {path} (run mfree_iwf-ul_cut_gpu_b200/build.py)")
+    probe = C.CDLL(str(path))
+    probe.mf_probe_fp64.argtypes = [C.c_int] + [C.c_void_p] * 5
+    probe.mf_probe_fp64.restype = C.c_int
     v = [C.c_double() for _ in range(5)]
-    rc = lib().mf_probe_fp64(device, *[C.byref(x) for x in v])
+    rc = probe.mf_probe_fp64(device, *[C.byref(x) for x in v])
     if rc != MF_OK:
         raise MfError(rc, "mf_probe_fp64")
     return {"fma_tflops": v[0].value, "pow_cycles": v[1].value, "log_cycles": v[2].value,

@@ -334,8 +334,16 @@ int launch_stage(mf_ctx *ctx, int stage) {
       }
       break;
     case 3:
-      if (fused_step(ctx)) TRY(launch_pdl(ctx, k_finish<true>, ctx->finish_blocks, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
-      else TRY(launch_pdl(ctx, k_finish<false>, ctx->finish_blocks, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+      if (ctx->P.fuse) {  // the next step's predictor runs here too: the whole state at once
+        if (fused_step(ctx))
+          TRY(launch_pdl(ctx, k_finish<true>, ctx->finish_blocks, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+        else
+          TRY(launch_pdl(ctx, k_finish<false>, ctx->finish_blocks, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+      } else {
+        const int fb = (N + FINISH_BLOCK - 1) / FINISH_BLOCK;
+        if (fused_step(ctx)) TRY(launch_pdl(ctx, k_finish_flat<true>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+        else TRY(launch_pdl(ctx, k_finish_flat<false>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+      }
       if (ctx->P.plastic) {
         if (ctx->P.jc_model == MF_JC_TANH)
           TRY(launch_pdl(ctx, k_plastic<false>, ctx->sm_count * PLASTIC_BLOCKS_PER_SM, BLOCK, ctx->P, ctx->D));
@@ -529,6 +537,7 @@ int mf_set_flags(mf_ctx *ctx, int flags) {
   if (!ctx) return MF_ERR_INVALID;
   ctx->flags = flags;
   ctx->P.keep_derivs = (flags & MF_OPT_KEEP_DERIVATIVES) ? 1 : 0;
+  ctx->P.smooth = (flags & MF_OPT_SMOOTH_MODEL) ? 1 : 0;
   drop_graphs(ctx);
   return MF_OK;
 }
@@ -859,6 +868,7 @@ int mf_set_options(mf_ctx *ctx, int thermal_solver, int jc_model, int precision)
 
 int mf_set_dt(mf_ctx *ctx, double dt) {
   if (!ctx || !(dt > 0.) || !std::isfinite(dt)) return MF_ERR_INVALID;
+  if (ctx->P.dt == dt) return MF_OK;  // nothing captured goes stale (the C++ mirror sets it every step)
   ctx->P.dt = dt;
   drop_graphs(ctx);
   return MF_OK;

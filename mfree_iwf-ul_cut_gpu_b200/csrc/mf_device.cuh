@@ -48,6 +48,10 @@ struct params {
   // between, each particle's candidates within 2 h + skin are kept in a list
   int verlet;
   int fuse;  // neighbour lists: the finish kernel also runs the next step's predictor
+  // differentiable form only (MF_OPT_SMOOTH_MODEL): full FP64 roots, angles and plastic
+  // increment instead of the reference's float-rounded ones, and a return map converged to
+  // 1e-13 relative instead of 1e-6 absolute
+  int smooth;
   float skin;
   double eos_c0;  // (double)sqrtf((float)(K / rho0)), the EOS sound speed (actions_gpu.cu:41-51)
   double dt;

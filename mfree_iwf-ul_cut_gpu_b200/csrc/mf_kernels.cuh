@@ -84,8 +84,11 @@ struct dev_buffers {
 #define MF_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
 #define MF_PDL_TRIGGER() asm volatile("griddepcontrol.launch_dependents;" ::: "memory")
 
+#ifndef MF_SCAN_ITEMS
+#define MF_SCAN_ITEMS 8
+#endif
 constexpr int SCAN_THREADS = 256;
-constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_ITEMS = MF_SCAN_ITEMS;  // cells per thread of k_scan (a multiple of 4)
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr int BLOCK = 256;
 // k_finish: a fixed grid of FINISH_BLOCKS_PER_SM blocks of FINISH_BLOCK threads per SM takes
@@ -363,19 +366,15 @@ static __global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D, 
 
 // ---------------------------------------------------------------------------------------
 // stable rank fix-up: inside a cell, the atomics gave the members in arbitrary order; the
-// stable sort wants them by previous array position. Position q of the sorted order holds
-// the member with exactly (q - cell_start) smaller previous positions.
-// u = perm_u[q]: particle, cell, cell start, cell end
-__device__ __forceinline__ int stable_member(const dev_buffers &D, int q, const int4 u) {
-  if (u.w - u.z == 1) return u.x;
-  const int k = q - u.z;
-  for (int m = u.z; m < u.w; ++m) {
-    const int v = D.perm_u[m].x;
-    int less = 0;
-    for (int m2 = u.z; m2 < u.w; ++m2) less += D.perm_u[m2].x < v;
-    if (less == k) return v;
-  }
-  return u.x;  // unreachable for a consistent cell list
+// stable sort wants them by previous array position. The member that the scatter put at
+// slot q (u = perm_u[q]: particle, cell, cell start, cell end) belongs at the cell's slot
+// start + (number of members with a smaller previous position): one pass over the cell, so a
+// cell of m particles costs O(m) per member (a crowded cell O(m^2) in all, not O(m^3)).
+__device__ __forceinline__ int stable_rank(const int4 *__restrict__ perm_u, const int4 u) {
+  if (u.w - u.z == 1) return 0;
+  int r = 0;
+  for (int m = u.z; m < u.w; ++m) r += perm_u[m].x < u.x ? 1 : 0;
+  return r;
 }
 
 // gather into the new order (grid_gpu_green.cu:22-116) and, if PREDICT, the predictor
@@ -512,12 +511,12 @@ template <bool PREDICT, bool MIXED>
 static __global__ void __launch_bounds__(BLOCK, REORDER_BLOCKS_PER_SM) k_reorder(params P, dev_buffers D) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= P.N) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= P.N) return;
   // with neighbour lists, a step without a sort keeps the order and the cells of the last
   // sort: the identity permutation
   const bool sort = !P.verlet || D.st->sort_now;
-  if (q == 0) {  // re-armed for the finish kernel of this step
+  if (t == 0) {  // re-armed for the finish kernel of this step
     *D.plastic_count = 0u;
     *D.finish_chunk = 0u;
     if (sort) D.st->sorts += 1ull;
@@ -525,12 +524,15 @@ static __global__ void __launch_bounds__(BLOCK, REORDER_BLOCKS_PER_SM) k_reorder
   // neighbour lists, no sort, and the previous step's finish (and plastic) kernels already ran
   // this step's predictor: nothing left to do
   if (PREDICT && !sort && D.st->predicted) return;
-  int p = q, hsh;
+  // thread t takes the particle the scatter put at slot t and moves it to its stable slot q
+  // (inside the same cell, so a warp's stores stay within a few neighbouring cells)
+  int p = t, q = t, hsh;
   if (sort) {
-    const int4 u = D.perm_u[q];
-    p = stable_member(D, q, u);
+    const int4 u = D.perm_u[t];
+    p = u.x;
+    q = u.z + stable_rank(D.perm_u, u);
     hsh = u.y;
-    if (q == u.z) D.count[hsh] = 0;  // the scatter's cursor, back to zero for the next counts
+    if (t == u.z) D.count[hsh] = 0;  // the scatter's cursor, back to zero for the next counts
     D.hash_cur[q] = hsh;
   } else {
     hsh = D.hash_cur[q];
@@ -994,6 +996,325 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
   f_out = f;
   fc_out = fc;
   ft_out = ft;
+}
+
+// The same corrector .. invalidate for one particle (not for the fused predictor, which needs
+// the whole state at once), in two phases that each load, update and store their own fields:
+// first velocity and position with the friction-heat input, contact, the kinematic boundary
+// conditions; then stress, density and temperature with the elastic test and the thermal
+// boundary condition. Fewer values are live at once than when every load is issued first, so
+// the kernel runs with fewer registers and more warps per SM. Every value is computed by the
+// same expressions from the same operands as in finish_particle: the results are equal bit for
+// bit. (eps_pl is not touched here: the corrector does not change it, the return map in
+// k_plastic does.)
+__device__ __forceinline__ void finish_particle_phased(const params &P, const dev_buffers &D,
+                                                       const mf_tool_state &TL, int q, double2 &pos_out,
+                                                       unsigned &f_out, double2 &fc_out, double2 &ft_out,
+                                                       unsigned &newly_blanked, bool &want_sort, bool identity) {
+  const state_set &A = D.A;
+  const state_set &B = D.B;
+  const double dt = P.dt;
+  unsigned f = B.flags[q];
+  const bool blanked = f & FLAG_BLANKED;
+  const bool tool = f & FLAG_TOOL;
+  const bool fixed = f & FLAG_FIXED;
+  const int p = identity ? q : D.perm[q];
+  // phase 1: kinematics
+  double2 pos = A.pos[p], vel = A.vel[p];
+  double2 pos_t = B.pos_t[q], vel_t = B.vel_t[q];
+  double2 fc = B.fc[q], ft = B.ft[q];
+  if (!blanked) {  // correct (leap_frog.cu:68-92)
+    pos.x = pos.x + dt * pos_t.x;
+    pos.y = pos.y + dt * pos_t.y;
+    vel.x = vel.x + dt * vel_t.x;
+    vel.y = vel.y + dt * vel_t.y;
+  }
+  // friction heat (actions_gpu.cu:135-162), previous step's ft and n: its increment now, added
+  // to the corrected temperature in phase 2
+  double dT_fric = 0.;
+  bool fric = false;
+  if (P.has_tool && P.fric_heat && !tool) {
+    const double f_fric_mag = (double)sqrtf((float)(ft.x * ft.x + ft.y * ft.y));
+    if (f_fric_mag != 0.) {
+      const double2 normal = D.n[q];
+      const double vdx = vel.x - TL.vel[0], vdy = vel.y - TL.vel[1];
+      const double vdn = vdx * normal.x + vdy * normal.y;
+      const double vrx = vdx - vdn, vry = vdy - vdn;
+      const double v_rel_mag = (double)sqrtf((float)(vrx * vrx + vry * vry));
+      dT_fric = P.trml_wp.eta * dt * f_fric_mag * v_rel_mag / (P.trml_wp.cp * P.phys.mass);
+      fric = true;
+    }
+  }
+  // tool particles move with the tool (tool_gpu.cu:210-221); contact (:151-207)
+  if (P.has_tool) {
+    if (tool) {
+      pos.x += dt * TL.vel[0];
+      pos.y += dt * TL.vel[1];
+    } else {
+      double cpx = 0., cpy = 0., nx = 0., ny = 0.;
+      const bool inside = establish_contact(TL, pos.x, pos.y, cpx, cpy, nx, ny);
+      if (!inside) {
+        fc = make_double2(0., 0.);
+        ft = make_double2(0., 0.);
+        D.n[q] = make_double2(0., 0.);
+      } else {
+        const double dt2 = dt * dt;
+        const double gN = (pos.x - cpx) * nx + (pos.y - cpy) * ny;
+        const double sc = -TL.slave_mass * gN;
+        double2 fN = make_double2(sc * nx, sc * ny);
+        fN.x = fN.x / dt2 * TL.contact_alpha;
+        fN.y = fN.y / dt2 * TL.contact_alpha;
+        double2 fT = make_double2(0., 0.);
+        if (TL.mu != 0.) {
+          const double vx = vel.x - TL.vel[0], vy = vel.y - TL.vel[1];
+          const double vrx = vx - vx * nx, vry = vy - vy * ny;
+          const double ks = TL.contact_alpha * TL.slave_mass;
+          const double kx = ks * vrx / dt, ky = ks * vry / dt;
+          const double fy = TL.mu * sqrt(fN.x * fN.x + fN.y * fN.y);
+          const double fsx = ft.x - kx, fsy = ft.y - ky;
+          const double lfs = sqrt(fsx * fsx + fsy * fsy);
+          if (lfs > fy) {
+            fT.x = fy * fsx / lfs;
+            fT.y = fy * fsy / lfs;
+          } else {
+            fT = make_double2(fsx, fsy);
+          }
+        }
+        fc = fN;
+        ft = fT;
+        D.n[q] = make_double2(nx, ny);
+      }
+    }
+  }
+  // boundary conditions (actions_gpu.cu:287-311)
+  if (!tool && fixed) {
+    vel = make_double2(0., 0.);
+    fc = make_double2(0., 0.);
+    pos_t = make_double2(0., 0.);
+    vel_t = make_double2(0., 0.);
+    B.pos_t[q] = pos_t;
+    B.vel_t[q] = vel_t;
+  }
+  bool invalid = !blanked && (isnaninf(pos_t.x) || isnaninf(pos_t.y) || isnaninf(vel_t.x) || isnaninf(vel_t.y));
+  // neighbour lists: the next step's predicted position against the list's build position
+  bool far = false;
+  if (P.verlet) {
+    const double2 pb = D.pos_build[q];
+    const double px = pos.x + 0.5 * dt * pos_t.x, py = pos.y + 0.5 * dt * pos_t.y;
+    const double ddx = px - pb.x, ddy = py - pb.y;
+    const double lim = 0.45 * (double)P.skin;
+    far = !(ddx * ddx + ddy * ddy <= lim * lim);
+  }
+  B.pos[q] = pos;
+  B.vel[q] = vel;
+  B.fc[q] = fc;
+  B.ft[q] = ft;
+  // phase 2: stress, density, temperature
+  double4 S = A.S[p];
+  double rho = A.rho[p], T = A.T[p];
+  const double4 S_t = B.S_t[q];
+  const double rho_t = B.rho_t[q], T_t = B.T_t[q];
+  if (!blanked) {
+    S.x = S.x + dt * S_t.x;
+    S.y = S.y + dt * S_t.y;
+    S.z = S.z + dt * S_t.z;
+    S.w = S.w + dt * S_t.w;
+    rho = rho + dt * rho_t;
+    T = T + dt * T_t;
+  }
+  if (fric) T += dT_fric;
+  // JC plasticity, radial return (actions_gpu.cu:226-285): the elastic lower bound of
+  // finish_particle, the rest in k_plastic
+  if (P.plastic && !tool) {
+    const double pr = B.pp[q];
+    const double Sxx = S.x, Syy = S.z, Szz = S.w, Sxy = S.y;
+    const double cxx = Sxx - pr, cyy = Syy - pr, czz = Szz - pr, cxy = Sxy;
+    const double svm = (double)sqrtf(
+        (float)((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy));
+    bool elastic = false;
+    if (P.jc_lower_bound) {
+      const mf_joco_constants &JC = P.joco;
+      const float theta_f = (float)(T - JC.Tref) * (1.f / (float)(JC.Tmelt - JC.Tref));
+      const double pow_hi = 1.00001 * (double)powf(theta_f, (float)JC.m);
+      elastic = svm < 0.999 * JC.A * (1.0 - pow_hi);
+    }
+    if (elastic) {
+      B.eps_pl_dot[q] = 0.;
+    } else {
+      const unsigned am = __activemask();
+      const int leader = __ffs(am) - 1;
+      unsigned base = 0u;
+      if ((int)lane_id() == leader) base = atomicAdd(D.plastic_count, (unsigned)__popc(am));
+      base = __shfl_sync(am, base, leader);
+      const unsigned rank = __popc(am & ((1u << lane_id()) - 1u));
+      D.plastic_list[base + rank] = plastic_item{T, svm, q, 0};
+    }
+  }
+  if (P.thermal_bc && fixed) T = P.trml_wp.T_init;
+  invalid = invalid || (!blanked && (isnaninf(S_t.x) || isnaninf(S_t.y) || isnaninf(S_t.z) || isnaninf(S_t.w) ||
+                                     isnaninf(rho_t) || isnaninf(T_t)));
+  B.S[q] = S;
+  B.rho[q] = rho;
+  B.T[q] = T;
+  if (invalid) {  // invalidate (actions_gpu.cu:317-349)
+    f |= FLAG_BLANKED;
+    newly_blanked += 1u;
+    B.flags[q] = f;
+  }
+  if (far && !(f & FLAG_BLANKED)) want_sort = true;
+  pos_out = pos;
+  f_out = f;
+  fc_out = fc;
+  ft_out = ft;
+}
+
+// Corrector .. invalidate for all particles plus the tool force (output.cu:31-39): one thread
+// per particle, one block per FINISH_BLOCK consecutive particles (the chunks of k_finish, so
+// that the force sums are the same numbers in the same tree: per warp, then the block's warps
+// in order, then the blocks in order in the last block to finish). Not for the fused predictor
+// (k_finish). With FUSE_HASH (locked grid) also the next step's hash and count.
+#ifndef FINISH_FLAT_MIN_BLOCKS
+#define FINISH_FLAT_MIN_BLOCKS 3
+#endif
+template <bool FUSE_HASH>
+__global__ void __launch_bounds__(FINISH_BLOCK, FINISH_FLAT_MIN_BLOCKS) k_finish_flat(params P, dev_buffers D,
+                                                                                    int num_scan_tiles) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
+  __shared__ mf_tool_state s_tool;
+  __shared__ ksum sm[FINISH_BLOCK / 32][4];
+  __shared__ unsigned smc[FINISH_BLOCK / 32][4];
+  __shared__ bool last;
+  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt);
+  const int q = blockIdx.x * FINISH_BLOCK + threadIdx.x;
+  const bool identity = P.verlet && !*(volatile unsigned *)&D.st->sort_now;
+  if (FUSE_HASH) {
+    const int stride = gridDim.x * FINISH_BLOCK;
+    for (int t = q; t < num_scan_tiles; t += stride) D.scan_status[t] = 0ull;
+  }
+  double2 fc = make_double2(0., 0.), ft = make_double2(0., 0.);
+  unsigned newly_blanked = 0, blanked_now = 0, oog = 0;
+  bool want_sort = false;
+  if (q < P.N) {
+    double2 pos;
+    unsigned f;
+    finish_particle_phased(P, D, s_tool, q, pos, f, fc, ft, newly_blanked, want_sort, identity);
+    blanked_now = (f & FLAG_BLANKED) ? 1u : 0u;
+    if (FUSE_HASH) {  // compute_hashes of the next step (grid.cu:34-51)
+      const geom g = *D.g;
+      long long hh;
+      if (f & FLAG_BLANKED) {
+        hh = D.hash_cur[q];
+      } else {
+        const int ix = __double2int_rz(P.verlet ? (pos.x - g.bbmin_x) * (1. / g.dx) : (pos.x - g.bbmin_x) / g.dx);
+        const int iy = __double2int_rz(P.verlet ? (pos.y - g.bbmin_y) * (1. / g.dx) : (pos.y - g.bbmin_y) / g.dx);
+        hh = (long long)ix * (long long)g.ny + (long long)iy;
+      }
+      if (hh < 0) { hh = 0; oog = 1; }
+      else if (hh >= g.num_cell) { hh = g.num_cell - 1; oog = 1; }
+      const int hsh = (int)hh;
+      D.hash_new[q] = hsh;
+      atomicAdd(&D.count[hsh], 1);
+    }
+  }
+  // the block's force sums (compensated), in the fixed tree of k_finish; warps whose forces are
+  // all zero skip the arithmetic ({+0, +0} is what the sums give for zeros)
+  const bool nz = fc.x != 0. || fc.y != 0. || ft.x != 0. || ft.y != 0.;
+  const int w = threadIdx.x >> 5;
+  if (__any_sync(0xffffffffu, nz)) {
+    ksum fcx{0., 0.}, fcy{0., 0.}, ftx{0., 0.}, fty{0., 0.};
+    ksum_add(fcx, fc.x);
+    ksum_add(fcy, fc.y);
+    ksum_add(ftx, ft.x);
+    ksum_add(fty, ft.y);
+    for (int o = 16; o > 0; o >>= 1) {
+      ksum a{__shfl_down_sync(0xffffffffu, fcx.s, o), __shfl_down_sync(0xffffffffu, fcx.c, o)};
+      ksum b{__shfl_down_sync(0xffffffffu, fcy.s, o), __shfl_down_sync(0xffffffffu, fcy.c, o)};
+      ksum c{__shfl_down_sync(0xffffffffu, ftx.s, o), __shfl_down_sync(0xffffffffu, ftx.c, o)};
+      ksum d{__shfl_down_sync(0xffffffffu, fty.s, o), __shfl_down_sync(0xffffffffu, fty.c, o)};
+      ksum_merge(fcx, a); ksum_merge(fcy, b); ksum_merge(ftx, c); ksum_merge(fty, d);
+    }
+    if (lane_id() == 0) {
+      sm[w][0] = fcx; sm[w][1] = fcy; sm[w][2] = ftx; sm[w][3] = fty;
+    }
+  } else if (lane_id() == 0) {
+    const ksum z{0., 0.};
+    sm[w][0] = z; sm[w][1] = z; sm[w][2] = z; sm[w][3] = z;
+  }
+  const unsigned nb = __reduce_add_sync(0xffffffffu, newly_blanked);
+  const unsigned nbl = __reduce_add_sync(0xffffffffu, blanked_now);
+  const unsigned noog = __reduce_add_sync(0xffffffffu, oog);
+  const unsigned nws = __ballot_sync(0xffffffffu, want_sort);
+  if (lane_id() == 0) {
+    smc[w][0] = nb; smc[w][1] = nbl; smc[w][2] = noog; smc[w][3] = nws;
+  }
+  const bool block_nz = __syncthreads_or(nz);  // sm and smc complete
+  if (threadIdx.x == 0) {
+    ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
+    if (block_nz) {
+      for (int k = 0; k < 4; ++k) r[k] = sm[0][k];
+      for (int v = 1; v < FINISH_BLOCK / 32; ++v)
+        for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[v][k]);
+    }
+    for (int k = 0; k < 4; ++k) {
+      D.partials[(size_t)blockIdx.x * 8 + 2 * k] = r[k].s;
+      D.partials[(size_t)blockIdx.x * 8 + 2 * k + 1] = r[k].c;
+    }
+    unsigned long long cnt[3] = {smc[0][0], smc[0][1], smc[0][2]};
+    unsigned ws = smc[0][3];
+    for (int v = 1; v < FINISH_BLOCK / 32; ++v) {
+      for (int k = 0; k < 3; ++k) cnt[k] += smc[v][k];
+      ws |= smc[v][3];
+    }
+    if (ws) D.st->want_sort = 1u;  // (before the fence and the ticket below)
+    if (cnt[0]) atomicAdd(&D.st->newly_blanked, cnt[0]);
+    if (cnt[1]) atomicAdd(&D.st->blanked, cnt[1]);
+    if (cnt[2]) atomicAdd(&D.st->out_of_grid, cnt[2]);
+    __threadfence();
+    const unsigned t = atomicAdd(&D.ticket[0], 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  // last block: fixed-order reduction of all block partials
+  __threadfence();
+  const int n_chunks = gridDim.x;
+  ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
+  for (int b = threadIdx.x; b < n_chunks; b += blockDim.x) {
+    const volatile double *pr = D.partials + (size_t)b * 8;
+    for (int k = 0; k < 4; ++k) {
+      ksum x{pr[2 * k], pr[2 * k + 1]};
+      ksum_merge(r[k], x);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 4; ++k) {
+      ksum x{__shfl_down_sync(0xffffffffu, r[k].s, o), __shfl_down_sync(0xffffffffu, r[k].c, o)};
+      ksum_merge(r[k], x);
+    }
+  __syncthreads();
+  if (lane_id() == 0)
+    for (int k = 0; k < 4; ++k) sm[w][k] = r[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int v = 1; v < FINISH_BLOCK / 32; ++v)
+      for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[v][k]);
+    const double Fx = (r[0].s + r[0].c) + (r[2].s + r[2].c);
+    const double Fy = (r[1].s + r[1].c) + (r[3].s + r[3].c);
+    D.force_last[0] = Fx;
+    D.force_last[1] = Fy;
+    const unsigned long long hd = D.st->force_log_head;
+    D.force_log[2 * (hd % FORCE_LOG_CAP)] = Fx;
+    D.force_log[2 * (hd % FORCE_LOG_CAP) + 1] = Fy;
+    D.st->force_log_head = hd + 1;
+    D.st->steps += 1;
+    if (P.verlet) {  // every particle is checked: the next step sorts if one asked for it
+      D.st->sort_now = D.st->want_sort;
+      D.st->want_sort = 0u;
+      D.st->predicted = 0u;
+    }
+    D.ticket[0] = 0u;
+  }
 }
 
 // Corrector .. invalidate for all particles plus the tool force (output.cu:31-39). A fixed

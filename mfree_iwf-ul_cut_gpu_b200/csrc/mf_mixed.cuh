@@ -50,23 +50,19 @@ __device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_con
   const unsigned fjw = (unsigned)__float_as_int(b0.z);
   const float rr2 = xij * xij + yij * yij;
   const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
-  float w = 0.f, dwr = 0.f;
-  if (in_support) {
-    const float rinv = rsqrtf(rr2);
-    const float qq = rr2 * rinv * I.h1;
-    float val, der;
-    if (qq > 1.f) {
-      const float t = 2.f - qq;
-      const float t2 = t * t;
-      val = 0.25f * t2 * t2 * t2;
-      der = -0.75f * t2 * I.h1 * rinv;
-    } else {
-      val = 1.f - 1.5f * qq * qq * (1.f - 0.5f * qq);
-      der = -3.0f * qq * (1.f - 0.75f * qq) * I.h1 * rinv;
-    }
-    w = val * I.fac;
-    dwr = der * I.fac;
-  }
+  // the reference's cubic spline (kernels.cuh:30-70) with both branches on q evaluated and one
+  // selected, so that the lanes of a warp do not split on it. The value keeps the reference's
+  // form: 1 - 1.5 q^2 (1 - q / 2) for q <= 1 and (2 - q)^6 / 4 (sic: _2mq2 cubed) for q > 1;
+  // the derivative -3 q (1 - 3 q / 4) and -3 (2 - q)^2 / 4 is written as 3 u^2 - 3 t^2 / 4 with
+  // t = 2 - q, u = max(1 - q, 0). Out of support (or at r^2 < 1e-8) both are 0.
+  const float rinv = rsqrtf(rr2);
+  const float qq = rr2 * rinv * I.h1;
+  const float t = 2.f - qq, u = fmaxf(1.f - qq, 0.f);
+  const float t2 = t * t, u2 = u * u;
+  const float val = qq > 1.f ? 0.25f * t2 * t2 * t2 : fmaf(-1.5f * qq * qq, fmaf(-0.5f, qq, 1.f), 1.f);
+  const float der = fmaf(3.f, u2, -0.75f * t2) * I.h1 * rinv;
+  const float w = in_support ? val * I.fac : 0.f;
+  const float dwr = in_support ? der * I.fac : 0.f;
   const float2 pij = f2(xij, yij);
   const float2 w_xy = __fmul2_rn(f2(dwr, dwr), pij);
   const float volj = b3.z;
@@ -86,11 +82,11 @@ __device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_con
     const float2 dvp = __fmul2_rn(dv, pij);
     const float vijposij = -(dvp.x + dvp.y);
     const float irhoij = __fdividef(2.f, I.rho + b3.x);
-    if (vijposij < 0.f) {
+    {  // Monaghan viscosity for approaching pairs, as a select rather than a branch
       const float cij = 0.5f * (I.c + b3.y);
       const float hij = 0.5f * (I.h + b2.w);
-      const float muij = hij * vijposij * __fdividef(1.f, rr2 + K.eta2 * hij * hij);
-      const float npi = (K.alpha * cij * muij - K.beta * muij * muij) * irhoij;  // -pi_ij
+      const float muij = hij * vijposij * __fdividef(1.f, fmaf(K.eta2 * hij, hij, rr2));
+      const float npi = vijposij < 0.f ? (K.alpha * cij - K.beta * muij) * muij * irhoij : 0.f;  // -pi_ij
       a.vt = __ffma2_rn(f2(npi, npi), w_xy, a.vt);
     }
     const float xs = w * irhoij;
