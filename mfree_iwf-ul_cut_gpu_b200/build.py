@@ -18,6 +18,10 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libmfree_b200.so"
+# benchmark-only measurement aid (FP64 FMA peak, pow/log/division latency), kept out of the
+# product library
+PROBE_SRC = PKG / "probe" / "mf_probe.cu"
+PROBE_LIB = LIB_DIR / "libmf_probe.so"
 OBJ = PKG / "_build"
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 
@@ -47,7 +51,16 @@ def _stale(target: Path) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
+def build_probe(force: bool = False) -> Path:
+    """The benchmark's FP64 probe library (lib/libmf_probe.so)."""
+    if force or not PROBE_LIB.exists() or PROBE_SRC.stat().st_mtime > PROBE_LIB.stat().st_mtime:
+        LIB_DIR.mkdir(parents=True, exist_ok=True)
+        _run([NVCC] + NVCC_FLAGS + ["-shared", "-o", PROBE_LIB, PROBE_SRC, "-lcudart"])
+    return PROBE_LIB
+
+
 def build(force: bool = False, ptxas_verbose: bool = False) -> Path:
+    build_probe(force)
     if not force and not _stale(LIB):
         return LIB
     OBJ.mkdir(parents=True, exist_ok=True)

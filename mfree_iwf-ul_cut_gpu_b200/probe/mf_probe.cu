@@ -1,6 +1,7 @@
-// Measurement aids (no counterpart in the reference): the FP64 FMA throughput of the device,
-// which the step's FP64 kernels are compared against, and the latency of the double-precision
-// calls on the return map's critical path (pow, log, division), measured with the SM clock.
+// Measurement aid for the benchmark only (no counterpart in the reference, not part of the
+// product library): the FP64 FMA throughput of the device, which the step's FP64 kernels are
+// compared against, and the latency of the double-precision calls on the return map's critical
+// path (pow, log, division), measured with the SM clock. Built into lib/libmf_probe.so.
 #include <cuda_runtime.h>
 
 #include "mfree_b200.h"
