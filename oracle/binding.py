@@ -158,6 +158,106 @@ def ref():
     return _ref
 
 
+REF_GPU_SO = HERE / "_ref" / "libref_gpu.so"
+_ref_gpu = None
+
+
+def ref_gpu():
+    """The reference's own FP64 CUDA step (oracle/_ref/libref_gpu.so), or None where it was not
+    built. Needs a CUDA device to run."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        if not REF_GPU_SO.exists():
+            return None
+        L = C.CDLL(str(REF_GPU_SO))
+        vp, d, i = C.c_void_p, C.c_double, C.c_int
+        L.refg_create.argtypes = [i] + [vp] * 7 + [d] * 5
+        L.refg_geometry.argtypes = [vp, vp]
+        L.refg_geometry.restype = None
+        L.refg_set_constants.argtypes = [vp] * 5 + [d]
+        L.refg_set_tool.argtypes = [C.POINTER(OrcTool), vp]
+        L.refg_get_tool.argtypes = [C.POINTER(OrcTool)]
+        L.refg_set_field.argtypes = [i, vp]
+        L.refg_get_field.argtypes = [i, vp]
+        L.refg_step.argtypes = [i]
+        L.refg_run_timed.argtypes = [i, vp]
+        L.refg_get_cells.argtypes = [vp, vp]
+        L.refg_report_force.argtypes = [vp]
+        _ref_gpu = L
+    return _ref_gpu
+
+
+class RefGPU:
+    """One system of the reference's own FP64 CUDA build (one per process at a time: the
+    reference keeps its constants and options process-wide)."""
+
+    def __init__(self, st: dict, phys7, corr6, joco12, trml_wp6, trml_tool6, tool: OrcTool):
+        self.L = ref_gpu()
+        if self.L is None:
+            raise RuntimeError(f"reference GPU build missing: {REF_GPU_SO}")
+        self.N = int(st["N"])
+        a = {k: np.ascontiguousarray(st[k], dtype=np.float64) for k in ("pos", "vel", "rho", "T", "h", "fixed",
+                                                                         "tool_p")}
+        bbmin, bbmax, h = st["grid"]
+        rc = self.L.refg_create(self.N, *[_ptr(a[k]) for k in ("pos", "vel", "rho", "T", "h", "fixed", "tool_p")],
+                                bbmin[0], bbmin[1], bbmax[0], bbmax[1], h)
+        self._check(rc, "refg_create")
+        self._c = [np.ascontiguousarray(x, dtype=np.float64) for x in (phys7, corr6, joco12, trml_wp6, trml_tool6)]
+        self._tool = tool
+        self._check(self.L.refg_set_tool(C.byref(tool), _ptr(self._c[0])), "refg_set_tool")
+        self._check(self.L.refg_set_constants(*[_ptr(x) for x in self._c], st["dt"]), "refg_set_constants")
+
+    @staticmethod
+    def _check(rc, where):
+        if rc != 0:
+            raise RuntimeError(f"{where} failed ({rc})")
+
+    def set_field(self, name: str, values) -> None:
+        fid, w = FIELDS[name]
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        v = np.ascontiguousarray(np.asarray(values, dtype=dt).reshape(self.N * w))
+        self._check(self.L.refg_set_field(fid, _ptr(v)), "refg_set_field")
+
+    def get(self, name: str) -> np.ndarray:
+        fid, w = FIELDS[name]
+        dt = np.int32 if name in INT_FIELDS else np.float64
+        out = np.zeros(self.N * w, dtype=dt)
+        self._check(self.L.refg_get_field(fid, _ptr(out)), "refg_get_field")
+        return out.reshape(self.N, w) if w > 1 else out
+
+    def step(self, n: int = 1) -> None:
+        self._check(self.L.refg_step(n), "refg_step")
+
+    def run_timed(self, n: int) -> float:
+        ms = C.c_float()
+        self._check(self.L.refg_run_timed(n, C.byref(ms)), "refg_run_timed")
+        return float(ms.value)
+
+    def geometry(self):
+        i3 = np.zeros(3, dtype=np.int32)
+        d3 = np.zeros(3)
+        self.L.refg_geometry(_ptr(i3), _ptr(d3))
+        return {"nx": int(i3[0]), "ny": int(i3[1]), "num_cell": int(i3[2]), "bbmin_x": d3[0], "bbmin_y": d3[1],
+                "dx": d3[2]}
+
+    def cells(self):
+        nc = self.geometry()["num_cell"]
+        st = np.zeros(nc, dtype=np.int32)
+        en = np.zeros(nc, dtype=np.int32)
+        self._check(self.L.refg_get_cells(_ptr(st), _ptr(en)), "refg_get_cells")
+        return st, en
+
+    def report_force(self):
+        out = np.zeros(2)
+        self._check(self.L.refg_report_force(_ptr(out)), "refg_report_force")
+        return out
+
+    def get_tool(self) -> OrcTool:
+        t = OrcTool()
+        self._check(self.L.refg_get_tool(C.byref(t)), "refg_get_tool")
+        return t
+
+
 def use_reference_functions(o) -> bool:
     """Run oracle state `o` on the reference's own host-compiled per-particle functions
     (kernels.cuh cubic_spline, lapl_pse; plasticity.cuh sigma_yield, solve_secant) instead of

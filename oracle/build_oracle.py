@@ -1,6 +1,6 @@
 """Build recipe for the oracle (test infrastructure; never part of the product path).
 
-Two artefacts:
+Three artefacts:
 
 * ``oracle/_build/liboracle.so``: the CPU restatement of the reference step
   (``oracle/sph_oracle.c``), plain C11 + OpenMP, built with gcc.
@@ -10,23 +10,32 @@ Two artefacts:
   host build of ``plasticity.cuh`` (``oracle/ref_host_plasticity.cpp``). It is only built
   when the reference tree is present; the GPU machines use the prebuilt file or skip.
 
-Both are loaded with ctypes by ``tests/`` and by ``bench.py``'s CPU-baseline leg only.
+* ``oracle/_ref/libref_gpu.so``: the reference's own FP64 CUDA step (its device sources,
+  unchanged, with the texture shim ``oracle/ref_gpu/ref_texture_shim.h`` force-included) and
+  the entry-point harness ``oracle/ref_gpu/ref_gpu_harness.cu``; built where the reference
+  tree is present, used on the GPU machine as the GPU oracle and the reference GPU baseline.
+
+All are loaded with ctypes by ``tests/`` and by ``bench.py``'s baseline legs only.
 """
 from __future__ import annotations
 
 import os
 import shutil
+from concurrent.futures import ThreadPoolExecutor
 import subprocess
 import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_SRC = Path(os.environ.get("MF_REFERENCE_SRC", "/root/reference/src"))
+# the reference's src/ directory: MF_REFERENCE_SRC, else a reference checkout beside this
+# repository (../reference/src); where neither exists only prebuilt files are used
+REF_SRC = Path(os.environ.get("MF_REFERENCE_SRC", str(HERE.parent.parent / "reference" / "src")))
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 CUDA_HOME = Path(NVCC).resolve().parent.parent
 
 ORACLE_LIB = HERE / "_build" / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libref_host.so"
+REF_GPU_LIB = HERE / "_ref" / "libref_gpu.so"
 
 
 def _run(cmd, cwd=None):
@@ -95,6 +104,39 @@ def build_ref(force: bool = False) -> Path | None:
     return REF_LIB
 
 
+def build_ref_gpu(force: bool = False) -> Path | None:
+    """The reference's own FP64 CUDA step for sm_100a (oracle/_ref/libref_gpu.so): its device
+    sources compiled unchanged where they lie, with the texture shim force-included and the
+    project's GLM subset, plus the entry-point harness oracle/ref_gpu/ref_gpu_harness.cu.
+    The reference's own makefile flags: -O3, whole-program per file (no relocatable device
+    code); its types.h selects FP64 and the Brookshaw heat solver."""
+    if not REF_SRC.is_dir():
+        return REF_GPU_LIB if REF_GPU_LIB.exists() else None
+    ref_files = ["actions_gpu.cu", "interactions_gpu.cu", "leap_frog.cu", "tool_gpu.cu", "grid.cu",
+                 "grid_gpu_green.cu", "particle_gpu.cu", "output.cu", "tool.cpp", "geometric_primitives.cpp",
+                 "constants_structs.cpp", "types.cpp"]
+    shim = HERE / "ref_gpu" / "ref_texture_shim.h"
+    harness = HERE / "ref_gpu" / "ref_gpu_harness.cu"
+    srcs = [shim, harness, HERE / "ref_shim" / "glm" / "glm.hpp", HERE / "sph_oracle.h"] + \
+        [REF_SRC / f for f in ref_files] + sorted(REF_SRC.glob("*.h")) + sorted(REF_SRC.glob("*.cuh"))
+    if not (force or _stale(REF_GPU_LIB, srcs)):
+        return REF_GPU_LIB
+    obj = HERE / "_ref" / "gpu_obj"
+    obj.mkdir(parents=True, exist_ok=True)
+    nv = [NVCC, "-O3", "-std=c++14", "-Xcompiler", "-fPIC", "-gencode", "arch=compute_100a,code=sm_100a",
+          "-include", str(shim), "-I", str(HERE / "ref_shim"), "-I", str(REF_SRC), "-I", str(HERE),
+          "-w", "-x", "cu", "-c"]
+    jobs = [(obj / ("refg_" + Path(f).stem + ".o"), REF_SRC / f) for f in ref_files]
+    jobs.append((obj / "ref_gpu_harness.o", harness))
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        list(pool.map(lambda j: _run(nv + ["-o", str(j[0]), str(j[1])]), jobs))
+    objs = [j[0] for j in jobs]
+    _run([NVCC, "-shared", "-Xcompiler", "-fPIC", "--cudart", "shared", "-Xlinker", "-Bsymbolic",
+          "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(REF_GPU_LIB)] + [str(x) for x in objs])
+    return REF_GPU_LIB
+
+
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     print(build_ref(force="--force" in sys.argv))
+    print(build_ref_gpu(force="--force" in sys.argv))

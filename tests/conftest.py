@@ -52,6 +52,29 @@ def orc():
 
 
 @pytest.fixture(scope="session")
+def c2_midcut(mf, tmp_path_factory):
+    """GPU: the ~150k-particle benchmark cut (176,695 particles, Brookshaw) after 0.05 mm of
+    plain FP64 cut (~182k steps), saved once per session to a state file; returns the scene,
+    its thermal solver, the file and the number of steps taken."""
+    import bench
+
+    p, solver, _ = bench.config_params(mf, "c2")
+    sc = mf.Scene.from_params(p)
+    ctx = mf.Context(0)
+    ctx.upload_scene(sc, mf.GRID_GREEN)
+    ctx.set_options(solver, mf.JC_JOHNSON_COOK, mf.PRECISION_FP64)
+    s = sc.s
+    steps = int(round(0.005 / (s.tool.vel[0] * s.dt)))
+    ctx.step(steps)
+    ctx.synchronize()
+    path = tmp_path_factory.mktemp("midcut") / "c2_midcut.mfstate"
+    ctx.state_save(str(path))
+    st = ctx.status()
+    ctx.close()
+    return {"scene": sc, "solver": solver, "path": path, "steps": steps, "status": st}
+
+
+@pytest.fixture(scope="session")
 def golden():
     def load(name):
         return dict(np.load(GOLDEN / f"{name}.npz"))

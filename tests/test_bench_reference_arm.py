@@ -9,6 +9,9 @@ ROOT = Path(__file__).resolve().parent.parent
 
 
 def test_reference_arm_prints_one_contract_line(mf, orc):
+    import scene_file
+
+    scene_file.build_scene_files(("c1",))  # the arm's inputs (written by build() on a GPU machine)
     r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--config", "c1", "--steps", "2",
                         "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
@@ -25,6 +28,23 @@ def test_reference_arm_prints_one_contract_line(mf, orc):
     assert cb["kind"] == ("reference" if orc.ref() is not None else "port")
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+    assert line["config"]["n_particles"] == 6149
+
+
+def test_reference_arm_does_not_load_the_product(mf, orc):
+    """The reference arm reads its scene from the scene file: the product library is never
+    loaded in its process (checked with the process's own memory map)."""
+    import scene_file
+
+    scene_file.build_scene_files(("c1",))
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--config', 'c1', '--steps', '1', "
+            "'--warmup', '1']\n"
+            "try:\n    runpy.run_path('bench.py', run_name='__main__')\nexcept SystemExit:\n    pass\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print('PRODUCT_LOADED' if 'libmfree_b200' in maps else 'PRODUCT_NOT_LOADED')")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "PRODUCT_NOT_LOADED" in r.stdout, r.stdout[-2000:]
 
 
 def test_benchmark_workloads_are_the_configurations(mf):
