@@ -82,6 +82,16 @@ WORKLOAD = {"workload": "orthogonal cut, Ti6Al4V 2.0 x 0.6 mm, 714x214 lattice d
             "lattice": [714, 214], "dx_um": 2.8, "thermal_solver": "brookshaw", "grid": "green (locked)"}
 
 
+WORKLOAD_BY_CONFIG = {
+    "c1": {"workload": "orthogonal cut, Ti6Al4V 2.0 x 0.6 mm, 143x43 lattice dx=14um, adiabatic, no tool particles",
+           "lattice": [143, 43], "dx_um": 14.0, "thermal_solver": "none", "grid": "green (locked)"},
+    "c2": dict(WORKLOAD),
+    "c3": {"workload": "orthogonal cut, Ti6Al4V 2.0 x 0.6 mm, 1290x387 lattice dx=1.55um + sampled tool particles, "
+                       "PSE thermal solver, thermal contact", "lattice": [1290, 387], "dx_um": 1.55,
+           "thermal_solver": "pse", "grid": "green (locked)"},
+}
+
+
 def config_params(mf, name, lattice_scale=1.0):
     """The scene parameters and workload description of a named configuration:
     c1 = 143 x 43 lattice, dx = 14 um, adiabatic, no tool particles (~6k);
@@ -90,15 +100,10 @@ def config_params(mf, name, lattice_scale=1.0):
     if name == "c1":
         p = cut_params(mf, nx=143, ny=43, dx=1.4e-3)
         p.sample_tool, p.use_thermals = 0, 0
-        return p, mf.THERMAL_BROOKSHAW, {"workload": "orthogonal cut, Ti6Al4V 2.0 x 0.6 mm, 143x43 lattice dx=14um, "
-                                                     "adiabatic, no tool particles", "lattice": [143, 43],
-                                         "dx_um": 14.0, "thermal_solver": "none", "grid": "green (locked)"}
+        return p, mf.THERMAL_BROOKSHAW, dict(WORKLOAD_BY_CONFIG["c1"])
     if name == "c3":
         p = cut_params(mf, nx=1290, ny=387, dx=1.55e-4)
-        return p, mf.THERMAL_PSE, {"workload": "orthogonal cut, Ti6Al4V 2.0 x 0.6 mm, 1290x387 lattice dx=1.55um + "
-                                               "sampled tool particles, PSE thermal solver, thermal contact",
-                                   "lattice": [1290, 387], "dx_um": 1.55, "thermal_solver": "pse",
-                                   "grid": "green (locked)"}
+        return p, mf.THERMAL_PSE, dict(WORKLOAD_BY_CONFIG["c3"])
     sc = lattice_scale
     p = cut_params(mf, nx=int(round(714 * sc)), ny=int(round(214 * sc)), dx=2.8e-4 / sc)
     return p, mf.THERMAL_BROOKSHAW, dict(WORKLOAD)
@@ -317,11 +322,13 @@ def load_state(mf, ctx, path):
     return int(d["steps"][0])
 
 
-def run_form(mf, scene, precision, steps, device, torch=None, state_out=None, flags=0, list_check_every=0):
+def run_form(mf, scene, precision, steps, device, torch=None, state_out=None, flags=0, list_check_every=0,
+             list_check_late=(0, 0)):
     """`steps` steps of one form from the scene's initial state. Returns the per-step tool
     force (steps x 2), the end state ordered by particle number, the device time (s) and the
     status. With neighbour lists (flags) and list_check_every > 0, the lists are checked by brute
-    force (mf_list_check) every that many steps, outside the timed chunks; the status then
+    force (mf_list_check) every that many steps, outside the timed chunks, and from step
+    list_check_late[0] on every list_check_late[1] steps when that is > 0; the status then
     carries the checks."""
     ctx = mf.Context(device)
     ctx.upload_scene(scene, mf.GRID_GREEN)
@@ -336,6 +343,12 @@ def run_form(mf, scene, precision, steps, device, torch=None, state_out=None, fl
         chunk = min(chunk, list_check_every)
     while left > 0:
         n = min(left, chunk)
+        done = steps - left
+        if checking and list_check_late[1] > 0:
+            if done >= list_check_late[0]:
+                n = min(n, list_check_late[1])
+            elif done + n > list_check_late[0]:
+                n = list_check_late[0] - done
         if torch is not None:
             stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -414,19 +427,21 @@ def accuracy(mf, scene, params, steps, device):
     return out
 
 
-def cut_run(mf, torch, scene, params, mm, device, state_out=None, lists=False, list_check_every=0):
+def cut_run(mf, torch, scene, params, mm, device, state_out=None, lists=False, list_check_every=0,
+            list_check_late=(0.0, 0)):
     """`mm` millimetres of cut in each form: device wall time per mm and the mixed form's errors
     (and, with state_out, the FP64 form's end state saved for --state-in). With `lists` the
     mixed form on neighbour lists (fused predictor) runs too, its lists checked every
     list_check_every steps when that is > 0."""
     steps = int(round(mm * steps_per_mm(scene, params)))
+    late = (int(round(list_check_late[0] * steps_per_mm(scene, params))), int(list_check_late[1]))
     f64, s64, t64, st64 = run_form(mf, scene, mf.PRECISION_FP64, steps, device, torch, state_out=state_out)
     fm, sm, tm, stm = run_form(mf, scene, mf.PRECISION_MIXED, steps, device, torch)
     lists_out = None
     if lists:
         fl, sl, tl, stl = run_form(mf, scene, mf.PRECISION_MIXED, steps, device, torch,
                                    flags=mf.OPT_NEIGHBOUR_LISTS | mf.OPT_FUSED_PREDICTOR,
-                                   list_check_every=list_check_every)
+                                   list_check_every=list_check_every, list_check_late=late)
         lists_out = {"wall_s_per_mm": tl / mm, "particle_steps_per_s": scene.N * steps / tl, "status": stl,
                      "errors": form_errors(scene, (f64, s64), (fl, sl)),
                      "mean_force_second_half": fl[steps // 2:].mean(axis=0).tolist()}
@@ -500,6 +515,7 @@ def batch_run(mf, torch, n_instances, steps, device):
     cs = contexts()
     b = mf.Batch(cs, steps_per_launch=0)
     k = b.steps_per_launch
+    fused, pair_block = b.fused, b.pair_block
     launches = max(1, steps // k)
     b.step(1)
     for c in cs:
@@ -515,7 +531,9 @@ def batch_run(mf, torch, n_instances, steps, device):
         c.close()
     return {"mode": "batch", "instances": n_instances, "particles_total": n_total,
             "particles_min_max": [min(sc.N for sc in scenes), max(sc.N for sc in scenes)],
-            "precision": "mixed", "steps_per_launch": k,
+            "precision": "mixed", "steps_per_launch": k, "batched_kernels": fused, "pair_block": pair_block,
+            "launches_per_step": ("one per step phase for all instances" if fused else
+                                  "one child graph per instance"),
             "one_at_a_time": {"steps": steps, "wall_s": one_s, "particle_steps_per_s": n_total * steps / one_s},
             "streams": {"steps": steps, "wall_s": seq_s, "particle_steps_per_s": n_total * steps / seq_s},
             "batched": {"steps": launches * k, "wall_s": bat_s,
@@ -562,6 +580,39 @@ def cpu_baseline(mf, scene, seconds=12.0, max_steps=5000):
                                     f"({what}), {dt:.1f} s"}
 
 
+def reference_gpu_baseline(mf, scene, steps=200, warmup=10):
+    """The reference's own FP64 CUDA build (its sources compiled unchanged for sm_100a with a
+    shim for the removed texture-reference API, oracle/_ref/libref_gpu.so; Brookshaw, the
+    build's solver) stepping the same scene on the same B200 through its leap_frog::step:
+    `steps` steps back to back between CUDA events on its stream (no L2 flush: compare with
+    the forms' back_to_back_ms_per_step). A reported baseline, not the product."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ctypes as C
+
+    import binding as orc
+
+    if orc.ref_gpu() is None:
+        return {"unavailable": "oracle/_ref/libref_gpu.so was not built (no reference tree where build() ran)"}
+    if SOLVER["thermal"] != mf.THERMAL_BROOKSHAW:
+        return {"unavailable": "the reference's build selects the Brookshaw solver in its types.h; this "
+                               "configuration uses PSE"}
+    st = scene_state(mf, scene)
+
+    def doubles(struct):
+        return [getattr(struct, f) for f, _ in struct._fields_]
+
+    tool = orc.OrcTool()
+    C.memmove(C.byref(tool), C.byref(st["tool"]), C.sizeof(orc.OrcTool))
+    r = orc.RefGPU(st, doubles(st["phys"]), doubles(st["corr"]), doubles(st["joco"]), doubles(st["trml_wp"]),
+                   doubles(st["trml_tool"]), tool)
+    r.step(warmup)
+    ms = r.run_timed(steps)
+    return {"value": scene.N * steps / (ms * 1e-3), "unit": "particle-steps/s", "ms_per_step": ms / steps,
+            "steps": steps, "warmup": warmup, "dtype": "f64",
+            "what": "the reference's own FP64 CUDA step (leap_frog::step, unchanged sources + texture shim, "
+                    "sm_100a), same scene, same GPU, steps back to back on its stream"}
+
+
 def scene_state(mf, scene):
     """The scene as the state dict tests/helpers.load_oracle expects."""
     import ctypes as C
@@ -588,23 +639,54 @@ def kernels_per_step(mf, precision):
     return 6
 
 
+def oracle_from_scene_file(orc, path):
+    """An oracle state holding a scene file's initial scene (oracle/scene_file.py): the inputs of
+    the reference arm, loaded without the product library."""
+    import ctypes as C
+
+    d = np.load(path)
+    N = int(d["pos"].shape[0])
+    o = orc.Oracle(N)
+    for k in ("pos", "vel", "rho", "T", "h", "fixed", "tool_p"):
+        o.set_field(k, d[k])
+    g = d["grid"]
+    o.L.orc_set_grid_locked(o.s, 0, g[0], g[1], g[2], g[3], g[4])
+    phys = orc.OrcPhys(*d["phys"])
+    corr = orc.OrcCorr(*d["corr"])
+    joco = orc.OrcJoco(*d["joco"])
+    tw, tt = orc.OrcTrml(*d["trml_wp"]), orc.OrcTrml(*d["trml_tool"])
+    o.L.orc_set_constants(o.s, C.byref(phys), C.byref(corr), C.byref(joco), C.byref(tw), C.byref(tt))
+    o.L.orc_set_options(o.s, int(d["thermal_solver"][0]), 0)
+    o.L.orc_set_dt(o.s, float(d["dt"][0]))
+    tool = orc.OrcTool()
+    C.memmove(C.byref(tool), d["tool"].tobytes(), C.sizeof(orc.OrcTool))
+    o.L.orc_set_tool(o.s, C.byref(tool))
+    o._keep = (phys, corr, joco, tw, tt, tool)
+    return o, N, int(d["n_tool"][0])
+
+
 def run_reference(args):
-    """--impl reference: the reference path's CPU restatement on the host cores."""
+    """--impl reference: the reference path's CPU implementation on the host cores (the
+    reference's own per-particle functions inside the oracle's OpenMP loops where they were
+    built, else the oracle's restatement), on the configuration's scene read from its scene
+    file (oracle/scene_file.py), so that this arm never loads the product library."""
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
-    mf = load_package()
-    params, solver, workload = config_params(mf, args.config)
-    scene = mf.Scene.from_params(params)
     sys.path.insert(0, str(ROOT / "oracle"))
-    sys.path.insert(0, str(ROOT / "tests"))
     import binding as orc
     import build_oracle
-    from helpers import load_oracle
+    import scene_file
 
     build_oracle.build_oracle()
-    o = load_oracle(orc, scene_state(mf, scene), thermal_solver=solver)
+    path = scene_file.scene_path(args.config)
+    if not path.exists():
+        print(json.dumps({"impl": "reference", "unavailable": f"scene file {path.name} missing: run "
+                          f"python oracle/scene_file.py {args.config} (or __graft_entry__.build())"}), flush=True)
+        return 0
+    o, N, n_tool = oracle_from_scene_file(orc, path)
     kind = cpu_kind(orc, o)
+    workload = dict(WORKLOAD_BY_CONFIG[args.config])
     # each "step" is one full oracle step; bound the run to a few minutes
     o.L.orc_step(o.s)
     t0 = time.perf_counter()
@@ -618,14 +700,15 @@ def run_reference(args):
     t0 = time.perf_counter()
     o.L.orc_steps(o.s, steps)
     dt = time.perf_counter() - t0
-    v = scene.N * steps / dt
+    v = N * steps / dt
     cores = int(orc.lib().orc_get_threads())
     line = {"metric": METRIC, "value": v, "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": steps,
             "warmup": warm, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": dict(workload, name=args.config, n_particles=scene.N, n_tool=scene.s.n_tool),
+            "config": dict(workload, name=args.config, n_particles=N, n_tool=n_tool,
+                           scene=f"oracle/_build/scenes/{path.name}"),
             "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": cores, "kind": kind,
-                             "sample": f"{steps} full steps of the {scene.N}-particle scene (requested "
+                             "sample": f"{steps} full steps of the {N}-particle scene (requested "
                                        f"{args.steps}), " + (REF_FUNCTIONS if kind == "reference" else
                                                              "C restatement of the reference step, OpenMP")},
             "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -654,6 +737,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched form's 64-instance sweep that the benchmark line carries")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own CUDA build on the same GPU (a reported baseline)")
     ap.add_argument("--e2e-steps", type=int, default=500)
     ap.add_argument("--accuracy-steps", type=int, default=20_000,
                     help="steps of the mixed-against-FP64 error report (0: off)")
@@ -665,6 +752,8 @@ def main():
     ap.add_argument("--list-check-every", type=int, default=0,
                     help="with --cut-lists: check the neighbour lists by brute force (mf_list_check) every "
                          "this many steps (0: never)")
+    ap.add_argument("--list-check-late", default="0,0",
+                    help="with --list-check-every: 'MM,STEPS' = from MM mm of cut on, check every STEPS steps")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"],
                     help="c2 (default): the ~150k-particle cut with thermal contact, the benchmark; "
                          "c1: the ~6k adiabatic cut; c3: the ~500k cut with the PSE solver")
@@ -717,8 +806,10 @@ def main():
         return 0
     if args.cut_mm > 0:
         if rank == 0:
+            lmm, lst = args.list_check_late.split(",")
             print(json.dumps(cut_run(mf, torch, scene, params, args.cut_mm, device, args.state_out,
-                                     lists=args.cut_lists, list_check_every=args.list_check_every)), flush=True)
+                                     lists=args.cut_lists, list_check_every=args.list_check_every,
+                                     list_check_late=(float(lmm), int(lst)))), flush=True)
         if world > 1:
             torch.distributed.barrier()
             torch.distributed.destroy_process_group()
@@ -776,21 +867,36 @@ def main():
     step_achieved = ALGO_BYTES_PER_PARTICLE_STEP * N / (head["ms_per_step"] * 1e-3) / 1e9
     traffic = profiled_traffic(ROOT / PAIR_PROFILE, N) if args.lattice_scale == 1.0 else None
 
-    e2e = None
+    e2e = e2e_fp64 = None
     if rank == 0:
-        secs, h2d, d2h, finite = e2e_form(mf, torch, scene, mf.PRECISION_MIXED, args.e2e_steps, device)
-        if not finite:
-            raise SystemExit("e2e: non-finite tool force in the end-to-end run")
-        e2e = {"value": N * args.e2e_steps / secs, "unit": "particle-steps/s",
-               "h2d_bytes_per_step": h2d / args.e2e_steps, "d2h_bytes_per_step": 16 + d2h / args.e2e_steps,
-               "steps": args.e2e_steps,
-               "what": "state in from pinned host memory, per step mf_step(1) + tool force to pinned host "
-                       "memory, final state out; wall clock"}
+        for prec in (mf.PRECISION_MIXED, mf.PRECISION_FP64):
+            secs, h2d, d2h, finite = e2e_form(mf, torch, scene, prec, args.e2e_steps, device)
+            if not finite:
+                raise SystemExit("e2e: non-finite tool force in the end-to-end run")
+            line_e2e = {"value": N * args.e2e_steps / secs, "unit": "particle-steps/s",
+                        "h2d_bytes_per_step": h2d / args.e2e_steps, "d2h_bytes_per_step": 16 + d2h / args.e2e_steps,
+                        "steps": args.e2e_steps,
+                        "what": "state in from pinned host memory, per step mf_step(1) + tool force to pinned host "
+                                "memory, final state out; wall clock"}
+            if prec == mf.PRECISION_MIXED:
+                e2e = line_e2e
+            else:
+                e2e_fp64 = dict(line_e2e, form="fp64")
     fp64_probe = mf.probe_fp64(device) if rank == 0 else None
     spm = steps_per_mm(scene, params)
-    cpu = None
+    batched = None
+    if rank == 0 and not args.no_batch:  # the batched form on the 64-instance parameter sweep
+        batched = batch_run(mf, torch, 64, 64, device)
+    cpu = ref_gpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(mf, scene)
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu_baseline(mf, scene)
+        if "ms_per_step" in ref_gpu:
+            ref_gpu["fp64_form_speedup_back_to_back"] = (ref_gpu["ms_per_step"]
+                                                        / results["fp64"]["back_to_back_ms_per_step"])
+            ref_gpu["mixed_form_speedup_back_to_back"] = (ref_gpu["ms_per_step"]
+                                                         / results["mixed"]["back_to_back_ms_per_step"])
     if world > 1:
         torch.distributed.barrier()
     if rank == 0:
@@ -829,7 +935,10 @@ def main():
             "gpu_launches": kernels_per_step(mf, mf.PRECISION_MIXED) * args.steps,
             "clocks": clocks,
             "e2e": e2e,
+            "e2e_fp64": e2e_fp64,
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
+            "batched_sweep": batched,
             "status": {k: v for k, v in results["mixed"]["status"].items()},
         }
         print(json.dumps(line), flush=True)

@@ -83,14 +83,6 @@ extern "C" {
                                      (faster; experimental: over a 1 mm cut of the ~150k-particle
                                      scene, 36 particles became non-finite after ~0.55 mm, which
                                      the form that sorts every step does not show) */
-#define MF_OPT_SMOOTH_MODEL 32     /* differentiable form only (mf_tangent_mean_force*): a smooth
-                                     model, no counterpart in the reference: FP64 roots, angles
-                                     and plastic increment where the reference rounds to float
-                                     (actions_gpu.cu:47,76-77,145,159,239,252,264-265;
-                                     kernels.cuh:50; interactions_gpu.cu:293-294) and the return
-                                     map converged to 1e-13 relative instead of the reference's
-                                     1e-6 absolute (plasticity.cuh:108), so that the objective
-                                     is differentiable and finite differences converge */
 
 /* ---- constants (constants_structs.h:25-82), same member order ---- */
 typedef struct { double E, nu, rho0, K, G, mass, mass_tool; } mf_phys_constants;
@@ -127,9 +119,10 @@ typedef struct {
   long long out_of_grid;      /* hashes outside [0, num_cell) clamped since creation */
   long long secant_cap_hits;  /* JC secant solves that hit the iteration cap */
   int max_cell_occupancy;     /* largest particles-per-cell seen in the last sort */
-  int error_flags;            /* bit 0: a bounded wait in the cell scan expired; bit 1: the
-                                 adaptive grid outgrew max_cell; bit 2: a neighbour list was
-                                 full (neighbours dropped) */
+  int error_flags;            /* bit 1: the adaptive grid outgrew max_cell; bit 2: a neighbour
+                                 list was full (neighbours dropped); bit 0 (a bounded wait in
+                                 the cell scan expired) is no longer raised: the scan waits
+                                 for nothing */
   long long secant_iterations; /* JC secant iterations since creation (cost diagnostic) */
   long long sorts;            /* cell-list sorts since creation (one per step, except for the
                                  mixed form with neighbour lists) */
@@ -234,8 +227,8 @@ int mf_status_get(mf_ctx *ctx, mf_status *status);
    (MF_ERR_RANGE beyond). A particle outside the grid is put into the nearest cell and counted;
    a cell of m particles costs O(m^2) in all. d_status (optional, caller-owned device memory,
    8-byte aligned; NULL: not written) receives, after every other kernel of the call, the
-   number of such clamped particles, the error flags (1: the scan's bounded wait expired, the
-   output is wrong) and the largest cell occupancy; a nonzero out_of_grid or error_flags means
+   number of such clamped particles, the error flags (0: the scan has no bounded waits left to
+   expire; the field is kept for callers that test it) and the largest cell occupancy; a nonzero out_of_grid or error_flags means
    the cell list is not the reference's. The return code covers the launches only (each
    launch's own error; an earlier error of the caller's work is neither read nor cleared). The
    first call on a device looks up the scratch array's address and caches it; make it before
@@ -246,7 +239,7 @@ int mf_status_get(mf_ctx *ctx, mf_status *status);
 #define MF_NOALLOC_MAX_CELLS (1 << 21)
 typedef struct {
   unsigned long long out_of_grid;        /* particles clamped into the grid */
-  unsigned long long error_flags;        /* 1: the scan's bounded wait expired */
+  unsigned long long error_flags;        /* 0 (the scan has no bounded waits) */
   unsigned long long max_cell_occupancy; /* largest number of particles in one cell */
 } mf_noalloc_status;
 int mf_cells_build_noalloc(const double *d_pos, int N, double bbmin_x, double bbmin_y, double dx, int nx, int ny,
@@ -366,11 +359,20 @@ int mf_vtk_write_tool(const mf_tool_state *tool, const char *path);
    It may be launched on any stream, also as a child of the caller's own graph; it stays
    valid until the context's buffers, constants, options, dt or flags change, and the steps it
    runs are counted on the device (mf_force_log) but not in mf_status.steps.
-   mf_batch_*: many contexts on one device advanced together by one graph launch: a parent
-   graph holding one child graph of steps_per_launch steps per context, with no edges between
-   them, so small instances run side by side instead of each underfilling the GPU.
-   steps_per_launch = 0 lets the batch pick it (2, 4, 8 or 16: the highest measured throughput
-   over a few launches, which advance the instances). After a host write to an instance its
+   mf_batch_*: many contexts on one device advanced together by one graph launch of
+   steps_per_launch steps, so that small instances run side by side instead of each
+   underfilling the GPU. Where every context steps a locked grid without neighbour lists and
+   all share the precision, heat solver, yield law and plasticity setting, each step of the
+   graph is one launch per phase (cell scan, scatter, reorder + predictor, pair sums, finish,
+   return map) over all instances: their constants and buffers are entries of a device array
+   (the reference keeps them in __constant__ memory, actions_gpu.cu:438-469,
+   interactions_gpu.cu:423-459, tool_gpu.cu:20-27, one system per process) and every block
+   finds its instance; each instance's results equal its own context's steps bit for bit.
+   Otherwise the graph holds one child graph per context, with no edges between them.
+   steps_per_launch = 0 lets the batch tune itself over a few launches, which advance the
+   instances: the block size of the batched pair kernel (64, 128 or 256 threads) and the steps
+   per launch (2, 4, 8 or 16), by the highest measured throughput; mf_batch_config reports the
+   choice (fused: 1 for the batched kernels). After a host write to an instance its
    cell counts are re-primed before the next launch; after a change that invalidates its
    graphs (buffers, constants, options, dt, flags) mf_batch_step returns MF_ERR_STATE and the
    batch must be rebuilt. */
@@ -379,6 +381,7 @@ int mf_graph_capture(mf_ctx *ctx, int n_steps, void **cuda_graph);
 int mf_graph_destroy(void *cuda_graph);
 int mf_batch_create(mf_ctx **ctxs, int n, int steps_per_launch, mf_batch **out);
 int mf_batch_steps_per_launch(const mf_batch *batch, int *steps_per_launch);
+int mf_batch_config(const mf_batch *batch, int *fused, int *pair_block, int *steps_per_launch);
 int mf_batch_step(mf_batch *batch, int n_launches); /* n_launches x steps_per_launch steps each */
 int mf_batch_destroy(mf_batch *batch);
 

@@ -25,7 +25,6 @@ THERMAL_BROOKSHAW, THERMAL_PSE = 0, 1
 JC_JOHNSON_COOK, JC_TANH = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 OPT_KEEP_DERIVATIVES, OPT_NO_GRAPHS, OPT_SORT_EVERY_STEP, OPT_FUSED_PREDICTOR, OPT_NEIGHBOUR_LISTS = 1, 2, 4, 8, 16
-OPT_SMOOTH_MODEL = 32  # differentiable form: the smooth model (FP64 roots, converged return map)
 
 # name -> (field id, doubles per particle, is_int)
 FIELDS = {
@@ -148,7 +147,7 @@ def lib():
         "mf_get_field_device": ([vp, i, vp, vp], i), "mf_set_field_device": ([vp, i, vp, vp], i),
         "mf_vtk_flush": ([vp], i), "mf_vtk_write_particle_arrays": ([C.c_char_p, i] + [vp] * 10, i),
         "mf_graph_capture": ([vp, i, C.POINTER(vp)], i), "mf_graph_destroy": ([vp], i),
-        "mf_batch_create": ([C.POINTER(vp), i, i, C.POINTER(vp)], i), "mf_batch_steps_per_launch": ([vp, ip], i),
+        "mf_batch_create": ([C.POINTER(vp), i, i, C.POINTER(vp)], i), "mf_batch_steps_per_launch": ([vp, ip], i), "mf_batch_config": ([vp, ip, ip, ip], i),
         "mf_batch_step": ([vp, i], i), "mf_batch_destroy": ([vp], i),
         "mf_get_constants": ([vp, C.POINTER(Phys), C.POINTER(Corr), C.POINTER(Joco), C.POINTER(Trml),
                               C.POINTER(Trml), ip], i),
@@ -486,9 +485,11 @@ class Batch:
         rc = self.L.mf_batch_create(arr, len(self.contexts), int(steps_per_launch), C.byref(self.h))
         if rc != MF_OK:
             raise MfError(rc, "mf_batch_create")
-        k = C.c_int()
-        self.L.mf_batch_steps_per_launch(self.h, C.byref(k))
+        k, fused, bs = C.c_int(), C.c_int(), C.c_int()
+        self.L.mf_batch_config(self.h, C.byref(fused), C.byref(bs), C.byref(k))
         self.steps_per_launch = k.value
+        self.fused = bool(fused.value)  # one launch per step phase for all instances
+        self.pair_block = bs.value
 
     def step(self, n_launches=1):
         rc = self.L.mf_batch_step(self.h, int(n_launches))

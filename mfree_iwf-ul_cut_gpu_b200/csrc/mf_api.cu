@@ -15,6 +15,7 @@
 
 #include "mf_kernels.cuh"
 #include "mf_mixed.cuh"
+#include "mf_batch.cuh"
 #include "mfree_b200.h"
 
 using namespace mf;
@@ -79,6 +80,7 @@ struct mf_ctx {
   bool mid_step = false; // stages 1-2 ran: reads see the step's buffer
   bool last_staged = false; // the last predictor ran staged (all intermediates stored)
   int scan_tiles = 0;   // tiles for max_cell + 1 entries
+  int *tsum[2] = {nullptr, nullptr};  // per-tile count totals: written with one parity, read with the other
   int finish_blocks = 0;
   int bbox_blocks = 0;
   int sm_count = 148;
@@ -172,6 +174,7 @@ int alloc_set(mf_ctx *ctx, state_set &s, int N) {
 int invalidate_counts(mf_ctx *ctx) {
   if (ctx->counts_ready && ctx->D.count) {
     CK(cudaMemsetAsync(ctx->D.count, 0, sizeof(int) * (size_t)ctx->G.max_cell, ctx->stream));
+    for (int k = 0; k < 2; ++k) CK(cudaMemsetAsync(ctx->tsum[k], 0, sizeof(int) * (size_t)ctx->scan_tiles, ctx->stream));
   }
   ctx->counts_ready = false;
   return MF_OK;
@@ -214,7 +217,8 @@ int alloc_grid(mf_ctx *ctx, int max_cell) {
   TRY(dalloc(ctx, L, &ctx->D.count, (size_t)max_cell));
   TRY(dalloc(ctx, L, &ctx->D.off, (size_t)max_cell + 1));
   ctx->scan_tiles = (max_cell + SCAN_TILE - 1) / SCAN_TILE + 1;
-  TRY(dalloc(ctx, L, &ctx->D.scan_status, (size_t)ctx->scan_tiles));
+  TRY(dalloc(ctx, L, &ctx->tsum[0], (size_t)ctx->scan_tiles));
+  TRY(dalloc(ctx, L, &ctx->tsum[1], (size_t)ctx->scan_tiles));
   ctx->counts_ready = false;
   return MF_OK;
 }
@@ -230,6 +234,10 @@ void bind_sets(mf_ctx *ctx) {
   ctx->D.B = ctx->set[ctx->cur ^ 1];
   ctx->D.tool_prev = ctx->tool_buf[ctx->cur];
   ctx->D.tool_next = ctx->tool_buf[ctx->cur ^ 1];
+  // a step's scan reads the tile totals the previous step's finish kernel (or the priming
+  // count) added to, and zeroes the ones this step's finish kernel adds to
+  ctx->D.tsum_r = ctx->tsum[ctx->cur ^ 1];
+  ctx->D.tsum_w = ctx->tsum[ctx->cur];
 }
 
 // the steady-state step of a locked grid starts at the scan: the previous step's k_finish
@@ -503,7 +511,6 @@ int mf_ctx_create(int device, mf_ctx **out) {
       ctx->sm_count = sms;
   }
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.ticket, 4);
-  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.scan_done, 1);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.force_log, (size_t)FORCE_LOG_CAP * 2);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.force_last, 2);
   if (rc != MF_OK) { mf_ctx_destroy(ctx); return rc; }
@@ -537,7 +544,6 @@ int mf_set_flags(mf_ctx *ctx, int flags) {
   if (!ctx) return MF_ERR_INVALID;
   ctx->flags = flags;
   ctx->P.keep_derivs = (flags & MF_OPT_KEEP_DERIVATIVES) ? 1 : 0;
-  ctx->P.smooth = (flags & MF_OPT_SMOOTH_MODEL) ? 1 : 0;
   drop_graphs(ctx);
   return MF_OK;
 }
@@ -1013,6 +1019,12 @@ struct mf_batch {
   cudaStream_t stream = nullptr;
   cudaGraphExec_t exec = nullptr;
   int K = 0;
+  // batched kernels: one launch per step phase for all systems (else one child graph per system)
+  bool fused = false;
+  int pair_bs = PAIR_BLOCK;          // block size of the batched pair kernel (tuned)
+  batch_entry *d_entries = nullptr;  // [2][n]: every system bound to each parity of its buffers
+  int *d_first = nullptr;            // 4 maps of n + 1 first blocks: scan, 256-thread phases, pair, plastic
+  int grid[4] = {0, 0, 0, 0};
 };
 
 namespace {
@@ -1022,8 +1034,137 @@ void batch_release(mf_batch *b) {
   b->exec = nullptr;
 }
 
-// one parent graph: a child graph of K steps per context, no edges between them
+// The batched kernels serve systems whose steps run the same kernel variants: locked grids,
+// steps launched whole (not staged), no neighbour lists, one precision, heat solver, yield
+// law and plasticity setting. Anything else keeps the child-graph batch.
+bool batch_can_fuse(mf_batch *b) {
+  const params &P0 = b->ctx[0]->P;
+  for (mf_ctx *c : b->ctx) {
+    set_list_mode(c);
+    const params &P = c->P;
+    if (!fused_step(c) || P.verlet || P.fuse || P.precision != P0.precision ||
+        P.thermal_solver != P0.thermal_solver || P.jc_model != P0.jc_model || P.plastic != P0.plastic ||
+        (P.thermal_solver == MF_THERMAL_PSE && (P.thermal_wp != 0) != (P0.thermal_wp != 0)))
+      return false;
+  }
+  return true;
+}
+
+extern "C++" {  // (this part of the file lies inside the C ABI's extern "C" block)
+template <typename... KArgs, typename... Args>
+int batch_kernel(mf_batch *b, void (*kernel)(KArgs...), int grid, int block, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.stream = b->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = MF_USE_PDL ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...) == cudaSuccess ? MF_OK : MF_ERR_CUDA;
+}
+
+// the pair phase (and PSE) of one step at the tuned block size
+template <int BS>
+int batch_pair(mf_batch *b, const params &P0, batch_map m) {
+  const bool mixed = P0.precision == MF_PRECISION_MIXED;
+  if (mixed) TRY(batch_kernel(b, kb_pair_mixed<BS>, b->grid[2], BS, m));
+  else TRY(batch_kernel(b, kb_pair_fp64<BS>, b->grid[2], BS, m));
+  if (P0.thermal_solver == MF_THERMAL_PSE && P0.thermal_wp) {
+    if (mixed) TRY(batch_kernel(b, kb_pse_mixed<BS>, b->grid[2], BS, m));
+    else TRY(batch_kernel(b, kb_pse<BS>, b->grid[2], BS, m));
+  }
+  return MF_OK;
+}
+}  // extern "C++"
+
+// Entries and block maps of every system, then K steps captured as one graph: per step one
+// launch per phase for all systems (scan, scatter, reorder + predictor, pair sums, finish,
+// return map), each launched as the single-system step launches it (programmatic dependent
+// launch), the systems bound to the parity of their buffers at that step.
+int batch_build_fused(mf_batch *b, int K) {
+  batch_release(b);
+  const int n = (int)b->ctx.size();
+  std::vector<batch_entry> e(2 * (size_t)n);
+  std::vector<int> first(4 * (size_t)(n + 1), 0);
+  long long total_n = 0;
+  for (mf_ctx *c : b->ctx) total_n += c->N;
+  const int sms = b->ctx[0]->sm_count;
+  for (int k = 0; k < n; ++k) {
+    mf_ctx *c = b->ctx[k];
+    c->P.N = c->N;
+    c->last_staged = false;
+    TRY(prime_counts(c));
+    const int saved = c->cur;
+    for (int par = 0; par < 2; ++par) {
+      c->cur = (saved + par) & 1;
+      bind_sets(c);
+      batch_entry &x = e[(size_t)par * n + k];
+      std::memset(&x, 0, sizeof(x));
+      x.P = c->P;
+      x.D = c->D;
+      x.scan_tiles = c->scan_tiles;
+    }
+    c->cur = saved;
+    bind_sets(c);
+    const int blocks[4] = {c->scan_tiles, (c->N + BLOCK - 1) / BLOCK, (c->N + b->pair_bs - 1) / b->pair_bs,
+                           (int)std::max<long long>(1, (long long)sms * PLASTIC_BLOCKS_PER_SM * c->N / total_n)};
+    for (int m = 0; m < 4; ++m) first[(size_t)m * (n + 1) + k + 1] = first[(size_t)m * (n + 1) + k] + blocks[m];
+  }
+  for (int m = 0; m < 4; ++m) b->grid[m] = first[(size_t)m * (n + 1) + n];
+  if (!b->d_entries) {
+    if (cudaMalloc(&b->d_entries, sizeof(batch_entry) * e.size()) != cudaSuccess) return MF_ERR_NOMEM;
+    if (cudaMalloc(&b->d_first, sizeof(int) * first.size()) != cudaSuccess) return MF_ERR_NOMEM;
+  }
+  if (cudaMemcpyAsync(b->d_entries, e.data(), sizeof(batch_entry) * e.size(), cudaMemcpyHostToDevice, b->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(b->d_first, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice, b->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(b->stream) != cudaSuccess)
+    return MF_ERR_CUDA;
+  const params &P0 = b->ctx[0]->P;
+  const bool mixed = P0.precision == MF_PRECISION_MIXED;
+  if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return MF_ERR_CUDA;
+  int rc = MF_OK;
+  for (int st = 0; st < K && rc == MF_OK; ++st) {
+    const batch_entry *ent = b->d_entries + (size_t)(st & 1) * n;
+    const batch_map m_scan{ent, b->d_first, n}, m_256{ent, b->d_first + (n + 1), n},
+        m_pair{ent, b->d_first + 2 * (n + 1), n}, m_pl{ent, b->d_first + 3 * (n + 1), n};
+    rc = batch_kernel(b, kb_scan, b->grid[0], SCAN_THREADS, m_scan);
+    if (rc == MF_OK) rc = batch_kernel(b, kb_scatter, b->grid[1], BLOCK, m_256);
+    if (rc == MF_OK) rc = mixed ? batch_kernel(b, kb_reorder<true>, b->grid[1], BLOCK, m_256)
+                                : batch_kernel(b, kb_reorder<false>, b->grid[1], BLOCK, m_256);
+    if (rc == MF_OK) {
+      switch (b->pair_bs) {
+        case 64: rc = batch_pair<64>(b, P0, m_pair); break;
+        case 256: rc = batch_pair<256>(b, P0, m_pair); break;
+        default: rc = batch_pair<128>(b, P0, m_pair); break;
+      }
+    }
+    if (rc == MF_OK) rc = batch_kernel(b, kb_finish, b->grid[1], FINISH_BLOCK, m_256);
+    if (rc == MF_OK && P0.plastic)
+      rc = P0.jc_model == MF_JC_TANH ? batch_kernel(b, kb_plastic<false>, b->grid[3], BLOCK, m_pl)
+                                     : batch_kernel(b, kb_plastic<true>, b->grid[3], BLOCK, m_pl);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(b->stream, &g);
+  if (rc != MF_OK || ec != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return rc != MF_OK ? rc : MF_ERR_CUDA;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&b->exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) return MF_ERR_CUDA;
+  for (int k = 0; k < n; ++k) b->gen[k] = b->ctx[k]->gen;
+  b->K = K;
+  return MF_OK;
+}
+
+// one parent graph: a child graph of K steps per context, no edges between them (or, where
+// the systems allow it, the batched kernels)
 int batch_build(mf_batch *b, int K) {
+  if (b->fused) return batch_build_fused(b, K);
   batch_release(b);
   cudaGraph_t parent = nullptr;
   cudaError_t e = cudaGraphCreate(&parent, 0);
@@ -1102,29 +1243,45 @@ int mf_batch_create(mf_ctx **ctxs, int n, int steps_per_launch, mf_batch **out) 
   }
   if (rc == MF_OK && cudaSetDevice(b->device) != cudaSuccess) rc = MF_ERR_CUDA;
   if (rc == MF_OK && cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) rc = MF_ERR_CUDA;
+  if (rc == MF_OK) b->fused = batch_can_fuse(b);
   if (rc == MF_OK && steps_per_launch > 0) rc = batch_build(b, steps_per_launch);
   if (rc == MF_OK && steps_per_launch == 0) {
-    // autotune: the steps per launch with the highest throughput over a few real launches
-    // (these launches advance the instances)
+    // autotune over a few real launches (which advance the instances): with the batched
+    // kernels first the pair kernel's block size at 4 steps per launch, then the steps per
+    // launch; the highest measured throughput wins
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = MF_ERR_CUDA;
+    auto measure = [&](int K, double *steps_per_ms) {
+      int r = batch_build(b, K);
+      if (r == MF_OK) r = batch_launch(b, 1);  // warm-up
+      if (r == MF_OK && cudaEventRecord(e0, b->stream) != cudaSuccess) r = MF_ERR_CUDA;
+      if (r == MF_OK) r = batch_launch(b, 2);
+      if (r == MF_OK && cudaEventRecord(e1, b->stream) != cudaSuccess) r = MF_ERR_CUDA;
+      float ms = 0.f;
+      if (r == MF_OK && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        r = MF_ERR_CUDA;
+      *steps_per_ms = 2.0 * K / (ms > 0.f ? ms : 1e-6f);
+      return r;
+    };
+    if (rc == MF_OK && b->fused) {
+      const int bs_cand[3] = {64, 128, 256};
+      double best = -1.;
+      int best_bs = PAIR_BLOCK;
+      for (int ci = 0; ci < 3 && rc == MF_OK; ++ci) {
+        b->pair_bs = bs_cand[ci];
+        double v = 0.;
+        rc = measure(4, &v);
+        if (rc == MF_OK && v > best) { best = v; best_bs = bs_cand[ci]; }
+      }
+      b->pair_bs = best_bs;
+    }
     const int cand[4] = {2, 4, 8, 16};
     double best = -1.;
     int best_k = 2;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = MF_ERR_CUDA;
     for (int ci = 0; ci < 4 && rc == MF_OK; ++ci) {
-      rc = batch_build(b, cand[ci]);
-      if (rc == MF_OK) rc = batch_launch(b, 1);  // warm-up
-      if (rc == MF_OK && cudaEventRecord(e0, b->stream) != cudaSuccess) rc = MF_ERR_CUDA;
-      if (rc == MF_OK) rc = batch_launch(b, 2);
-      if (rc == MF_OK && cudaEventRecord(e1, b->stream) != cudaSuccess) rc = MF_ERR_CUDA;
-      float ms = 0.f;
-      if (rc == MF_OK && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
-        rc = MF_ERR_CUDA;
-      const double steps_per_ms = 2.0 * cand[ci] / (ms > 0.f ? ms : 1e-6f);
-      if (rc == MF_OK && steps_per_ms > best) {
-        best = steps_per_ms;
-        best_k = cand[ci];
-      }
+      double v = 0.;
+      rc = measure(cand[ci], &v);
+      if (rc == MF_OK && v > best) { best = v; best_k = cand[ci]; }
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -1144,6 +1301,14 @@ int mf_batch_steps_per_launch(const mf_batch *b, int *k) {
   return MF_OK;
 }
 
+int mf_batch_config(const mf_batch *b, int *fused, int *pair_block, int *steps_per_launch) {
+  if (!b) return MF_ERR_INVALID;
+  if (fused) *fused = b->fused ? 1 : 0;
+  if (pair_block) *pair_block = b->fused ? b->pair_bs : PAIR_BLOCK;
+  if (steps_per_launch) *steps_per_launch = b->K;
+  return MF_OK;
+}
+
 int mf_batch_step(mf_batch *b, int n_launches) {
   nvtx_range range("mf_batch_step");
   if (!b || n_launches < 0) return MF_ERR_INVALID;
@@ -1157,6 +1322,8 @@ int mf_batch_destroy(mf_batch *b) {
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   batch_release(b);
+  if (b->d_entries) cudaFree(b->d_entries);
+  if (b->d_first) cudaFree(b->d_first);
   for (cudaEvent_t e : b->ev)
     if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);

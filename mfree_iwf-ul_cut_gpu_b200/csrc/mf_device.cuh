@@ -48,10 +48,6 @@ struct params {
   // between, each particle's candidates within 2 h + skin are kept in a list
   int verlet;
   int fuse;  // neighbour lists: the finish kernel also runs the next step's predictor
-  // differentiable form only (MF_OPT_SMOOTH_MODEL): full FP64 roots, angles and plastic
-  // increment instead of the reference's float-rounded ones, and a return map converged to
-  // 1e-13 relative instead of 1e-6 absolute
-  int smooth;
   float skin;
   double eos_c0;  // (double)sqrtf((float)(K / rho0)), the EOS sound speed (actions_gpu.cu:41-51)
   double dt;
@@ -78,7 +74,7 @@ struct dev_status {
   int max_cell_occupancy;
   int error_flags;
   unsigned int force_ticket;
-  unsigned int scan_tile_counter;
+  unsigned int scan_tile_counter;  // (unused: the cell scan takes no tile tickets)
   unsigned long long force_log_head;
   unsigned long long secant_iterations;
   unsigned long long sorts;  // cell-list sorts (every step, except with neighbour lists)
@@ -91,7 +87,7 @@ struct dev_status {
 };
 
 constexpr int FORCE_LOG_CAP = 1 << 16;
-constexpr int ERR_SCAN_WAIT = 1;
+constexpr int ERR_SCAN_WAIT = 1;  // (no longer raised: the cell scan has no bounded waits)
 constexpr int ERR_GRID_BUDGET = 2;
 constexpr int ERR_LIST_OVERFLOW = 4;  // a neighbour list was full: neighbours were dropped
 

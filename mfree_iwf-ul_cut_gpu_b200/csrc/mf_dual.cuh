@@ -148,33 +148,4 @@ __device__ __forceinline__ dn<ND> dsinf_narrow(const dn<ND> &x) {
   return dchain((double)sinf((float)x.v), cos(x.v), x);
 }
 
-// The same five roots and angle functions with a switch: the reference's float-rounded values
-// (smooth = false, the plain FP64 step's arithmetic) or full FP64 values (smooth = true, the
-// opt-in smooth model of the differentiable form, whose objective has no float staircase)
-template <int ND>
-__device__ __forceinline__ dn<ND> dsqrt_sel(const dn<ND> &x, bool smooth) {
-  return smooth ? dsqrt(x) : dsqrtf_narrow(x);
-}
-
-template <int ND>
-__device__ __forceinline__ dn<ND> datan2_sel(const dn<ND> &y, const dn<ND> &x, bool smooth) {
-  if (!smooth) return datan2f_narrow(y, x);
-  dn<ND> r;
-  r.v = atan2(y.v, x.v);
-  const double den = x.v * x.v + y.v * y.v;
-#pragma unroll
-  for (int k = 0; k < ND; ++k) r.d[k] = den > 0. ? (x.v * y.d[k] - y.v * x.d[k]) / den : 0.;
-  return r;
-}
-
-template <int ND>
-__device__ __forceinline__ dn<ND> dcos_sel(const dn<ND> &x, bool smooth) {
-  return smooth ? dchain(cos(x.v), -sin(x.v), x) : dcosf_narrow(x);
-}
-
-template <int ND>
-__device__ __forceinline__ dn<ND> dsin_sel(const dn<ND> &x, bool smooth) {
-  return smooth ? dchain(sin(x.v), cos(x.v), x) : dsinf_narrow(x);
-}
-
 }  // namespace mf

@@ -55,9 +55,9 @@ struct dev_buffers {
   int *hash_new, *perm;
   int4 *perm_u;         // per sorted slot: {particle, cell, cell start, cell end} (unranked)
   int *count;           // per-cell counts (max_cell)
+  int *tsum_r, *tsum_w; // per-tile totals of the counts: read by this step's scan / added to by
+                        // this step's counting for the next (two arrays, swapped every step)
   int *off;             // cell offsets (max_cell + 1)
-  unsigned long long *scan_status;
-  unsigned *scan_done;
   double *partials;     // per-block partial sums (force / bbox)
   unsigned *ticket;     // last-block tickets: [0] force, [1] bbox, [2] tool wear
   double *force_log;    // FORCE_LOG_CAP x 2
@@ -107,11 +107,16 @@ constexpr int PAIR_BLOCK = 128;
 #ifndef REORDER_BLOCKS_PER_SM
 #define REORDER_BLOCKS_PER_SM 5
 #endif
-constexpr unsigned long long SCAN_FLAG_AGG = 1ull << 62;
-constexpr unsigned long long SCAN_FLAG_PREFIX = 2ull << 62;
-constexpr long long SCAN_SPIN_LIMIT = 1ll << 24;
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+// A kernel body's block index and block count within its particle system: the grid's own for a
+// kernel launched for one context, the system's share of the grid in a batched launch that
+// steps many systems at once (mf_batch_*). Bodies use these instead of blockIdx.x / gridDim.x.
+struct blk {
+  int x, n;
+};
+__device__ __forceinline__ blk grid_blk() { return blk{(int)blockIdx.x, (int)gridDim.x}; }
 
 // ---------------------------------------------------------------------------------------
 // adaptive geometry (grid_base::update_geometry, grid.cu:97-136)
@@ -179,12 +184,21 @@ static __global__ void __launch_bounds__(BLOCK) k_bbox(int N, const double2 *__r
 }
 
 // ---------------------------------------------------------------------------------------
+// one particle counted into its cell and into its cell's scan tile (the scan's per-tile totals);
+// the lanes of a warp with the same tile add their total in one atomic
+__device__ __forceinline__ void count_particle(int *count, int *tsum, int hsh) {
+  atomicAdd(&count[hsh], 1);  // no return value: a fire-and-forget reduction
+  const int tile = hsh / SCAN_TILE;
+  const unsigned peers = __match_any_sync(__activemask(), tile);
+  if ((int)lane_id() == __ffs(peers) - 1) atomicAdd(&tsum[tile], __popc(peers));
+}
+
+// ---------------------------------------------------------------------------------------
 // cell hash + count (compute_hashes, grid.cu:34-51)
 static __global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A, dev_buffers D, int num_scan_tiles) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  for (int t = gid; t < num_scan_tiles; t += gridDim.x * blockDim.x) D.scan_status[t] = 0ull;
   unsigned oog = 0;
   if (gid < N) {
     const geom g = *D.g;
@@ -202,157 +216,112 @@ static __global__ void __launch_bounds__(BLOCK) k_hash_count(int N, state_set A,
     else if (hh >= g.num_cell) { hh = g.num_cell - 1; oog = 1; }
     const int hsh = (int)hh;
     D.hash_new[gid] = hsh;
-    atomicAdd(&D.count[hsh], 1);  // no return value: a fire-and-forget reduction
+    count_particle(D.count, D.tsum_r, hsh);  // read by the scan that follows
   }
   unsigned any = __ballot_sync(0xffffffffu, oog);
   if (any && lane_id() == 0) atomicAdd(&D.st->out_of_grid, (unsigned long long)__popc(any));
 }
 
 // ---------------------------------------------------------------------------------------
-// exclusive scan of the cell counts -> offsets, single pass with decoupled look-back.
-// Tile ids come from an atomic ticket, so every tile waits only on tiles that are already
-// running; the wait is bounded and reports ERR_SCAN_WAIT instead of hanging.
-static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int N, int verlet) {
-  MF_PDL_WAIT();
-  MF_PDL_TRIGGER();
+// exclusive scan of the cell counts -> offsets. Whoever counted the particles into their cells
+// (the previous step's finish kernel, or k_hash_count) also added each one to its tile's total
+// (tsum_r, a tile = SCAN_TILE cells), so block b knows where its tile starts by summing the
+// totals of the tiles before it: no block waits for another. Each block also zeroes the counts
+// of its tile and the total the next counting adds to (tsum_w; one block per tile).
+__device__ __forceinline__ void scan_body(const dev_buffers &D, int N, int verlet, blk bk) {
+  const int num_cell = D.g->num_cell;
+  if (threadIdx.x == 0) D.tsum_w[bk.x] = 0;
   if (verlet && !D.st->sort_now) {
     // neighbour lists, no sort this step: the counts the finish kernel made go unused; back
-    // to zero for the next step's (block b clears tile b; the grid has a block per tile)
-    const int num_cell = D.g->num_cell;
-    for (int c = blockIdx.x * SCAN_TILE + threadIdx.x; c < min(num_cell, (blockIdx.x + 1) * SCAN_TILE);
+    // to zero for the next step's
+    for (int c = bk.x * SCAN_TILE + threadIdx.x; c < min(num_cell, (bk.x + 1) * SCAN_TILE);
          c += SCAN_THREADS)
       D.count[c] = 0;
     return;
   }
-  __shared__ int s_tile;
   __shared__ int s_warp[SCAN_THREADS / 32];
   __shared__ int s_excl;
   __shared__ int s_max[SCAN_THREADS / 32];
-  const int num_cell = D.g->num_cell;
   const int num_tiles = (num_cell + SCAN_TILE - 1) / SCAN_TILE;
-  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&D.st->scan_tile_counter, 1u);
-  __syncthreads();
-  const int tile = s_tile;
-  if (tile < num_tiles) {
-    const int base = tile * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
-    static_assert(SCAN_ITEMS % 4 == 0, "whole int4 per thread");
-    const bool full = base + SCAN_ITEMS <= num_cell;  // base: a multiple of SCAN_ITEMS, 16-byte aligned
-    int v[SCAN_ITEMS];
-    if (full) {
+  const int tile = bk.x;
+  if (tile >= num_tiles) return;
+  if (threadIdx.x < 32) {  // the tile's start: the totals of the tiles before it
+    int v = 0;
+    for (int t = (int)lane_id(); t < tile; t += 32) v += __ldcg(D.tsum_r + t);
+    v = __reduce_add_sync(0xffffffffu, v);
+    if (lane_id() == 0) s_excl = v;
+  }
+  const int base = tile * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  static_assert(SCAN_ITEMS % 4 == 0, "whole int4 per thread");
+  const bool full = base + SCAN_ITEMS <= num_cell;  // base: a multiple of SCAN_ITEMS, 16-byte aligned
+  int v[SCAN_ITEMS];
+  if (full) {
 #pragma unroll
-      for (int k = 0; k < SCAN_ITEMS / 4; ++k) {
-        const int4 c = reinterpret_cast<const int4 *>(D.count + base)[k];
-        v[4 * k] = c.x; v[4 * k + 1] = c.y; v[4 * k + 2] = c.z; v[4 * k + 3] = c.w;
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < SCAN_ITEMS; ++k) v[k] = base + k < num_cell ? D.count[base + k] : 0;
+    for (int k = 0; k < SCAN_ITEMS / 4; ++k) {
+      const int4 c = reinterpret_cast<const int4 *>(D.count + base)[k];
+      v[4 * k] = c.x; v[4 * k + 1] = c.y; v[4 * k + 2] = c.z; v[4 * k + 3] = c.w;
     }
-    int tsum = 0, tmax = 0;
+  } else {
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) v[k] = base + k < num_cell ? D.count[base + k] : 0;
+  }
+  int tsum = 0, tmax = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    const int x = v[k];
+    v[k] = tsum;
+    tsum += x;
+    tmax = max(tmax, x);
+  }
+  // warp inclusive scan of thread sums
+  int incl = tsum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if ((int)lane_id() >= o) incl += y;
+  }
+  tmax = __reduce_max_sync(0xffffffffu, tmax);
+  if (lane_id() == 31) s_warp[threadIdx.x >> 5] = incl;
+  if (lane_id() == 0) s_max[threadIdx.x >> 5] = tmax;
+  __syncthreads();
+  int warp_excl = 0, agg = 0, bmax = 0;
+  for (int w = 0; w < SCAN_THREADS / 32; ++w) {
+    if (w < (int)(threadIdx.x >> 5)) warp_excl += s_warp[w];
+    agg += s_warp[w];
+    bmax = max(bmax, s_max[w]);
+  }
+  if (threadIdx.x == 0 && bmax > 0) atomicMax(&D.st->max_cell_occupancy, bmax);
+  const int excl = s_excl + warp_excl + incl - tsum;
+  if (full) {
+    int4 *o = reinterpret_cast<int4 *>(D.off + base);
+    int4 *z = reinterpret_cast<int4 *>(D.count + base);  // ready for the next step
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS / 4; ++k) {
+      o[k] = make_int4(excl + v[4 * k], excl + v[4 * k + 1], excl + v[4 * k + 2], excl + v[4 * k + 3]);
+      z[k] = make_int4(0, 0, 0, 0);
+    }
+  } else {
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS; ++k) {
-      const int x = v[k];
-      v[k] = tsum;
-      tsum += x;
-      tmax = max(tmax, x);
-    }
-    // warp inclusive scan of thread sums
-    int incl = tsum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, incl, o);
-      if ((int)lane_id() >= o) incl += y;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) tmax = max(tmax, __shfl_down_sync(0xffffffffu, tmax, o));
-    if (lane_id() == 31) s_warp[threadIdx.x >> 5] = incl;
-    if (lane_id() == 0) s_max[threadIdx.x >> 5] = tmax;
-    __syncthreads();
-    int warp_excl = 0, agg = 0, bmax = 0;
-    for (int w = 0; w < SCAN_THREADS / 32; ++w) {
-      if (w < (int)(threadIdx.x >> 5)) warp_excl += s_warp[w];
-      agg += s_warp[w];
-      bmax = max(bmax, s_max[w]);
-    }
-    const int thread_excl = warp_excl + incl - tsum;
-    if (threadIdx.x < 32) {
-      // warp-wide look-back: lane l inspects tile (base - l); aggregates of the tiles up to
-      // the nearest inclusive prefix are summed in one round trip per 32 tiles
-      const unsigned lane = lane_id();
-      if (lane == 0 && bmax > 0) atomicMax(&D.st->max_cell_occupancy, bmax);
-      int excl = 0;
-      if (tile == 0) {
-        if (lane == 0) atomicExch(&D.scan_status[0], SCAN_FLAG_PREFIX | (unsigned long long)(unsigned)agg);
-      } else {
-        if (lane == 0) atomicExch(&D.scan_status[tile], SCAN_FLAG_AGG | (unsigned long long)(unsigned)agg);
-        int base = tile - 1;
-        long long spins = 0;
-        bool done = false;
-        while (!done) {
-          const int t = base - (int)lane;
-          unsigned long long w = 2ull << 62;  // before tile 0: an inclusive prefix of 0
-          if (t >= 0) w = *((volatile unsigned long long *)&D.scan_status[t]);
-          while (__any_sync(0xffffffffu, (w & (3ull << 62)) == 0ull)) {
-            if (++spins > SCAN_SPIN_LIMIT) {
-              if (lane == 0) atomicOr(&D.st->error_flags, ERR_SCAN_WAIT);
-              w = 2ull << 62;  // give up: the offsets of this step are wrong, flagged
-              break;
-            }
-            if ((w & (3ull << 62)) == 0ull) w = *((volatile unsigned long long *)&D.scan_status[t]);
-          }
-          const unsigned pre = __ballot_sync(0xffffffffu, (w & (3ull << 62)) == SCAN_FLAG_PREFIX);
-          const int last = pre ? __ffs(pre) - 1 : 31;  // nearest prefix (or the whole window)
-          int v = (int)lane <= last ? (int)(unsigned)(w & 0xffffffffull) : 0;
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-          excl += v;
-          done = pre != 0u;
-          base -= 32;
-        }
-        if (lane == 0)
-          atomicExch(&D.scan_status[tile], SCAN_FLAG_PREFIX | (unsigned long long)(unsigned)(excl + agg));
+      const int c = base + k;
+      if (c < num_cell) {
+        D.off[c] = excl + v[k];
+        D.count[c] = 0;
       }
-      if (lane == 0) s_excl = excl;
-    }
-    __syncthreads();
-    const int excl = s_excl + thread_excl;
-    if (full) {
-      int4 *o = reinterpret_cast<int4 *>(D.off + base);
-      int4 *z = reinterpret_cast<int4 *>(D.count + base);  // ready for the next step
-#pragma unroll
-      for (int k = 0; k < SCAN_ITEMS / 4; ++k) {
-        o[k] = make_int4(excl + v[4 * k], excl + v[4 * k + 1], excl + v[4 * k + 2], excl + v[4 * k + 3]);
-        z[k] = make_int4(0, 0, 0, 0);
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < SCAN_ITEMS; ++k) {
-        const int c = base + k;
-        if (c < num_cell) {
-          D.off[c] = excl + v[k];
-          D.count[c] = 0;
-        }
-      }
-    }
-    if (tile == num_tiles - 1 && threadIdx.x == 0) D.off[num_cell] = s_excl + agg;
-  }
-  // the last block to finish re-arms the tile ticket
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    unsigned d = atomicAdd(D.scan_done, 1u);
-    if (d == gridDim.x - 1) {
-      D.st->scan_tile_counter = 0u;
-      *D.scan_done = 0u;
     }
   }
+  if (tile == num_tiles - 1 && threadIdx.x == 0) D.off[num_cell] = s_excl + agg;
   (void)N;
 }
 
-static __global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D, int verlet) {
+static __global__ void __launch_bounds__(SCAN_THREADS) k_scan(dev_buffers D, int N, int verlet) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  scan_body(D, N, verlet, grid_blk());
+}
+
+__device__ __forceinline__ void scatter_body(int N, const dev_buffers &D, int verlet, blk bk) {
+  const int q = bk.x * blockDim.x + threadIdx.x;
   if (q >= N) return;
   if (verlet && !D.st->sort_now) return;  // neighbour lists, no sort this step
   const int c = D.hash_new[q];
@@ -362,6 +331,12 @@ static __global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D, 
   // needs one load.
   const int slot = atomicAdd(&D.count[c], 1);
   D.perm_u[s + slot] = make_int4(q, c, s, D.off[c + 1]);
+}
+
+static __global__ void __launch_bounds__(BLOCK) k_scatter(int N, dev_buffers D, int verlet) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
+  scatter_body(N, D, verlet, grid_blk());
 }
 
 // ---------------------------------------------------------------------------------------
@@ -508,10 +483,8 @@ __device__ __forceinline__ void predict_particle(const params &P, const dev_buff
 }
 
 template <bool PREDICT, bool MIXED>
-static __global__ void __launch_bounds__(BLOCK, REORDER_BLOCKS_PER_SM) k_reorder(params P, dev_buffers D) {
-  MF_PDL_WAIT();
-  MF_PDL_TRIGGER();
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void reorder_body(const params &P, const dev_buffers &D, blk bk) {
+  const int t = bk.x * blockDim.x + threadIdx.x;
   if (t >= P.N) return;
   // with neighbour lists, a step without a sort keeps the order and the cells of the last
   // sort: the identity permutation
@@ -574,6 +547,13 @@ static __global__ void __launch_bounds__(BLOCK, REORDER_BLOCKS_PER_SM) k_reorder
   predict_particle<MIXED>(P, D, B, q, hsh, pos, vel, S, rho, T, pos_t, vel_t, S_t, rho_t, T_t, f, h, sort);
 }
 
+template <bool PREDICT, bool MIXED>
+static __global__ void __launch_bounds__(BLOCK, REORDER_BLOCKS_PER_SM) k_reorder(params P, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
+  reorder_body<PREDICT, MIXED>(P, D, grid_blk());
+}
+
 // ---------------------------------------------------------------------------------------
 // pair sums over the 5x5 cell window + rates, plain FP64 (interactions_gpu.cu:147-345,
 // actions_gpu.cu:99-224). With hash = ix*ny + iy, the five cells of one window column are
@@ -594,10 +574,7 @@ __device__ __forceinline__ void load_rec(const double *__restrict__ rec, int N, 
   }
 }
 
-static __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_pair_fp64(params P, dev_buffers D) {
-  MF_PDL_WAIT();
-  MF_PDL_TRIGGER();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void pair_fp64_particle(const params &P, const dev_buffers &D, int q) {
   if (q >= P.N) return;
   const double *__restrict__ rec = D.rec;
   const int N = P.N;
@@ -742,12 +719,21 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_pair_fp64(params P, de
   if (thermal) B.T_t[q] = thermal_alpha * T_lapl;
 }
 
-// PSE heat Laplacian (interactions_gpu.cu:88-144): every particle of the window, blanked
-// ones included; alpha taken through the reference's half-length texture binding (:405).
-static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers D) {
+// the FP64 pair sums of block bk.x's particles
+__device__ __forceinline__ void pair_fp64_body(const params &P, const dev_buffers &D, blk bk) {
+  pair_fp64_particle(P, D, bk.x * blockDim.x + threadIdx.x);
+}
+
+static __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_pair_fp64(params P, dev_buffers D) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  pair_fp64_body(P, D, grid_blk());
+}
+
+// PSE heat Laplacian (interactions_gpu.cu:88-144): every particle of the window, blanked
+// ones included; alpha taken through the reference's half-length texture binding (:405).
+__device__ __forceinline__ void pse_body(const params &P, const dev_buffers &D, blk bk) {
+  const int q = bk.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const double *__restrict__ rec = D.rec;
   const int N = P.N;
@@ -784,11 +770,18 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers
   D.B.T_t[q] = alpha * T_ti;
 }
 
+static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
+  pse_body(P, D, grid_blk());
+}
+
 // ---------------------------------------------------------------------------------------
 // the rigid tool of this step, advanced in shared memory: tool::update_tool (tool.cpp:211-221)
 // with IEEE-rounded operations (bitwise equal to the host's double arithmetic), one lane per
 // segment and one for the fillet; block 0 stores it for the next step
-__device__ __forceinline__ void tool_advance_shared(mf_tool_state &T, const dev_buffers &D, double dt) {
+__device__ __forceinline__ void tool_advance_shared(mf_tool_state &T, const dev_buffers &D, double dt,
+                                                    bool first_block) {
   // copied word by word by the block's threads
   static_assert(sizeof(mf_tool_state) % sizeof(double) == 0, "tool state is a whole number of doubles");
   constexpr int WORDS = (int)(sizeof(mf_tool_state) / sizeof(double));
@@ -809,7 +802,7 @@ __device__ __forceinline__ void tool_advance_shared(mf_tool_state &T, const dev_
     T.fillet.p[1] = __dadd_rn(T.fillet.p[1], sy);
   }
   __syncthreads();
-  if (blockIdx.x == 0 && threadIdx.x == 0) *D.tool_next = T;
+  if (first_block && threadIdx.x == 0) *D.tool_next = T;
 }
 
 // corrector .. invalidate for one particle (leap_frog.cu:68-92, actions_gpu.cu:135-162,
@@ -1177,21 +1170,16 @@ __device__ __forceinline__ void finish_particle_phased(const params &P, const de
 #define FINISH_FLAT_MIN_BLOCKS 3
 #endif
 template <bool FUSE_HASH>
-__global__ void __launch_bounds__(FINISH_BLOCK, FINISH_FLAT_MIN_BLOCKS) k_finish_flat(params P, dev_buffers D,
-                                                                                    int num_scan_tiles) {
-  MF_PDL_WAIT();
-  MF_PDL_TRIGGER();
+__device__ __forceinline__ void finish_flat_body(const params &P, const dev_buffers &D,
+                                                                                    int num_scan_tiles, blk bk) {
   __shared__ mf_tool_state s_tool;
   __shared__ ksum sm[FINISH_BLOCK / 32][4];
   __shared__ unsigned smc[FINISH_BLOCK / 32][4];
   __shared__ bool last;
-  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt);
-  const int q = blockIdx.x * FINISH_BLOCK + threadIdx.x;
+  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt, bk.x == 0);
+  const int q = bk.x * FINISH_BLOCK + threadIdx.x;
   const bool identity = P.verlet && !*(volatile unsigned *)&D.st->sort_now;
-  if (FUSE_HASH) {
-    const int stride = gridDim.x * FINISH_BLOCK;
-    for (int t = q; t < num_scan_tiles; t += stride) D.scan_status[t] = 0ull;
-  }
+  (void)num_scan_tiles;
   double2 fc = make_double2(0., 0.), ft = make_double2(0., 0.);
   unsigned newly_blanked = 0, blanked_now = 0, oog = 0;
   bool want_sort = false;
@@ -1214,7 +1202,7 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_FLAT_MIN_BLOCKS) k_finish
       else if (hh >= g.num_cell) { hh = g.num_cell - 1; oog = 1; }
       const int hsh = (int)hh;
       D.hash_new[q] = hsh;
-      atomicAdd(&D.count[hsh], 1);
+      count_particle(D.count, D.tsum_w, hsh);  // read by the next step's scan
     }
   }
   // the block's force sums (compensated), in the fixed tree of k_finish; warps whose forces are
@@ -1257,8 +1245,8 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_FLAT_MIN_BLOCKS) k_finish
         for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[v][k]);
     }
     for (int k = 0; k < 4; ++k) {
-      D.partials[(size_t)blockIdx.x * 8 + 2 * k] = r[k].s;
-      D.partials[(size_t)blockIdx.x * 8 + 2 * k + 1] = r[k].c;
+      D.partials[(size_t)bk.x * 8 + 2 * k] = r[k].s;
+      D.partials[(size_t)bk.x * 8 + 2 * k + 1] = r[k].c;
     }
     unsigned long long cnt[3] = {smc[0][0], smc[0][1], smc[0][2]};
     unsigned ws = smc[0][3];
@@ -1272,13 +1260,13 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_FLAT_MIN_BLOCKS) k_finish
     if (cnt[2]) atomicAdd(&D.st->out_of_grid, cnt[2]);
     __threadfence();
     const unsigned t = atomicAdd(&D.ticket[0], 1u);
-    last = (t == gridDim.x - 1);
+    last = (t == bk.n - 1);
   }
   __syncthreads();
   if (!last) return;
   // last block: fixed-order reduction of all block partials
   __threadfence();
-  const int n_chunks = gridDim.x;
+  const int n_chunks = bk.n;
   ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
   for (int b = threadIdx.x; b < n_chunks; b += blockDim.x) {
     const volatile double *pr = D.partials + (size_t)b * 8;
@@ -1317,6 +1305,13 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_FLAT_MIN_BLOCKS) k_finish
   }
 }
 
+template <bool FUSE_HASH>
+__global__ void __launch_bounds__(FINISH_BLOCK, FINISH_FLAT_MIN_BLOCKS) k_finish_flat(params P, dev_buffers D, int num_scan_tiles) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
+  finish_flat_body<FUSE_HASH>(P, D, num_scan_tiles, grid_blk());
+}
+
 // Corrector .. invalidate for all particles plus the tool force (output.cu:31-39). A fixed
 // grid of blocks takes chunks of BLOCK consecutive particles from an atomic counter, so the
 // blocks that meet the costly particles (yield tests, contact) do not set the kernel's length.
@@ -1340,7 +1335,7 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
     s_jc = P.joco;
     s_chunk[0] = (int)atomicAdd(D.finish_chunk, 1u);
   }
-  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt);  // (its first barrier also covers s_jc, s_chunk)
+  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt, blockIdx.x == 0);  // (its first barrier also covers s_jc, s_chunk)
   else __syncthreads();
   const int stride = gridDim.x * blockDim.x;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1357,8 +1352,8 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
   if (FUSE_HASH) {
     g = *D.g;
     inv_dx = 1. / g.dx;
-    for (int t = gid; t < num_scan_tiles; t += stride) D.scan_status[t] = 0ull;
   }
+  (void)num_scan_tiles;
   for (int buf = 0;; buf ^= 1) {
     const int chunk = s_chunk[buf];
     if (chunk >= n_chunks) break;
@@ -1387,7 +1382,7 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
         else if (hh >= g.num_cell) { hh = g.num_cell - 1; ++oog; }
         const int hsh = (int)hh;
         D.hash_new[q] = hsh;
-        atomicAdd(&D.count[hsh], 1);
+        count_particle(D.count, D.tsum_w, hsh);  // read by the next step's scan
       }
     }
     // the chunk's force sums (compensated), in a fixed tree: warps, then warps in order. Only
@@ -1560,9 +1555,7 @@ __device__ __forceinline__ double solve_secant_pair(const mf_joco_constants &jc,
 }
 
 template <bool PAIRED>
-static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic(params P, dev_buffers D) {
-  MF_PDL_WAIT();
-  MF_PDL_TRIGGER();
+__device__ __forceinline__ void plastic_body(const params &P, const dev_buffers &D, blk bk) {
   __shared__ mf_joco_constants s_jc;  // by reference into the out-of-line functions
   __shared__ unsigned long long s_cnt[BLOCK / 32][2];
   if (threadIdx.x == 0) s_jc = P.joco;
@@ -1578,8 +1571,8 @@ static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic
   const unsigned sub = PAIRED ? (lane_id() & 1u) : 0u;
   const unsigned pmask = PAIRED ? (0x3u << (lane_id() & ~1u)) : 0xffffffffu;
   unsigned capped = 0u, iters_sum = 0u;
-  const unsigned stride = gridDim.x * blockDim.x / LANES;
-  for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) / LANES; i < n; i += stride) {
+  const unsigned stride = bk.n * blockDim.x / LANES;
+  for (unsigned i = (bk.x * blockDim.x + threadIdx.x) / LANES; i < n; i += stride) {
     const plastic_item it = D.plastic_list[i];
     const int q = it.q;
     double T = it.T;
@@ -1659,6 +1652,13 @@ static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic
     if (c) atomicAdd(&D.st->secant_cap_hits, c);
     if (itn) atomicAdd(&D.st->secant_iterations, itn);
   }
+}
+
+template <bool PAIRED>
+static __global__ void __launch_bounds__(BLOCK, PLASTIC_BLOCKS_PER_SM) k_plastic(params P, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
+  plastic_body<PAIRED>(P, D, grid_blk());
 }
 
 // Usui tool wear rate (tool_wear.cu:20-64) on the current state, on the device instead of

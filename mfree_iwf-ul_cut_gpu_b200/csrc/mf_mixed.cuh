@@ -43,26 +43,38 @@ struct mixed_const {
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
+// r^2 with its one fused multiply-add written out, so that every kernel that tests or uses a
+// pair's distance (window, list build, list) rounds it the same way: the list form and the
+// window form then give the same sums bit for bit on a step that builds the lists
+__device__ __forceinline__ float dist2(float x, float y) { return fmaf(x, x, __fmul_rn(y, y)); }
+
 // one neighbour j (records b0..b3) of particle i at offset (xij, yij)
 __device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_const &K, mixed_acc &a, float xij,
                                                float yij, const float4 &b0, const float4 &b1, const float4 &b2,
                                                const float4 &b3) {
   const unsigned fjw = (unsigned)__float_as_int(b0.z);
-  const float rr2 = xij * xij + yij * yij;
+  const float rr2 = dist2(xij, yij);
   const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
-  // the reference's cubic spline (kernels.cuh:30-70) with both branches on q evaluated and one
-  // selected, so that the lanes of a warp do not split on it. The value keeps the reference's
-  // form: 1 - 1.5 q^2 (1 - q / 2) for q <= 1 and (2 - q)^6 / 4 (sic: _2mq2 cubed) for q > 1;
-  // the derivative -3 q (1 - 3 q / 4) and -3 (2 - q)^2 / 4 is written as 3 u^2 - 3 t^2 / 4 with
-  // t = 2 - q, u = max(1 - q, 0). Out of support (or at r^2 < 1e-8) both are 0.
-  const float rinv = rsqrtf(rr2);
-  const float qq = rr2 * rinv * I.h1;
-  const float t = 2.f - qq, u = fmaxf(1.f - qq, 0.f);
-  const float t2 = t * t, u2 = u * u;
-  const float val = qq > 1.f ? 0.25f * t2 * t2 * t2 : fmaf(-1.5f * qq * qq, fmaf(-0.5f, qq, 1.f), 1.f);
-  const float der = fmaf(3.f, u2, -0.75f * t2) * I.h1 * rinv;
-  const float w = in_support ? val * I.fac : 0.f;
-  const float dwr = in_support ? der * I.fac : 0.f;
+  // the reference's cubic spline (kernels.cuh:30-70), its value (2 - q)^6 / 4 for q > 1 (sic:
+  // _2mq2 cubed) included. (Evaluating both branches and selecting, to keep a warp's lanes
+  // together, measured 8 us slower on the ~150k-particle cut.)
+  float w = 0.f, dwr = 0.f;
+  if (in_support) {
+    const float rinv = rsqrtf(rr2);
+    const float qq = rr2 * rinv * I.h1;
+    float val, der;
+    if (qq > 1.f) {
+      const float t = 2.f - qq;
+      const float t2 = t * t;
+      val = 0.25f * t2 * t2 * t2;
+      der = -0.75f * t2 * I.h1 * rinv;
+    } else {
+      val = fmaf(-1.5f * qq * qq, fmaf(-0.5f, qq, 1.f), 1.f);
+      der = -3.0f * qq * fmaf(-0.75f, qq, 1.f) * I.h1 * rinv;
+    }
+    w = val * I.fac;
+    dwr = der * I.fac;
+  }
   const float2 pij = f2(xij, yij);
   const float2 w_xy = __fmul2_rn(f2(dwr, dwr), pij);
   const float volj = b3.z;
@@ -82,11 +94,11 @@ __device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_con
     const float2 dvp = __fmul2_rn(dv, pij);
     const float vijposij = -(dvp.x + dvp.y);
     const float irhoij = __fdividef(2.f, I.rho + b3.x);
-    {  // Monaghan viscosity for approaching pairs, as a select rather than a branch
+    if (vijposij < 0.f) {  // Monaghan viscosity for approaching pairs
       const float cij = 0.5f * (I.c + b3.y);
       const float hij = 0.5f * (I.h + b2.w);
       const float muij = hij * vijposij * __fdividef(1.f, fmaf(K.eta2 * hij, hij, rr2));
-      const float npi = vijposij < 0.f ? (K.alpha * cij - K.beta * muij) * muij * irhoij : 0.f;  // -pi_ij
+      const float npi = fmaf(K.alpha, cij, -K.beta * muij) * muij * irhoij;  // -pi_ij
       a.vt = __ffma2_rn(f2(npi, npi), w_xy, a.vt);
     }
     const float xs = w * irhoij;
@@ -116,14 +128,14 @@ __device__ __forceinline__ int build_list(const dev_buffers &D, const float4 *__
     const int col = ii * g.ny;
     const int j0 = __ldg(D.off + col + low_j);
     const int j1 = __ldg(D.off + col + high_j);
-    const float ox = (float)(gi - ii) * dxc + I.x;
+    const float ox = fmaf((float)(gi - ii), dxc, I.x);
     const unsigned tag = (unsigned)(gi - ii + 3) << LIST_INDEX_BITS;
     for (int j = j0; j < j1; ++j) {
       const float4 b0 = __ldg(r0 + j);
       const unsigned fjw = (unsigned)__float_as_int(b0.z);
       const float xij = ox - b0.x;
       const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
-      const float rr2 = xij * xij + yij * yij;
+      const float rr2 = dist2(xij, yij);
       if (!(fjw & FLAG_BLANKED) && (!(rr2 >= R2) || (fjw & FLAG_NONFINITE))) {
         if (cnt < LIST_CAP) row[cnt] = (unsigned)j | tag;
         ++cnt;
@@ -189,10 +201,7 @@ static __global__ void k_list_check(params P, dev_buffers D, const double2 *__re
 // LIST: the neighbour-list form (steps with P.verlet). 80 registers (6 blocks of 128 per SM)
 // keep both forms free of spills; the list form measured slower at 7 and 8 blocks per SM
 template <bool LIST>
-static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, dev_buffers D) {
-  MF_PDL_WAIT();
-  MF_PDL_TRIGGER();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_buffers &D, int q) {
   if (q >= P.N) return;
   // record planes (structure of arrays): plane k of particle j at [k * N + j]
   const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
@@ -256,12 +265,12 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
         const bool live = k0 + u < cnt;
         const unsigned e = live ? ev[u] : (unsigned)q | (3u << LIST_INDEX_BITS);
         const int j = (int)(e & LIST_INDEX_MASK);
-        const float ox = (float)((int)(e >> LIST_INDEX_BITS) - 3) * dxc + I.x;
+        const float ox = fmaf((float)((int)(e >> LIST_INDEX_BITS) - 3), dxc, I.x);
         const float4 b0 = __ldg(r0 + j), b1 = __ldg(r1 + j), b2 = __ldg(r2 + j), b3 = __ldg(r3 + j);
         const unsigned fjw = (unsigned)__float_as_int(b0.z);
         const float xij = ox - b0.x;
         const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
-        const float rr2 = xij * xij + yij * yij;
+        const float rr2 = dist2(xij, yij);
         const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
         if (live && !(fjw & FLAG_BLANKED) && (in_support || (fjw & FLAG_NONFINITE)))
           mixed_interact(I, K, acc, xij, yij, b0, b1, b2, b3);
@@ -276,7 +285,7 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
       const int col = ii * g.ny;
       const int j0 = __ldg(D.off + col + low_j);
       const int j1 = __ldg(D.off + col + high_j);
-      const float ox = (float)(gi - ii) * dxc + I.x;
+      const float ox = fmaf((float)(gi - ii), dxc, I.x);
       // chunks of up to 32 candidates: mark the contributing ones, then visit them in order
       for (int jb = j0; jb < j1; jb += 32) {
         const int jn = min(32, j1 - jb);
@@ -287,7 +296,7 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
           const unsigned fjw = (unsigned)__float_as_int(b0.z);
           const float xij = ox - b0.x;
           const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
-          const float rr2 = xij * xij + yij * yij;
+          const float rr2 = dist2(xij, yij);
           const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
           const bool take = !(fjw & FLAG_BLANKED) && (in_support || I.nonfinite || (fjw & FLAG_NONFINITE));
           mask |= (take ? 1u : 0u) << k;
@@ -347,14 +356,25 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, d
   if (thermal) B.T_t[q] = thermal_alpha * (double)T_lapl;
 }
 
+// the mixed pair sums of block bk.x's particles
+template <bool LIST>
+__device__ __forceinline__ void pair_mixed_body(const params &P, const dev_buffers &D, blk bk) {
+  pair_mixed_particle<LIST>(P, D, bk.x * blockDim.x + threadIdx.x);
+}
+
+template <bool LIST>
+static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
+  pair_mixed_body<LIST>(P, D, grid_blk());
+}
+
 // PSE heat Laplacian (interactions_gpu.cu:88-144, kernels.cuh:72-89) in FP32 for the mixed
 // form, on the FP32 records: the same window (every particle of the 5x5 cells, blanked ones
 // included, no support cut-off) and the same alpha through the half-length texture binding;
 // exp from the hardware approximation, temperatures relative to the initial temperature.
-static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse_mixed(params P, dev_buffers D) {
-  MF_PDL_WAIT();
-  MF_PDL_TRIGGER();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void pse_mixed_body(const params &P, const dev_buffers &D, blk bk) {
+  const int q = bk.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
   const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
   const float4 *__restrict__ r2 = r0 + 2 * (size_t)P.N;
@@ -395,6 +415,12 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse_mixed(params P, dev_b
     }
   }
   D.B.T_t[q] = alpha * (double)T_ti;
+}
+
+static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse_mixed(params P, dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
+  pse_mixed_body(P, D, grid_blk());
 }
 
 }  // namespace mf

@@ -39,10 +39,9 @@ struct noalloc_scratch {
   int count[NA_MAX_CELLS];
   int off[NA_MAX_CELLS + 1];
   int hash_new[NA_MAX_PARTICLES];
-  unsigned long long scan_status[NA_SCAN_TILES];
+  int tsum[2][NA_SCAN_TILES];  // per-tile count totals: [0] counted into, [1] zeroed by the scan
   geom g;
   dev_status st;
-  unsigned scan_done;
 };
 static_assert(sizeof(noalloc_scratch) < (27u << 20), "the scratch array stays near 26 MiB");
 
@@ -67,18 +66,17 @@ int scratch_for_current_device(noalloc_scratch **out) {
   return MF_OK;
 }
 
-// zero the counts, the scan's tile states, tickets and status; store the geometry
+// zero the counts, the scan's per-tile totals and the status; store the geometry
 __global__ void k_na_clear(noalloc_scratch *S, geom g) {
   const int stride = gridDim.x * blockDim.x;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   for (int c = gid; c < g.num_cell; c += stride) S->count[c] = 0;
   const int tiles = (g.num_cell + SCAN_TILE - 1) / SCAN_TILE + 1;
-  for (int t = gid; t < tiles; t += stride) S->scan_status[t] = 0ull;
+  for (int t = gid; t < tiles; t += stride) S->tsum[0][t] = 0;
   if (gid == 0) {
     S->g = g;
     dev_status z{};
     S->st = z;
-    S->scan_done = 0u;
   }
 }
 
@@ -97,7 +95,7 @@ __global__ void k_na_hash(const double2 *__restrict__ pos, int N, noalloc_scratc
     else if (hh >= g.num_cell) { hh = g.num_cell - 1; oog = 1; }
     const int h = (int)hh;
     S->hash_new[i] = h;
-    atomicAdd(&S->count[h], 1);
+    count_particle(S->count, S->tsum[0], h);
   }
   const unsigned any = __ballot_sync(0xffffffffu, oog);
   if (any && (threadIdx.x & 31u) == 0) atomicAdd(&S->st.out_of_grid, (unsigned long long)__popc(any));
@@ -175,8 +173,8 @@ extern "C" int mf_cells_build_noalloc(const double *d_pos, int N, double bbmin_x
   D.off = S->off;
   D.hash_new = S->hash_new;
   D.perm_u = S->perm_u;
-  D.scan_status = S->scan_status;
-  D.scan_done = &S->scan_done;
+  D.tsum_r = S->tsum[0];
+  D.tsum_w = S->tsum[1];
   D.g = &S->g;
   D.st = &S->st;
   const int scan_tiles = (g.num_cell + SCAN_TILE - 1) / SCAN_TILE + 1;

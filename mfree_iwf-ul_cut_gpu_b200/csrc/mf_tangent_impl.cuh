@@ -48,11 +48,11 @@ __global__ void k_t_posv(int N, tbuf T) {
 
 // artificial stress (actions_gpu.cu:35-39, 53-97) on duals
 __device__ void t_artificial_stress(const DN &rhoi, const DN &pi, const DN &Sx, const DN &Sy, const DN &Sz,
-                                    double eps, DN &Rxx, DN &Rxy, DN &Ryy, bool smooth) {
+                                    double eps, DN &Rxx, DN &Rxy, DN &Ryy) {
   const DN sxx = Sx - pi, sxy = Sy, syy = Sz - pi;
   const DN rhoi21 = 1. / (rhoi * rhoi);
-  const DN theta = 0.5 * datan2_sel(2. * sxy, sxx - syy, smooth);
-  const DN ct = dcos_sel(theta, smooth), st = dsin_sel(theta, smooth);
+  const DN theta = 0.5 * datan2f_narrow(2. * sxy, sxx - syy);
+  const DN ct = dcosf_narrow(theta), st = dsinf_narrow(theta);
   const DN ct2 = ct * ct, st2 = st * st;
   const DN rot_sxx = ct2 * sxx + 2.0 * ct * st * sxy + st2 * syy;
   const DN rot_syy = st2 * sxx - 2.0 * ct * st * sxy + ct2 * syy;
@@ -90,9 +90,9 @@ __global__ void k_t_reorder(params P, dev_buffers D, tbuf T) {
   DN prs = dconst<ND>(0.), Rxx = dconst<ND>(0.), Rxy = dconst<ND>(0.), Ryy = dconst<ND>(0.);
   if (!tool) {
     const double rho0 = P.phys.rho0;
-    const double c0 = P.smooth ? sqrt(P.phys.K / rho0) : (double)sqrtf((float)(P.phys.K / rho0));
+    const double c0 = (double)sqrtf((float)(P.phys.K / rho0));
     prs = c0 * c0 * (s.rho - rho0);
-    t_artificial_stress(s.rho, prs, s.S[0], s.S[1], s.S[2], P.corr.stresseps, Rxx, Rxy, Ryy, P.smooth != 0);
+    t_artificial_stress(s.rho, prs, s.S[0], s.S[1], s.S[2], P.corr.stresseps, Rxx, Rxy, Ryy);
   }
   T.pp[q] = prs;
   const DN rho21 = 1. / (s.rho * s.rho);
@@ -101,7 +101,7 @@ __global__ void k_t_reorder(params P, dev_buffers D, tbuf T) {
   r.sxx = (s.S[0] - prs) * rho21; r.sxy = s.S[1] * rho21; r.syy = (s.S[2] - prs) * rho21;
   r.Rxx = Rxx; r.Rxy = Rxy; r.Ryy = Ryy;
   r.rho = s.rho;
-  r.c = dsqrt_sel(P.phys.K / s.rho, P.smooth != 0);
+  r.c = dsqrtf_narrow(P.phys.K / s.rho);
   r.vol = P.phys.mass / s.rho;
   r.T = s.T;
   r.h = s.h;
@@ -143,7 +143,7 @@ __global__ void k_t_pair(params P, dev_buffers D, tbuf T) {
       const DN rr2 = xij * xij + yij * yij;
       if (rr2.v >= fourh2 || rr2.v < 1e-8) continue;  // outside the support: W = 0
       // cubic spline (kernels.cuh:30-70), rad = (double)sqrtf((float)rr2)
-      const DN rad = dsqrt_sel(rr2, P.smooth != 0);
+      const DN rad = dsqrtf_narrow(rr2);
       const DN qq = rad * h1;
       DN val, der;
       if (qq.v > 1) {
@@ -227,15 +227,10 @@ __device__ DN t_sigma_yield(const params &P, const tparams &TP, const DN &eps_pl
 }
 
 // secant radial return (plasticity.cuh:74-119) iterated on duals: the derivative of the
-// iterate the reference returns. The reference stops at an absolute change below 1e-6
-// (plasticity.cuh:108), a few per cent of a typical increment, so its converged increment jumps
-// whenever a particle's iteration count changes; the smooth model (P.smooth) iterates until the
-// change is below 1e-13 of the increment, where the iterate and its derivative are those of the
-// exact root (at most 100 iterations either way).
+// iterate the reference returns
 __device__ DN t_solve_secant(const params &P, const tparams &TP, const DN &init, const DN &norm_Strial,
                              const DN &eps_pl_init, const DN &t, double delta_t, double mu) {
-  const double s23 = sqrt(2.0 / 3.0);
-  const bool smooth = P.smooth != 0;
+  const double s23 = sqrt(2.0 / 3.0), tol = 1e-6;
   DN dl = init, dl_old = init;
   int iter = 0;
   while (true) {
@@ -248,8 +243,7 @@ __device__ DN t_solve_secant(const params &P, const tparams &TP, const DN &init,
     dl_old = dl;
     dl = dl - g / slope;
     if (dl.v < 0.) dl = -0.1 * dl;
-    const double tol = smooth ? 1e-13 * fabs(dl.v) : 1e-6;
-    if (fabs(dl.v - dl_old.v) < tol || (smooth && dl.v == dl_old.v)) return dl;
+    if (fabs(dl.v - dl_old.v) < tol) return dl;
     if (iter > 100) return dl;
     iter++;
   }
@@ -326,23 +320,23 @@ __global__ void __launch_bounds__(128) k_t_finish(params P, dev_buffers D, tbuf 
     DN eps_pl = B.eps, eps_pl_dot = B.epsd;
     DN fc[2] = {B.fc[0], B.fc[1]}, ft[2] = {B.ft[0], B.ft[1]};
     if (P.has_tool && P.fric_heat && !tool) {  // friction heat (actions_gpu.cu:135-162)
-      const DN f_fric_mag = dsqrt_sel(ft[0] * ft[0] + ft[1] * ft[1], P.smooth != 0);
+      const DN f_fric_mag = dsqrtf_narrow(ft[0] * ft[0] + ft[1] * ft[1]);
       if (f_fric_mag.v != 0.) {
         const DN vdx = vel[0] - TL.vel[0], vdy = vel[1] - TL.vel[1];
         const DN vdn = vdx * T.n2[2 * q] + vdy * T.n2[2 * q + 1];
         const DN vrx = vdx - vdn, vry = vdy - vdn;
-        const DN v_rel_mag = dsqrt_sel(vrx * vrx + vry * vry, P.smooth != 0);
+        const DN v_rel_mag = dsqrtf_narrow(vrx * vrx + vry * vry);
         Tm += P.trml_wp.eta * dt * f_fric_mag * v_rel_mag / (P.trml_wp.cp * P.phys.mass);
       }
     }
     if (P.plastic && !tool) {  // JC radial return (actions_gpu.cu:226-285)
       const double mu = P.phys.G;
       const DN Sxx = S[0], Syy = S[2], Szz = S[3], Sxy = S[1];
-      const DN norm_Strial = dsqrt_sel(Sxx * Sxx + Syy * Syy + Szz * Szz + Sxy * Sxy, P.smooth != 0);
+      const DN norm_Strial = dsqrtf_narrow(Sxx * Sxx + Syy * Syy + Szz * Szz + Sxy * Sxy);
       const DN pr = T.pp[q];
       const DN cxx = Sxx - pr, cyy = Syy - pr, czz = Szz - pr, cxy = Sxy;
-      const DN svm = dsqrt_sel((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz +
-                                   3.0 * cxy * cxy, P.smooth != 0);
+      const DN svm = dsqrtf_narrow((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz +
+                                   3.0 * cxy * cxy);
       const DN sigma_Y = t_sigma_yield(P, TP, eps_pl, eps_pl_dot, Tm);
       if (svm.v < sigma_Y.v) {
         eps_pl_dot = dconst<ND>(0.);
@@ -350,10 +344,9 @@ __global__ void __launch_bounds__(128) k_t_finish(params P, dev_buffers D, tbuf 
         DN init = eps_pl_dot * dt * sqrt(2. / 3.);
         if (!(init.v > 1e-8)) init = dconst<ND>(fmax(init.v, 1e-8));
         const DN dl = t_solve_secant(P, TP, init, norm_Strial, eps_pl, Tm, dt, mu);
-        // (double)(sqrtf(2/3) * fmaxf((float)dl, 0)): float-rounded value, exact derivative; the
-        // smooth model keeps the increment in FP64
+        // (double)(sqrtf(2/3) * fmaxf((float)dl, 0)): float-rounded value, exact derivative
         const float s23f = sqrtf((float)(2.0 / 3.0));
-        const double inc_v = P.smooth ? sqrt(2.0 / 3.0) * fmax(dl.v, 0.) : (double)(s23f * fmaxf((float)dl.v, 0.f));
+        const double inc_v = (double)(s23f * fmaxf((float)dl.v, 0.f));
         const DN inc = dl.v > 0. ? dchain(inc_v, sqrt(2.0 / 3.0), dl) : dconst<ND>(inc_v);
         const DN eps_pl_new = eps_pl + inc;
         const DN eps_pl_dot_new = inc / dt;
@@ -538,8 +531,8 @@ int run_mean_force(mf_ctx *ctx, int device, params P, const dev_buffers &Dctx, i
   D.count = al.get<int>((size_t)G.max_cell);
   D.off = al.get<int>((size_t)G.max_cell + 1);
   const int scan_tiles = (G.max_cell + SCAN_TILE - 1) / SCAN_TILE + 1;
-  D.scan_status = al.get<unsigned long long>((size_t)scan_tiles);
-  D.scan_done = al.get<unsigned>(1);
+  D.tsum_r = al.get<int>((size_t)scan_tiles);
+  D.tsum_w = al.get<int>((size_t)scan_tiles);
   D.st = al.get<dev_status>(1);
   D.hash_cur = al.get<int>(N);
   D.hash_new = al.get<int>(N);
@@ -574,6 +567,7 @@ int run_mean_force(mf_ctx *ctx, int device, params P, const dev_buffers &Dctx, i
     k_t_posv<<<nb, 128>>>(N, TB);
     k_hash_count<<<hb, 128>>>(N, As, D, scan_tiles);
     k_scan<<<scan_tiles, SCAN_THREADS>>>(D, N, 0);
+    std::swap(D.tsum_r, D.tsum_w);  // the scan zeroed the other one for the next count
     k_scatter<<<(N + BLOCK - 1) / BLOCK, BLOCK>>>(N, D, 0);
     k_t_reorder<<<nb, 128>>>(P, D, TB);
     k_t_pair<<<nb, 128>>>(P, D, TB);

@@ -1,7 +1,10 @@
 """The batched form: several instances advanced by one graph launch (mf_batch_*).
 
 Each instance inside the batch runs exactly its own step sequence, so after any number of
-launches its state must equal, bit for bit, that of a separate context stepped as often.
+launches its state must equal, bit for bit, that of a separate context stepped as often: with
+the batched kernels (one launch per step phase for all instances; three perturbed reference
+scenes, and the 64-instance parameter sweep of uneven sizes) and with the child-graph batch
+that serves instances the batched kernels do not (neighbour lists).
 """
 import numpy as np
 import pytest
@@ -31,7 +34,7 @@ def test_batch_equals_separate_contexts(mf, precision):
     batched = [load_product(mf, st, precision=precision) for st in sts]
     single = [load_product(mf, st, precision=precision) for st in sts]
     b = mf.Batch(batched, steps_per_launch=4)
-    assert b.steps_per_launch == 4
+    assert b.steps_per_launch == 4 and b.fused
     b.step(3)
     for c in single:
         c.step(12)
@@ -59,6 +62,7 @@ def test_batch_autotune_and_graph_capture(mf):
     batched = [load_product(mf, st) for st in sts]
     b = mf.Batch(batched, steps_per_launch=0)
     assert b.steps_per_launch in (2, 4, 8, 16)
+    assert b.fused and b.pair_block in (64, 128, 256)
     b.close()
     # a captured graph: created and destroyed through the C ABI
     import ctypes as C
@@ -66,3 +70,55 @@ def test_batch_autotune_and_graph_capture(mf):
     assert mf.lib().mf_graph_capture(batched[0].h, 4, C.byref(g)) == 0 and g.value
     assert mf.lib().mf_graph_destroy(g) == 0
     assert mf.lib().mf_graph_capture(batched[0].h, 3, C.byref(g)) != 0  # odd: refused
+
+
+def sweep_contexts(mf, n, precision):
+    import bench
+
+    out = []
+    for p in bench.sweep_params(mf, n):
+        sc = mf.Scene.from_params(p)
+        c = mf.Context(0)
+        c.upload_scene(sc, mf.GRID_GREEN)
+        c.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, precision)
+        out.append(c)
+    return out
+
+
+def test_sweep_of_64_instances_equals_separate_contexts(mf):
+    """The batched parameter sweep (64 instances, 3k-45k particles, speeds, rakes, depths of
+    cut and JC A, B drawn per instance; mixed precision): after two launches of 4 steps with
+    a tuned pair block size, every instance equals its own context bit for bit."""
+    batched = sweep_contexts(mf, 64, mf.PRECISION_MIXED)
+    single = sweep_contexts(mf, 64, mf.PRECISION_MIXED)
+    sizes = [c.N for c in batched]
+    assert min(sizes) < 8000 and max(sizes) > 30000
+    b = mf.Batch(batched, steps_per_launch=0)
+    assert b.fused
+    steps0 = [c.status()["steps"] for c in batched]  # the tuning launches advanced the instances
+    for c, s0 in zip(single, steps0):
+        c.step(s0)
+    b.step(2)
+    for c in single:
+        c.step(2 * b.steps_per_launch)
+    for x, y in zip(batched, single):
+        assert x.status()["steps"] == y.status()["steps"]
+        assert_same(x, y)
+    b.close()
+    for c in batched + single:
+        c.close()
+
+
+def test_instances_on_neighbour_lists_take_the_child_graph_batch(mf):
+    sts = scenes(mf)
+    flags = mf.OPT_NEIGHBOUR_LISTS
+    batched = [load_product(mf, st, precision=1, flags=flags) for st in sts]
+    single = [load_product(mf, st, precision=1, flags=flags) for st in sts]
+    b = mf.Batch(batched, steps_per_launch=2)
+    assert not b.fused
+    b.step(3)
+    for c in single:
+        c.step(6)
+    for x, y in zip(batched, single):
+        assert_same(x, y)
+    b.close()

@@ -115,3 +115,50 @@ def test_unsupported_settings_are_rejected(mf):
     ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_TANH, mf.PRECISION_FP64)
     with pytest.raises(mf.MfError):
         ctx.tangent_mean_force(0, 5, 0)
+
+
+def config5_context(mf):
+    """Benchmark configuration 5: the cut at dx = 7.7 um (260 x 78 lattice + sampled tool
+    particles, 23,416), Brookshaw, thermal contact, plain FP64 forward."""
+    import bench
+
+    p = bench.cut_params(mf, nx=260, ny=78, dx=7.7e-4)
+    sc = mf.Scene.from_params(p)
+    ctx = mf.Context(0)
+    ctx.upload_scene(sc, mf.GRID_GREEN)
+    ctx.set_options(mf.THERMAL_BROOKSHAW, mf.JC_JOHNSON_COOK, mf.PRECISION_FP64)
+    return ctx
+
+
+def test_config5_gradient_while_elastic(mf):
+    """Configuration 5's scene over the steps before its first particle yields: the tool force
+    averaged over steps 1,000-2,000 (the tool in contact, friction acting) and its derivatives
+    with respect to JC A, B, n, C, m and mu in one six-direction pass. The Johnson-Cook
+    derivatives are zero, as their central differences are (no particle reaches the yield
+    surface); d/dmu agrees with the FP64 central difference at a relative step of 1e-4 within
+    1e-3 relative. (Over the configuration's own window, steps 3,001-5,000, where the chip
+    starts to yield, the central differences at relative steps 1e-3, 1e-4 and 1e-5 disagree
+    with each other for A, C and mu: the objective is not differentiable at those scales.)"""
+    ad = autodiff_module()
+    ctx = config5_context(mf)
+    theta0 = ad.current_parameters(ctx)
+    skip, window = 1000, 1000
+    mean, d6 = ctx.tangent_mean_force_all(skip, window)
+    assert mean[0] != 0.0
+    fds = []
+    for k in range(6):
+        h = 1e-4 * abs(theta0[k])
+        th = list(theta0)
+        th[k] += h
+        ad.apply_parameters(ctx, th)
+        fp, _ = ctx.tangent_mean_force(skip, window, -1)
+        th[k] -= 2 * h
+        ad.apply_parameters(ctx, th)
+        fm, _ = ctx.tangent_mean_force(skip, window, -1)
+        ad.apply_parameters(ctx, theta0)
+        fds.append((fp - fm) / (2 * h))
+    for k in range(5):  # A, B, n, C, m
+        assert np.all(d6[k] == 0.0) and np.all(fds[k] == 0.0), ad.PARAMS[k]
+    rel = np.abs(d6[5] - fds[5]) / np.abs(fds[5])
+    assert np.all(rel <= 1e-3), (d6[5], fds[5], rel)
+    ctx.close()
