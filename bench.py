@@ -36,7 +36,7 @@ METRIC = "particle-steps/s at ~150k particles w/ thermal contact: mixed vs FP64,
 ALGO_BYTES_PER_PARTICLE_STEP = 480.0
 # ncu summary of the pair kernel on this workload; its "dram bytes per launch" line is the
 # roofline's measured traffic
-PAIR_PROFILE = "profiles/k_pair_mixed_cut714x214.txt"
+PAIR_PROFILE = "profiles/k_pair_mixed_list_cut714x214.txt"  # the headline form's pair kernel
 FLUSH_BYTES = 256 << 20
 
 
@@ -255,7 +255,7 @@ E2E_FIELDS = ("pos", "vel", "h", "rho", "T", "fixed", "blanked", "tool_p", "S", 
               "n", "pos_t", "vel_t", "rho_t", "S_t", "T_t")
 
 
-def e2e_form(mf, torch, scene, precision, steps, device):
+def e2e_form(mf, torch, scene, precision, steps, device, flags=0):
     """End to end through the C ABI with host buffers. Outside the timed region: context,
     device buffers and the step graphs (created once per run). Inside: the complete particle
     state copied in from pinned host memory (mf_set_field, all per-particle fields, in one
@@ -265,6 +265,7 @@ def e2e_form(mf, torch, scene, precision, steps, device):
     ctx.upload_scene(scene, mf.GRID_GREEN)
     ctx.set_options(SOLVER["thermal"], mf.JC_JOHNSON_COOK, precision)
     ctx.set_neighbour_skin(SOLVER["skin"])
+    ctx.set_flags(flags)
     ctx.step(2)  # builds the graphs
     ctx.synchronize()
     n = scene.N
@@ -323,7 +324,7 @@ def load_state(mf, ctx, path):
 
 
 def run_form(mf, scene, precision, steps, device, torch=None, state_out=None, flags=0, list_check_every=0,
-             list_check_late=(0, 0)):
+             list_check_late=(0, 0), stop_on_nonfinite=False):
     """`steps` steps of one form from the scene's initial state. Returns the per-step tool
     force (steps x 2), the end state ordered by particle number, the device time (s) and the
     status. With neighbour lists (flags) and list_check_every > 0, the lists are checked by brute
@@ -336,7 +337,7 @@ def run_form(mf, scene, precision, steps, device, torch=None, state_out=None, fl
     ctx.set_neighbour_skin(SOLVER["skin"])
     ctx.set_flags(flags)
     checking = list_check_every > 0 and bool(flags & mf.OPT_NEIGHBOUR_LISTS)
-    checks = []
+    checks, timeline = [], []
     forces, left, secs = [], steps, 0.0
     chunk = 50_000  # below the device force log's 65,536 entries
     if checking:
@@ -361,14 +362,21 @@ def run_form(mf, scene, precision, steps, device, torch=None, state_out=None, fl
             ctx.step(n)
         forces.append(ctx.force_log())
         left -= n
+        st = ctx.status()
+        if not timeline or st["blanked"] != timeline[-1][1] or st["secant_cap_hits"] != timeline[-1][2]:
+            timeline.append((steps - left, int(st["blanked"]), int(st["secant_cap_hits"])))
+        if stop_on_nonfinite and not np.isfinite(forces[-1]).all():
+            break
         if checking:
             c = ctx.list_check()
             st = ctx.status()
             checks.append({"steps": steps - left, "pairs": c["pairs"], "missing": c["missing"], "stale": c["stale"],
                            "blanked": st["blanked"], "sorts": st["sorts"], "secant_cap_hits": st["secant_cap_hits"]})
     order = np.argsort(ctx.get("id"))
-    state = {k: ctx.get(k)[order] for k in ("S", "p", "eps_pl", "T", "tool_p", "blanked")}
+    state = {k: ctx.get(k)[order] for k in ("S", "p", "eps_pl", "T", "tool_p", "blanked", "pos")}
     status = ctx.status()
+    # (steps done, blanked, capped secant solves) where either changed: when a run went wrong
+    status["timeline"] = timeline
     if checking:
         valid = [c for c in checks if not c["stale"]]
         bad = [c["steps"] for c in valid if c["missing"] > 0]
@@ -388,26 +396,60 @@ def von_mises(S, p):
                               + 3.0 * cxy * cxy, 0.0))
 
 
+def finite_prefix(forces):
+    """Steps before the first step whose tool force is not finite (all steps if none)."""
+    bad = np.flatnonzero(~np.isfinite(forces).all(axis=1))
+    return int(bad[0]) if bad.size else len(forces)
+
+
+def chip_summary(scene, st):
+    """Peak temperature rise over the workpiece and plastic strain of the chip (workpiece
+    particles above the initial uncut surface), blanked particles left out."""
+    y_top = scene.array("pos")[scene.array("tool_p") == 0.0, 1].max()
+    wp = (st["tool_p"] == 0.0) & (st["blanked"] == 0.0)
+    chip = wp & (st["pos"][:, 1] > y_top)
+    T0 = scene.s.trml_wp.T_init
+    return {"dT_peak": float(st["T"][wp].max() - T0),
+            "eps_chip_max": float(st["eps_pl"][chip].max()) if chip.any() else 0.0,
+            "eps_chip_mean": float(st["eps_pl"][chip].mean()) if chip.any() else 0.0,
+            "n_chip": int(chip.sum())}
+
+
 def form_errors(scene, ref, test):
-    """Mixed (test) against FP64 (ref): relative error of the mean tool force over the run and
-    relative L2 errors of the end fields over the workpiece particles blanked in neither."""
+    """Mixed (test) against FP64 (ref): relative error of the mean tool force over the steps
+    both forms' forces are finite (all of them in a clean run), of the peak temperature rise and
+    the chip's plastic strain, and relative L2 errors of the end fields over the workpiece
+    particles blanked in neither."""
     (f64, s64), (fm, sm) = ref, test
+    n = min(finite_prefix(f64), finite_prefix(fm))
     mask = (s64["tool_p"] == 0.0) & (s64["blanked"] == 0.0) & (sm["blanked"] == 0.0)
+    c64, cm = chip_summary(scene, s64), chip_summary(scene, sm)
+
+    def rel(a, b):
+        return abs(a - b) / abs(b) if b else None
 
     def rel_l2(a, b):
         den = float(np.linalg.norm(b))
         return float(np.linalg.norm(a - b)) / den if den > 0 else float(np.linalg.norm(a - b))
 
     T0 = scene.s.trml_wp.T_init
-    mean64, meanm = f64.mean(axis=0), fm.mean(axis=0)
+    mean64, meanm = f64[:n].mean(axis=0), fm[:n].mean(axis=0)
     return {
+        "force_steps": n,
+        "first_nonfinite_force_step": {"fp64": finite_prefix(f64) if finite_prefix(f64) < len(f64) else None,
+                                       "test": finite_prefix(fm) if finite_prefix(fm) < len(fm) else None},
         "mean_fc": [float(meanm[0]), float(mean64[0])],
+        "mean_ff": [float(meanm[1]), float(mean64[1])],
         "mean_fc_rel_err": abs(float(meanm[0] - mean64[0])) / abs(float(mean64[0])) if mean64[0] else None,
         "mean_ff_rel_err": abs(float(meanm[1] - mean64[1])) / abs(float(mean64[1])) if mean64[1] else None,
         "von_mises_rel_l2": rel_l2(von_mises(sm["S"], sm["p"])[mask], von_mises(s64["S"], s64["p"])[mask]),
         "eps_pl_rel_l2": rel_l2(sm["eps_pl"][mask], s64["eps_pl"][mask]),
         "T_rise_rel_l2": rel_l2(sm["T"][mask] - T0, s64["T"][mask] - T0),
         "blanked": [int((sm["blanked"] != 0).sum()), int((s64["blanked"] != 0).sum())],
+        "chip": {"test": cm, "fp64": c64},
+        "dT_peak_rel_err": rel(cm["dT_peak"], c64["dT_peak"]),
+        "eps_chip_max_rel_err": rel(cm["eps_chip_max"], c64["eps_chip_max"]),
+        "eps_chip_mean_rel_err": rel(cm["eps_chip_mean"], c64["eps_chip_mean"]),
     }
 
 
@@ -416,10 +458,11 @@ def steps_per_mm(scene, params):
     return 0.1 / (params.speed * scene.s.dt)
 
 
-def accuracy(mf, scene, params, steps, device):
-    """Mixed against FP64 over the first `steps` steps of the cut, both from the same state."""
+def accuracy(mf, scene, params, steps, device, flags=0):
+    """Mixed (with option flags) against FP64 over the first `steps` steps of the cut, both from
+    the same state."""
     f64, s64, _, _ = run_form(mf, scene, mf.PRECISION_FP64, steps, device)
-    fm, sm, _, stm = run_form(mf, scene, mf.PRECISION_MIXED, steps, device)
+    fm, sm, _, stm = run_form(mf, scene, mf.PRECISION_MIXED, steps, device, flags=flags)
     out = {"steps": steps, "tool_travel_um": steps * scene.s.dt * params.speed * 1e4,
            "against": "the FP64 form (single steps equal to the oracle to 1e-12) from the same initial state",
            "mixed_sorts": int(stm["sorts"]), "mixed_error_flags": int(stm["error_flags"])}
@@ -427,34 +470,135 @@ def accuracy(mf, scene, params, steps, device):
     return out
 
 
-def cut_run(mf, torch, scene, params, mm, device, state_out=None, lists=False, list_check_every=0,
-            list_check_late=(0.0, 0)):
-    """`mm` millimetres of cut in each form: device wall time per mm and the mixed form's errors
-    (and, with state_out, the FP64 form's end state saved for --state-in). With `lists` the
-    mixed form on neighbour lists (fused predictor) runs too, its lists checked every
-    list_check_every steps when that is > 0."""
+# the forms by name: precision and option flags. "mixed" (the headline): FP32 pair sums on
+# neighbour lists kept between cell-list sorts; "mixed_sorted": the same sums with the cell list
+# sorted every step, as the FP64 form does; "mixed_lists_fused": lists with the next step's
+# predictor run in the finish kernel (measured slower; profiling only)
+FORMS = {"fp64": ("PRECISION_FP64", ()), "mixed": ("PRECISION_MIXED", ("OPT_NEIGHBOUR_LISTS",)),
+         "mixed_sorted": ("PRECISION_MIXED", ("OPT_SORT_EVERY_STEP",)),
+         "mixed_lists_fused": ("PRECISION_MIXED", ("OPT_NEIGHBOUR_LISTS", "OPT_FUSED_PREDICTOR"))}
+HEADLINE_FORMS = ("fp64", "mixed", "mixed_sorted")
+CUT_FORMS = FORMS
+
+
+def form_flags(mf, name):
+    flags = 0
+    for f in FORMS[name][1]:
+        flags |= getattr(mf, f)
+    return getattr(mf, FORMS[name][0]), flags
+
+
+def cut_together(mf, scene, params, mm, forms, device, out_dir, list_check_every=0, list_check_late=(0.0, 0),
+                 state_out=None):
+    """`mm` millimetres of cut in several forms at once, one context per form on its own
+    stream, their steps launched in turns of 500 so that the forms' latency-bound kernels
+    share the GPU (no per-form device time then); each form's run saved as cut_<form>.npz in
+    out_dir (cut_compare reads them). A form whose tool force stops being finite is stopped
+    at the end of that chunk; list checks as in run_form. With state_out, the FP64 form's end
+    state is saved there (for --state-in)."""
     steps = int(round(mm * steps_per_mm(scene, params)))
     late = (int(round(list_check_late[0] * steps_per_mm(scene, params))), int(list_check_late[1]))
-    f64, s64, t64, st64 = run_form(mf, scene, mf.PRECISION_FP64, steps, device, torch, state_out=state_out)
-    fm, sm, tm, stm = run_form(mf, scene, mf.PRECISION_MIXED, steps, device, torch)
-    lists_out = None
-    if lists:
-        fl, sl, tl, stl = run_form(mf, scene, mf.PRECISION_MIXED, steps, device, torch,
-                                   flags=mf.OPT_NEIGHBOUR_LISTS | mf.OPT_FUSED_PREDICTOR,
-                                   list_check_every=list_check_every, list_check_late=late)
-        lists_out = {"wall_s_per_mm": tl / mm, "particle_steps_per_s": scene.N * steps / tl, "status": stl,
-                     "errors": form_errors(scene, (f64, s64), (fl, sl)),
-                     "mean_force_second_half": fl[steps // 2:].mean(axis=0).tolist()}
-    out = {"mode": "cut", "mm": mm, "steps": steps, "n_particles": scene.N,
-           "wall_s_per_mm": {"fp64": t64 / mm, "mixed": tm / mm},
-           "particle_steps_per_s": {"fp64": scene.N * steps / t64, "mixed": scene.N * steps / tm},
-           "status": {"fp64": st64, "mixed": stm}}
-    out.update(form_errors(scene, (f64, s64), (fm, sm)))
-    # time-averaged force over the second half of the run (past the entry transient)
-    h = steps // 2
-    out["mean_force_second_half"] = {"fp64": f64[h:].mean(axis=0).tolist(), "mixed": fm[h:].mean(axis=0).tolist()}
-    if lists_out is not None:
-        out["mixed_lists"] = lists_out
+    runs = {}
+    for form in forms:
+        prec, flags = form_flags(mf, form)
+        ctx = mf.Context(device)
+        ctx.upload_scene(scene, mf.GRID_GREEN)
+        ctx.set_options(SOLVER["thermal"], mf.JC_JOHNSON_COOK, prec)
+        ctx.set_neighbour_skin(SOLVER["skin"])
+        ctx.set_flags(flags)
+        runs[form] = {"ctx": ctx, "forces": [], "timeline": [], "checks": [], "done": 0, "stopped": False,
+                      "checking": list_check_every > 0 and bool(flags & mf.OPT_NEIGHBOUR_LISTS)}
+    chunk = 20_000  # below the device force log's 65,536 entries
+    if list_check_every > 0:
+        chunk = min(chunk, list_check_every)
+    t0 = time.time()
+    while any(not r["stopped"] and r["done"] < steps for r in runs.values()):
+        n = min(chunk, steps - min(r["done"] for r in runs.values() if not r["stopped"] and r["done"] < steps))
+        if late[1] > 0:
+            d = min(r["done"] for r in runs.values() if not r["stopped"] and r["done"] < steps)
+            if d >= late[0]:
+                n = min(n, late[1])
+            elif d + n > late[0]:
+                n = late[0] - d
+        active = [r for r in runs.values() if not r["stopped"] and r["done"] < steps]
+        for k0 in range(0, n, 500):
+            for r in active:
+                r["ctx"].step(min(500, n - k0))
+        for r in active:
+            ctx = r["ctx"]
+            r["forces"].append(ctx.force_log())
+            r["done"] += n
+            st = ctx.status()
+            tl = r["timeline"]
+            if not tl or st["blanked"] != tl[-1][1] or st["secant_cap_hits"] != tl[-1][2]:
+                tl.append((r["done"], int(st["blanked"]), int(st["secant_cap_hits"])))
+            if r["checking"]:
+                c = ctx.list_check()
+                r["checks"].append({"steps": r["done"], "pairs": c["pairs"], "missing": c["missing"],
+                                    "stale": c["stale"], "blanked": st["blanked"], "sorts": st["sorts"]})
+            if not np.isfinite(r["forces"][-1]).all():
+                r["stopped"] = True
+    wall = time.time() - t0
+    out = {}
+    for form, r in runs.items():
+        ctx = r["ctx"]
+        if state_out and form == "fp64":
+            save_state(mf, ctx, state_out, r["done"])
+        order = np.argsort(ctx.get("id"))
+        st = {k: ctx.get(k)[order] for k in ("S", "p", "eps_pl", "T", "tool_p", "blanked", "pos")}
+        status = ctx.status()
+        status["timeline"] = r["timeline"]
+        if r["checking"]:
+            valid = [c for c in r["checks"] if not c["stale"]]
+            bad = [c["steps"] for c in valid if c["missing"] > 0]
+            status["list_checks"] = {"every": list_check_every, "checked": len(valid),
+                                     "missing_total": int(sum(c["missing"] for c in valid)),
+                                     "first_step_missing": bad[0] if bad else None}
+        ctx.close()
+        f = np.concatenate(r["forces"])
+        path = Path(out_dir) / f"cut_{form}.npz"
+        np.savez(path, forces=f, secs=np.array([np.nan]), status=np.array([json.dumps(status)]),
+                 steps_planned=np.array([steps]), **{"state_" + k: v for k, v in st.items()})
+        out[form] = str(path)
+    return out, wall
+
+
+def cut_compare(mf, scene, paths):
+    """Errors between the saved runs of cut_one: every form against the FP64 form (over the
+    steps both forces are finite; end fields only where both runs reached the planned end)
+    and the list forms against the sorted mixed form."""
+    runs = {}
+    for p in paths:
+        d = np.load(p)
+        st = {k[6:]: d[k] for k in d.files if k.startswith("state_")}
+        status = json.loads(str(d["status"][0]))
+        runs[Path(p).stem.replace("cut_", "")] = (d["forces"], st, float(d["secs"][0]), status,
+                                                 int(d["steps_planned"][0]))
+    out = {"forms": {}}
+    for name, (f, st, secs, status, planned) in runs.items():
+        lc = status.get("list_checks")
+        out["forms"][name] = {"steps": int(len(f)), "steps_planned": planned, "completed": len(f) == planned,
+                              "first_nonfinite_force_step": finite_prefix(f) if finite_prefix(f) < len(f) else None,
+                              "mean_force": f[:finite_prefix(f)].mean(axis=0).tolist(),
+                              "device_s": secs, "blanked": int(status["blanked"]),
+                              "secant_cap_hits": int(status["secant_cap_hits"]), "sorts": int(status["sorts"]),
+                              "timeline": status.get("timeline"), "chip": chip_summary(scene, st),
+                              "list_checks": None if lc is None else {k: v for k, v in lc.items() if k != "log"}}
+
+    def errs(ref, test):
+        (fr, sr, _, _, pr), (ft, stt, _, _, pt) = runs[ref], runs[test]
+        e = form_errors(scene, (fr, sr), (ft, stt))
+        if not (len(fr) == pr and len(ft) == pt):  # a run stopped early: its end state is not the same instant
+            for k in ("von_mises_rel_l2", "eps_pl_rel_l2", "T_rise_rel_l2", "chip", "dT_peak_rel_err",
+                      "eps_chip_max_rel_err", "eps_chip_mean_rel_err"):
+                e[k] = None
+        return e
+
+    for name in runs:
+        if name != "fp64" and "fp64" in runs:
+            out["forms"][name]["errors_against_fp64"] = errs("fp64", name)
+        if name != "mixed_sorted" and name != "fp64" and "mixed_sorted" in runs:
+            out["forms"][name]["errors_against_mixed_sorted"] = errs("mixed_sorted", name)
     return out
 
 
@@ -726,7 +870,7 @@ def profiled_traffic(path, n_particles):
         return None
     for line in text.splitlines():
         if line.startswith("dram bytes per launch (read + write):"):
-            return float(line.split(":", 1)[1])
+            return float(line.split(":", 1)[1].split()[0])
     return None
 
 
@@ -745,15 +889,17 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=20_000,
                     help="steps of the mixed-against-FP64 error report (0: off)")
     ap.add_argument("--cut-mm", type=float, default=0.0,
-                    help="instead of the benchmark: run this many mm of cut in both forms and report "
-                         "wall time per mm and the mixed form's errors")
-    ap.add_argument("--cut-lists", action="store_true",
-                    help="with --cut-mm: also run the mixed form on neighbour lists (fused predictor)")
+                    help="instead of the benchmark: run this many mm of cut in the --cut-forms (together on the "
+                         "GPU, one context and stream each) and report each form's errors against the FP64 form")
+    ap.add_argument("--cut-forms", default="fp64,mixed,mixed_sorted")
     ap.add_argument("--list-check-every", type=int, default=0,
-                    help="with --cut-lists: check the neighbour lists by brute force (mf_list_check) every "
+                    help="with --cut-mm: check the list forms' neighbour lists by brute force (mf_list_check) every "
                          "this many steps (0: never)")
     ap.add_argument("--list-check-late", default="0,0",
                     help="with --list-check-every: 'MM,STEPS' = from MM mm of cut on, check every STEPS steps")
+    ap.add_argument("--cut-dir", default="/tmp", help="with --cut-mm: where each form's run is saved (.npz)")
+    ap.add_argument("--cut-compare", nargs="+", default=None,
+                    help="instead of the benchmark: errors between runs saved by --cut-mm (cut_<form>.npz)")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"],
                     help="c2 (default): the ~150k-particle cut with thermal contact, the benchmark; "
                          "c1: the ~6k adiabatic cut; c3: the ~500k cut with the PSE solver")
@@ -768,7 +914,7 @@ def main():
     ap.add_argument("--skin", type=float, default=0.0,
                     help="neighbour-list skin of the mixed form as a fraction of the cell size (0: the "
                          "library's default, a tenth)")
-    ap.add_argument("--forms", default="fp64,mixed,mixed_lists",
+    ap.add_argument("--forms", default=",".join(HEADLINE_FORMS),
                     help="comma-separated forms to time (all three for the benchmark line; one, e.g. "
                          "'mixed', for a profiling run)")
     ap.add_argument("--lattice-scale", type=float, default=1.0,
@@ -804,12 +950,19 @@ def main():
             torch.distributed.barrier()
             torch.distributed.destroy_process_group()
         return 0
+    if args.cut_compare:
+        print(json.dumps(cut_compare(mf, scene, args.cut_compare)), flush=True)
+        return 0
     if args.cut_mm > 0:
         if rank == 0:
             lmm, lst = args.list_check_late.split(",")
-            print(json.dumps(cut_run(mf, torch, scene, params, args.cut_mm, device, args.state_out,
-                                     lists=args.cut_lists, list_check_every=args.list_check_every,
-                                     list_check_late=(float(lmm), int(lst)))), flush=True)
+            paths, wall = cut_together(mf, scene, params, args.cut_mm, args.cut_forms.split(","), device,
+                                       args.cut_dir, list_check_every=args.list_check_every,
+                                       list_check_late=(float(lmm), int(lst)), state_out=args.state_out)
+            res = cut_compare(mf, scene, list(paths.values()))
+            res.update({"mode": "cut", "mm": args.cut_mm, "wall_s_all_forms": wall, "n_particles": N,
+                        "steps_per_mm": steps_per_mm(scene, params)})
+            print(json.dumps(res), flush=True)
         if world > 1:
             torch.distributed.barrier()
             torch.distributed.destroy_process_group()
@@ -817,9 +970,7 @@ def main():
 
     results = {}
     clocks = None
-    forms = [f for f in (("fp64", mf.PRECISION_FP64, 0), ("mixed", mf.PRECISION_MIXED, 0),
-                         ("mixed_lists", mf.PRECISION_MIXED, mf.OPT_NEIGHBOUR_LISTS | mf.OPT_FUSED_PREDICTOR))
-             if f[0] in args.forms.split(",")]
+    forms = [(name,) + form_flags(mf, name) for name in FORMS if name in args.forms.split(",")]
     for name, prec, flags in forms:
         if world > 1:
             torch.distributed.barrier()
@@ -832,7 +983,7 @@ def main():
         total_ms = max_over_ranks(float(step_ms.sum()), world, device=f"cuda:{device}")
         results[name] = {"ms_per_step": total_ms / args.steps, "pair_kernel_ms": float(np.median(pair_ms)),
                          "status": st, **extra}
-    if set(results) != {"fp64", "mixed", "mixed_lists"}:  # a profiling run: no benchmark line
+    if set(results) != set(HEADLINE_FORMS):  # a profiling run: no benchmark line
         if rank == 0:
             print(json.dumps({"forms": {f: {k: v for k, v in r.items() if k != "status"}
                                         for f, r in results.items()}}), flush=True)
@@ -841,13 +992,15 @@ def main():
         return 0
     acc = None
     if rank == 0 and args.accuracy_steps > 0:
-        acc = accuracy(mf, scene, params, args.accuracy_steps, device)
+        acc = accuracy(mf, scene, params, args.accuracy_steps, device, flags=form_flags(mf, "mixed")[1])
     # neighbour lists: the timed steps may hold fewer sorts than a run; charge each step its
     # share of a sorting step's extra time, at the context's steps per sort
-    ml = results["mixed_lists"]
-    ml["timed_ms_per_step"] = ml["ms_per_step"]
-    if ml["sorts_in_timed_steps"] < args.steps:  # (without lists, e.g. PSE, every timed step sorted)
-        ml["ms_per_step"] += max(0.0, ml["sort_step_ms"] - ml["timed_ms_per_step"]) / ml["steps_per_sort"]
+    for ml in results.values():
+        if "sort_step_ms" not in ml:
+            continue
+        ml["timed_ms_per_step"] = ml["ms_per_step"]
+        if ml["sorts_in_timed_steps"] < args.steps:  # (without lists, e.g. PSE, every timed step sorted)
+            ml["ms_per_step"] += max(0.0, ml["sort_step_ms"] - ml["timed_ms_per_step"]) / ml["steps_per_sort"]
     particles = sum_over_ranks(float(N), world, device=f"cuda:{device}")
     for name, r in results.items():
         r["value"] = particles / (r["ms_per_step"] * 1e-3)
@@ -870,7 +1023,8 @@ def main():
     e2e = e2e_fp64 = None
     if rank == 0:
         for prec in (mf.PRECISION_MIXED, mf.PRECISION_FP64):
-            secs, h2d, d2h, finite = e2e_form(mf, torch, scene, prec, args.e2e_steps, device)
+            flags = form_flags(mf, "mixed")[1] if prec == mf.PRECISION_MIXED else 0
+            secs, h2d, d2h, finite = e2e_form(mf, torch, scene, prec, args.e2e_steps, device, flags)
             if not finite:
                 raise SystemExit("e2e: non-finite tool force in the end-to-end run")
             line_e2e = {"value": N * args.e2e_steps / secs, "unit": "particle-steps/s",
@@ -909,20 +1063,21 @@ def main():
                            n_tool=scene.s.n_tool,
                            start_state=(f"saved state {args.state_in}" if args.state_in else "initial scene"),
                            parallelism=f"replicas x{world}", l2="flushed between timed steps (256 MiB write)",
+                           mixed_form="FP32 pair sums on neighbour lists (MF_OPT_NEIGHBOUR_LISTS), the cell list "
+                                      "sorted when a particle moved 0.45 skin from its list's build position",
                            global_particles=N * world),
             "forms": dict(
                 {f: {k: v for k, v in r.items() if k != "status"} for f, r in results.items()},
                 mixed_over_fp64=results["mixed"]["value"] / results["fp64"]["value"],
                 mixed_over_fp64_back_to_back=(results["fp64"]["back_to_back_ms_per_step"]
                                               / results["mixed"]["back_to_back_ms_per_step"]),
-                mixed_lists_over_fp64=results["mixed_lists"]["value"] / results["fp64"]["value"],
+                mixed_sorted_over_fp64=results["mixed_sorted"]["value"] / results["fp64"]["value"],
                 wall_s_per_mm_cut={f: r["ms_per_step"] * 1e-3 * spm for f, r in results.items()},
                 steps_per_mm_cut=spm,
-                note="mixed (the headline): FP32 pair sums, the cell list sorted every step as in the FP64 "
-                     "form; mixed_lists: the same sums on neighbour lists kept between sorts, with the fused "
-                     "predictor (experimental: it "
-                     "failed a 1 mm cut; ms_per_step = timed steps + each step's share of a sorting step's extra "
-                     "time at steps_per_sort); pair_kernel_ms: median "
+                note="mixed (the headline): FP32 pair sums on neighbour lists kept between cell-list sorts "
+                     "(MF_OPT_NEIGHBOUR_LISTS; ms_per_step = timed steps + each step's share of a sorting step's "
+                     "extra time at steps_per_sort); mixed_sorted: the same sums with the cell list sorted every "
+                     "step, as in the FP64 form; pair_kernel_ms: median "
                      "of steps launched kernel by kernel (mf_step_timed) after an L2 flush; "
                      "back_to_back_ms_per_step: the same number of steps without flushes, one event pair "
                      "(reported beside the flushed headline)"),
@@ -930,7 +1085,8 @@ def main():
             "fp64_probe": fp64_probe,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                         "kernel": "k_pair_mixed", "algorithmic_bytes_per_particle": ALGO_BYTES_PER_PARTICLE_STEP,
+                         "kernel": "k_pair_mixed<true> (neighbour lists)",
+                         "algorithmic_bytes_per_particle": ALGO_BYTES_PER_PARTICLE_STEP,
                          "step_achieved": step_achieved, "step_frac": step_achieved / peak},
             "gpu_launches": kernels_per_step(mf, mf.PRECISION_MIXED) * args.steps,
             "clocks": clocks,

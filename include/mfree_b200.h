@@ -120,9 +120,11 @@ typedef struct {
   long long secant_cap_hits;  /* JC secant solves that hit the iteration cap */
   int max_cell_occupancy;     /* largest particles-per-cell seen in the last sort */
   int error_flags;            /* bit 1: the adaptive grid outgrew max_cell; bit 2: a neighbour
-                                 list was full (neighbours dropped); bit 0 (a bounded wait in
-                                 the cell scan expired) is no longer raised: the scan waits
-                                 for nothing */
+                                 list was full (neighbours dropped); bit 3: a block of the
+                                 pair kernel did not receive its staged candidates in time
+                                 (its particles' rates of that step were not written); bit 0
+                                 (a bounded wait in the cell scan expired) is no longer
+                                 raised: the scan waits for nothing */
   long long secant_iterations; /* JC secant iterations since creation (cost diagnostic) */
   long long sorts;            /* cell-list sorts since creation (one per step, except for the
                                  mixed form with neighbour lists) */

@@ -277,11 +277,11 @@ void set_list_mode(mf_ctx *ctx) {
 // drains (programmatic dependent launch); the kernel waits for its predecessor before it
 // touches memory (MF_PDL_WAIT)
 template <typename... KArgs, typename... Args>
-int launch_pdl(mf_ctx *ctx, void (*kernel)(KArgs...), int grid, int block, Args... args) {
+int launch_pdl_smem(mf_ctx *ctx, void (*kernel)(KArgs...), int grid, int block, size_t smem, Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid);
   cfg.blockDim = dim3((unsigned)block);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = ctx->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -294,6 +294,11 @@ int launch_pdl(mf_ctx *ctx, void (*kernel)(KArgs...), int grid, int block, Args.
     return MF_ERR_CUDA;
   }
   return MF_OK;
+}
+
+template <typename... KArgs, typename... Args>
+int launch_pdl(mf_ctx *ctx, void (*kernel)(KArgs...), int grid, int block, Args... args) {
+  return launch_pdl_smem(ctx, kernel, grid, block, 0, args...);
 }
 
 // cell-list build into the other buffer (k_hash_count .. k_reorder); PREDICT adds the
@@ -312,6 +317,17 @@ int launch_cells(mf_ctx *ctx, bool step_mode) {
   TRY(launch_pdl(ctx, k_scan, ctx->scan_tiles, SCAN_THREADS, ctx->D, N, verlet));
   TRY(launch_pdl(ctx, k_scatter, nb, BLOCK, N, ctx->D, verlet));
   return MF_OK;
+}
+
+#ifndef MF_PAIR_STAGED
+#define MF_PAIR_STAGED 0
+#endif
+// grid of the mixed pair kernels: npb blocks, or with SM-major placement the next multiple of
+// the SM count (the blocks past the last particle return at once)
+int pair_grid(const mf_ctx *ctx, int npb) {
+  if (!MF_PAIR_SM_MAJOR) return npb;
+  const int s = ctx->sm_count;
+  return (npb + s - 1) / s * s;
 }
 
 int launch_stage(mf_ctx *ctx, int stage) {
@@ -333,8 +349,10 @@ int launch_stage(mf_ctx *ctx, int stage) {
       else TRY(launch_pdl(ctx, k_reorder<true, false>, nb, BLOCK, ctx->P, ctx->D));
       break;
     case 2:
-      if (mixed && ctx->P.verlet) TRY(launch_pdl(ctx, k_pair_mixed<true>, npb, PAIR_BLOCK, ctx->P, ctx->D));
-      else if (mixed) TRY(launch_pdl(ctx, k_pair_mixed<false>, npb, PAIR_BLOCK, ctx->P, ctx->D));
+      if (mixed && ctx->P.verlet) TRY(launch_pdl(ctx, k_pair_mixed<true>, pair_grid(ctx, npb), PAIR_BLOCK, ctx->P, ctx->D));
+      else if (mixed && MF_PAIR_STAGED)
+        TRY(launch_pdl_smem(ctx, k_pair_mixed_staged, pair_grid(ctx, npb), PAIR_BLOCK, (size_t)STAGE_BYTES, ctx->P, ctx->D));
+      else if (mixed) TRY(launch_pdl(ctx, k_pair_mixed<false>, pair_grid(ctx, npb), PAIR_BLOCK, ctx->P, ctx->D));
       else TRY(launch_pdl(ctx, k_pair_fp64, npb, PAIR_BLOCK, ctx->P, ctx->D));
       if (ctx->P.thermal_solver == MF_THERMAL_PSE && ctx->P.thermal_wp) {
         if (mixed) TRY(launch_pdl(ctx, k_pse_mixed, npb, PAIR_BLOCK, ctx->P, ctx->D));
@@ -509,6 +527,11 @@ int mf_ctx_create(int device, mf_ctx **out) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
       ctx->sm_count = sms;
+    ctx->P.sm_count = ctx->sm_count;
+    if (MF_PAIR_STAGED &&
+        cudaFuncSetAttribute(k_pair_mixed_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_BYTES) !=
+            cudaSuccess)
+      rc = MF_ERR_CUDA;
   }
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.ticket, 4);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.force_log, (size_t)FORCE_LOG_CAP * 2);

@@ -42,6 +42,7 @@ struct params {
   int precision;
   int plastic, fric_heat, thermal_bc, thermal_wp, thermal_tool_on, has_tool, keep_derivs;
   int staged;  // step run stage by stage (mf_step_stage): keep every intermediate array
+  int sm_count;  // SMs of the device (block placement of the pair kernels)
   int jc_lower_bound;  // A > 0, B >= 0, C >= 0: the yield stress is bounded below by A (1 - theta^m)
   // mixed form with neighbour lists: the cell list is sorted only on steps where some
   // particle's predicted position is more than 0.45 skin from where its list was built; in
@@ -90,6 +91,7 @@ constexpr int FORCE_LOG_CAP = 1 << 16;
 constexpr int ERR_SCAN_WAIT = 1;  // (no longer raised: the cell scan has no bounded waits)
 constexpr int ERR_GRID_BUDGET = 2;
 constexpr int ERR_LIST_OVERFLOW = 4;  // a neighbour list was full: neighbours were dropped
+constexpr int ERR_STAGE_WAIT = 8;     // a pair block's staged candidate copies did not complete in time
 
 // neighbour list entry: particle index in the low LIST_INDEX_BITS bits, above them the
 // column offset of the pair's cells (i's column - j's column) + 3, in [0, 6]

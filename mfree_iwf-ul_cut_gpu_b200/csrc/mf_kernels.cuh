@@ -482,8 +482,49 @@ __device__ __forceinline__ void predict_particle(const params &P, const dev_buff
   }
 }
 
+// The rigid tool of this step: tool::update_tool (tool.cpp:211-221) with IEEE-rounded
+// operations (bitwise equal to the host's double arithmetic), by warp 0 of block 0 of the
+// step's reorder/predictor kernel: tool_prev copied to tool_next word by word, then lane
+// k < num_seg moves segment k and lane 5 the fillet. The finish kernel, which runs later in the
+// step, reads tool_next; computing it there keeps this division chain out of every finish
+// block's start. (A function of its own, not inlined, so that it adds no registers to the
+// kernel that calls it.)
+static __device__ __noinline__ void tool_advance_warp(const mf_tool_state *prev, mf_tool_state *next, double dt) {
+  static_assert(sizeof(mf_tool_state) % sizeof(double) == 0, "tool state is a whole number of doubles");
+  constexpr int WORDS = (int)(sizeof(mf_tool_state) / sizeof(double));
+  const int l = (int)lane_id();
+  const double *src = reinterpret_cast<const double *>(prev);
+  double *dst = reinterpret_cast<double *>(next);
+  for (int w = l; w < WORDS; w += 32) dst[w] = src[w];
+  __syncwarp();  // the copy's stores before the lanes' own below
+  const mf_tool_state &T0 = *prev;
+  const double sx = __dmul_rn(dt, T0.vel[0]), sy = __dmul_rn(dt, T0.vel[1]);
+  if (l < T0.num_seg) {
+    mf_segment s = T0.seg[l];
+    s.left[0] = __dadd_rn(s.left[0], sx);
+    s.left[1] = __dadd_rn(s.left[1], sy);
+    s.right[0] = __dadd_rn(s.right[0], sx);
+    s.right[1] = __dadd_rn(s.right[1], sy);
+    line_through_rn(s.left[0], s.left[1], s.right[0], s.right[1], s.a, s.b, s.vertical);
+    next->seg[l] = s;
+  } else if (l == 5 && T0.has_fillet) {
+    next->fillet.p[0] = __dadd_rn(T0.fillet.p[0], sx);
+    next->fillet.p[1] = __dadd_rn(T0.fillet.p[1], sy);
+  }
+}
+
+// the step's tool (written by the pair kernel) into shared memory, copied word by word by the
+// block's threads
+__device__ __forceinline__ void tool_load_shared(mf_tool_state &T, const dev_buffers &D) {
+  constexpr int WORDS = (int)(sizeof(mf_tool_state) / sizeof(double));
+  for (int w = threadIdx.x; w < WORDS; w += blockDim.x)
+    reinterpret_cast<double *>(&T)[w] = reinterpret_cast<const double *>(D.tool_next)[w];
+  __syncthreads();
+}
+
 template <bool PREDICT, bool MIXED>
 __device__ __forceinline__ void reorder_body(const params &P, const dev_buffers &D, blk bk) {
+  if (PREDICT && P.has_tool && bk.x == 0 && threadIdx.x < 32) tool_advance_warp(D.tool_prev, D.tool_next, P.dt);
   const int t = bk.x * blockDim.x + threadIdx.x;
   if (t >= P.N) return;
   // with neighbour lists, a step without a sort keeps the order and the cells of the last
@@ -560,6 +601,7 @@ static __global__ void __launch_bounds__(BLOCK, REORDER_BLOCKS_PER_SM) k_reorder
 // consecutive hashes, so their particles form one contiguous range of the sorted order;
 // visiting the columns in x order and each range in array order is the reference's
 // neighbour order (x-cell outer, y-cell inner, sorted order within a cell).
+
 // plane k of the FP64 record of particle j
 __device__ __forceinline__ double2 rec_plane(const double *__restrict__ rec, int N, int k, int j) {
   return __ldg(reinterpret_cast<const double2 *>(rec) + (size_t)k * N + j);
@@ -724,7 +766,10 @@ __device__ __forceinline__ void pair_fp64_body(const params &P, const dev_buffer
   pair_fp64_particle(P, D, bk.x * blockDim.x + threadIdx.x);
 }
 
-static __global__ void __launch_bounds__(PAIR_BLOCK, 4) k_pair_fp64(params P, dev_buffers D) {
+#ifndef MF_PAIR64_MIN_BLOCKS
+#define MF_PAIR64_MIN_BLOCKS 4
+#endif
+static __global__ void __launch_bounds__(PAIR_BLOCK, MF_PAIR64_MIN_BLOCKS) k_pair_fp64(params P, dev_buffers D) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
   pair_fp64_body(P, D, grid_blk());
@@ -777,33 +822,6 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers
 }
 
 // ---------------------------------------------------------------------------------------
-// the rigid tool of this step, advanced in shared memory: tool::update_tool (tool.cpp:211-221)
-// with IEEE-rounded operations (bitwise equal to the host's double arithmetic), one lane per
-// segment and one for the fillet; block 0 stores it for the next step
-__device__ __forceinline__ void tool_advance_shared(mf_tool_state &T, const dev_buffers &D, double dt,
-                                                    bool first_block) {
-  // copied word by word by the block's threads
-  static_assert(sizeof(mf_tool_state) % sizeof(double) == 0, "tool state is a whole number of doubles");
-  constexpr int WORDS = (int)(sizeof(mf_tool_state) / sizeof(double));
-  for (int w = threadIdx.x; w < WORDS; w += blockDim.x)
-    reinterpret_cast<double *>(&T)[w] = reinterpret_cast<const double *>(D.tool_prev)[w];
-  __syncthreads();
-  const double sx = __dmul_rn(dt, T.vel[0]), sy = __dmul_rn(dt, T.vel[1]);
-  const int t = threadIdx.x;
-  if (t < T.num_seg) {
-    mf_segment &s = T.seg[t];
-    s.left[0] = __dadd_rn(s.left[0], sx);
-    s.left[1] = __dadd_rn(s.left[1], sy);
-    s.right[0] = __dadd_rn(s.right[0], sx);
-    s.right[1] = __dadd_rn(s.right[1], sy);
-    line_through_rn(s.left[0], s.left[1], s.right[0], s.right[1], s.a, s.b, s.vertical);
-  } else if (t == 5 && T.has_fillet) {
-    T.fillet.p[0] = __dadd_rn(T.fillet.p[0], sx);
-    T.fillet.p[1] = __dadd_rn(T.fillet.p[1], sy);
-  }
-  __syncthreads();
-  if (first_block && threadIdx.x == 0) *D.tool_next = T;
-}
 
 // corrector .. invalidate for one particle (leap_frog.cu:68-92, actions_gpu.cu:135-162,
 // 226-349, tool_gpu.cu:151-221); returns the final position and flags
@@ -1161,6 +1179,45 @@ __device__ __forceinline__ void finish_particle_phased(const params &P, const de
   ft_out = ft;
 }
 
+// The step's tool force from the n per-block partials (8 doubles each: the compensated sums
+// s, c of fc.x, fc.y, ft.x, ft.y), by warp 0 of the last block to finish, in a fixed tree:
+// lane l merges partials l, l + 32, ... in order, then the lanes by a shuffle tree; lane 0
+// stores the force (report_force, output.cu:31-39: contact plus friction force), logs it and
+// closes the step's counters. `predicted`: the next step's predictor ran in this kernel.
+__device__ __forceinline__ void force_sums_last_warp(const params &P, const dev_buffers &D, int n, bool predicted) {
+  __threadfence();
+  ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
+  for (int b = (int)lane_id(); b < n; b += 32) {
+    const volatile double *pr = D.partials + (size_t)b * 8;
+    for (int k = 0; k < 4; ++k) {
+      ksum x{pr[2 * k], pr[2 * k + 1]};
+      ksum_merge(r[k], x);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 4; ++k) {
+      ksum x{__shfl_down_sync(0xffffffffu, r[k].s, o), __shfl_down_sync(0xffffffffu, r[k].c, o)};
+      ksum_merge(r[k], x);
+    }
+  if (lane_id() == 0) {
+    const double Fx = (r[0].s + r[0].c) + (r[2].s + r[2].c);
+    const double Fy = (r[1].s + r[1].c) + (r[3].s + r[3].c);
+    D.force_last[0] = Fx;
+    D.force_last[1] = Fy;
+    const unsigned long long hd = D.st->force_log_head;
+    D.force_log[2 * (hd % FORCE_LOG_CAP)] = Fx;
+    D.force_log[2 * (hd % FORCE_LOG_CAP) + 1] = Fy;
+    D.st->force_log_head = hd + 1;
+    D.st->steps += 1;
+    if (P.verlet) {  // every particle is checked: the next step sorts if one asked for it
+      D.st->sort_now = D.st->want_sort;
+      D.st->want_sort = 0u;
+      D.st->predicted = predicted ? 1u : 0u;
+    }
+    D.ticket[0] = 0u;
+  }
+}
+
 // Corrector .. invalidate for all particles plus the tool force (output.cu:31-39): one thread
 // per particle, one block per FINISH_BLOCK consecutive particles (the chunks of k_finish, so
 // that the force sums are the same numbers in the same tree: per warp, then the block's warps
@@ -1175,8 +1232,7 @@ __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buff
   __shared__ mf_tool_state s_tool;
   __shared__ ksum sm[FINISH_BLOCK / 32][4];
   __shared__ unsigned smc[FINISH_BLOCK / 32][4];
-  __shared__ bool last;
-  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt, bk.x == 0);
+  if (P.has_tool) tool_load_shared(s_tool, D);
   const int q = bk.x * FINISH_BLOCK + threadIdx.x;
   const bool identity = P.verlet && !*(volatile unsigned *)&D.st->sort_now;
   (void)num_scan_tiles;
@@ -1237,6 +1293,10 @@ __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buff
     smc[w][0] = nb; smc[w][1] = nbl; smc[w][2] = noog; smc[w][3] = nws;
   }
   const bool block_nz = __syncthreads_or(nz);  // sm and smc complete
+  // warp 0 closes the block (the block's sums into its partial, the counters, the ticket) and,
+  // in the last block, the step; the other warps are done
+  if (threadIdx.x >= 32) return;
+  unsigned is_last = 0u;
   if (threadIdx.x == 0) {
     ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
     if (block_nz) {
@@ -1259,50 +1319,10 @@ __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buff
     if (cnt[1]) atomicAdd(&D.st->blanked, cnt[1]);
     if (cnt[2]) atomicAdd(&D.st->out_of_grid, cnt[2]);
     __threadfence();
-    const unsigned t = atomicAdd(&D.ticket[0], 1u);
-    last = (t == bk.n - 1);
+    is_last = atomicAdd(&D.ticket[0], 1u) == (unsigned)(bk.n - 1) ? 1u : 0u;
   }
-  __syncthreads();
-  if (!last) return;
-  // last block: fixed-order reduction of all block partials
-  __threadfence();
-  const int n_chunks = bk.n;
-  ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
-  for (int b = threadIdx.x; b < n_chunks; b += blockDim.x) {
-    const volatile double *pr = D.partials + (size_t)b * 8;
-    for (int k = 0; k < 4; ++k) {
-      ksum x{pr[2 * k], pr[2 * k + 1]};
-      ksum_merge(r[k], x);
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1)
-    for (int k = 0; k < 4; ++k) {
-      ksum x{__shfl_down_sync(0xffffffffu, r[k].s, o), __shfl_down_sync(0xffffffffu, r[k].c, o)};
-      ksum_merge(r[k], x);
-    }
-  __syncthreads();
-  if (lane_id() == 0)
-    for (int k = 0; k < 4; ++k) sm[w][k] = r[k];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int v = 1; v < FINISH_BLOCK / 32; ++v)
-      for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[v][k]);
-    const double Fx = (r[0].s + r[0].c) + (r[2].s + r[2].c);
-    const double Fy = (r[1].s + r[1].c) + (r[3].s + r[3].c);
-    D.force_last[0] = Fx;
-    D.force_last[1] = Fy;
-    const unsigned long long hd = D.st->force_log_head;
-    D.force_log[2 * (hd % FORCE_LOG_CAP)] = Fx;
-    D.force_log[2 * (hd % FORCE_LOG_CAP) + 1] = Fy;
-    D.st->force_log_head = hd + 1;
-    D.st->steps += 1;
-    if (P.verlet) {  // every particle is checked: the next step sorts if one asked for it
-      D.st->sort_now = D.st->want_sort;
-      D.st->want_sort = 0u;
-      D.st->predicted = 0u;
-    }
-    D.ticket[0] = 0u;
-  }
+  if (!__shfl_sync(0xffffffffu, is_last, 0)) return;
+  force_sums_last_warp(P, D, bk.n, false);
 }
 
 template <bool FUSE_HASH>
@@ -1330,12 +1350,11 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
   __shared__ ksum sm[FINISH_BLOCK / 32][4];
   __shared__ unsigned smc[FINISH_BLOCK / 32][3];
   __shared__ int s_chunk[2];  // this chunk and the next, taken while this one runs
-  __shared__ bool last;
   if (threadIdx.x == 0) {
     s_jc = P.joco;
     s_chunk[0] = (int)atomicAdd(D.finish_chunk, 1u);
   }
-  if (P.has_tool) tool_advance_shared(s_tool, D, P.dt, blockIdx.x == 0);  // (its first barrier also covers s_jc, s_chunk)
+  if (P.has_tool) tool_load_shared(s_tool, D);  // (its barrier also covers s_jc, s_chunk)
   else __syncthreads();
   const int stride = gridDim.x * blockDim.x;
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1436,6 +1455,8 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
   // with neighbour lists the hashes and counts above serve the next step only if it sorts,
   // which is known once every particle has been checked (last block, below)
   const bool block_wants_sort = __syncthreads_or(want_sort);
+  if (threadIdx.x >= 32) return;  // warp 0 closes the block and, in the last block, the step
+  unsigned is_last = 0u;
   if (threadIdx.x == 0) {
     unsigned long long cnt[3] = {smc[0][0], smc[0][1], smc[0][2]};
     for (int w = 1; w < FINISH_BLOCK / 32; ++w)
@@ -1445,50 +1466,10 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
     if (cnt[1]) atomicAdd(&D.st->blanked, cnt[1]);
     if (cnt[2]) atomicAdd(&D.st->out_of_grid, cnt[2]);
     __threadfence();
-    const unsigned t = atomicAdd(&D.ticket[0], 1u);
-    last = (t == gridDim.x - 1);
+    is_last = atomicAdd(&D.ticket[0], 1u) == gridDim.x - 1 ? 1u : 0u;
   }
-  __syncthreads();
-  if (!last) return;
-  // last block: fixed-order reduction of all chunk partials
-  __threadfence();
-  ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
-  for (int b = threadIdx.x; b < n_chunks; b += blockDim.x) {
-    const volatile double *pr = D.partials + (size_t)b * 8;
-    for (int k = 0; k < 4; ++k) {
-      ksum x{pr[2 * k], pr[2 * k + 1]};
-      ksum_merge(r[k], x);
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1)
-    for (int k = 0; k < 4; ++k) {
-      ksum x{__shfl_down_sync(0xffffffffu, r[k].s, o), __shfl_down_sync(0xffffffffu, r[k].c, o)};
-      ksum_merge(r[k], x);
-    }
-  __syncthreads();
-  if (lane_id() == 0)
-    for (int k = 0; k < 4; ++k) sm[threadIdx.x >> 5][k] = r[k];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int w = 1; w < FINISH_BLOCK / 32; ++w)
-      for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
-    // report_force: total contact force plus total friction force
-    const double Fx = (r[0].s + r[0].c) + (r[2].s + r[2].c);
-    const double Fy = (r[1].s + r[1].c) + (r[3].s + r[3].c);
-    D.force_last[0] = Fx;
-    D.force_last[1] = Fy;
-    const unsigned long long hd = D.st->force_log_head;
-    D.force_log[2 * (hd % FORCE_LOG_CAP)] = Fx;
-    D.force_log[2 * (hd % FORCE_LOG_CAP) + 1] = Fy;
-    D.st->force_log_head = hd + 1;
-    D.st->steps += 1;
-    if (P.verlet) {  // every particle is checked: the next step sorts if one asked for it
-      D.st->sort_now = D.st->want_sort;
-      D.st->want_sort = 0u;
-      D.st->predicted = fuse ? 1u : 0u;
-    }
-    D.ticket[0] = 0u;
-  }
+  if (!__shfl_sync(0xffffffffu, is_last, 0)) return;
+  force_sums_last_warp(P, D, n_chunks, fuse);
 }
 
 // JC plasticity (actions_gpu.cu:226-285) for the particles the finish kernel listed: the

@@ -198,36 +198,55 @@ static __global__ void k_list_check(params P, dev_buffers D, const double2 *__re
   if (missing) atomicAdd(out + 1, missing);
 }
 
-// LIST: the neighbour-list form (steps with P.verlet). 80 registers (6 blocks of 128 per SM)
-// keep both forms free of spills; the list form measured slower at 7 and 8 blocks per SM
-template <bool LIST>
-__device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_buffers &D, int q) {
-  if (q >= P.N) return;
+// Records of the candidates: the record planes in global memory (read through the read-only
+// path), or a block's staged copy of them in shared memory (STAGE_CAP entries per plane).
+struct rec_global {
+  const float4 *__restrict__ r0, *__restrict__ r1, *__restrict__ r2, *__restrict__ r3;
+  __device__ __forceinline__ float4 p0(int j) const { return __ldg(r0 + j); }
+  __device__ __forceinline__ void all(int j, float4 &b0, float4 &b1, float4 &b2, float4 &b3) const {
+    b0 = __ldg(r0 + j); b1 = __ldg(r1 + j); b2 = __ldg(r2 + j); b3 = __ldg(r3 + j);
+  }
+};
+
+#ifndef MF_STAGE_CAP
+#define MF_STAGE_CAP 1024
+#endif
+constexpr int STAGE_CAP = MF_STAGE_CAP;              // staged candidates per block
+constexpr int STAGE_BYTES = 4 * STAGE_CAP * 16;      // four planes of float4
+
+struct rec_staged {
+  const float4 *s;  // plane k at s[k * STAGE_CAP + j]
+  __device__ __forceinline__ float4 p0(int j) const { return s[j]; }
+  __device__ __forceinline__ void all(int j, float4 &b0, float4 &b1, float4 &b2, float4 &b3) const {
+    b0 = s[j]; b1 = s[STAGE_CAP + j]; b2 = s[2 * STAGE_CAP + j]; b3 = s[3 * STAGE_CAP + j];
+  }
+};
+
+// The i particle of slot q: its records and the constants of its sums. False when q has no
+// pair sums (past the end, blanked, a tool particle without Brookshaw heat).
+__device__ __forceinline__ bool mixed_begin(const params &P, const dev_buffers &D, int q, mixed_i &I,
+                                            mixed_const &K, double &thermal_alpha) {
+  if (q >= P.N) return false;
   // record planes (structure of arrays): plane k of particle j at [k * N + j]
   const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
-  const float4 *__restrict__ r1 = r0 + P.N;
-  const float4 *__restrict__ r2 = r1 + P.N;
-  const float4 *__restrict__ r3 = r2 + P.N;
   const float4 a0 = __ldg(r0 + q);  // x, y, flags|cy, vx
   const unsigned fi = (unsigned)__float_as_int(a0.z) & 0xffu;
-  if (fi & FLAG_BLANKED) return;
+  if (fi & FLAG_BLANKED) return false;
   const bool tool_i = fi & FLAG_TOOL;
   const bool brookshaw = P.thermal_solver == MF_THERMAL_BROOKSHAW;
-  if (!brookshaw && tool_i) return;
-  const float4 a1 = __ldg(r1 + q);  // vy, sxx, sxy, syy
-  const float4 a2 = __ldg(r2 + q);  // Rxx, Rxy, Ryy, h
-  const float4 a3 = __ldg(r3 + q);  // rho, c, vol, T - T_init
+  if (!brookshaw && tool_i) return false;
+  const float4 a1 = __ldg(r0 + P.N + q);          // vy, sxx, sxy, syy
+  const float4 a2 = __ldg(r0 + 2 * P.N + q);      // Rxx, Rxy, Ryy, h
+  const float4 a3 = __ldg(r0 + 3 * P.N + q);      // rho, c, vol, T - T_init
 
-  mixed_const K;
   K.inv_wdeltap = (float)(1. / P.corr.wdeltap);
   K.alpha = (float)P.corr.alpha;
   K.beta = (float)P.corr.beta;
   const float eta = (float)P.corr.eta;
   K.eta2 = eta * eta;
-  double thermal_alpha = 0.;
+  thermal_alpha = 0.;
   if (brookshaw) thermal_alpha = !tool_i ? P.trml_wp.alpha : (P.thermal_tool_on ? P.trml_tool.alpha : 0.);
 
-  mixed_i I;
   I.thermal = thermal_alpha != 0.;
   I.nonfinite = fi & FLAG_NONFINITE;
   I.mech = !tool_i;
@@ -238,81 +257,44 @@ __device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_b
   I.h1 = 1.f / I.h;
   I.fourh2 = 4.f * I.h * I.h;
   I.fac = 0.454728408833987f * I.h1 * I.h1;
+  return true;
+}
 
-  const geom g = *D.g;
-  const float dxc = (float)g.dx;
-  const int hashi = D.hash_cur[q];
-  const int gi = hashi / g.ny;
-  const int gj = hashi - gi * g.ny;
-
-  mixed_acc acc;
-  acc.vd01 = acc.vd23 = acc.sd_xw = acc.sd_zy = acc.vt = acc.xt = f2(0.f, 0.f);
-  acc.T_lapl = 0.f;
-
-  if (LIST && !I.nonfinite) {
-    // neighbour list: built on a sorting step, then read; each entry passes the same
-    // support test as a window candidate. A particle's row is contiguous: four entries per
-    // 16-byte load; an entry past the count reads the particle's own record (always valid,
-    // so the loads need no guard) and is skipped.
-    const int cnt = D.st->sort_now ? build_list(D, r0, q, I, g, gi, gj, dxc, P.skin) : D.ncount[q];
-    const uint4 *row = reinterpret_cast<const uint4 *>(D.nlist + (size_t)q * LIST_CAP);
-    uint4 e4 = row[0];  // (a row is LIST_CAP entries: the first four are always there)
-    for (int k0 = 0; k0 < cnt; k0 += 4) {
-      const unsigned ev[4] = {e4.x, e4.y, e4.z, e4.w};
-      if (k0 + 4 < cnt) e4 = row[(k0 >> 2) + 1];  // the next four, in flight during these
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const bool live = k0 + u < cnt;
-        const unsigned e = live ? ev[u] : (unsigned)q | (3u << LIST_INDEX_BITS);
-        const int j = (int)(e & LIST_INDEX_MASK);
-        const float ox = fmaf((float)((int)(e >> LIST_INDEX_BITS) - 3), dxc, I.x);
-        const float4 b0 = __ldg(r0 + j), b1 = __ldg(r1 + j), b2 = __ldg(r2 + j), b3 = __ldg(r3 + j);
-        const unsigned fjw = (unsigned)__float_as_int(b0.z);
-        const float xij = ox - b0.x;
-        const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
-        const float rr2 = dist2(xij, yij);
-        const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
-        if (live && !(fjw & FLAG_BLANKED) && (in_support || (fjw & FLAG_NONFINITE)))
-          mixed_interact(I, K, acc, xij, yij, b0, b1, b2, b3);
-      }
-    }
-  } else {  // the 5x5 window (interactions_gpu.cu:147-345)
-    const int low_i = gi - 2 < 0 ? 0 : gi - 2;
-    const int low_j = gj - 2 < 0 ? 0 : gj - 2;
-    const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
-    const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
-    for (int ii = low_i; ii < high_i; ++ii) {
-      const int col = ii * g.ny;
-      const int j0 = __ldg(D.off + col + low_j);
-      const int j1 = __ldg(D.off + col + high_j);
-      const float ox = fmaf((float)(gi - ii), dxc, I.x);
-      // chunks of up to 32 candidates: mark the contributing ones, then visit them in order
-      for (int jb = j0; jb < j1; jb += 32) {
-        const int jn = min(32, j1 - jb);
-        unsigned mask = 0u;
+// The candidates j0 .. j1 - 1 of one window column (indices into R), in chunks of up to 32: mark
+// the contributing ones, then visit them in order.
+template <class REC>
+__device__ __forceinline__ void mixed_column(const REC &R, int j0, int j1, float ox, int gj, float dxc,
+                                             const mixed_i &I, const mixed_const &K, mixed_acc &acc) {
+  for (int jb = j0; jb < j1; jb += 32) {
+    const int jn = min(32, j1 - jb);
+    unsigned mask = 0u;
 #pragma unroll 4
-        for (int k = 0; k < jn; ++k) {
-          const float4 b0 = __ldg(r0 + jb + k);
-          const unsigned fjw = (unsigned)__float_as_int(b0.z);
-          const float xij = ox - b0.x;
-          const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
-          const float rr2 = dist2(xij, yij);
-          const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
-          const bool take = !(fjw & FLAG_BLANKED) && (in_support || I.nonfinite || (fjw & FLAG_NONFINITE));
-          mask |= (take ? 1u : 0u) << k;
-        }
-        while (mask) {
-          const int k = __ffs(mask) - 1;
-          mask &= mask - 1u;
-          const int j = jb + k;
-          // all four planes at once: one load latency per neighbour
-          const float4 b0 = __ldg(r0 + j), b1 = __ldg(r1 + j), b2 = __ldg(r2 + j), b3 = __ldg(r3 + j);
-          const float yij = fmaf((float)(gj - (int)((unsigned)__float_as_int(b0.z) >> 8)), dxc, I.y - b0.y);
-          mixed_interact(I, K, acc, ox - b0.x, yij, b0, b1, b2, b3);
-        }
-      }
+    for (int k = 0; k < jn; ++k) {
+      const float4 b0 = R.p0(jb + k);
+      const unsigned fjw = (unsigned)__float_as_int(b0.z);
+      const float xij = ox - b0.x;
+      const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
+      const float rr2 = dist2(xij, yij);
+      const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
+      const bool take = !(fjw & FLAG_BLANKED) && (in_support || I.nonfinite || (fjw & FLAG_NONFINITE));
+      mask |= (take ? 1u : 0u) << k;
+    }
+    while (mask) {
+      const int k = __ffs(mask) - 1;
+      mask &= mask - 1u;
+      // all four planes at once: one load latency per neighbour
+      float4 b0, b1, b2, b3;
+      R.all(jb + k, b0, b1, b2, b3);
+      const float yij = fmaf((float)(gj - (int)((unsigned)__float_as_int(b0.z) >> 8)), dxc, I.y - b0.y);
+      mixed_interact(I, K, acc, ox - b0.x, yij, b0, b1, b2, b3);
     }
   }
+}
+
+// the rates of slot q from its pair sums: Jaumann stress rate, continuity, momentum, advection
+// and heat (actions_gpu.cu:100-132, interactions_gpu.cu:331-345)
+__device__ __forceinline__ void mixed_end(const params &P, const dev_buffers &D, int q, const mixed_i &I,
+                                          const mixed_acc &acc, double thermal_alpha) {
   const float mass = (float)P.phys.mass;
   const float m_eps = (float)P.corr.xspheps * mass;
   const float vdx = acc.vd01.x, vdy = acc.vd01.y, vdz = acc.vd23.x, vdw = acc.vd23.y;
@@ -356,17 +338,258 @@ __device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_b
   if (thermal) B.T_t[q] = thermal_alpha * (double)T_lapl;
 }
 
+// LIST: the neighbour-list form (steps with P.verlet). 80 registers (6 blocks of 128 per SM)
+// keep both forms free of spills; the list form measured slower at 7 and 8 blocks per SM
+template <bool LIST>
+__device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_buffers &D, int q) {
+  mixed_i I;
+  mixed_const K;
+  double thermal_alpha;
+  if (!mixed_begin(P, D, q, I, K, thermal_alpha)) return;
+  const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
+  const rec_global R{r0, r0 + P.N, r0 + 2 * (size_t)P.N, r0 + 3 * (size_t)P.N};
+
+  const geom g = *D.g;
+  const float dxc = (float)g.dx;
+  const int hashi = D.hash_cur[q];
+  const int gi = hashi / g.ny;
+  const int gj = hashi - gi * g.ny;
+
+  mixed_acc acc;
+  acc.vd01 = acc.vd23 = acc.sd_xw = acc.sd_zy = acc.vt = acc.xt = f2(0.f, 0.f);
+  acc.T_lapl = 0.f;
+
+  if (LIST && !I.nonfinite) {
+    // neighbour list: built on a sorting step, then read; each entry passes the same
+    // support test as a window candidate. A particle's row is contiguous: four entries per
+    // 16-byte load; an entry past the count reads the particle's own record (always valid,
+    // so the loads need no guard) and is skipped.
+    const int cnt = D.st->sort_now ? build_list(D, r0, q, I, g, gi, gj, dxc, P.skin) : D.ncount[q];
+    const uint4 *row = reinterpret_cast<const uint4 *>(D.nlist + (size_t)q * LIST_CAP);
+    uint4 e4 = row[0];  // (a row is LIST_CAP entries: the first four are always there)
+    for (int k0 = 0; k0 < cnt; k0 += 4) {
+      const unsigned ev[4] = {e4.x, e4.y, e4.z, e4.w};
+      if (k0 + 4 < cnt) e4 = row[(k0 >> 2) + 1];  // the next four, in flight during these
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool live = k0 + u < cnt;
+        const unsigned e = live ? ev[u] : (unsigned)q | (3u << LIST_INDEX_BITS);
+        const int j = (int)(e & LIST_INDEX_MASK);
+        const float ox = fmaf((float)((int)(e >> LIST_INDEX_BITS) - 3), dxc, I.x);
+        float4 b0, b1, b2, b3;
+        R.all(j, b0, b1, b2, b3);
+        const unsigned fjw = (unsigned)__float_as_int(b0.z);
+        const float xij = ox - b0.x;
+        const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
+        const float rr2 = dist2(xij, yij);
+        const bool in_support = !(rr2 >= I.fourh2 || rr2 < 1e-8f);
+        if (live && !(fjw & FLAG_BLANKED) && (in_support || (fjw & FLAG_NONFINITE)))
+          mixed_interact(I, K, acc, xij, yij, b0, b1, b2, b3);
+      }
+    }
+  } else {  // the 5x5 window (interactions_gpu.cu:147-345)
+    const int low_i = gi - 2 < 0 ? 0 : gi - 2;
+    const int low_j = gj - 2 < 0 ? 0 : gj - 2;
+    const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
+    const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
+    for (int ii = low_i; ii < high_i; ++ii) {
+      const int col = ii * g.ny;
+      const int j0 = __ldg(D.off + col + low_j);
+      const int j1 = __ldg(D.off + col + high_j);
+      mixed_column(R, j0, j1, fmaf((float)(gi - ii), dxc, I.x), gj, dxc, I, K, acc);
+    }
+  }
+  mixed_end(P, D, q, I, acc, thermal_alpha);
+}
+
 // the mixed pair sums of block bk.x's particles
 template <bool LIST>
 __device__ __forceinline__ void pair_mixed_body(const params &P, const dev_buffers &D, blk bk) {
   pair_mixed_particle<LIST>(P, D, bk.x * blockDim.x + threadIdx.x);
 }
 
+#ifndef MF_PAIR_SM_MAJOR
+#define MF_PAIR_SM_MAJOR 0
+#endif
+// Block b of a grid of W * S blocks (S = the device's SM count) takes chunk (b mod S) W + b / S.
+// When the hardware hands out blocks to the SMs in turn, the blocks resident on one SM at the
+// same time (b, b + S, b + 2 S, ...) then take consecutive chunks of the sorted particles, and
+// their neighbour windows overlap in that SM's L1.
+__device__ __forceinline__ blk sm_major_blk(int sms) {
+  const int w = (int)gridDim.x / sms;
+  return blk{(int)(blockIdx.x % (unsigned)sms) * w + (int)(blockIdx.x / (unsigned)sms), (int)gridDim.x};
+}
+
 template <bool LIST>
 static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, dev_buffers D) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
-  pair_mixed_body<LIST>(P, D, grid_blk());
+  pair_mixed_body<LIST>(P, D, MF_PAIR_SM_MAJOR ? sm_major_blk(P.sm_count) : grid_blk());
+}
+
+// ---- window form with the block's candidates staged in shared memory by bulk copies ----
+//
+// The block's particles (consecutive sorted slots) lie in at most two cell columns (groups);
+// for group k in column c_k with cell rows r_min .. r_max, its particles' windows together are
+// the rows r_min - 2 .. r_max + 2 of the columns c_k - 2 .. c_k + 2, and each of those five
+// row spans is one contiguous range of the sorted records. Up to ten ranges (four planes each)
+// are copied into shared memory by the tensor memory accelerator, one bulk copy per range and
+// plane, completing on one mbarrier; each particle then reads its candidates there instead of
+// through L1/L2. A block whose particles span more than two columns, or whose ranges hold more
+// than STAGE_CAP records, reads from global memory as k_pair_mixed does. Same candidates in
+// the same order, so the sums are those of k_pair_mixed bit for bit.
+struct stage_table {
+  int g0[10], n[10], s0[10];  // per (group, column offset): first record, count, staged position
+  int gi0;                    // the column of group 0
+  int ok;                     // 1: staged; 0: read from global memory
+  int rmin[2], rmax[2];       // cell rows of each group
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+// bounded wait for phase 0 of the mbarrier: false if it did not complete in `limit` polls
+__device__ __forceinline__ bool mbar_wait_phase0(unsigned long long *bar, long limit) {
+  const unsigned a = smem_u32(bar);
+  for (long it = 0; it < limit; ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(0u)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void pair_mixed_staged_body(const params &P, const dev_buffers &D, blk bk,
+                                                       float4 *s_rec) {
+  __shared__ stage_table T;
+  __shared__ __align__(8) unsigned long long s_bar;
+  const int q0 = bk.x * (int)blockDim.x;
+  if (q0 >= P.N) return;  // (a block past the last particle: the whole block leaves)
+  const geom g = *D.g;
+  const int q = q0 + (int)threadIdx.x;
+  if (threadIdx.x == 0) {
+    T.gi0 = __ldg(D.hash_cur + q0) / g.ny;
+    T.ok = 1;
+    T.rmin[0] = T.rmin[1] = 0x7fffffff;
+    T.rmax[0] = T.rmax[1] = -1;
+  }
+  __syncthreads();
+  int gi = 0, gj = 0;
+  if (q < P.N) {
+    const int h = __ldg(D.hash_cur + q);
+    gi = h / g.ny;
+    gj = h - gi * g.ny;
+    const int grp = gi - T.gi0;
+    if (grp < 0 || grp > 1) {
+      T.ok = 0;
+    } else {
+      atomicMin(&T.rmin[grp], gj);
+      atomicMax(&T.rmax[grp], gj);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int total = 0;
+    for (int k = 0; k < 10; ++k) {
+      const int grp = k / 5;
+      const int col = T.gi0 + grp + (k % 5) - 2;
+      int j0 = 0, j1 = 0;
+      if (T.rmax[grp] >= 0 && col >= 0 && col < g.nx) {
+        const int lo = max(T.rmin[grp] - 2, 0), hi = min(T.rmax[grp] + 3, g.ny);
+        j0 = __ldg(D.off + col * g.ny + lo);
+        j1 = __ldg(D.off + col * g.ny + hi);
+      }
+      T.g0[k] = j0;
+      T.n[k] = j1 - j0;
+      T.s0[k] = total;
+      total += j1 - j0;
+    }
+    if (total > STAGE_CAP || total == 0) T.ok = 0;
+    if (T.ok) {
+      const unsigned bar = smem_u32(&s_bar);
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      unsigned long long state;
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+                   : "=l"(state)
+                   : "r"(bar), "r"((unsigned)total * 64u)
+                   : "memory");
+      (void)state;
+      const float4 *src = reinterpret_cast<const float4 *>(D.recf);
+      for (int k = 0; k < 10; ++k) {
+        if (T.n[k] == 0) continue;
+        for (int pl = 0; pl < 4; ++pl) {
+          const float4 *from = src + (size_t)pl * P.N + T.g0[k];
+          const unsigned to = smem_u32(s_rec + pl * STAGE_CAP + T.s0[k]);
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(to),
+              "l"(from), "r"((unsigned)T.n[k] * 16u), "r"(bar)
+              : "memory");
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const bool staged = T.ok;
+  if (staged && !mbar_wait_phase0(&s_bar, 1L << 22)) {
+    // the copies did not complete: report it, give them a second bounded wait so that none is
+    // still writing when the block exits, and leave this block's rates unwritten
+    if (threadIdx.x == 0) atomicOr(&D.st->error_flags, ERR_STAGE_WAIT);
+    mbar_wait_phase0(&s_bar, 1L << 22);
+    return;
+  }
+  mixed_i I;
+  mixed_const K;
+  double thermal_alpha;
+  if (!mixed_begin(P, D, q, I, K, thermal_alpha)) return;
+  const float dxc = (float)g.dx;
+  mixed_acc acc;
+  acc.vd01 = acc.vd23 = acc.sd_xw = acc.sd_zy = acc.vt = acc.xt = f2(0.f, 0.f);
+  acc.T_lapl = 0.f;
+  const int low_i = gi - 2 < 0 ? 0 : gi - 2;
+  const int low_j = gj - 2 < 0 ? 0 : gj - 2;
+  const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
+  const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
+  if (staged) {
+    const rec_staged R{s_rec};
+    const int kb = (gi - T.gi0) * 5 - (gi - 2);  // range of column ii: kb + ii
+    for (int ii = low_i; ii < high_i; ++ii) {
+      const int col = ii * g.ny;
+      const int k = kb + ii;
+      const int d = T.s0[k] - T.g0[k];  // staged position = record index + d
+      const int j0 = __ldg(D.off + col + low_j) + d;
+      const int j1 = __ldg(D.off + col + high_j) + d;
+      mixed_column(R, j0, j1, fmaf((float)(gi - ii), dxc, I.x), gj, dxc, I, K, acc);
+    }
+  } else {
+    const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
+    const rec_global R{r0, r0 + P.N, r0 + 2 * (size_t)P.N, r0 + 3 * (size_t)P.N};
+    for (int ii = low_i; ii < high_i; ++ii) {
+      const int col = ii * g.ny;
+      const int j0 = __ldg(D.off + col + low_j);
+      const int j1 = __ldg(D.off + col + high_j);
+      mixed_column(R, j0, j1, fmaf((float)(gi - ii), dxc, I.x), gj, dxc, I, K, acc);
+    }
+  }
+  mixed_end(P, D, q, I, acc, thermal_alpha);
+}
+
+#ifndef MF_STAGED_BLOCKS_PER_SM
+#define MF_STAGED_BLOCKS_PER_SM 3
+#endif
+static __global__ void __launch_bounds__(PAIR_BLOCK, MF_STAGED_BLOCKS_PER_SM) k_pair_mixed_staged(params P,
+                                                                                                  dev_buffers D) {
+  MF_PDL_WAIT();
+  MF_PDL_TRIGGER();
+  extern __shared__ __align__(128) float4 s_dyn[];
+  pair_mixed_staged_body(P, D, MF_PAIR_SM_MAJOR ? sm_major_blk(P.sm_count) : grid_blk(), s_dyn);
 }
 
 // PSE heat Laplacian (interactions_gpu.cu:88-144, kernels.cuh:72-89) in FP32 for the mixed
