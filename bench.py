@@ -482,10 +482,12 @@ CUT_FORMS = FORMS
 
 
 def form_flags(mf, name):
+    """Precision and option flags of a form; a name "<form>@p" is that form from initial
+    positions moved by at most 1e-12 of the lattice spacing (cut runs only)."""
     flags = 0
-    for f in FORMS[name][1]:
+    for f in FORMS[name.split("@")[0]][1]:
         flags |= getattr(mf, f)
-    return getattr(mf, FORMS[name][0]), flags
+    return getattr(mf, FORMS[name.split("@")[0]][0]), flags
 
 
 def cut_together(mf, scene, params, mm, forms, device, out_dir, list_check_every=0, list_check_late=(0.0, 0),
@@ -506,6 +508,10 @@ def cut_together(mf, scene, params, mm, forms, device, out_dir, list_check_every
         ctx.set_options(SOLVER["thermal"], mf.JC_JOHNSON_COOK, prec)
         ctx.set_neighbour_skin(SOLVER["skin"])
         ctx.set_flags(flags)
+        if form.endswith("@p"):  # a rounding-sized perturbation of the initial positions
+            rng = np.random.default_rng(12345)
+            pos = ctx.get("pos")
+            ctx.set("pos", pos + (rng.random(pos.shape) - 0.5) * 2e-12 * params.dx)
         runs[form] = {"ctx": ctx, "forces": [], "timeline": [], "checks": [], "done": 0, "stopped": False,
                       "checking": list_check_every > 0 and bool(flags & mf.OPT_NEIGHBOUR_LISTS)}
     chunk = 20_000  # below the device force log's 65,536 entries
@@ -575,11 +581,16 @@ def cut_compare(mf, scene, paths):
         runs[Path(p).stem.replace("cut_", "")] = (d["forces"], st, float(d["secs"][0]), status,
                                                  int(d["steps_planned"][0]))
     out = {"forms": {}}
+    blocks = 10  # mean force per tenth of the planned run, over its finite steps
     for name, (f, st, secs, status, planned) in runs.items():
         lc = status.get("list_checks")
         out["forms"][name] = {"steps": int(len(f)), "steps_planned": planned, "completed": len(f) == planned,
                               "first_nonfinite_force_step": finite_prefix(f) if finite_prefix(f) < len(f) else None,
                               "mean_force": f[:finite_prefix(f)].mean(axis=0).tolist(),
+                              "block_mean_force": [f[k * planned // blocks:min((k + 1) * planned // blocks,
+                                                                               finite_prefix(f))].mean(axis=0).tolist()
+                                                   if k * planned // blocks < finite_prefix(f) else None
+                                                   for k in range(blocks)],
                               "device_s": secs, "blanked": int(status["blanked"]),
                               "secant_cap_hits": int(status["secant_cap_hits"]), "sorts": int(status["sorts"]),
                               "timeline": status.get("timeline"), "chip": chip_summary(scene, st),
@@ -597,6 +608,8 @@ def cut_compare(mf, scene, paths):
     for name in runs:
         if name != "fp64" and "fp64" in runs:
             out["forms"][name]["errors_against_fp64"] = errs("fp64", name)
+        if name.endswith("@p") and name.split("@")[0] in runs:
+            out["forms"][name]["errors_against_unperturbed"] = errs(name.split("@")[0], name)
         if name != "mixed_sorted" and name != "fp64" and "mixed_sorted" in runs:
             out["forms"][name]["errors_against_mixed_sorted"] = errs("mixed_sorted", name)
     return out

@@ -78,11 +78,13 @@ extern "C" {
 #define MF_OPT_SORT_EVERY_STEP 4  /* mixed form: sort the cell list every step, as the FP64 form
                                      does (the default; overrides MF_OPT_NEIGHBOUR_LISTS) */
 #define MF_OPT_FUSED_PREDICTOR 8  /* with MF_OPT_NEIGHBOUR_LISTS: run the next step's predictor in
-                                     the finish kernel instead of the reorder kernel (faster) */
-#define MF_OPT_NEIGHBOUR_LISTS 16 /* mixed form: keep neighbour lists between cell-list sorts
-                                     (faster; experimental: over a 1 mm cut of the ~150k-particle
-                                     scene, 36 particles became non-finite after ~0.55 mm, which
-                                     the form that sorts every step does not show) */
+                                     the finish kernel instead of the reorder kernel (measured
+                                     ~3 % slower per step on the ~150k-particle cut) */
+#define MF_OPT_NEIGHBOUR_LISTS 16 /* mixed form: keep neighbour lists between cell-list sorts,
+                                     sorting when a particle's next predicted position is more
+                                     than 0.45 skin from where its list was built (the fastest
+                                     form; over a 1 mm cut of the ~150k-particle scene no pair
+                                     was missing from the lists in 1,053 brute-force checks) */
 
 /* ---- constants (constants_structs.h:25-82), same member order ---- */
 typedef struct { double E, nu, rho0, K, G, mass, mass_tool; } mf_phys_constants;
@@ -120,11 +122,9 @@ typedef struct {
   long long secant_cap_hits;  /* JC secant solves that hit the iteration cap */
   int max_cell_occupancy;     /* largest particles-per-cell seen in the last sort */
   int error_flags;            /* bit 1: the adaptive grid outgrew max_cell; bit 2: a neighbour
-                                 list was full (neighbours dropped); bit 3: a block of the
-                                 pair kernel did not receive its staged candidates in time
-                                 (its particles' rates of that step were not written); bit 0
-                                 (a bounded wait in the cell scan expired) is no longer
-                                 raised: the scan waits for nothing */
+                                 list was full (neighbours dropped); bit 0 (a bounded wait in
+                                 the cell scan expired) is no longer raised: the scan waits
+                                 for nothing */
   long long secant_iterations; /* JC secant iterations since creation (cost diagnostic) */
   long long sorts;            /* cell-list sorts since creation (one per step, except for the
                                  mixed form with neighbour lists) */

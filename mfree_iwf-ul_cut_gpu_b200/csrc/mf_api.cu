@@ -202,9 +202,13 @@ int alloc_particles(mf_ctx *ctx, int N) {
   TRY(dalloc(ctx, L, &D.pos_build, N));
   ctx->finish_blocks = std::min((N + FINISH_BLOCK - 1) / FINISH_BLOCK, ctx->sm_count * FINISH_BLOCKS_PER_SM);
   ctx->bbox_blocks = std::min((N + BLOCK - 1) / BLOCK, ctx->sm_count * 4);
-  // per-chunk force partials of the finish kernel (or per-block partials of the bbox pass)
+  // per-chunk force partials of the finish kernel and their group sums (or per-block partials of
+  // the bbox pass), the force sum's group tickets
   const int finish_chunks = (N + FINISH_BLOCK - 1) / FINISH_BLOCK;
-  TRY(dalloc(ctx, L, &D.partials, (size_t)std::max(std::max(finish_chunks, ctx->bbox_blocks), 1) * 8));
+  const int force_groups = (finish_chunks + FORCE_GROUP - 1) / FORCE_GROUP;
+  TRY(dalloc(ctx, L, &D.partials,
+             (size_t)std::max(std::max(finish_chunks + force_groups, ctx->bbox_blocks), 1) * 8));
+  TRY(dalloc(ctx, L, &D.gticket, (size_t)std::max(force_groups, 1)));
   TRY(invalidate_counts(ctx));
   ctx->N = N;
   return MF_OK;
@@ -319,17 +323,6 @@ int launch_cells(mf_ctx *ctx, bool step_mode) {
   return MF_OK;
 }
 
-#ifndef MF_PAIR_STAGED
-#define MF_PAIR_STAGED 0
-#endif
-// grid of the mixed pair kernels: npb blocks, or with SM-major placement the next multiple of
-// the SM count (the blocks past the last particle return at once)
-int pair_grid(const mf_ctx *ctx, int npb) {
-  if (!MF_PAIR_SM_MAJOR) return npb;
-  const int s = ctx->sm_count;
-  return (npb + s - 1) / s * s;
-}
-
 int launch_stage(mf_ctx *ctx, int stage) {
   static const char *const names[4] = {"mf stage 0: cell list", "mf stage 1: predictor",
                                        "mf stage 2: pair sums", "mf stage 3: finish + return map"};
@@ -349,10 +342,8 @@ int launch_stage(mf_ctx *ctx, int stage) {
       else TRY(launch_pdl(ctx, k_reorder<true, false>, nb, BLOCK, ctx->P, ctx->D));
       break;
     case 2:
-      if (mixed && ctx->P.verlet) TRY(launch_pdl(ctx, k_pair_mixed<true>, pair_grid(ctx, npb), PAIR_BLOCK, ctx->P, ctx->D));
-      else if (mixed && MF_PAIR_STAGED)
-        TRY(launch_pdl_smem(ctx, k_pair_mixed_staged, pair_grid(ctx, npb), PAIR_BLOCK, (size_t)STAGE_BYTES, ctx->P, ctx->D));
-      else if (mixed) TRY(launch_pdl(ctx, k_pair_mixed<false>, pair_grid(ctx, npb), PAIR_BLOCK, ctx->P, ctx->D));
+      if (mixed && ctx->P.verlet) TRY(launch_pdl(ctx, k_pair_mixed<true>, npb, PAIR_BLOCK, ctx->P, ctx->D));
+      else if (mixed) TRY(launch_pdl(ctx, k_pair_mixed<false>, npb, PAIR_BLOCK, ctx->P, ctx->D));
       else TRY(launch_pdl(ctx, k_pair_fp64, npb, PAIR_BLOCK, ctx->P, ctx->D));
       if (ctx->P.thermal_solver == MF_THERMAL_PSE && ctx->P.thermal_wp) {
         if (mixed) TRY(launch_pdl(ctx, k_pse_mixed, npb, PAIR_BLOCK, ctx->P, ctx->D));
@@ -527,11 +518,6 @@ int mf_ctx_create(int device, mf_ctx **out) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
       ctx->sm_count = sms;
-    ctx->P.sm_count = ctx->sm_count;
-    if (MF_PAIR_STAGED &&
-        cudaFuncSetAttribute(k_pair_mixed_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_BYTES) !=
-            cudaSuccess)
-      rc = MF_ERR_CUDA;
   }
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.ticket, 4);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.force_log, (size_t)FORCE_LOG_CAP * 2);
@@ -687,7 +673,7 @@ int mf_get_field(mf_ctx *ctx, int field, void *host) {
       std::vector<float> rec(N * F_WIDTH);
       CK(cudaMemcpy(rec.data(), ctx->D.recf, sizeof(float) * N * F_WIDTH, cudaMemcpyDeviceToHost));
       for (size_t i = 0; i < N; ++i) {
-        auto at = [&](int f) { return rec[(size_t)(f / 4) * N * 4 + (size_t)i * 4 + f % 4]; };
+        auto at = [&](int f) { return rec[recf_word(f / 4, (int)i, (int)N) * 4 + f % 4]; };
         o[4 * i] = at(F_RXX);
         o[4 * i + 1] = at(F_RXY);
         o[4 * i + 2] = at(F_RYY);

@@ -34,6 +34,16 @@ enum : int {
   F_WIDTH
 };
 
+#ifndef MF_REC_AOS
+#define MF_REC_AOS 0
+#endif
+// index of float4 word k (0..3) of particle j's FP32 pair record among N records: four planes
+// (word k of every particle together, at k N + j), or with MF_REC_AOS each particle's 64 bytes
+// together (at 4 j + k)
+__host__ __device__ __forceinline__ size_t recf_word(int k, int j, int N) {
+  return MF_REC_AOS ? (size_t)4 * (size_t)j + (size_t)k : (size_t)k * (size_t)N + (size_t)j;
+}
+
 struct params {
   int N;
   int grid_kind;
@@ -42,7 +52,6 @@ struct params {
   int precision;
   int plastic, fric_heat, thermal_bc, thermal_wp, thermal_tool_on, has_tool, keep_derivs;
   int staged;  // step run stage by stage (mf_step_stage): keep every intermediate array
-  int sm_count;  // SMs of the device (block placement of the pair kernels)
   int jc_lower_bound;  // A > 0, B >= 0, C >= 0: the yield stress is bounded below by A (1 - theta^m)
   // mixed form with neighbour lists: the cell list is sorted only on steps where some
   // particle's predicted position is more than 0.45 skin from where its list was built; in
@@ -91,7 +100,6 @@ constexpr int FORCE_LOG_CAP = 1 << 16;
 constexpr int ERR_SCAN_WAIT = 1;  // (no longer raised: the cell scan has no bounded waits)
 constexpr int ERR_GRID_BUDGET = 2;
 constexpr int ERR_LIST_OVERFLOW = 4;  // a neighbour list was full: neighbours were dropped
-constexpr int ERR_STAGE_WAIT = 8;     // a pair block's staged candidate copies did not complete in time
 
 // neighbour list entry: particle index in the low LIST_INDEX_BITS bits, above them the
 // column offset of the pair's cells (i's column - j's column) + 3, in [0, 6]

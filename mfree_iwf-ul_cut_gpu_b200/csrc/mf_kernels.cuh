@@ -58,8 +58,10 @@ struct dev_buffers {
   int *tsum_r, *tsum_w; // per-tile totals of the counts: read by this step's scan / added to by
                         // this step's counting for the next (two arrays, swapped every step)
   int *off;             // cell offsets (max_cell + 1)
-  double *partials;     // per-block partial sums (force / bbox)
+  double *partials;     // per-block partial sums (force / bbox); the force's group sums follow the
+                        // block partials (at [8 * number of block partials])
   unsigned *ticket;     // last-block tickets: [0] force, [1] bbox, [2] tool wear
+  unsigned *gticket;    // per-group tickets of the force sums (one per FORCE_GROUP block partials)
   double *force_log;    // FORCE_LOG_CAP x 2
   double *force_last;   // 2
   plastic_item *plastic_list;  // particles whose return map k_plastic runs (this step)
@@ -470,11 +472,11 @@ __device__ __forceinline__ void predict_particle(const params &P, const dev_buff
     fr[1] = (float)(pos.y - oy);
     fr[2] = __int_as_float((int)(rf | ((unsigned)cj << 8)));
     fr[15] = (float)(T - P.trml_wp.T_init);
-    // four planes of float4 (structure of arrays): plane k of particle q at [k * N + q]
+    // four float4 words (recf_word: four planes, or each record's words together)
     float4 *fd = reinterpret_cast<float4 *>(D.recf);
 #pragma unroll
     for (int k = 0; k < F_WIDTH / 4; ++k)
-      fd[(size_t)k * P.N + q] = make_float4(fr[4 * k], fr[4 * k + 1], fr[4 * k + 2], fr[4 * k + 3]);
+      fd[recf_word(k, q, P.N)] = make_float4(fr[4 * k], fr[4 * k + 1], fr[4 * k + 2], fr[4 * k + 3]);
     // the lists stay valid while every particle is within skin / 2 of where it was at the
     // last sort (then every pair closer than 2 h was closer than 2 h + skin there); each step's
     // finish kernel checks the next step's predicted positions against 0.45 skin
@@ -1179,43 +1181,78 @@ __device__ __forceinline__ void finish_particle_phased(const params &P, const de
   ft_out = ft;
 }
 
-// The step's tool force from the n per-block partials (8 doubles each: the compensated sums
-// s, c of fc.x, fc.y, ft.x, ft.y), by warp 0 of the last block to finish, in a fixed tree:
-// lane l merges partials l, l + 32, ... in order, then the lanes by a shuffle tree; lane 0
-// stores the force (report_force, output.cu:31-39: contact plus friction force), logs it and
-// closes the step's counters. `predicted`: the next step's predictor ran in this kernel.
-__device__ __forceinline__ void force_sums_last_warp(const params &P, const dev_buffers &D, int n, bool predicted) {
-  __threadfence();
-  ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
-  for (int b = (int)lane_id(); b < n; b += 32) {
-    const volatile double *pr = D.partials + (size_t)b * 8;
-    for (int k = 0; k < 4; ++k) {
-      ksum x{pr[2 * k], pr[2 * k + 1]};
-      ksum_merge(r[k], x);
-    }
-  }
+// The step's tool force from the per-block partials (8 doubles each: the compensated sums s, c
+// of fc.x, fc.y, ft.x, ft.y) in a fixed two-level tree: the partials of each group of
+// FORCE_GROUP consecutive blocks summed by one warp (lane l takes the group's l-th partial,
+// then a shuffle tree), then the group sums by one warp (lane l takes groups l, l + 32, ... in
+// order, then the same tree). In the flat finish kernel the block that completes a group sums
+// it and the block that completes the last group sums the groups: each step of the tree is one
+// load per lane and a shuffle tree, so no block waits long and no warp walks a long chain.
+constexpr int FORCE_GROUP = 32;
+
+__device__ __forceinline__ void ksum4_shuffle_tree(ksum r[4]) {
   for (int o = 16; o > 0; o >>= 1)
     for (int k = 0; k < 4; ++k) {
       ksum x{__shfl_down_sync(0xffffffffu, r[k].s, o), __shfl_down_sync(0xffffffffu, r[k].c, o)};
       ksum_merge(r[k], x);
     }
-  if (lane_id() == 0) {
-    const double Fx = (r[0].s + r[0].c) + (r[2].s + r[2].c);
-    const double Fy = (r[1].s + r[1].c) + (r[3].s + r[3].c);
-    D.force_last[0] = Fx;
-    D.force_last[1] = Fy;
-    const unsigned long long hd = D.st->force_log_head;
-    D.force_log[2 * (hd % FORCE_LOG_CAP)] = Fx;
-    D.force_log[2 * (hd % FORCE_LOG_CAP) + 1] = Fy;
-    D.st->force_log_head = hd + 1;
-    D.st->steps += 1;
-    if (P.verlet) {  // every particle is checked: the next step sorts if one asked for it
-      D.st->sort_now = D.st->want_sort;
-      D.st->want_sort = 0u;
-      D.st->predicted = predicted ? 1u : 0u;
+}
+
+// lane 0: the sum of group g of the nb block partials (read through L2: other blocks wrote them
+// before their fence and ticket)
+__device__ __forceinline__ void force_group_sum(const double *partials, int g, int nb, ksum r[4]) {
+  const int b = g * FORCE_GROUP + (int)lane_id();
+  for (int k = 0; k < 4; ++k) r[k] = ksum{0., 0.};
+  if (b < nb) {
+    const double2 *pr = reinterpret_cast<const double2 *>(partials) + (size_t)b * 4;
+    for (int k = 0; k < 4; ++k) {
+      const double2 v = __ldcg(pr + k);
+      r[k] = ksum{v.x, v.y};
     }
-    D.ticket[0] = 0u;
   }
+  ksum4_shuffle_tree(r);
+}
+
+__device__ __forceinline__ void store_ksum4(double *dst, const ksum r[4]) {
+  for (int k = 0; k < 4; ++k) {
+    dst[2 * k] = r[k].s;
+    dst[2 * k + 1] = r[k].c;
+  }
+}
+
+// lane 0: the sum of the ng group sums
+__device__ __forceinline__ void force_final_sum(const double *gsums, int ng, ksum r[4]) {
+  for (int k = 0; k < 4; ++k) r[k] = ksum{0., 0.};
+  const double2 *pr = reinterpret_cast<const double2 *>(gsums);
+  for (int g = (int)lane_id(); g < ng; g += 32)
+    for (int k = 0; k < 4; ++k) {
+      const double2 v = __ldcg(pr + (size_t)g * 4 + k);
+      ksum x{v.x, v.y};
+      ksum_merge(r[k], x);
+    }
+  ksum4_shuffle_tree(r);
+}
+
+// lane 0 of the warp that finished the sum: report_force (output.cu:31-39: contact plus
+// friction force) into force_last and the log, the step's counters, the tickets re-armed.
+// `predicted`: the next step's predictor ran in this kernel.
+__device__ __forceinline__ void force_close_step(const params &P, const dev_buffers &D, const ksum r[4],
+                                                 bool predicted) {
+  const double Fx = (r[0].s + r[0].c) + (r[2].s + r[2].c);
+  const double Fy = (r[1].s + r[1].c) + (r[3].s + r[3].c);
+  D.force_last[0] = Fx;
+  D.force_last[1] = Fy;
+  const unsigned long long hd = D.st->force_log_head;
+  D.force_log[2 * (hd % FORCE_LOG_CAP)] = Fx;
+  D.force_log[2 * (hd % FORCE_LOG_CAP) + 1] = Fy;
+  D.st->force_log_head = hd + 1;
+  D.st->steps += 1;
+  if (P.verlet) {  // every particle is checked: the next step sorts if one asked for it
+    D.st->sort_now = D.st->want_sort;
+    D.st->want_sort = 0u;
+    D.st->predicted = predicted ? 1u : 0u;
+  }
+  D.ticket[0] = 0u;
 }
 
 // Corrector .. invalidate for all particles plus the tool force (output.cu:31-39): one thread
@@ -1319,10 +1356,29 @@ __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buff
     if (cnt[1]) atomicAdd(&D.st->blanked, cnt[1]);
     if (cnt[2]) atomicAdd(&D.st->out_of_grid, cnt[2]);
     __threadfence();
-    is_last = atomicAdd(&D.ticket[0], 1u) == (unsigned)(bk.n - 1) ? 1u : 0u;
+    const int g = bk.x / FORCE_GROUP;
+    const int gsize = min(FORCE_GROUP, bk.n - g * FORCE_GROUP);
+    is_last = atomicAdd(&D.gticket[g], 1u) == (unsigned)(gsize - 1) ? 1u : 0u;
   }
   if (!__shfl_sync(0xffffffffu, is_last, 0)) return;
-  force_sums_last_warp(P, D, bk.n, false);
+  // this block completed its group: the group's sum, then the group ticket
+  __threadfence();
+  const int g = bk.x / FORCE_GROUP;
+  const int ng = (bk.n + FORCE_GROUP - 1) / FORCE_GROUP;
+  double *gsums = D.partials + (size_t)bk.n * 8;
+  ksum r[4];
+  force_group_sum(D.partials, g, bk.n, r);
+  unsigned last = 0u;
+  if (lane_id() == 0) {
+    store_ksum4(gsums + (size_t)g * 8, r);
+    D.gticket[g] = 0u;
+    __threadfence();
+    last = atomicAdd(&D.ticket[0], 1u) == (unsigned)(ng - 1) ? 1u : 0u;
+  }
+  if (!__shfl_sync(0xffffffffu, last, 0)) return;
+  __threadfence();
+  force_final_sum(gsums, ng, r);
+  if (lane_id() == 0) force_close_step(P, D, r, false);
 }
 
 template <bool FUSE_HASH>
@@ -1455,8 +1511,7 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
   // with neighbour lists the hashes and counts above serve the next step only if it sorts,
   // which is known once every particle has been checked (last block, below)
   const bool block_wants_sort = __syncthreads_or(want_sort);
-  if (threadIdx.x >= 32) return;  // warp 0 closes the block and, in the last block, the step
-  unsigned is_last = 0u;
+  __shared__ unsigned s_last;
   if (threadIdx.x == 0) {
     unsigned long long cnt[3] = {smc[0][0], smc[0][1], smc[0][2]};
     for (int w = 1; w < FINISH_BLOCK / 32; ++w)
@@ -1466,10 +1521,24 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
     if (cnt[1]) atomicAdd(&D.st->blanked, cnt[1]);
     if (cnt[2]) atomicAdd(&D.st->out_of_grid, cnt[2]);
     __threadfence();
-    is_last = atomicAdd(&D.ticket[0], 1u) == gridDim.x - 1 ? 1u : 0u;
+    s_last = atomicAdd(&D.ticket[0], 1u) == gridDim.x - 1 ? 1u : 0u;
   }
-  if (!__shfl_sync(0xffffffffu, is_last, 0)) return;
-  force_sums_last_warp(P, D, n_chunks, fuse);
+  __syncthreads();
+  if (!s_last) return;
+  // the last block: the same two-level tree as k_finish_flat, every group by one of its warps
+  __threadfence();
+  const int ng = (n_chunks + FORCE_GROUP - 1) / FORCE_GROUP;
+  double *gsums = D.partials + (size_t)n_chunks * 8;
+  ksum r[4];
+  for (int g = (int)(threadIdx.x >> 5); g < ng; g += FINISH_BLOCK / 32) {
+    force_group_sum(D.partials, g, n_chunks, r);
+    if (lane_id() == 0) store_ksum4(gsums + (size_t)g * 8, r);
+  }
+  __threadfence_block();
+  __syncthreads();
+  if (threadIdx.x >= 32) return;
+  force_final_sum(gsums, ng, r);
+  if (lane_id() == 0) force_close_step(P, D, r, fuse);
 }
 
 // JC plasticity (actions_gpu.cu:226-285) for the particles the finish kernel listed: the

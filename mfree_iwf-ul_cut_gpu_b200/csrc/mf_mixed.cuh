@@ -108,12 +108,26 @@ __device__ __forceinline__ void mixed_interact(const mixed_i &I, const mixed_con
   if (I.thermal && rr2 > 1e-16f) a.T_lapl = fmaf(volj * (I.T - b3.w), dwr, a.T_lapl);
 }
 
+// Records of the candidates in global memory, read through the read-only path (word k of
+// record j at recf_word(k, j, N)). (A block's candidates staged in shared memory by bulk copies
+// on one mbarrier measured 25-30 % slower on the ~150k-particle cut: fewer resident warps and
+// the copy's wait before any arithmetic, against loads that L1 already served 84 % of.)
+struct rec_global {
+  const float4 *__restrict__ r;
+  int N;
+  __device__ __forceinline__ float4 p0(int j) const { return __ldg(r + recf_word(0, j, N)); }
+  __device__ __forceinline__ void all(int j, float4 &b0, float4 &b1, float4 &b2, float4 &b3) const {
+    b0 = __ldg(r + recf_word(0, j, N)); b1 = __ldg(r + recf_word(1, j, N));
+    b2 = __ldg(r + recf_word(2, j, N)); b3 = __ldg(r + recf_word(3, j, N));
+  }
+};
+
 // Neighbour list of particle q, built on a step that sorted: the candidates within
 // 2 h_i + skin over the 7x7 cells around its own (the 5x5 window widened by one cell, which
 // covers that radius for h_i up to the cell size), blanked ones left out, non-finite ones
 // kept (their pair terms carry the NaN). Columns in x order and each column's range in array
 // order, so the in-support candidates come in the order of the 5x5 window.
-__device__ __forceinline__ int build_list(const dev_buffers &D, const float4 *__restrict__ r0, int q,
+__device__ __forceinline__ int build_list(const dev_buffers &D, const rec_global &REC, int q,
                                           const mixed_i &I, const geom &g, int gi, int gj, float dxc,
                                           float skin) {
   const float R = 2.f * I.h + skin;
@@ -131,7 +145,7 @@ __device__ __forceinline__ int build_list(const dev_buffers &D, const float4 *__
     const float ox = fmaf((float)(gi - ii), dxc, I.x);
     const unsigned tag = (unsigned)(gi - ii + 3) << LIST_INDEX_BITS;
     for (int j = j0; j < j1; ++j) {
-      const float4 b0 = __ldg(r0 + j);
+      const float4 b0 = REC.p0(j);
       const unsigned fjw = (unsigned)__float_as_int(b0.z);
       const float xij = ox - b0.x;
       const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
@@ -160,7 +174,7 @@ __device__ __forceinline__ int build_list(const dev_buffers &D, const float4 *__
 static __global__ void k_list_abs(int N, dev_buffers D, double2 *abs) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= N) return;
-  const float4 b0 = reinterpret_cast<const float4 *>(D.recf)[j];
+  const float4 b0 = reinterpret_cast<const float4 *>(D.recf)[recf_word(0, j, N)];
   const geom g = *D.g;
   const int hj = D.hash_cur[j];
   const int cx = hj / g.ny, cy = hj - cx * g.ny;
@@ -172,10 +186,10 @@ static __global__ void k_list_check(params P, dev_buffers D, const double2 *__re
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.N) return;
   const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
-  const unsigned fi = (unsigned)__float_as_int(r0[i].z) & 0xffu;
+  const unsigned fi = (unsigned)__float_as_int(r0[recf_word(0, i, P.N)].z) & 0xffu;
   if (fi & (FLAG_BLANKED | FLAG_NONFINITE)) return;
   if ((fi & FLAG_TOOL) && P.thermal_solver != MF_THERMAL_BROOKSHAW) return;  // no pair sums
-  const double h = (double)r0[2 * (size_t)P.N + i].w;
+  const double h = (double)r0[recf_word(2, i, P.N)].w;
   const double lim = 4. * h * h * (1. - 1e-5);
   const double2 xi = abs[i];
   const unsigned *row = D.nlist + (size_t)i * LIST_CAP;
@@ -183,7 +197,7 @@ static __global__ void k_list_check(params P, dev_buffers D, const double2 *__re
   unsigned long long pairs = 0, missing = 0;
   for (int j = 0; j < P.N; ++j) {
     if (j == i) continue;
-    const unsigned fj = (unsigned)__float_as_int(r0[j].z);
+    const unsigned fj = (unsigned)__float_as_int(r0[recf_word(0, j, P.N)].z);
     if (fj & (FLAG_BLANKED | FLAG_NONFINITE)) continue;
     const double2 xj = abs[j];
     const double dx = xi.x - xj.x, dy = xi.y - xj.y;
@@ -198,46 +212,21 @@ static __global__ void k_list_check(params P, dev_buffers D, const double2 *__re
   if (missing) atomicAdd(out + 1, missing);
 }
 
-// Records of the candidates: the record planes in global memory (read through the read-only
-// path), or a block's staged copy of them in shared memory (STAGE_CAP entries per plane).
-struct rec_global {
-  const float4 *__restrict__ r0, *__restrict__ r1, *__restrict__ r2, *__restrict__ r3;
-  __device__ __forceinline__ float4 p0(int j) const { return __ldg(r0 + j); }
-  __device__ __forceinline__ void all(int j, float4 &b0, float4 &b1, float4 &b2, float4 &b3) const {
-    b0 = __ldg(r0 + j); b1 = __ldg(r1 + j); b2 = __ldg(r2 + j); b3 = __ldg(r3 + j);
-  }
-};
-
-#ifndef MF_STAGE_CAP
-#define MF_STAGE_CAP 1024
-#endif
-constexpr int STAGE_CAP = MF_STAGE_CAP;              // staged candidates per block
-constexpr int STAGE_BYTES = 4 * STAGE_CAP * 16;      // four planes of float4
-
-struct rec_staged {
-  const float4 *s;  // plane k at s[k * STAGE_CAP + j]
-  __device__ __forceinline__ float4 p0(int j) const { return s[j]; }
-  __device__ __forceinline__ void all(int j, float4 &b0, float4 &b1, float4 &b2, float4 &b3) const {
-    b0 = s[j]; b1 = s[STAGE_CAP + j]; b2 = s[2 * STAGE_CAP + j]; b3 = s[3 * STAGE_CAP + j];
-  }
-};
-
 // The i particle of slot q: its records and the constants of its sums. False when q has no
 // pair sums (past the end, blanked, a tool particle without Brookshaw heat).
 __device__ __forceinline__ bool mixed_begin(const params &P, const dev_buffers &D, int q, mixed_i &I,
                                             mixed_const &K, double &thermal_alpha) {
   if (q >= P.N) return false;
-  // record planes (structure of arrays): plane k of particle j at [k * N + j]
   const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
-  const float4 a0 = __ldg(r0 + q);  // x, y, flags|cy, vx
+  const float4 a0 = __ldg(r0 + recf_word(0, q, P.N));  // x, y, flags|cy, vx
   const unsigned fi = (unsigned)__float_as_int(a0.z) & 0xffu;
   if (fi & FLAG_BLANKED) return false;
   const bool tool_i = fi & FLAG_TOOL;
   const bool brookshaw = P.thermal_solver == MF_THERMAL_BROOKSHAW;
   if (!brookshaw && tool_i) return false;
-  const float4 a1 = __ldg(r0 + P.N + q);          // vy, sxx, sxy, syy
-  const float4 a2 = __ldg(r0 + 2 * P.N + q);      // Rxx, Rxy, Ryy, h
-  const float4 a3 = __ldg(r0 + 3 * P.N + q);      // rho, c, vol, T - T_init
+  const float4 a1 = __ldg(r0 + recf_word(1, q, P.N));  // vy, sxx, sxy, syy
+  const float4 a2 = __ldg(r0 + recf_word(2, q, P.N));  // Rxx, Rxy, Ryy, h
+  const float4 a3 = __ldg(r0 + recf_word(3, q, P.N));  // rho, c, vol, T - T_init
 
   K.inv_wdeltap = (float)(1. / P.corr.wdeltap);
   K.alpha = (float)P.corr.alpha;
@@ -346,8 +335,7 @@ __device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_b
   mixed_const K;
   double thermal_alpha;
   if (!mixed_begin(P, D, q, I, K, thermal_alpha)) return;
-  const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
-  const rec_global R{r0, r0 + P.N, r0 + 2 * (size_t)P.N, r0 + 3 * (size_t)P.N};
+  const rec_global R{reinterpret_cast<const float4 *>(D.recf), P.N};
 
   const geom g = *D.g;
   const float dxc = (float)g.dx;
@@ -364,7 +352,7 @@ __device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_b
     // support test as a window candidate. A particle's row is contiguous: four entries per
     // 16-byte load; an entry past the count reads the particle's own record (always valid,
     // so the loads need no guard) and is skipped.
-    const int cnt = D.st->sort_now ? build_list(D, r0, q, I, g, gi, gj, dxc, P.skin) : D.ncount[q];
+    const int cnt = D.st->sort_now ? build_list(D, R, q, I, g, gi, gj, dxc, P.skin) : D.ncount[q];
     const uint4 *row = reinterpret_cast<const uint4 *>(D.nlist + (size_t)q * LIST_CAP);
     uint4 e4 = row[0];  // (a row is LIST_CAP entries: the first four are always there)
     for (int k0 = 0; k0 < cnt; k0 += 4) {
@@ -408,188 +396,11 @@ __device__ __forceinline__ void pair_mixed_body(const params &P, const dev_buffe
   pair_mixed_particle<LIST>(P, D, bk.x * blockDim.x + threadIdx.x);
 }
 
-#ifndef MF_PAIR_SM_MAJOR
-#define MF_PAIR_SM_MAJOR 0
-#endif
-// Block b of a grid of W * S blocks (S = the device's SM count) takes chunk (b mod S) W + b / S.
-// When the hardware hands out blocks to the SMs in turn, the blocks resident on one SM at the
-// same time (b, b + S, b + 2 S, ...) then take consecutive chunks of the sorted particles, and
-// their neighbour windows overlap in that SM's L1.
-__device__ __forceinline__ blk sm_major_blk(int sms) {
-  const int w = (int)gridDim.x / sms;
-  return blk{(int)(blockIdx.x % (unsigned)sms) * w + (int)(blockIdx.x / (unsigned)sms), (int)gridDim.x};
-}
-
 template <bool LIST>
 static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, dev_buffers D) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
-  pair_mixed_body<LIST>(P, D, MF_PAIR_SM_MAJOR ? sm_major_blk(P.sm_count) : grid_blk());
-}
-
-// ---- window form with the block's candidates staged in shared memory by bulk copies ----
-//
-// The block's particles (consecutive sorted slots) lie in at most two cell columns (groups);
-// for group k in column c_k with cell rows r_min .. r_max, its particles' windows together are
-// the rows r_min - 2 .. r_max + 2 of the columns c_k - 2 .. c_k + 2, and each of those five
-// row spans is one contiguous range of the sorted records. Up to ten ranges (four planes each)
-// are copied into shared memory by the tensor memory accelerator, one bulk copy per range and
-// plane, completing on one mbarrier; each particle then reads its candidates there instead of
-// through L1/L2. A block whose particles span more than two columns, or whose ranges hold more
-// than STAGE_CAP records, reads from global memory as k_pair_mixed does. Same candidates in
-// the same order, so the sums are those of k_pair_mixed bit for bit.
-struct stage_table {
-  int g0[10], n[10], s0[10];  // per (group, column offset): first record, count, staged position
-  int gi0;                    // the column of group 0
-  int ok;                     // 1: staged; 0: read from global memory
-  int rmin[2], rmax[2];       // cell rows of each group
-};
-
-__device__ __forceinline__ unsigned smem_u32(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-
-// bounded wait for phase 0 of the mbarrier: false if it did not complete in `limit` polls
-__device__ __forceinline__ bool mbar_wait_phase0(unsigned long long *bar, long limit) {
-  const unsigned a = smem_u32(bar);
-  for (long it = 0; it < limit; ++it) {
-    unsigned done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(0u)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void pair_mixed_staged_body(const params &P, const dev_buffers &D, blk bk,
-                                                       float4 *s_rec) {
-  __shared__ stage_table T;
-  __shared__ __align__(8) unsigned long long s_bar;
-  const int q0 = bk.x * (int)blockDim.x;
-  if (q0 >= P.N) return;  // (a block past the last particle: the whole block leaves)
-  const geom g = *D.g;
-  const int q = q0 + (int)threadIdx.x;
-  if (threadIdx.x == 0) {
-    T.gi0 = __ldg(D.hash_cur + q0) / g.ny;
-    T.ok = 1;
-    T.rmin[0] = T.rmin[1] = 0x7fffffff;
-    T.rmax[0] = T.rmax[1] = -1;
-  }
-  __syncthreads();
-  int gi = 0, gj = 0;
-  if (q < P.N) {
-    const int h = __ldg(D.hash_cur + q);
-    gi = h / g.ny;
-    gj = h - gi * g.ny;
-    const int grp = gi - T.gi0;
-    if (grp < 0 || grp > 1) {
-      T.ok = 0;
-    } else {
-      atomicMin(&T.rmin[grp], gj);
-      atomicMax(&T.rmax[grp], gj);
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int total = 0;
-    for (int k = 0; k < 10; ++k) {
-      const int grp = k / 5;
-      const int col = T.gi0 + grp + (k % 5) - 2;
-      int j0 = 0, j1 = 0;
-      if (T.rmax[grp] >= 0 && col >= 0 && col < g.nx) {
-        const int lo = max(T.rmin[grp] - 2, 0), hi = min(T.rmax[grp] + 3, g.ny);
-        j0 = __ldg(D.off + col * g.ny + lo);
-        j1 = __ldg(D.off + col * g.ny + hi);
-      }
-      T.g0[k] = j0;
-      T.n[k] = j1 - j0;
-      T.s0[k] = total;
-      total += j1 - j0;
-    }
-    if (total > STAGE_CAP || total == 0) T.ok = 0;
-    if (T.ok) {
-      const unsigned bar = smem_u32(&s_bar);
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-      unsigned long long state;
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
-                   : "=l"(state)
-                   : "r"(bar), "r"((unsigned)total * 64u)
-                   : "memory");
-      (void)state;
-      const float4 *src = reinterpret_cast<const float4 *>(D.recf);
-      for (int k = 0; k < 10; ++k) {
-        if (T.n[k] == 0) continue;
-        for (int pl = 0; pl < 4; ++pl) {
-          const float4 *from = src + (size_t)pl * P.N + T.g0[k];
-          const unsigned to = smem_u32(s_rec + pl * STAGE_CAP + T.s0[k]);
-          asm volatile(
-              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(to),
-              "l"(from), "r"((unsigned)T.n[k] * 16u), "r"(bar)
-              : "memory");
-        }
-      }
-    }
-  }
-  __syncthreads();
-  const bool staged = T.ok;
-  if (staged && !mbar_wait_phase0(&s_bar, 1L << 22)) {
-    // the copies did not complete: report it, give them a second bounded wait so that none is
-    // still writing when the block exits, and leave this block's rates unwritten
-    if (threadIdx.x == 0) atomicOr(&D.st->error_flags, ERR_STAGE_WAIT);
-    mbar_wait_phase0(&s_bar, 1L << 22);
-    return;
-  }
-  mixed_i I;
-  mixed_const K;
-  double thermal_alpha;
-  if (!mixed_begin(P, D, q, I, K, thermal_alpha)) return;
-  const float dxc = (float)g.dx;
-  mixed_acc acc;
-  acc.vd01 = acc.vd23 = acc.sd_xw = acc.sd_zy = acc.vt = acc.xt = f2(0.f, 0.f);
-  acc.T_lapl = 0.f;
-  const int low_i = gi - 2 < 0 ? 0 : gi - 2;
-  const int low_j = gj - 2 < 0 ? 0 : gj - 2;
-  const int high_i = gi + 3 > g.nx ? g.nx : gi + 3;
-  const int high_j = gj + 3 > g.ny ? g.ny : gj + 3;
-  if (staged) {
-    const rec_staged R{s_rec};
-    const int kb = (gi - T.gi0) * 5 - (gi - 2);  // range of column ii: kb + ii
-    for (int ii = low_i; ii < high_i; ++ii) {
-      const int col = ii * g.ny;
-      const int k = kb + ii;
-      const int d = T.s0[k] - T.g0[k];  // staged position = record index + d
-      const int j0 = __ldg(D.off + col + low_j) + d;
-      const int j1 = __ldg(D.off + col + high_j) + d;
-      mixed_column(R, j0, j1, fmaf((float)(gi - ii), dxc, I.x), gj, dxc, I, K, acc);
-    }
-  } else {
-    const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
-    const rec_global R{r0, r0 + P.N, r0 + 2 * (size_t)P.N, r0 + 3 * (size_t)P.N};
-    for (int ii = low_i; ii < high_i; ++ii) {
-      const int col = ii * g.ny;
-      const int j0 = __ldg(D.off + col + low_j);
-      const int j1 = __ldg(D.off + col + high_j);
-      mixed_column(R, j0, j1, fmaf((float)(gi - ii), dxc, I.x), gj, dxc, I, K, acc);
-    }
-  }
-  mixed_end(P, D, q, I, acc, thermal_alpha);
-}
-
-#ifndef MF_STAGED_BLOCKS_PER_SM
-#define MF_STAGED_BLOCKS_PER_SM 3
-#endif
-static __global__ void __launch_bounds__(PAIR_BLOCK, MF_STAGED_BLOCKS_PER_SM) k_pair_mixed_staged(params P,
-                                                                                                  dev_buffers D) {
-  MF_PDL_WAIT();
-  MF_PDL_TRIGGER();
-  extern __shared__ __align__(128) float4 s_dyn[];
-  pair_mixed_staged_body(P, D, MF_PAIR_SM_MAJOR ? sm_major_blk(P.sm_count) : grid_blk(), s_dyn);
+  pair_mixed_body<LIST>(P, D, grid_blk());
 }
 
 // PSE heat Laplacian (interactions_gpu.cu:88-144, kernels.cuh:72-89) in FP32 for the mixed
@@ -599,14 +410,12 @@ static __global__ void __launch_bounds__(PAIR_BLOCK, MF_STAGED_BLOCKS_PER_SM) k_
 __device__ __forceinline__ void pse_mixed_body(const params &P, const dev_buffers &D, blk bk) {
   const int q = bk.x * blockDim.x + threadIdx.x;
   if (q >= P.N) return;
-  const float4 *__restrict__ r0 = reinterpret_cast<const float4 *>(D.recf);
-  const float4 *__restrict__ r2 = r0 + 2 * (size_t)P.N;
-  const float4 *__restrict__ r3 = r0 + 3 * (size_t)P.N;
-  const float4 a0 = __ldg(r0 + q);  // x, y, flags|cy, vx
+  const float4 *__restrict__ r = reinterpret_cast<const float4 *>(D.recf);
+  const float4 a0 = __ldg(r + recf_word(0, q, P.N));  // x, y, flags|cy, vx
   const unsigned fi = (unsigned)__float_as_int(a0.z) & 0xffu;
   if (fi & FLAG_BLANKED) return;
-  const float hi = __ldg(r2 + q).w;
-  const float Ti = __ldg(r3 + q).w;
+  const float hi = __ldg(r + recf_word(2, q, P.N)).w;
+  const float Ti = __ldg(r + recf_word(3, q, P.N)).w;
   const long long tex_elems = ((long long)sizeof(int) * P.N) / 8;
   const bool tool_i = q < tex_elems ? (fi & FLAG_TOOL) != 0 : false;
   const double alpha = tool_i ? P.trml_tool.alpha : P.trml_wp.alpha;
@@ -629,8 +438,8 @@ __device__ __forceinline__ void pse_mixed_body(const params &P, const dev_buffer
     const float ox = (float)(gi - ii) * dxc + a0.x;
 #pragma unroll 4
     for (int j = j0; j < j1; ++j) {
-      const float4 b0 = __ldg(r0 + j);
-      const float4 b3 = __ldg(r3 + j);  // rho, c, vol, T - T_init
+      const float4 b0 = __ldg(r + recf_word(0, j, P.N));
+      const float4 b3 = __ldg(r + recf_word(3, j, P.N));  // rho, c, vol, T - T_init
       const float xij = ox - b0.x;
       const float yij = fmaf((float)(gj - (int)((unsigned)__float_as_int(b0.z) >> 8)), dxc, a0.y - b0.y);
       const float w2 = coef * __expf(-(xij * xij + yij * yij) * inv_h2);
