@@ -34,14 +34,12 @@ enum : int {
   F_WIDTH
 };
 
-#ifndef MF_REC_AOS
-#define MF_REC_AOS 0
-#endif
-// index of float4 word k (0..3) of particle j's FP32 pair record among N records: four planes
-// (word k of every particle together, at k N + j), or with MF_REC_AOS each particle's 64 bytes
-// together (at 4 j + k)
+// index of float4 word k (0..3) of particle j's FP32 pair record among N records: four planes,
+// word k of every particle together at k N + j. (Each particle's 64 bytes together, at 4 j + k,
+// measured 68 % slower in the list pair kernel: a warp's 16-byte loads then touch four times as
+// many cache lines, and L1 throughput becomes the limit.)
 __host__ __device__ __forceinline__ size_t recf_word(int k, int j, int N) {
-  return MF_REC_AOS ? (size_t)4 * (size_t)j + (size_t)k : (size_t)k * (size_t)N + (size_t)j;
+  return (size_t)k * (size_t)N + (size_t)j;
 }
 
 struct params {
