@@ -89,6 +89,9 @@ struct dev_status {
   unsigned int sort_now;     // neighbour lists: this step sorts (set by the previous step)
   unsigned int want_sort;    // neighbour lists: a particle's next predicted position is more
                              // than 0.45 skin from where its list was built
+  unsigned int sorted_prev;  // the last step sorted the cell list: the set this step writes
+                             // holds the order of two steps ago, so this step's reorder writes
+                             // the order, particle numbers and smoothing lengths again
   unsigned int predicted;    // neighbour lists: the last finish kernel also ran the next step's
                              // predictor (it did not follow a sort); the next step, if it does
                              // not sort, skips the reorder kernel

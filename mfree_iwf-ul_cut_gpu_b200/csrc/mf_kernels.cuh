@@ -484,6 +484,15 @@ __device__ __forceinline__ void predict_particle(const params &P, const dev_buff
   }
 }
 
+// the last step's contact and friction forces of the particle at slot q (start-of-step slot p):
+// from the step's start set (the Rothlin grid does not gather ft: it stays in place,
+// grid_gpu_rothlin.cu:138-250)
+__device__ __forceinline__ void prev_contact_forces(const params &P, const dev_buffers &D, int q, int p,
+                                                    double2 &fc, double2 &ft) {
+  fc = D.A.fc[p];
+  ft = D.A.ft[P.grid_kind == MF_GRID_GREEN ? p : q];
+}
+
 // The rigid tool of this step: tool::update_tool (tool.cpp:211-221) with IEEE-rounded
 // operations (bitwise equal to the host's double arithmetic), by warp 0 of block 0 of the
 // step's reorder/predictor kernel: tool_prev copied to tool_next word by word, then lane
@@ -555,9 +564,15 @@ __device__ __forceinline__ void reorder_body(const params &P, const dev_buffers 
   }
   const state_set &A = D.A;
   const state_set &B = D.B;
-  D.perm[q] = p;
-  B.idx[q] = P.grid_kind == MF_GRID_GREEN ? p : A.idx[p];
-  B.id[q] = A.id[p];
+  // the order, numbers and smoothing lengths: unchanged on a step that keeps the order after a
+  // step that kept it too (neighbour lists), when this step's set already holds them from two
+  // steps ago
+  const bool moved = sort || !PREDICT || P.staged || D.st->sorted_prev;
+  if (moved) {
+    D.perm[q] = p;
+    B.idx[q] = P.grid_kind == MF_GRID_GREEN ? p : A.idx[p];
+    B.id[q] = A.id[p];
+  }
 
   double2 pos = A.pos[p], vel = A.vel[p];
   double4 S = A.S[p];
@@ -569,10 +584,15 @@ __device__ __forceinline__ void reorder_body(const params &P, const dev_buffers 
   const double h = A.h[p];
   B.eps_pl[q] = A.eps_pl[p];
   B.eps_pl_dot[q] = A.eps_pl_dot[p];
-  B.fc[q] = A.fc[p];
-  // the Rothlin grid does not gather ft (grid_gpu_rothlin.cu:138-250): it stays in place
-  B.ft[q] = P.grid_kind == MF_GRID_GREEN ? A.ft[p] : A.ft[q];
-  B.h[q] = h;
+  if (!PREDICT || P.staged) {
+    // the last step's contact forces: within a step the pair and finish kernels read them from
+    // the start set (prev_contact_forces); a sort outside a step, or a staged step whose
+    // intermediate state is read back, moves them too
+    B.fc[q] = A.fc[p];
+    // the Rothlin grid does not gather ft (grid_gpu_rothlin.cu:138-250): it stays in place
+    B.ft[q] = P.grid_kind == MF_GRID_GREEN ? A.ft[p] : A.ft[q];
+  }
+  if (moved) B.h[q] = h;
   if (!PREDICT) {  // a sort outside a step: the state moves as it is
     B.pos_t[q] = pos_t;
     B.vel_t[q] = vel_t;
@@ -648,6 +668,7 @@ __device__ __forceinline__ void pair_fp64_particle(const params &P, const dev_bu
 
   const geom g = *D.g;
   const int hashi = D.hash_cur[q];
+  const int p = __ldg(D.perm + q);  // the start slot (last contact forces), loaded during the sums
   const int gi = hashi / g.ny;
   const int gj = hashi - gi * g.ny;
   const int low_i = gi - 2 < 0 ? 0 : gi - 2;
@@ -750,7 +771,8 @@ __device__ __forceinline__ void pair_fp64_particle(const params &P, const dev_bu
     jaumann(P.phys.G, vdx, vdy, vdz, vdw, S.x, S.y, S.z, S.w, tx, ty, tz, tw);
     B.S_t[q] = make_double4(tx, ty, tz, tw);
     B.rho_t[q] = -rhoi * (vdx + vdw);
-    const double2 fc = B.fc[q], ft = B.ft[q];
+    double2 fc, ft;
+    prev_contact_forces(P, D, q, p, fc, ft);
     double2 vel_t;
     vel_t.x = vtx + (sdx + sdy + fc.x / mass + ft.x / mass);
     vel_t.y = vty + (sdz + sdw + fc.y / mass + ft.y / mass);
@@ -847,7 +869,8 @@ __device__ __forceinline__ void finish_particle(const params &P, const dev_buffe
   const double4 S_t = B.S_t[q];
   const double rho_t = B.rho_t[q], T_t = B.T_t[q];
   double eps_pl = B.eps_pl[q], eps_pl_dot = B.eps_pl_dot[q];
-  double2 fc = B.fc[q], ft = B.ft[q];
+  double2 fc, ft;
+  prev_contact_forces(P, D, q, p, fc, ft);
   const double2 normal = D.n[q];
   const double pr = B.pp[q];
   double2 pos = A.pos[p], vel = A.vel[p];
@@ -1035,7 +1058,8 @@ __device__ __forceinline__ void finish_particle_phased(const params &P, const de
   // phase 1: kinematics
   double2 pos = A.pos[p], vel = A.vel[p];
   double2 pos_t = B.pos_t[q], vel_t = B.vel_t[q];
-  double2 fc = B.fc[q], ft = B.ft[q];
+  double2 fc, ft;
+  prev_contact_forces(P, D, q, p, fc, ft);
   if (!blanked) {  // correct (leap_frog.cu:68-92)
     pos.x = pos.x + dt * pos_t.x;
     pos.y = pos.y + dt * pos_t.y;
@@ -1237,7 +1261,7 @@ __device__ __forceinline__ void force_final_sum(const double *gsums, int ng, ksu
 // friction force) into force_last and the log, the step's counters, the tickets re-armed.
 // `predicted`: the next step's predictor ran in this kernel.
 __device__ __forceinline__ void force_close_step(const params &P, const dev_buffers &D, const ksum r[4],
-                                                 bool predicted) {
+                                                 bool predicted, bool sorted) {
   const double Fx = (r[0].s + r[0].c) + (r[2].s + r[2].c);
   const double Fy = (r[1].s + r[1].c) + (r[3].s + r[3].c);
   D.force_last[0] = Fx;
@@ -1252,6 +1276,7 @@ __device__ __forceinline__ void force_close_step(const params &P, const dev_buff
     D.st->want_sort = 0u;
     D.st->predicted = predicted ? 1u : 0u;
   }
+  D.st->sorted_prev = sorted ? 1u : 0u;
   D.ticket[0] = 0u;
 }
 
@@ -1378,7 +1403,7 @@ __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buff
   if (!__shfl_sync(0xffffffffu, last, 0)) return;
   __threadfence();
   force_final_sum(gsums, ng, r);
-  if (lane_id() == 0) force_close_step(P, D, r, false);
+  if (lane_id() == 0) force_close_step(P, D, r, false, !identity);
 }
 
 template <bool FUSE_HASH>
@@ -1538,7 +1563,7 @@ __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(p
   __syncthreads();
   if (threadIdx.x >= 32) return;
   force_final_sum(gsums, ng, r);
-  if (lane_id() == 0) force_close_step(P, D, r, fuse);
+  if (lane_id() == 0) force_close_step(P, D, r, fuse, !identity);
 }
 
 // JC plasticity (actions_gpu.cu:226-285) for the particles the finish kernel listed: the

@@ -282,7 +282,7 @@ __device__ __forceinline__ void mixed_column(const REC &R, int j0, int j1, float
 
 // the rates of slot q from its pair sums: Jaumann stress rate, continuity, momentum, advection
 // and heat (actions_gpu.cu:100-132, interactions_gpu.cu:331-345)
-__device__ __forceinline__ void mixed_end(const params &P, const dev_buffers &D, int q, const mixed_i &I,
+__device__ __forceinline__ void mixed_end(const params &P, const dev_buffers &D, int q, int p, const mixed_i &I,
                                           const mixed_acc &acc, double thermal_alpha) {
   const float mass = (float)P.phys.mass;
   const float m_eps = (float)P.corr.xspheps * mass;
@@ -314,7 +314,8 @@ __device__ __forceinline__ void mixed_end(const params &P, const dev_buffers &D,
     const float tw = -g2 * t3;
     B.S_t[q] = make_double4(tx, ty, tz, tw);
     B.rho_t[q] = -(double)rhoi * (double)(vdx + vdw);
-    const double2 fc = B.fc[q], ft = B.ft[q];
+    double2 fc, ft;
+    prev_contact_forces(P, D, q, p, fc, ft);
     const double m = P.phys.mass;
     const double2 vp = B.vel[q];
     B.vel_t[q] = make_double2((double)(vtx + (sdx + sdy)) + fc.x / m + ft.x / m,
@@ -336,6 +337,11 @@ __device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_b
   double thermal_alpha;
   if (!mixed_begin(P, D, q, I, K, thermal_alpha)) return;
   const rec_global R{reinterpret_cast<const float4 *>(D.recf), P.N};
+  // the particle's slot at the start of the step (its last contact forces are read there at the
+  // end): loaded now, so that the load's latency passes during the sums; a list step without a
+  // sort keeps the order
+  const bool sorting = !LIST || D.st->sort_now;
+  const int p = sorting ? __ldg(D.perm + q) : q;
 
   const geom g = *D.g;
   const float dxc = (float)g.dx;
@@ -352,7 +358,7 @@ __device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_b
     // support test as a window candidate. A particle's row is contiguous: four entries per
     // 16-byte load; an entry past the count reads the particle's own record (always valid,
     // so the loads need no guard) and is skipped.
-    const int cnt = D.st->sort_now ? build_list(D, R, q, I, g, gi, gj, dxc, P.skin) : D.ncount[q];
+    const int cnt = sorting ? build_list(D, R, q, I, g, gi, gj, dxc, P.skin) : D.ncount[q];
     const uint4 *row = reinterpret_cast<const uint4 *>(D.nlist + (size_t)q * LIST_CAP);
     uint4 e4 = row[0];  // (a row is LIST_CAP entries: the first four are always there)
     for (int k0 = 0; k0 < cnt; k0 += 4) {
@@ -387,7 +393,7 @@ __device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_b
       mixed_column(R, j0, j1, fmaf((float)(gi - ii), dxc, I.x), gj, dxc, I, K, acc);
     }
   }
-  mixed_end(P, D, q, I, acc, thermal_alpha);
+  mixed_end(P, D, q, p, I, acc, thermal_alpha);
 }
 
 // the mixed pair sums of block bk.x's particles
