@@ -112,6 +112,11 @@ def test_lists_track_sorting_every_step_long(mf):
         assert rel_err(by_id(a, f), by_id(b, f)) < 1e-3, (f, rel_err(by_id(a, f), by_id(b, f)), sa["sorts"])
     fa, fb = a.force_log(), b.force_log()
     assert rel_err(fa.mean(axis=0), fb.mean(axis=0)) < 1e-4
+    # the fields a list step without a sort does not rewrite (order, numbers, smoothing lengths)
+    # after sorts and runs of steps without one: every particle still carries its own
+    assert np.array_equal(np.sort(a.get("id")), np.arange(st["N"]))
+    assert np.array_equal(by_id(a, "h"), by_id(b, "h"))
+    assert np.array_equal(by_id(a, "tool_p"), by_id(b, "tool_p"))
 
 
 def test_sorts_every_step_outside_list_mode(mf):
