@@ -81,11 +81,10 @@ struct mf_ctx {
   bool last_staged = false; // the last predictor ran staged (all intermediates stored)
   int scan_tiles = 0;   // tiles for max_cell + 1 entries
   int *tsum[2] = {nullptr, nullptr};  // per-tile count totals: written with one parity, read with the other
-  int finish_blocks = 0;
   int bbox_blocks = 0;
   int sm_count = 148;
   mf_tool_state *tool_buf[2] = {nullptr, nullptr};  // tool after the last step, by parity
-  // k_finish of the last step already hashed and counted the particles for the next one
+  // k_finish_flat of the last step already hashed and counted the particles for the next one
   // (locked grid): the next step starts at the scan
   bool counts_ready = false;
   double skin = 0.;  // neighbour-list skin (mixed form); <= 0: a tenth of the cell size
@@ -170,7 +169,7 @@ int alloc_set(mf_ctx *ctx, state_set &s, int N) {
   return MF_OK;
 }
 
-// the counts the last step's k_finish prepared are stale once the host changes the state
+// the counts the last step's k_finish_flat prepared are stale once the host changes the state
 int invalidate_counts(mf_ctx *ctx) {
   if (ctx->counts_ready && ctx->D.count) {
     CK(cudaMemsetAsync(ctx->D.count, 0, sizeof(int) * (size_t)ctx->G.max_cell, ctx->stream));
@@ -200,7 +199,6 @@ int alloc_particles(mf_ctx *ctx, int N) {
   TRY(dalloc(ctx, L, &D.nlist, (size_t)LIST_CAP * N));
   TRY(dalloc(ctx, L, &D.ncount, N));
   TRY(dalloc(ctx, L, &D.pos_build, N));
-  ctx->finish_blocks = std::min((N + FINISH_BLOCK - 1) / FINISH_BLOCK, ctx->sm_count * FINISH_BLOCKS_PER_SM);
   ctx->bbox_blocks = std::min((N + BLOCK - 1) / BLOCK, ctx->sm_count * 4);
   // per-chunk force partials of the finish kernel and their group sums (or per-block partials of
   // the bbox pass), the force sum's group tickets
@@ -244,7 +242,7 @@ void bind_sets(mf_ctx *ctx) {
   ctx->D.tsum_w = ctx->tsum[ctx->cur];
 }
 
-// the steady-state step of a locked grid starts at the scan: the previous step's k_finish
+// the steady-state step of a locked grid starts at the scan: the previous step's k_finish_flat
 // hashed and counted the particles
 bool fused_step(const mf_ctx *ctx) { return ctx->G.locked && !ctx->P.staged; }
 
@@ -351,15 +349,18 @@ int launch_stage(mf_ctx *ctx, int stage) {
       }
       break;
     case 3:
-      if (ctx->P.fuse) {  // the next step's predictor runs here too: the whole state at once
-        if (fused_step(ctx))
-          TRY(launch_pdl(ctx, k_finish<true>, ctx->finish_blocks, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
-        else
-          TRY(launch_pdl(ctx, k_finish<false>, ctx->finish_blocks, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
-      } else {
+      {
         const int fb = (N + FINISH_BLOCK - 1) / FINISH_BLOCK;
-        if (fused_step(ctx)) TRY(launch_pdl(ctx, k_finish_flat<true>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
-        else TRY(launch_pdl(ctx, k_finish_flat<false>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+        if (ctx->P.fuse) {  // the next step's predictor runs here too
+          if (fused_step(ctx))
+            TRY(launch_pdl(ctx, k_finish_flat<true, true>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+          else
+            TRY(launch_pdl(ctx, k_finish_flat<false, true>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+        } else if (fused_step(ctx)) {
+          TRY(launch_pdl(ctx, k_finish_flat<true, false>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+        } else {
+          TRY(launch_pdl(ctx, k_finish_flat<false, false>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+        }
       }
       if (ctx->P.plastic) {
         if (ctx->P.jc_model == MF_JC_TANH)
@@ -381,7 +382,7 @@ int launch_step(mf_ctx *ctx) {
   return MF_OK;
 }
 
-// hash + count for the first fused step (afterwards each step's k_finish prepares them)
+// hash + count for the first fused step (afterwards each step's k_finish_flat prepares them)
 int prime_counts(mf_ctx *ctx) {
   if (!fused_step(ctx) || ctx->counts_ready) return MF_OK;
   bind_sets(ctx);
@@ -511,7 +512,6 @@ int mf_ctx_create(int device, mf_ctx **out) {
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.g, 1);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.st, 1);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.plastic_count, 1);
-  if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->D.finish_chunk, 1);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->tool_buf[0], 1);
   if (rc == MF_OK) rc = dalloc(ctx, ctx->fixed_allocs, &ctx->tool_buf[1], 1);
   if (rc == MF_OK) {

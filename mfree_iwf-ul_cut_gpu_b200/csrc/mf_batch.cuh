@@ -121,7 +121,7 @@ static __global__ void __launch_bounds__(FINISH_BLOCK, 2) kb_finish(batch_map M)
   MF_PDL_TRIGGER();
   __shared__ batch_entry s;
   const blk b = batch_block(M, s);
-  finish_flat_body<true>(s.P, s.D, s.scan_tiles, b);
+  finish_flat_body<true, false>(s.P, s.D, s.scan_tiles, b);
 }
 
 template <bool PAIRED>

@@ -3,23 +3,24 @@
 // Per step, on one stream (captured once into a CUDA graph):
 //   k_bbox        adaptive grid only: min/max reduction -> geometry     (grid.cu:97-136)
 //   k_hash_count  cell hash per particle + atomic per-cell count       (grid.cu:34-51);
-//                 with a locked grid only before the first step, after that k_finish of
-//                 the previous step has done it
-//   k_scan        single-pass decoupled look-back exclusive scan of the
-//                 counts -> cell offsets (the cell_start/cell_end lists)
+//                 with a locked grid only before the first step, after that k_finish_flat
+//                 of the previous step has done it
+//   k_scan        exclusive scan of the counts -> cell offsets (the cell_start/cell_end
+//                 lists), each tile starting from the preceding tiles' totals
 //   k_scatter     particle -> slot inside its cell (atomic cursor per cell)
 //   k_reorder     stable rank fix-up inside each cell (equal to thrust's stable sort_by_key),
 //                 gather of the persistent state into the other buffer, and - in a step - the
-//                 predictor, EOS, artificial stress and the neighbour pair records
-//                 (grid_gpu_green.cu:22-116, leap_frog.cu:30-66, actions_gpu.cu:41-97)
+//                 predictor, EOS, artificial stress, the neighbour pair records and the rigid
+//                 tool's advance (grid_gpu_green.cu:22-116, leap_frog.cu:30-66,
+//                 actions_gpu.cu:41-97, tool.cpp:211-221)
 //   k_pair_fp64   the pair sums over the 5x5 cell window (interactions_gpu.cu:147-345) and the
 //                 rates: Jaumann, continuity, momentum, advection (actions_gpu.cu:99-224)
 //   k_pse         PSE heat Laplacian (interactions_gpu.cu:88-144), PSE solver only
-//   k_finish      corrector, friction heat, JC plasticity, the rigid tool's advance, tool
-//                 particles, contact, boundary conditions, invalidation and the compensated
-//                 tool-force reduction; with a locked grid also the next step's hashes and
-//                 counts (leap_frog.cu:68-92, actions_gpu.cu:135-162,226-349, tool.cpp:211-221,
-//                 tool_gpu.cu:151-221, output.cu:31-39)
+//   k_finish_flat corrector, friction heat, the JC elastic test, tool particles, contact,
+//                 boundary conditions, invalidation and the compensated tool-force reduction;
+//                 with a locked grid also the next step's hashes and counts (leap_frog.cu:68-92,
+//                 actions_gpu.cu:135-162,226-349, tool_gpu.cu:151-221, output.cu:31-39)
+//   k_plastic     the JC return map of the particles the elastic test did not settle
 #pragma once
 
 #include "mf_device.cuh"
@@ -66,14 +67,13 @@ struct dev_buffers {
   double *force_last;   // 2
   plastic_item *plastic_list;  // particles whose return map k_plastic runs (this step)
   unsigned *plastic_count;
-  unsigned *finish_chunk;     // next chunk of the finish kernel (zeroed by the reorder)
   // neighbour lists (mixed form): entry k of particle q at nlist[q * LIST_CAP + k], ncount[q]
   // entries; pos_build[q] the predicted position the list was built from
   unsigned *nlist;
   int *ncount;
   double2 *pos_build;
   mf_tool_state *tool_prev;  // tool after the previous step (read)
-  mf_tool_state *tool_next;  // tool after this step (written by k_finish)
+  mf_tool_state *tool_next;  // tool after this step (written by k_reorder, read by k_finish_flat)
   geom *g;
   dev_status *st;
 };
@@ -93,13 +93,9 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = MF_SCAN_ITEMS;  // cells per thread of k_scan (a multiple of 4)
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr int BLOCK = 256;
-// k_finish: a fixed grid of FINISH_BLOCKS_PER_SM blocks of FINISH_BLOCK threads per SM takes
-// FINISH_BLOCK-particle chunks from an atomic counter
+// k_finish_flat: threads per block (one particle per thread)
 #ifndef FINISH_BLOCK
 #define FINISH_BLOCK 256
-#endif
-#ifndef FINISH_BLOCKS_PER_SM
-#define FINISH_BLOCKS_PER_SM 2
 #endif
 // k_plastic: fixed grid of this many 256-thread blocks per SM over the plastic list
 constexpr int PLASTIC_BLOCKS_PER_SM = 4;
@@ -543,7 +539,6 @@ __device__ __forceinline__ void reorder_body(const params &P, const dev_buffers 
   const bool sort = !P.verlet || D.st->sort_now;
   if (t == 0) {  // re-armed for the finish kernel of this step
     *D.plastic_count = 0u;
-    *D.finish_chunk = 0u;
     if (sort) D.st->sorts += 1ull;
   }
   // neighbour lists, no sort, and the previous step's finish (and plastic) kernels already ran
@@ -847,206 +842,20 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers
 
 // ---------------------------------------------------------------------------------------
 
-// corrector .. invalidate for one particle (leap_frog.cu:68-92, actions_gpu.cu:135-162,
-// 226-349, tool_gpu.cu:151-221); returns the final position and flags
-__device__ __forceinline__ void finish_particle(const params &P, const dev_buffers &D, const mf_tool_state &TL,
-                                               const mf_joco_constants &JC, int q,
-                                               double2 &pos_out, unsigned &f_out, double2 &fc_out, double2 &ft_out,
-                                               unsigned &newly_blanked, bool &want_sort, bool identity,
-                                               bool fuse) {
-  const state_set &A = D.A;
-  const state_set &B = D.B;
-  const double dt = P.dt;
-  unsigned f = B.flags[q];
-  const bool blanked = f & FLAG_BLANKED;
-  const bool tool = f & FLAG_TOOL;
-  const bool fixed = f & FLAG_FIXED;
-  // the state at the start of the step, in the new order (predict/correct skip blanked
-  // particles, so for them it is also the state at the end of the step)
-  // every load is issued here, before any store, so that they are all in flight together
-  const int p = identity ? q : D.perm[q];
-  double2 pos_t = B.pos_t[q], vel_t = B.vel_t[q];
-  const double4 S_t = B.S_t[q];
-  const double rho_t = B.rho_t[q], T_t = B.T_t[q];
-  double eps_pl = B.eps_pl[q], eps_pl_dot = B.eps_pl_dot[q];
-  double2 fc, ft;
-  prev_contact_forces(P, D, q, p, fc, ft);
-  const double2 normal = D.n[q];
-  const double pr = B.pp[q];
-  double2 pos = A.pos[p], vel = A.vel[p];
-  double4 S = A.S[p];
-  double rho = A.rho[p], T = A.T[p];
-  if (!blanked) {  // correct (leap_frog.cu:68-92)
-    pos.x = pos.x + dt * pos_t.x;
-    pos.y = pos.y + dt * pos_t.y;
-    vel.x = vel.x + dt * vel_t.x;
-    vel.y = vel.y + dt * vel_t.y;
-    S.x = S.x + dt * S_t.x;
-    S.y = S.y + dt * S_t.y;
-    S.z = S.z + dt * S_t.z;
-    S.w = S.w + dt * S_t.w;
-    rho = rho + dt * rho_t;
-    T = T + dt * T_t;
-  }
-  // friction heat (actions_gpu.cu:135-162), previous step's ft and n
-  if (P.has_tool && P.fric_heat && !tool) {
-    const double f_fric_mag = (double)sqrtf((float)(ft.x * ft.x + ft.y * ft.y));
-    if (f_fric_mag != 0.) {
-      const double vdx = vel.x - TL.vel[0], vdy = vel.y - TL.vel[1];
-      const double vdn = vdx * normal.x + vdy * normal.y;
-      const double vrx = vdx - vdn, vry = vdy - vdn;
-      const double v_rel_mag = (double)sqrtf((float)(vrx * vrx + vry * vry));
-      T += P.trml_wp.eta * dt * f_fric_mag * v_rel_mag / (P.trml_wp.cp * P.phys.mass);
-    }
-  }
-  // JC plasticity, radial return (actions_gpu.cu:226-285)
-  if (P.plastic && !tool) {
-    const double Sxx = S.x, Syy = S.z, Szz = S.w, Sxy = S.y;
-    const double cxx = Sxx - pr, cyy = Syy - pr, czz = Szz - pr, cxy = Sxy;
-    const double svm = (double)sqrtf(
-        (float)((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy));
-    // With A > 0 and B, C >= 0 the yield stress is at least A * (1 - theta^m): (A + B eps^n)
-    // >= A and the rate factor >= 1. A von Mises stress clearly below that bound is elastic
-    // without any FP64 pow: theta^m comes from powf, whose error (a few float ulps, plus the
-    // float rounding of theta and m) the factor 1.00001 covers, and the 0.1 % margin covers
-    // the rounding of the full yield stress. Every other particle goes to k_plastic, which
-    // runs the reference's full FP64 yield test and, where it yields, the return map over a
-    // compacted list with every lane busy; the trial stress, eps_pl, eps_pl_dot and rho
-    // written below are its inputs. Keeping the FP64 pow/log of the full test out of this
-    // kernel keeps its register budget small.
-    bool elastic = false;
-    if (P.jc_lower_bound) {
-      // theta in float: three float roundings (about 2e-7 relative), far inside the margin
-      const float theta_f = (float)(T - JC.Tref) * (1.f / (float)(JC.Tmelt - JC.Tref));
-      const double pow_hi = 1.00001 * (double)powf(theta_f, (float)JC.m);
-      elastic = svm < 0.999 * JC.A * (1.0 - pow_hi);
-    }
-    if (elastic) {
-      eps_pl_dot = 0.;
-    } else {
-      const unsigned am = __activemask();
-      const int leader = __ffs(am) - 1;
-      unsigned base = 0u;
-      if ((int)lane_id() == leader) base = atomicAdd(D.plastic_count, (unsigned)__popc(am));
-      base = __shfl_sync(am, base, leader);
-      const unsigned rank = __popc(am & ((1u << lane_id()) - 1u));
-      D.plastic_list[base + rank] = plastic_item{T, svm, q, 0};
-    }
-  }
-  // tool particles move with the tool (tool_gpu.cu:210-221); contact (:151-207)
-  if (P.has_tool) {
-    if (tool) {
-      pos.x += dt * TL.vel[0];
-      pos.y += dt * TL.vel[1];
-    } else {
-      double cpx = 0., cpy = 0., nx = 0., ny = 0.;
-      const bool inside = establish_contact(TL, pos.x, pos.y, cpx, cpy, nx, ny);
-      if (!inside) {
-        fc = make_double2(0., 0.);
-        ft = make_double2(0., 0.);
-        D.n[q] = make_double2(0., 0.);
-      } else {
-        const double dt2 = dt * dt;
-        const double gN = (pos.x - cpx) * nx + (pos.y - cpy) * ny;
-        const double sc = -TL.slave_mass * gN;
-        double2 fN = make_double2(sc * nx, sc * ny);
-        fN.x = fN.x / dt2 * TL.contact_alpha;
-        fN.y = fN.y / dt2 * TL.contact_alpha;
-        double2 fT = make_double2(0., 0.);
-        if (TL.mu != 0.) {
-          const double vx = vel.x - TL.vel[0], vy = vel.y - TL.vel[1];
-          const double vrx = vx - vx * nx, vry = vy - vy * ny;
-          const double ks = TL.contact_alpha * TL.slave_mass;
-          const double kx = ks * vrx / dt, ky = ks * vry / dt;
-          const double fy = TL.mu * sqrt(fN.x * fN.x + fN.y * fN.y);
-          const double fsx = ft.x - kx, fsy = ft.y - ky;
-          const double lfs = sqrt(fsx * fsx + fsy * fsy);
-          if (lfs > fy) {
-            fT.x = fy * fsx / lfs;
-            fT.y = fy * fsy / lfs;
-          } else {
-            fT = make_double2(fsx, fsy);
-          }
-        }
-        fc = fN;
-        ft = fT;
-        D.n[q] = make_double2(nx, ny);
-      }
-    }
-  }
-  // boundary conditions (actions_gpu.cu:287-311)
-  if (!tool && fixed) {
-    vel = make_double2(0., 0.);
-    fc = make_double2(0., 0.);
-    pos_t = make_double2(0., 0.);
-    vel_t = make_double2(0., 0.);
-    B.pos_t[q] = pos_t;
-    B.vel_t[q] = vel_t;
-  }
-  if (P.thermal_bc && fixed) T = P.trml_wp.T_init;
-  // invalidate (actions_gpu.cu:317-349)
-  if (!blanked) {
-    bool invalid = isnaninf(pos_t.x) || isnaninf(pos_t.y) || isnaninf(vel_t.x) || isnaninf(vel_t.y) ||
-                   isnaninf(S_t.x) || isnaninf(S_t.y) || isnaninf(S_t.z) || isnaninf(S_t.w) ||
-                   isnaninf(rho_t) || isnaninf(T_t);
-    if (invalid) {
-      f |= FLAG_BLANKED;
-      newly_blanked += 1u;
-      B.flags[q] = f;
-    }
-  }
-  // neighbour lists: the next step's predictor moves the particle to pos + dt/2 pos_t
-  // (leap_frog.cu:30-66); a sort is asked for when that is more than 0.45 skin from where its
-  // list was built (the lists hold while every particle stays within skin / 2)
-  if (P.verlet && !(f & FLAG_BLANKED)) {
-    const double2 pb = D.pos_build[q];
-    const double px = pos.x + 0.5 * dt * pos_t.x, py = pos.y + 0.5 * dt * pos_t.y;
-    const double ddx = px - pb.x, ddy = py - pb.y;
-    const double lim = 0.45 * (double)P.skin;
-    if (!(ddx * ddx + ddy * ddy <= lim * lim)) want_sort = true;
-  }
-  B.pos[q] = pos;
-  B.vel[q] = vel;
-  B.S[q] = S;
-  B.rho[q] = rho;
-  B.T[q] = T;
-  B.eps_pl[q] = eps_pl;
-  B.eps_pl_dot[q] = eps_pl_dot;
-  B.fc[q] = fc;
-  B.ft[q] = ft;
-  if (fuse) {
-    // neighbour lists, a step without a sort: the next step keeps this order, so its
-    // predictor runs here, on the final state still in registers, into the set the next step
-    // writes (this step's start set, read above by this thread only). If the next step sorts,
-    // its reorder kernel redoes it; k_plastic redoes it for the particles it changes.
-    const state_set &N1 = D.A;
-    N1.idx[q] = P.grid_kind == MF_GRID_GREEN ? q : B.idx[q];
-    N1.eps_pl[q] = eps_pl;
-    N1.eps_pl_dot[q] = eps_pl_dot;
-    N1.fc[q] = fc;
-    N1.ft[q] = ft;
-    predict_particle<true>(P, D, N1, q, D.hash_cur[q], pos, vel, S, rho, T, pos_t, vel_t, S_t, rho_t, T_t, f, B.h[q],
-                           false);
-  }
-  pos_out = pos;
-  f_out = f;
-  fc_out = fc;
-  ft_out = ft;
-}
-
-// The same corrector .. invalidate for one particle (not for the fused predictor, which needs
-// the whole state at once), in two phases that each load, update and store their own fields:
-// first velocity and position with the friction-heat input, contact, the kinematic boundary
-// conditions; then stress, density and temperature with the elastic test and the thermal
-// boundary condition. Fewer values are live at once than when every load is issued first, so
-// the kernel runs with fewer registers and more warps per SM. Every value is computed by the
-// same expressions from the same operands as in finish_particle: the results are equal bit for
-// bit. (eps_pl is not touched here: the corrector does not change it, the return map in
-// k_plastic does.)
+// Corrector .. invalidate for one particle (leap_frog.cu:68-92, actions_gpu.cu:135-162,
+// 226-349, tool_gpu.cu:151-221), in two phases that each load, update and store their own
+// fields: first velocity and position with the friction-heat input, contact, the kinematic
+// boundary conditions; then stress, density and temperature with the elastic test and the
+// thermal boundary condition. Fewer values are live at once than when every load is issued
+// first, so the kernel runs with fewer registers and more warps per SM. (eps_pl is not touched
+// here: the corrector does not change it, the return map in k_plastic does.) With FUSE_PRED and
+// `fuse`, also the next step's predictor (neighbour lists, a step without a sort).
+template <bool FUSE_PRED>
 __device__ __forceinline__ void finish_particle_phased(const params &P, const dev_buffers &D,
                                                        const mf_tool_state &TL, int q, double2 &pos_out,
                                                        unsigned &f_out, double2 &fc_out, double2 &ft_out,
-                                                       unsigned &newly_blanked, bool &want_sort, bool identity) {
+                                                       unsigned &newly_blanked, bool &want_sort, bool identity,
+                                                       bool fuse) {
   const state_set &A = D.A;
   const state_set &B = D.B;
   const double dt = P.dt;
@@ -1162,13 +971,13 @@ __device__ __forceinline__ void finish_particle_phased(const params &P, const de
   if (fric) T += dT_fric;
   // JC plasticity, radial return (actions_gpu.cu:226-285): the elastic lower bound of
   // finish_particle, the rest in k_plastic
+  bool elastic = false;
   if (P.plastic && !tool) {
     const double pr = B.pp[q];
     const double Sxx = S.x, Syy = S.z, Szz = S.w, Sxy = S.y;
     const double cxx = Sxx - pr, cyy = Syy - pr, czz = Szz - pr, cxy = Sxy;
     const double svm = (double)sqrtf(
         (float)((cxx * cxx + cyy * cyy + czz * czz) - cxx * cyy - cxx * czz - cyy * czz + 3.0 * cxy * cxy));
-    bool elastic = false;
     if (P.jc_lower_bound) {
       const mf_joco_constants &JC = P.joco;
       const float theta_f = (float)(T - JC.Tref) * (1.f / (float)(JC.Tmelt - JC.Tref));
@@ -1199,6 +1008,20 @@ __device__ __forceinline__ void finish_particle_phased(const params &P, const de
     B.flags[q] = f;
   }
   if (far && !(f & FLAG_BLANKED)) want_sort = true;
+  if (FUSE_PRED && fuse) {
+    // neighbour lists, a step without a sort: the next step keeps this order, so its predictor
+    // runs here, on the final state (position, velocity and the kinematic rates read back, the
+    // rest still in registers), into the set the next step writes (this step's start set, read
+    // above by this thread only). If the next step sorts, its reorder kernel redoes it; k_plastic
+    // redoes it for the particles it changes. The next step reads the last contact forces from
+    // its start set, this step's end set.
+    const state_set &N1 = D.A;
+    N1.idx[q] = P.grid_kind == MF_GRID_GREEN ? q : B.idx[q];
+    N1.eps_pl[q] = B.eps_pl[q];
+    N1.eps_pl_dot[q] = (P.plastic && !tool && elastic) ? 0. : B.eps_pl_dot[q];
+    predict_particle<true>(P, D, N1, q, D.hash_cur[q], B.pos[q], B.vel[q], S, rho, T, B.pos_t[q], B.vel_t[q], S_t,
+                           rho_t, T_t, f, B.h[q], false);
+  }
   pos_out = pos;
   f_out = f;
   fc_out = fc;
@@ -1281,14 +1104,16 @@ __device__ __forceinline__ void force_close_step(const params &P, const dev_buff
 }
 
 // Corrector .. invalidate for all particles plus the tool force (output.cu:31-39): one thread
-// per particle, one block per FINISH_BLOCK consecutive particles (the chunks of k_finish, so
-// that the force sums are the same numbers in the same tree: per warp, then the block's warps
-// in order, then the blocks in order in the last block to finish). Not for the fused predictor
-// (k_finish). With FUSE_HASH (locked grid) also the next step's hash and count.
+// per particle, one block per FINISH_BLOCK consecutive particles; the force sums per warp, then
+// the block's warps in order, then the two-level group tree. With FUSE_HASH (locked grid) also
+// the next step's hash and count; with FUSE_PRED the next step's predictor on list steps
+// without a sort (MF_OPT_FUSED_PREDICTOR). (A persistent variant of the fused kernel, blocks
+// taking 256-particle chunks from a counter at 128 registers, measured 44 against these 38 us
+// and gave the same bits.)
 #ifndef FINISH_FLAT_MIN_BLOCKS
 #define FINISH_FLAT_MIN_BLOCKS 3
 #endif
-template <bool FUSE_HASH>
+template <bool FUSE_HASH, bool FUSE_PRED>
 __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buffers &D,
                                                                                     int num_scan_tiles, blk bk) {
   __shared__ mf_tool_state s_tool;
@@ -1297,6 +1122,7 @@ __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buff
   if (P.has_tool) tool_load_shared(s_tool, D);
   const int q = bk.x * FINISH_BLOCK + threadIdx.x;
   const bool identity = P.verlet && !*(volatile unsigned *)&D.st->sort_now;
+  const bool fuse = FUSE_PRED && identity && P.fuse;  // the next step's predictor runs here too
   (void)num_scan_tiles;
   double2 fc = make_double2(0., 0.), ft = make_double2(0., 0.);
   unsigned newly_blanked = 0, blanked_now = 0, oog = 0;
@@ -1304,7 +1130,7 @@ __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buff
   if (q < P.N) {
     double2 pos;
     unsigned f;
-    finish_particle_phased(P, D, s_tool, q, pos, f, fc, ft, newly_blanked, want_sort, identity);
+    finish_particle_phased<FUSE_PRED>(P, D, s_tool, q, pos, f, fc, ft, newly_blanked, want_sort, identity, fuse);
     blanked_now = (f & FLAG_BLANKED) ? 1u : 0u;
     if (FUSE_HASH) {  // compute_hashes of the next step (grid.cu:34-51)
       const geom g = *D.g;
@@ -1323,7 +1149,7 @@ __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buff
       count_particle(D.count, D.tsum_w, hsh);  // read by the next step's scan
     }
   }
-  // the block's force sums (compensated), in the fixed tree of k_finish; warps whose forces are
+  // the block's force sums (compensated), in a fixed tree; warps whose forces are
   // all zero skip the arithmetic ({+0, +0} is what the sums give for zeros)
   const bool nz = fc.x != 0. || fc.y != 0. || ft.x != 0. || ft.y != 0.;
   const int w = threadIdx.x >> 5;
@@ -1403,167 +1229,14 @@ __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buff
   if (!__shfl_sync(0xffffffffu, last, 0)) return;
   __threadfence();
   force_final_sum(gsums, ng, r);
-  if (lane_id() == 0) force_close_step(P, D, r, false, !identity);
+  if (lane_id() == 0) force_close_step(P, D, r, fuse, !identity);
 }
 
-template <bool FUSE_HASH>
+template <bool FUSE_HASH, bool FUSE_PRED>
 __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_FLAT_MIN_BLOCKS) k_finish_flat(params P, dev_buffers D, int num_scan_tiles) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
-  finish_flat_body<FUSE_HASH>(P, D, num_scan_tiles, grid_blk());
-}
-
-// Corrector .. invalidate for all particles plus the tool force (output.cu:31-39). A fixed
-// grid of blocks takes chunks of BLOCK consecutive particles from an atomic counter, so the
-// blocks that meet the costly particles (yield tests, contact) do not set the kernel's length.
-// Each chunk's force sum goes to its own partial, and the last block to finish adds the
-// partials in chunk order: the result does not depend on which block took which chunk. With
-// FUSE_HASH (locked grid) the kernel also computes the next step's cell hash and per-cell
-// count from the final positions (the work of k_hash_count) and re-arms the scan.
-template <bool FUSE_HASH>
-__global__ void __launch_bounds__(FINISH_BLOCK, FINISH_BLOCKS_PER_SM) k_finish(params P, dev_buffers D, int num_scan_tiles) {
-  MF_PDL_WAIT();
-  MF_PDL_TRIGGER();
-  __shared__ mf_tool_state s_tool;
-  // the JC constants in shared memory: the out-of-line yield functions take them by
-  // reference, which for a kernel parameter would mean a copy on every thread's stack
-  __shared__ mf_joco_constants s_jc;
-  __shared__ ksum sm[FINISH_BLOCK / 32][4];
-  __shared__ unsigned smc[FINISH_BLOCK / 32][3];
-  __shared__ int s_chunk[2];  // this chunk and the next, taken while this one runs
-  if (threadIdx.x == 0) {
-    s_jc = P.joco;
-    s_chunk[0] = (int)atomicAdd(D.finish_chunk, 1u);
-  }
-  if (P.has_tool) tool_load_shared(s_tool, D);  // (its barrier also covers s_jc, s_chunk)
-  else __syncthreads();
-  const int stride = gridDim.x * blockDim.x;
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n_chunks = (P.N + FINISH_BLOCK - 1) / FINISH_BLOCK;
-  unsigned newly_blanked = 0, blanked_now = 0, oog = 0;
-  bool want_sort = false;
-  // neighbour lists, a step without a sort: the order is the previous step's (the last block
-  // sets sort_now for the next step only after every block has read it here); such a step
-  // also runs the next step's predictor
-  const bool identity = P.verlet && !*(volatile unsigned *)&D.st->sort_now;
-  const bool fuse = identity && P.fuse;
-  geom g{};
-  double inv_dx = 0.;
-  if (FUSE_HASH) {
-    g = *D.g;
-    inv_dx = 1. / g.dx;
-  }
-  (void)num_scan_tiles;
-  for (int buf = 0;; buf ^= 1) {
-    const int chunk = s_chunk[buf];
-    if (chunk >= n_chunks) break;
-    // the next chunk's index: its atomic runs while this chunk is processed (every thread
-    // read s_chunk[buf ^ 1] before the previous chunk's barriers)
-    if (threadIdx.x == 0) s_chunk[buf ^ 1] = (int)atomicAdd(D.finish_chunk, 1u);
-    const int q = chunk * FINISH_BLOCK + threadIdx.x;
-    double2 fc = make_double2(0., 0.), ft = make_double2(0., 0.);
-    if (q < P.N) {
-      double2 pos;
-      unsigned f;
-      finish_particle(P, D, s_tool, s_jc, q, pos, f, fc, ft, newly_blanked, want_sort, identity, fuse);
-      blanked_now += (f & FLAG_BLANKED) ? 1u : 0u;
-      if (FUSE_HASH) {  // compute_hashes of the next step (grid.cu:34-51)
-        long long hh;
-        if (f & FLAG_BLANKED) {
-          hh = D.hash_cur[q];
-        } else {
-          // (the FP64 form divides as the reference does; the mixed form with neighbour lists,
-          // which needs no particular cell for a particle on a cell edge, multiplies)
-          const int ix = __double2int_rz(P.verlet ? (pos.x - g.bbmin_x) * inv_dx : (pos.x - g.bbmin_x) / g.dx);
-          const int iy = __double2int_rz(P.verlet ? (pos.y - g.bbmin_y) * inv_dx : (pos.y - g.bbmin_y) / g.dx);
-          hh = (long long)ix * (long long)g.ny + (long long)iy;
-        }
-        if (hh < 0) { hh = 0; ++oog; }
-        else if (hh >= g.num_cell) { hh = g.num_cell - 1; ++oog; }
-        const int hsh = (int)hh;
-        D.hash_new[q] = hsh;
-        count_particle(D.count, D.tsum_w, hsh);  // read by the next step's scan
-      }
-    }
-    // the chunk's force sums (compensated), in a fixed tree: warps, then warps in order. Only
-    // particles in contact carry a force; a warp or chunk whose forces are all zero has the
-    // partial {+0, +0}, which is what the sums give for zeros, so their arithmetic is skipped.
-    const bool nz = fc.x != 0. || fc.y != 0. || ft.x != 0. || ft.y != 0.;
-    if (__any_sync(0xffffffffu, nz)) {
-      ksum fcx{0., 0.}, fcy{0., 0.}, ftx{0., 0.}, fty{0., 0.};
-      ksum_add(fcx, fc.x);
-      ksum_add(fcy, fc.y);
-      ksum_add(ftx, ft.x);
-      ksum_add(fty, ft.y);
-      for (int o = 16; o > 0; o >>= 1) {
-        ksum a{__shfl_down_sync(0xffffffffu, fcx.s, o), __shfl_down_sync(0xffffffffu, fcx.c, o)};
-        ksum b{__shfl_down_sync(0xffffffffu, fcy.s, o), __shfl_down_sync(0xffffffffu, fcy.c, o)};
-        ksum c{__shfl_down_sync(0xffffffffu, ftx.s, o), __shfl_down_sync(0xffffffffu, ftx.c, o)};
-        ksum d{__shfl_down_sync(0xffffffffu, fty.s, o), __shfl_down_sync(0xffffffffu, fty.c, o)};
-        ksum_merge(fcx, a); ksum_merge(fcy, b); ksum_merge(ftx, c); ksum_merge(fty, d);
-      }
-      if (lane_id() == 0) {
-        sm[threadIdx.x >> 5][0] = fcx; sm[threadIdx.x >> 5][1] = fcy;
-        sm[threadIdx.x >> 5][2] = ftx; sm[threadIdx.x >> 5][3] = fty;
-      }
-    } else if (lane_id() == 0) {
-      const ksum z{0., 0.};
-      sm[threadIdx.x >> 5][0] = z; sm[threadIdx.x >> 5][1] = z;
-      sm[threadIdx.x >> 5][2] = z; sm[threadIdx.x >> 5][3] = z;
-    }
-    const bool chunk_nz = __syncthreads_or(nz);  // sm complete
-    if (threadIdx.x == 0) {
-      ksum r[4] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
-      if (chunk_nz) {
-        for (int k = 0; k < 4; ++k) r[k] = sm[0][k];
-        for (int w = 1; w < FINISH_BLOCK / 32; ++w)
-          for (int k = 0; k < 4; ++k) ksum_merge(r[k], sm[w][k]);
-      }
-      for (int k = 0; k < 4; ++k) {
-        D.partials[(size_t)chunk * 8 + 2 * k] = r[k].s;
-        D.partials[(size_t)chunk * 8 + 2 * k + 1] = r[k].c;
-      }
-    }
-    __syncthreads();  // sm is reused, s_chunk[buf ^ 1] is set for the next chunk
-  }
-  // the block's counters
-  const unsigned nb = __reduce_add_sync(0xffffffffu, newly_blanked);
-  const unsigned nbl = __reduce_add_sync(0xffffffffu, blanked_now);
-  const unsigned noog = __reduce_add_sync(0xffffffffu, oog);
-  if (lane_id() == 0) {
-    smc[threadIdx.x >> 5][0] = nb; smc[threadIdx.x >> 5][1] = nbl; smc[threadIdx.x >> 5][2] = noog;
-  }
-  // with neighbour lists the hashes and counts above serve the next step only if it sorts,
-  // which is known once every particle has been checked (last block, below)
-  const bool block_wants_sort = __syncthreads_or(want_sort);
-  __shared__ unsigned s_last;
-  if (threadIdx.x == 0) {
-    unsigned long long cnt[3] = {smc[0][0], smc[0][1], smc[0][2]};
-    for (int w = 1; w < FINISH_BLOCK / 32; ++w)
-      for (int k = 0; k < 3; ++k) cnt[k] += smc[w][k];
-    if (block_wants_sort) D.st->want_sort = 1u;  // (before the fence and the ticket below)
-    if (cnt[0]) atomicAdd(&D.st->newly_blanked, cnt[0]);
-    if (cnt[1]) atomicAdd(&D.st->blanked, cnt[1]);
-    if (cnt[2]) atomicAdd(&D.st->out_of_grid, cnt[2]);
-    __threadfence();
-    s_last = atomicAdd(&D.ticket[0], 1u) == gridDim.x - 1 ? 1u : 0u;
-  }
-  __syncthreads();
-  if (!s_last) return;
-  // the last block: the same two-level tree as k_finish_flat, every group by one of its warps
-  __threadfence();
-  const int ng = (n_chunks + FORCE_GROUP - 1) / FORCE_GROUP;
-  double *gsums = D.partials + (size_t)n_chunks * 8;
-  ksum r[4];
-  for (int g = (int)(threadIdx.x >> 5); g < ng; g += FINISH_BLOCK / 32) {
-    force_group_sum(D.partials, g, n_chunks, r);
-    if (lane_id() == 0) store_ksum4(gsums + (size_t)g * 8, r);
-  }
-  __threadfence_block();
-  __syncthreads();
-  if (threadIdx.x >= 32) return;
-  force_final_sum(gsums, ng, r);
-  if (lane_id() == 0) force_close_step(P, D, r, fuse, !identity);
+  finish_flat_body<FUSE_HASH, FUSE_PRED>(P, D, num_scan_tiles, grid_blk());
 }
 
 // JC plasticity (actions_gpu.cu:226-285) for the particles the finish kernel listed: the

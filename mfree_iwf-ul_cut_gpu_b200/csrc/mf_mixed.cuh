@@ -402,8 +402,11 @@ __device__ __forceinline__ void pair_mixed_body(const params &P, const dev_buffe
   pair_mixed_particle<LIST>(P, D, bk.x * blockDim.x + threadIdx.x);
 }
 
+#ifndef MF_PAIR_MIXED_MIN_BLOCKS
+#define MF_PAIR_MIXED_MIN_BLOCKS 6
+#endif
 template <bool LIST>
-static __global__ void __launch_bounds__(PAIR_BLOCK, 6) k_pair_mixed(params P, dev_buffers D) {
+static __global__ void __launch_bounds__(PAIR_BLOCK, MF_PAIR_MIXED_MIN_BLOCKS) k_pair_mixed(params P, dev_buffers D) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
   pair_mixed_body<LIST>(P, D, grid_blk());
