@@ -342,7 +342,7 @@ int launch_stage(mf_ctx *ctx, int stage) {
     case 2:
       if (mixed && ctx->P.verlet) TRY(launch_pdl(ctx, k_pair_mixed<true>, npb, PAIR_BLOCK, ctx->P, ctx->D));
       else if (mixed) TRY(launch_pdl(ctx, k_pair_mixed<false>, npb, PAIR_BLOCK, ctx->P, ctx->D));
-      else TRY(launch_pdl(ctx, k_pair_fp64, npb, PAIR_BLOCK, ctx->P, ctx->D));
+      else TRY(launch_pdl(ctx, k_pair_fp64, (N + PAIR64_BLOCK - 1) / PAIR64_BLOCK, PAIR64_BLOCK, ctx->P, ctx->D));
       if (ctx->P.thermal_solver == MF_THERMAL_PSE && ctx->P.thermal_wp) {
         if (mixed) TRY(launch_pdl(ctx, k_pse_mixed, npb, PAIR_BLOCK, ctx->P, ctx->D));
         else TRY(launch_pdl(ctx, k_pse, npb, PAIR_BLOCK, ctx->P, ctx->D));

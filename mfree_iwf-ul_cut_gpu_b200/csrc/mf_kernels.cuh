@@ -99,11 +99,14 @@ constexpr int BLOCK = 256;
 #endif
 // k_plastic: fixed grid of this many 256-thread blocks per SM over the plastic list
 constexpr int PLASTIC_BLOCKS_PER_SM = 4;
-constexpr int PAIR_BLOCK = 128;
+#ifndef MF_PAIR_BLOCK
+#define MF_PAIR_BLOCK 128
+#endif
+constexpr int PAIR_BLOCK = MF_PAIR_BLOCK;
 // k_reorder: blocks per SM its register budget allows (REORDER_BLOCKS_PER_SM x 256 threads per
 // SM, so that a ~180k-particle grid runs in one wave)
 #ifndef REORDER_BLOCKS_PER_SM
-#define REORDER_BLOCKS_PER_SM 5
+#define REORDER_BLOCKS_PER_SM 3
 #endif
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
@@ -785,10 +788,14 @@ __device__ __forceinline__ void pair_fp64_body(const params &P, const dev_buffer
   pair_fp64_particle(P, D, bk.x * blockDim.x + threadIdx.x);
 }
 
+// the FP64 pair kernel in blocks of 64 at 8 per SM (128 registers): 110.6 against 112.6 us in
+// blocks of 128 at 4, 114.7 in blocks of 256 at 2 (the ~150k-particle cut); at 3 blocks of 128
+// (153 registers, no spills) 121.8
+constexpr int PAIR64_BLOCK = 64;
 #ifndef MF_PAIR64_MIN_BLOCKS
-#define MF_PAIR64_MIN_BLOCKS 4
+#define MF_PAIR64_MIN_BLOCKS 8
 #endif
-static __global__ void __launch_bounds__(PAIR_BLOCK, MF_PAIR64_MIN_BLOCKS) k_pair_fp64(params P, dev_buffers D) {
+static __global__ void __launch_bounds__(PAIR64_BLOCK, MF_PAIR64_MIN_BLOCKS) k_pair_fp64(params P, dev_buffers D) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
   pair_fp64_body(P, D, grid_blk());

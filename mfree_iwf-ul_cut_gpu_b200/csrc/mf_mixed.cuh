@@ -328,8 +328,7 @@ __device__ __forceinline__ void mixed_end(const params &P, const dev_buffers &D,
   if (thermal) B.T_t[q] = thermal_alpha * (double)T_lapl;
 }
 
-// LIST: the neighbour-list form (steps with P.verlet). 80 registers (6 blocks of 128 per SM)
-// keep both forms free of spills; the list form measured slower at 7 and 8 blocks per SM
+// LIST: the neighbour-list form (steps with P.verlet)
 template <bool LIST>
 __device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_buffers &D, int q) {
   mixed_i I;
@@ -402,11 +401,11 @@ __device__ __forceinline__ void pair_mixed_body(const params &P, const dev_buffe
   pair_mixed_particle<LIST>(P, D, bk.x * blockDim.x + threadIdx.x);
 }
 
-#ifndef MF_PAIR_MIXED_MIN_BLOCKS
-#define MF_PAIR_MIXED_MIN_BLOCKS 6
-#endif
+// blocks per SM: the window kernel at 6 (80 registers, no spills); the list kernel at 5 (92
+// registers, no spills; at 6 it spills a little and ran ~1.5 us slower, at 9 with 56 registers
+// 13 us slower)
 template <bool LIST>
-static __global__ void __launch_bounds__(PAIR_BLOCK, MF_PAIR_MIXED_MIN_BLOCKS) k_pair_mixed(params P, dev_buffers D) {
+static __global__ void __launch_bounds__(PAIR_BLOCK, LIST ? 5 : 6) k_pair_mixed(params P, dev_buffers D) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
   pair_mixed_body<LIST>(P, D, grid_blk());
