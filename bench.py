@@ -673,6 +673,7 @@ def batch_run(mf, torch, n_instances, steps, device):
     b = mf.Batch(cs, steps_per_launch=0)
     k = b.steps_per_launch
     fused, pair_block = b.fused, b.pair_block
+    form, bps = b.form, b.blocks_per_sm
     launches = max(1, steps // k)
     b.step(1)
     for c in cs:
@@ -682,6 +683,27 @@ def batch_run(mf, torch, n_instances, steps, device):
     for c in cs:
         c.synchronize()
     bat_s = time.perf_counter() - t0
+    # each launch form at a fixed setting, on the same (advancing) instances
+    forms = {}
+    if fused:
+        for name, fm, fb, fk in (("phases_k16", mf.BATCH_PHASES, 0, 16), ("persistent_1_per_sm_k16", mf.BATCH_PERSISTENT, 1, 16),
+                                 ("persistent_2_per_sm_k16", mf.BATCH_PERSISTENT, 2, 16)):
+            try:
+                b.set_form(fm, fb, fk)
+            except mf.MfError as e:
+                forms[name] = {"error": str(e)}
+                continue
+            nl = max(1, steps // fk)
+            b.step(1)
+            for c in cs:
+                c.synchronize()
+            t0 = time.perf_counter()
+            b.step(nl)
+            for c in cs:
+                c.synchronize()
+            w = time.perf_counter() - t0
+            forms[name] = {"steps": nl * fk, "wall_s": w, "particle_steps_per_s": n_total * nl * fk / w,
+                           "blocks_per_sm": b.blocks_per_sm}
     st = [c.status() for c in cs]
     b.close()
     for c in cs:
@@ -689,8 +711,11 @@ def batch_run(mf, torch, n_instances, steps, device):
     return {"mode": "batch", "instances": n_instances, "particles_total": n_total,
             "particles_min_max": [min(sc.N for sc in scenes), max(sc.N for sc in scenes)],
             "precision": "mixed", "steps_per_launch": k, "batched_kernels": fused, "pair_block": pair_block,
-            "launches_per_step": ("one per step phase for all instances" if fused else
-                                  "one child graph per instance"),
+            "form": ("persistent" if form == mf.BATCH_PERSISTENT else "phases"), "persistent_blocks_per_sm": bps,
+            "launches_per_step": (f"one cooperative launch per {k} steps for all instances ({bps} blocks per SM)"
+                                  if form == mf.BATCH_PERSISTENT else "one per step phase for all instances"
+                                  if fused else "one child graph per instance"),
+            "forms": forms,
             "one_at_a_time": {"steps": steps, "wall_s": one_s, "particle_steps_per_s": n_total * steps / one_s},
             "streams": {"steps": steps, "wall_s": seq_s, "particle_steps_per_s": n_total * steps / seq_s},
             "batched": {"steps": launches * k, "wall_s": bat_s,

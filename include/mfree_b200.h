@@ -122,7 +122,8 @@ typedef struct {
   long long secant_cap_hits;  /* JC secant solves that hit the iteration cap */
   int max_cell_occupancy;     /* largest particles-per-cell seen in the last sort */
   int error_flags;            /* bit 1: the adaptive grid outgrew max_cell; bit 2: a neighbour
-                                 list was full (neighbours dropped); bit 0 (a bounded wait in
+                                 list was full (neighbours dropped); bit 3: a persistent batch
+                                 launch's barrier wait expired (mf_batch_set_form); bit 0 (a bounded wait in
                                  the cell scan expired) is no longer raised: the scan waits
                                  for nothing */
   long long secant_iterations; /* JC secant iterations since creation (cost diagnostic) */
@@ -385,6 +386,24 @@ int mf_batch_create(mf_ctx **ctxs, int n, int steps_per_launch, mf_batch **out);
 int mf_batch_steps_per_launch(const mf_batch *batch, int *steps_per_launch);
 int mf_batch_config(const mf_batch *batch, int *fused, int *pair_block, int *steps_per_launch);
 int mf_batch_step(mf_batch *batch, int n_launches); /* n_launches x steps_per_launch steps each */
+/* Launch form of a batch on the batched kernels. MF_BATCH_PHASES: each step one launch per
+   phase, as above. MF_BATCH_PERSISTENT: the K steps of a launch run inside ONE cooperative
+   launch (captured in the batch's graph) of blocks_per_sm 256-thread blocks per SM (0: as many
+   as are resident); its blocks take each phase's blocks of all instances in turn and meet at a
+   grid-wide barrier between phases, every instance's results still equal to its own context's
+   bit for bit. Each barrier wait is bounded (mf_batch_set_wait_limit, default 2 s): if one
+   expires the launch ends early and every instance's mf_status.error_flags gets bit 3.
+   The persistent form steps mixed-precision batches only (an FP64 build of it contracted the
+   pair sums' multiply-adds differently, ~1e-16 relative off the single-system step).
+   mf_batch_set_form rebuilds the batch's graph (MF_ERR_INVALID for a child-graph or FP64 batch
+   in the persistent form, an odd or < 2 steps_per_launch); the tuner of steps_per_launch = 0
+   also measures the persistent form of a mixed batch (1 and 2 blocks per SM, 4 and 16 steps
+   per launch) and keeps the fastest form. ---- */
+#define MF_BATCH_PHASES 0
+#define MF_BATCH_PERSISTENT 1
+int mf_batch_set_form(mf_batch *batch, int form, int blocks_per_sm, int steps_per_launch);
+int mf_batch_form(const mf_batch *batch, int *form, int *blocks_per_sm);
+int mf_batch_set_wait_limit(mf_batch *batch, double seconds);
 int mf_batch_destroy(mf_batch *batch);
 
 /* ---- differentiable form (no counterpart in the reference): from the context's current

@@ -25,6 +25,8 @@ THERMAL_BROOKSHAW, THERMAL_PSE = 0, 1
 JC_JOHNSON_COOK, JC_TANH = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 OPT_KEEP_DERIVATIVES, OPT_NO_GRAPHS, OPT_SORT_EVERY_STEP, OPT_FUSED_PREDICTOR, OPT_NEIGHBOUR_LISTS = 1, 2, 4, 8, 16
+BATCH_PHASES, BATCH_PERSISTENT = 0, 1
+ERRF_BATCH_WAIT = 8  # mf_status.error_flags bit 3: a persistent batch launch's barrier wait expired
 
 # name -> (field id, doubles per particle, is_int)
 FIELDS = {
@@ -149,6 +151,8 @@ def lib():
         "mf_graph_capture": ([vp, i, C.POINTER(vp)], i), "mf_graph_destroy": ([vp], i),
         "mf_batch_create": ([C.POINTER(vp), i, i, C.POINTER(vp)], i), "mf_batch_steps_per_launch": ([vp, ip], i), "mf_batch_config": ([vp, ip, ip, ip], i),
         "mf_batch_step": ([vp, i], i), "mf_batch_destroy": ([vp], i),
+        "mf_batch_set_form": ([vp, i, i, i], i), "mf_batch_form": ([vp, ip, ip], i),
+        "mf_batch_set_wait_limit": ([vp, d], i),
         "mf_get_constants": ([vp, C.POINTER(Phys), C.POINTER(Corr), C.POINTER(Joco), C.POINTER(Trml),
                               C.POINTER(Trml), ip], i),
         "mf_force_log": ([vp, vp, i, ip], i), "mf_force_last_async": ([vp, vp], i), "mf_status_get": ([vp, C.POINTER(Status)], i),
@@ -485,11 +489,28 @@ class Batch:
         rc = self.L.mf_batch_create(arr, len(self.contexts), int(steps_per_launch), C.byref(self.h))
         if rc != MF_OK:
             raise MfError(rc, "mf_batch_create")
-        k, fused, bs = C.c_int(), C.c_int(), C.c_int()
+        self._read_config()
+
+    def _read_config(self):
+        k, fused, bs, form, bps = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
         self.L.mf_batch_config(self.h, C.byref(fused), C.byref(bs), C.byref(k))
+        self.L.mf_batch_form(self.h, C.byref(form), C.byref(bps))
         self.steps_per_launch = k.value
-        self.fused = bool(fused.value)  # one launch per step phase for all instances
+        self.fused = bool(fused.value)  # batched kernels over all instances
         self.pair_block = bs.value
+        self.form = form.value  # BATCH_PHASES: a launch per phase; BATCH_PERSISTENT: one per K steps
+        self.blocks_per_sm = bps.value  # of the persistent form
+
+    def set_form(self, form, blocks_per_sm=0, steps_per_launch=4):
+        rc = self.L.mf_batch_set_form(self.h, int(form), int(blocks_per_sm), int(steps_per_launch))
+        if rc != MF_OK:
+            raise MfError(rc, "mf_batch_set_form")
+        self._read_config()
+
+    def set_wait_limit(self, seconds):
+        rc = self.L.mf_batch_set_wait_limit(self.h, float(seconds))
+        if rc != MF_OK:
+            raise MfError(rc, "mf_batch_set_wait_limit")
 
     def step(self, n_launches=1):
         rc = self.L.mf_batch_step(self.h, int(n_launches))

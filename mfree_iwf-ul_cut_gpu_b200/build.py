@@ -8,9 +8,11 @@ tree so that it travels with the repository to the GPU machine.
 """
 from __future__ import annotations
 
+import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -66,15 +68,18 @@ def build(force: bool = False, ptxas_verbose: bool = False) -> Path:
     OBJ.mkdir(parents=True, exist_ok=True)
     LIB_DIR.mkdir(parents=True, exist_ok=True)
     objs = []
-    log = []
+    cmds = []
     for src in sources():
         o = OBJ / (src.stem + ".o")
         if src.suffix == ".cu":
             extra = ["-Xptxas", "-v"] if ptxas_verbose else []
-            log.append(_run([NVCC] + NVCC_FLAGS + extra + ["-c", "-o", o, src]))
+            cmds.append([NVCC] + NVCC_FLAGS + extra + ["-c", "-o", o, src])
         else:
-            log.append(_run(["g++"] + CXX_FLAGS + ["-c", "-o", o, src]))
+            cmds.append(["g++"] + CXX_FLAGS + ["-c", "-o", o, src])
         objs.append(o)
+    # the translation units compile independently: side by side
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+        log = list(pool.map(_run, cmds))
     tmp = LIB.with_suffix(".so.tmp")
     _run([NVCC, "-shared", "-Xcompiler", "-fPIC"] + ARCH + ["-o", tmp] + objs + ["-lcudart"])
     tmp.replace(LIB)

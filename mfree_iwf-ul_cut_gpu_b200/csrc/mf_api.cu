@@ -16,6 +16,7 @@
 #include "mf_kernels.cuh"
 #include "mf_mixed.cuh"
 #include "mf_batch.cuh"
+#include "mf_persist.h"
 #include "mfree_b200.h"
 
 using namespace mf;
@@ -1034,6 +1035,12 @@ struct mf_batch {
   batch_entry *d_entries = nullptr;  // [2][n]: every system bound to each parity of its buffers
   int *d_first = nullptr;            // 4 maps of n + 1 first blocks: scan, 256-thread phases, pair, plastic
   int grid[4] = {0, 0, 0, 0};
+  // MF_BATCH_PERSISTENT: K steps in one cooperative launch of persist_bps blocks per SM
+  int form = MF_BATCH_PHASES;
+  int persist_bps = 0;           // 0: as many as are resident
+  unsigned long long *d_bar = nullptr;  // the persistent kernel's barrier word
+  double wait_s = 2.0;           // limit of one barrier wait
+  int persist_used = 0;          // blocks per SM of the built persistent launch
 };
 
 namespace {
@@ -1117,7 +1124,8 @@ int batch_build_fused(mf_batch *b, int K) {
     }
     c->cur = saved;
     bind_sets(c);
-    const int blocks[4] = {c->scan_tiles, (c->N + BLOCK - 1) / BLOCK, (c->N + b->pair_bs - 1) / b->pair_bs,
+    const int pair_bs = b->form == MF_BATCH_PERSISTENT ? PERSIST_BLOCK : b->pair_bs;
+    const int blocks[4] = {c->scan_tiles, (c->N + BLOCK - 1) / BLOCK, (c->N + pair_bs - 1) / pair_bs,
                            (int)std::max<long long>(1, (long long)sms * PLASTIC_BLOCKS_PER_SM * c->N / total_n)};
     for (int m = 0; m < 4; ++m) first[(size_t)m * (n + 1) + k + 1] = first[(size_t)m * (n + 1) + k] + blocks[m];
   }
@@ -1134,9 +1142,36 @@ int batch_build_fused(mf_batch *b, int K) {
     return MF_ERR_CUDA;
   const params &P0 = b->ctx[0]->P;
   const bool mixed = P0.precision == MF_PRECISION_MIXED;
+  persist_args A = {};
+  int pgrid = 0;
+  if (b->form == MF_BATCH_PERSISTENT) {
+    int resident = 0;
+    if (!mixed) return MF_ERR_INVALID;
+    if (persist_blocks_per_sm(&resident) != 0) return MF_ERR_CUDA;
+    const int bps = b->persist_bps > 0 ? std::min(b->persist_bps, resident) : resident;
+    if (bps < 1) return MF_ERR_CUDA;
+    pgrid = bps * sms;
+    b->persist_used = bps;
+    if (!b->d_bar && cudaMalloc(&b->d_bar, sizeof(unsigned long long)) != cudaSuccess) return MF_ERR_NOMEM;
+    A.e = b->d_entries;
+    A.first = b->d_first;
+    A.n = n;
+    A.K = K;
+    for (int m = 0; m < 4; ++m) A.grid[m] = b->grid[m];
+    A.pse = P0.thermal_solver == MF_THERMAL_PSE && P0.thermal_wp ? 1 : 0;
+    A.plastic = P0.plastic ? 1 : 0;
+    A.paired = P0.jc_model == MF_JC_TANH ? 0 : 1;
+    A.bar = b->d_bar;
+    A.wait_ns = (unsigned long long)(b->wait_s * 1e9);
+  }
   if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return MF_ERR_CUDA;
   int rc = MF_OK;
-  for (int st = 0; st < K && rc == MF_OK; ++st) {
+  if (b->form == MF_BATCH_PERSISTENT) {  // the barrier word starts at zero in every launch
+    if (cudaMemsetAsync(b->d_bar, 0, sizeof(unsigned long long), b->stream) != cudaSuccess ||
+        persist_launch(b->stream, pgrid, A) != 0)
+      rc = MF_ERR_CUDA;
+  }
+  for (int st = 0; st < K && rc == MF_OK && b->form != MF_BATCH_PERSISTENT; ++st) {
     const batch_entry *ent = b->d_entries + (size_t)(st & 1) * n;
     const batch_map m_scan{ent, b->d_first, n}, m_256{ent, b->d_first + (n + 1), n},
         m_pair{ent, b->d_first + 2 * (n + 1), n}, m_pl{ent, b->d_first + 3 * (n + 1), n};
@@ -1292,6 +1327,30 @@ int mf_batch_create(mf_ctx **ctxs, int n, int steps_per_launch, mf_batch **out) 
       rc = measure(cand[ci], &v);
       if (rc == MF_OK && v > best) { best = v; best_k = cand[ci]; }
     }
+    if (rc == MF_OK && b->fused && b->ctx[0]->P.precision == MF_PRECISION_MIXED) {
+      // then the persistent kernel (one launch per K steps) at 1 and 2 blocks per SM and 4 or
+      // 16 steps per launch; it replaces the per-phase launches where it measures faster
+      int resident = 0;
+      if (persist_blocks_per_sm(&resident) != 0) resident = 0;
+      int best_bps = 0, best_pk = 0;
+      for (int bps = 1; bps <= std::min(resident, 2) && rc == MF_OK; ++bps) {
+        for (int pk : {4, 16}) {
+          b->form = MF_BATCH_PERSISTENT;
+          b->persist_bps = bps;
+          double v = 0.;
+          const int r = measure(pk, &v);
+          if (r == MF_ERR_CUDA) {  // (a launch form the device refuses: kept out)
+            cudaGetLastError();
+            continue;
+          }
+          rc = r;
+          if (rc == MF_OK && v > best) { best = v; best_bps = bps; best_pk = pk; }
+        }
+      }
+      b->form = best_bps ? MF_BATCH_PERSISTENT : MF_BATCH_PHASES;
+      b->persist_bps = best_bps;
+      if (best_bps) best_k = best_pk;
+    }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (rc == MF_OK) rc = batch_build(b, best_k);
@@ -1318,6 +1377,34 @@ int mf_batch_config(const mf_batch *b, int *fused, int *pair_block, int *steps_p
   return MF_OK;
 }
 
+int mf_batch_set_form(mf_batch *b, int form, int blocks_per_sm, int steps_per_launch) {
+  if (!b || (form != MF_BATCH_PHASES && form != MF_BATCH_PERSISTENT) || blocks_per_sm < 0 || steps_per_launch < 2 ||
+      (steps_per_launch & 1))
+    return MF_ERR_INVALID;
+  // child-graph batches have no phases; the persistent kernel steps the mixed form only
+  if (form == MF_BATCH_PERSISTENT && (!b->fused || b->ctx[0]->P.precision != MF_PRECISION_MIXED))
+    return MF_ERR_INVALID;
+  if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamSynchronize(b->stream) != cudaSuccess) return MF_ERR_CUDA;
+  b->form = form;
+  b->persist_bps = blocks_per_sm;
+  return batch_build(b, steps_per_launch);
+}
+
+int mf_batch_form(const mf_batch *b, int *form, int *blocks_per_sm) {
+  if (!b) return MF_ERR_INVALID;
+  if (form) *form = b->form;
+  if (blocks_per_sm) *blocks_per_sm = b->form == MF_BATCH_PERSISTENT ? b->persist_used : 0;
+  return MF_OK;
+}
+
+int mf_batch_set_wait_limit(mf_batch *b, double seconds) {
+  if (!b || !(seconds >= 0.) || seconds > 3600.) return MF_ERR_INVALID;
+  b->wait_s = seconds;
+  if (!b->exec) return MF_OK;
+  if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamSynchronize(b->stream) != cudaSuccess) return MF_ERR_CUDA;
+  return batch_build(b, b->K);  // the limit is an argument of the captured launch
+}
+
 int mf_batch_step(mf_batch *b, int n_launches) {
   nvtx_range range("mf_batch_step");
   if (!b || n_launches < 0) return MF_ERR_INVALID;
@@ -1333,6 +1420,7 @@ int mf_batch_destroy(mf_batch *b) {
   batch_release(b);
   if (b->d_entries) cudaFree(b->d_entries);
   if (b->d_first) cudaFree(b->d_first);
+  if (b->d_bar) cudaFree(b->d_bar);
   for (cudaEvent_t e : b->ev)
     if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);

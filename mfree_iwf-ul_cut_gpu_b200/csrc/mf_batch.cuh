@@ -27,15 +27,17 @@ struct batch_map {
   int n;
 };
 
-// The block's system (the largest k with first[k] <= blockIdx.x), its entry copied into shared
-// memory by the block's threads (16-byte words), and the block's index and count within it.
-__device__ __forceinline__ blk batch_block(const batch_map &M, batch_entry &s) {
+// The system of batched block vb (the largest k with first[k] <= vb), its entry copied into
+// shared memory by the block's threads (16-byte words), and the block's index and count within
+// it. A batched launch passes its own block index; the persistent kernel each phase block it
+// takes.
+__device__ __forceinline__ blk batch_block_at(const batch_map &M, batch_entry &s, int vb) {
   __shared__ int s_k;
   if (threadIdx.x == 0) {
     int lo = 0, hi = M.n - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (__ldg(M.first + mid) <= (int)blockIdx.x) lo = mid;
+      if (__ldg(M.first + mid) <= vb) lo = mid;
       else hi = mid - 1;
     }
     s_k = lo;
@@ -48,7 +50,10 @@ __device__ __forceinline__ blk batch_block(const batch_map &M, batch_entry &s) {
   for (int w = threadIdx.x; w < (int)(sizeof(batch_entry) / 16); w += blockDim.x) dst[w] = __ldg(src + w);
   __syncthreads();
   const int f0 = __ldg(M.first + k), f1 = __ldg(M.first + k + 1);
-  return blk{(int)blockIdx.x - f0, f1 - f0};
+  return blk{vb - f0, f1 - f0};
+}
+__device__ __forceinline__ blk batch_block(const batch_map &M, batch_entry &s) {
+  return batch_block_at(M, s, (int)blockIdx.x);
 }
 
 static __global__ void __launch_bounds__(SCAN_THREADS) kb_scan(batch_map M) {

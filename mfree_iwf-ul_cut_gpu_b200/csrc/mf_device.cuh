@@ -101,6 +101,7 @@ constexpr int FORCE_LOG_CAP = 1 << 16;
 constexpr int ERR_SCAN_WAIT = 1;  // (no longer raised: the cell scan has no bounded waits)
 constexpr int ERR_GRID_BUDGET = 2;
 constexpr int ERR_LIST_OVERFLOW = 4;  // a neighbour list was full: neighbours were dropped
+constexpr int ERR_BATCH_WAIT = 8;     // a persistent batch launch's grid barrier wait expired
 
 // neighbour list entry: particle index in the low LIST_INDEX_BITS bits, above them the
 // column offset of the pair's cells (i's column - j's column) + 3, in [0, 6]

@@ -122,3 +122,99 @@ def test_instances_on_neighbour_lists_take_the_child_graph_batch(mf):
     for x, y in zip(batched, single):
         assert_same(x, y)
     b.close()
+
+
+@pytest.mark.parametrize("blocks_per_sm", [0, 1, 2])
+def test_persistent_batch_equals_separate_contexts(mf, blocks_per_sm):
+    """The persistent form (mixed precision): K steps of every instance in one cooperative
+    launch whose blocks take each phase's blocks in turn and meet at a grid barrier between
+    phases. Every instance equals its own context bit for bit, over two builds of the batch's
+    graph and back to the per-phase launches."""
+    precision = 1
+    sts = scenes(mf)
+    batched = [load_product(mf, st, precision=precision) for st in sts]
+    single = [load_product(mf, st, precision=precision) for st in sts]
+    b = mf.Batch(batched, steps_per_launch=4)
+    b.set_form(mf.BATCH_PERSISTENT, blocks_per_sm, 4)
+    assert b.form == mf.BATCH_PERSISTENT and b.fused and b.steps_per_launch == 4
+    assert b.blocks_per_sm >= 1 and (blocks_per_sm == 0 or b.blocks_per_sm == blocks_per_sm)
+    b.step(3)
+    for c in single:
+        c.step(12)
+    for x, y in zip(batched, single):
+        assert x.status()["steps"] == 12 and x.status()["error_flags"] == 0
+        assert_same(x, y)
+    b.set_form(mf.BATCH_PERSISTENT, blocks_per_sm, 2)  # rebuilt: the barrier word restarts at zero
+    b.step(2)
+    for c in single:
+        c.step(4)
+    for x, y in zip(batched, single):
+        assert x.status()["error_flags"] == 0
+        assert_same(x, y)
+    b.set_form(mf.BATCH_PHASES, 0, 2)  # and back to one launch per phase
+    assert b.form == mf.BATCH_PHASES
+    b.step(1)
+    for c in single:
+        c.step(2)
+    for x, y in zip(batched, single):
+        assert_same(x, y)
+    b.close()
+
+
+def test_persistent_sweep_of_64_instances_equals_separate_contexts(mf):
+    """The 64-instance sweep (mixed precision) in the persistent form, 16 steps per launch."""
+    batched = sweep_contexts(mf, 64, mf.PRECISION_MIXED)
+    single = sweep_contexts(mf, 64, mf.PRECISION_MIXED)
+    b = mf.Batch(batched, steps_per_launch=2)
+    b.set_form(mf.BATCH_PERSISTENT, 0, 16)
+    b.step(2)
+    for c in single:
+        c.step(32)
+    for x, y in zip(batched, single):
+        assert x.status()["steps"] == y.status()["steps"] == 32
+        assert x.status()["error_flags"] == 0
+        assert_same(x, y)
+    b.close()
+    for c in batched + single:
+        c.close()
+
+
+def test_persistent_barrier_wait_limit(mf):
+    """A barrier wait that runs out ends the persistent launch early with an error the host
+    reads: with a zero wait limit the first block that has to wait gives up, the barrier then
+    releases no block, and every instance's status carries error bit 3; the device stays
+    usable (a fresh context steps and equals a second fresh context)."""
+    sts = scenes(mf)
+    batched = [load_product(mf, st, precision=1) for st in sts]
+    b = mf.Batch(batched, steps_per_launch=2)
+    b.set_form(mf.BATCH_PERSISTENT, 0, 8)
+    b.set_wait_limit(0.0)
+    b.step(1)
+    for x in batched:
+        assert x.status()["error_flags"] & mf.ERRF_BATCH_WAIT
+    b.close()
+    for x in batched:
+        x.close()
+    fresh = [load_product(mf, sts[0], precision=1) for _ in range(2)]
+    fresh[0].step(4)
+    fresh[1].step(4)
+    assert fresh[0].status()["error_flags"] == 0
+    assert_same(fresh[0], fresh[1])
+    with pytest.raises(mf.MfError):
+        b2 = mf.Batch(fresh, steps_per_launch=2)
+        b2.set_wait_limit(-1.0)
+
+
+def test_persistent_form_refused_for_fp64_and_child_graph_batches(mf):
+    sts = scenes(mf)
+    fp64 = [load_product(mf, st, precision=0) for st in sts]
+    b = mf.Batch(fp64, steps_per_launch=2)
+    with pytest.raises(mf.MfError):
+        b.set_form(mf.BATCH_PERSISTENT, 0, 4)
+    b.close()
+    lists = [load_product(mf, st, precision=1, flags=mf.OPT_NEIGHBOUR_LISTS) for st in sts]
+    b = mf.Batch(lists, steps_per_launch=2)
+    assert not b.fused
+    with pytest.raises(mf.MfError):
+        b.set_form(mf.BATCH_PERSISTENT, 0, 4)
+    b.close()
