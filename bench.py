@@ -190,6 +190,9 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+SORT_RATE_STEPS = 1000  # untimed steps over which the list form's sort rate is counted
+
+
 def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None, flags=0):
     """Per-step CUDA-event times (ms) of mf_step(1) with the L2 flushed between steps, then
     a few steps run kernel by kernel (mf_step_timed, L2 flushed) for the device time of each
@@ -230,6 +233,14 @@ def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None,
         b.record(stream)
     torch.cuda.synchronize(device)
     extra["back_to_back_ms_per_step"] = a.elapsed_time(b) / steps
+    if precision == mf.PRECISION_MIXED and flags & mf.OPT_NEIGHBOUR_LISTS:
+        # the trajectory's sort rate over a window longer than the timed steps (untimed): the
+        # sorting steps' extra time is amortised at this rate
+        ctx.step(SORT_RATE_STEPS)
+        ctx.synchronize()
+        n_run = warmup + 2 * steps + SORT_RATE_STEPS
+        extra["steps_per_sort"] = n_run / max(ctx.status()["sorts"], 1)
+        extra["sort_rate_window_steps"] = n_run
     stages = []
     with torch.cuda.stream(stream):
         for _ in range(max(5, min(20, steps // 4))):
@@ -1114,7 +1125,8 @@ def main():
                 steps_per_mm_cut=spm,
                 note="mixed (the headline): FP32 pair sums on neighbour lists kept between cell-list sorts "
                      "(MF_OPT_NEIGHBOUR_LISTS; ms_per_step = timed steps + each step's share of a sorting step's "
-                     "extra time at steps_per_sort); mixed_sorted: the same sums with the cell list sorted every "
+                     "extra time at steps_per_sort, the sort rate counted over sort_rate_window_steps steps of the same "
+                     "run, warm-up, timed and back-to-back steps included); mixed_sorted: the same sums with the cell list sorted every "
                      "step, as in the FP64 form; pair_kernel_ms: median "
                      "of steps launched kernel by kernel (mf_step_timed) after an L2 flush; "
                      "back_to_back_ms_per_step: the same number of steps without flushes, one event pair "

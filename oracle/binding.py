@@ -159,17 +159,19 @@ def ref():
 
 
 REF_GPU_SO = HERE / "_ref" / "libref_gpu.so"
-_ref_gpu = None
+REF_GPU_PSE_SO = HERE / "_ref" / "libref_gpu_pse.so"
+_ref_gpu = {}
 
 
-def ref_gpu():
-    """The reference's own FP64 CUDA step (oracle/_ref/libref_gpu.so), or None where it was not
-    built. Needs a CUDA device to run."""
-    global _ref_gpu
-    if _ref_gpu is None:
-        if not REF_GPU_SO.exists():
+def ref_gpu(solver: str = "brookshaw"):
+    """The reference's own FP64 CUDA step (oracle/_ref/libref_gpu.so; solver="pse": its PSE heat
+    solver build, libref_gpu_pse.so), or None where it was not built. Needs a CUDA device to
+    run."""
+    if solver not in _ref_gpu:
+        so = REF_GPU_PSE_SO if solver == "pse" else REF_GPU_SO
+        if not so.exists():
             return None
-        L = C.CDLL(str(REF_GPU_SO))
+        L = C.CDLL(str(so))
         vp, d, i = C.c_void_p, C.c_double, C.c_int
         L.refg_create.argtypes = [i] + [vp] * 7 + [d] * 5
         L.refg_geometry.argtypes = [vp, vp]
@@ -183,18 +185,19 @@ def ref_gpu():
         L.refg_run_timed.argtypes = [i, vp]
         L.refg_get_cells.argtypes = [vp, vp]
         L.refg_report_force.argtypes = [vp]
-        _ref_gpu = L
-    return _ref_gpu
+        _ref_gpu[solver] = L
+    return _ref_gpu[solver]
 
 
 class RefGPU:
     """One system of the reference's own FP64 CUDA build (one per process at a time: the
     reference keeps its constants and options process-wide)."""
 
-    def __init__(self, st: dict, phys7, corr6, joco12, trml_wp6, trml_tool6, tool: OrcTool):
-        self.L = ref_gpu()
+    def __init__(self, st: dict, phys7, corr6, joco12, trml_wp6, trml_tool6, tool: OrcTool,
+                 solver: str = "brookshaw"):
+        self.L = ref_gpu(solver)
         if self.L is None:
-            raise RuntimeError(f"reference GPU build missing: {REF_GPU_SO}")
+            raise RuntimeError(f"reference GPU build missing ({solver})")
         self.N = int(st["N"])
         a = {k: np.ascontiguousarray(st[k], dtype=np.float64) for k in ("pos", "vel", "rho", "T", "h", "fixed",
                                                                          "tool_p")}

@@ -104,39 +104,65 @@ def build_ref(force: bool = False) -> Path | None:
     return REF_LIB
 
 
-def build_ref_gpu(force: bool = False) -> Path | None:
+def _pse_types_header(out_dir: Path) -> Path:
+    """The reference's types.h with its heat-solver switch turned to PSE (types.h selects the
+    solver with a #define and no way to override it from the command line): generated from the
+    reference's own file at build time into oracle/_ref, never committed, and force-included
+    after the texture shim, so that its include guard makes the sources' own types.h a no-op."""
+    text = (REF_SRC / "types.h").read_text()
+    on, off = "#define Thermal_Conduction_Brookshaw", "//#define Thermal_Conduction_PSE"
+    if text.count(on) != 1 or text.count(off) != 1:
+        raise RuntimeError("types.h: the heat-solver switch is not where the PSE build expects it")
+    text = text.replace(off, "#define Thermal_Conduction_PSE").replace(on, "//#define Thermal_Conduction_Brookshaw")
+    out = out_dir / "types_pse.h"
+    if not out.exists() or out.read_text() != text:
+        out.write_text(text)
+    return out
+
+
+REF_GPU_PSE_LIB = HERE / "_ref" / "libref_gpu_pse.so"
+
+
+def build_ref_gpu(force: bool = False, solver: str = "brookshaw") -> Path | None:
     """The reference's own FP64 CUDA step for sm_100a (oracle/_ref/libref_gpu.so): its device
     sources compiled unchanged where they lie, with the texture shim force-included and the
     project's GLM subset, plus the entry-point harness oracle/ref_gpu/ref_gpu_harness.cu.
     The reference's own makefile flags: -O3, whole-program per file (no relocatable device
-    code); its types.h selects FP64 and the Brookshaw heat solver."""
+    code); its types.h selects FP64 and the Brookshaw heat solver. solver="pse": the same
+    sources built with the switch in types.h turned to its PSE solver
+    (oracle/_ref/libref_gpu_pse.so)."""
+    pse = solver == "pse"
+    lib = REF_GPU_PSE_LIB if pse else REF_GPU_LIB
     if not REF_SRC.is_dir():
-        return REF_GPU_LIB if REF_GPU_LIB.exists() else None
+        return lib if lib.exists() else None
     ref_files = ["actions_gpu.cu", "interactions_gpu.cu", "leap_frog.cu", "tool_gpu.cu", "grid.cu",
                  "grid_gpu_green.cu", "particle_gpu.cu", "output.cu", "tool.cpp", "geometric_primitives.cpp",
                  "constants_structs.cpp", "types.cpp"]
     shim = HERE / "ref_gpu" / "ref_texture_shim.h"
     harness = HERE / "ref_gpu" / "ref_gpu_harness.cu"
-    srcs = [shim, harness, HERE / "ref_shim" / "glm" / "glm.hpp", HERE / "sph_oracle.h"] + \
+    srcs = [shim, harness, HERE / "ref_shim" / "glm" / "glm.hpp", HERE / "sph_oracle.h", Path(__file__)] + \
         [REF_SRC / f for f in ref_files] + sorted(REF_SRC.glob("*.h")) + sorted(REF_SRC.glob("*.cuh"))
-    if not (force or _stale(REF_GPU_LIB, srcs)):
-        return REF_GPU_LIB
-    obj = HERE / "_ref" / "gpu_obj"
+    if not (force or _stale(lib, srcs)):
+        return lib
+    obj = HERE / "_ref" / ("gpu_obj_pse" if pse else "gpu_obj")
     obj.mkdir(parents=True, exist_ok=True)
     nv = [NVCC, "-O3", "-std=c++14", "-Xcompiler", "-fPIC", "-gencode", "arch=compute_100a,code=sm_100a",
-          "-include", str(shim), "-I", str(HERE / "ref_shim"), "-I", str(REF_SRC), "-I", str(HERE),
-          "-w", "-x", "cu", "-c"]
+          "-include", str(shim)]
+    if pse:
+        nv += ["-include", str(_pse_types_header(obj))]
+    nv += ["-I", str(HERE / "ref_shim"), "-I", str(REF_SRC), "-I", str(HERE), "-w", "-x", "cu", "-c"]
     jobs = [(obj / ("refg_" + Path(f).stem + ".o"), REF_SRC / f) for f in ref_files]
     jobs.append((obj / "ref_gpu_harness.o", harness))
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
         list(pool.map(lambda j: _run(nv + ["-o", str(j[0]), str(j[1])]), jobs))
     objs = [j[0] for j in jobs]
     _run([NVCC, "-shared", "-Xcompiler", "-fPIC", "--cudart", "shared", "-Xlinker", "-Bsymbolic",
-          "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(REF_GPU_LIB)] + [str(x) for x in objs])
-    return REF_GPU_LIB
+          "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(lib)] + [str(x) for x in objs])
+    return lib
 
 
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     print(build_ref(force="--force" in sys.argv))
     print(build_ref_gpu(force="--force" in sys.argv))
+    print(build_ref_gpu(force="--force" in sys.argv, solver="pse"))

@@ -4,9 +4,11 @@
 // compiled unchanged where they lie (actions_gpu.cu, interactions_gpu.cu, leap_frog.cu,
 // tool_gpu.cu, grid*.cu, particle_gpu.cu, output.cu, and the host files they need) with the
 // texture shim (ref_texture_shim.h, force-included) and the project's GLM subset, into
-// oracle/_ref/libref_gpu.so by oracle/build_oracle.py (build_ref_gpu). This is the
+// oracle/_ref/libref_gpu.so by oracle/build_oracle.py (build_ref_gpu). That is the
 // reference's default build: USE_DOUBLE and the Brookshaw heat solver are #defined in its
-// types.h; the PSE build would need types.h edited and is not made.
+// types.h. oracle/_ref/libref_gpu_pse.so is the same sources and harness with its PSE heat
+// solver: a copy of types.h with the solver switch turned, generated into oracle/_ref at build
+// time, is force-included so that its guard makes the sources' own types.h a no-op.
 //
 // The harness does what the reference's main() (mfree_gpu.cpp:206-308) and setup_ref_cut
 // (benchmarks.cpp:255-537) do, from caller-given arrays instead of a built-in scene: a

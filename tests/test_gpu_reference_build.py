@@ -19,8 +19,11 @@ moves it by a float ulp); the tool force within 1e-9 of the total contact force 
 (thrust::reduce sums in an unspecified order). Cell lists, blanking and the tool bit for bit.
 
 The reference keeps its constants and option flags process-wide, so every reference system
-here uses the same options: Johnson-Cook plasticity, heat (Brookshaw, its build's solver),
-friction heat and a tool.
+here uses the same options: Johnson-Cook plasticity, heat, friction heat and a tool. Its heat
+solver is chosen at compile time (types.h): the default build runs Brookshaw, a second build
+(oracle/_ref/libref_gpu_pse.so, the switch turned in a generated copy of types.h) its PSE
+solver, which pins the product's PSE path on a perturbed scene and on the ~500k-particle
+configuration.
 """
 import ctypes as C
 
@@ -42,13 +45,13 @@ def _doubles(struct):
     return [getattr(struct, f) for f, _ in struct._fields_]
 
 
-def ref_gpu_from(orc, st):
-    if orc.ref_gpu() is None:
+def ref_gpu_from(orc, st, solver="brookshaw"):
+    if orc.ref_gpu(solver) is None:
         pytest.skip("the reference's GPU build was not made (no reference tree where the build ran)")
     tool = orc.OrcTool()
     C.memmove(C.byref(tool), C.byref(st["tool"]), C.sizeof(orc.OrcTool))
     r = orc.RefGPU(st, _doubles(st["phys"]), _doubles(st["corr"]), _doubles(st["joco"]), _doubles(st["trml_wp"]),
-                   _doubles(st["trml_tool"]), tool)
+                   _doubles(st["trml_tool"]), tool, solver=solver)
     for k in EXTRA:
         r.set_field(k, st[k])
     return r
@@ -192,4 +195,56 @@ def test_product_against_reference_build_mid_cut(mf, orc, c2_midcut):
         plastic = max(plastic, int(np.count_nonzero(r.get("eps_pl_dot")[nb])))
     assert np.count_nonzero(np.abs(r.get("fc")).sum(axis=1)) >= 10
     assert plastic >= 10
+    ctx.close()
+
+
+def product_steps_against(orc, ctx, r, steps):
+    """`steps` full steps of both, compared after each (as in the Brookshaw tests above)."""
+    for k in range(steps):
+        ctx.step(1)
+        r.step(1)
+        assert np.array_equal(ctx.get("idx"), r.get("idx")), k
+        assert np.array_equal(ctx.get("hash"), r.get("hash")), k
+        assert np.array_equal(ctx.get("blanked"), r.get("blanked")), k
+        nb = r.get("blanked") == 0.0
+        wp = nb & (r.get("tool_p") == 0.0)
+        compare(ctx.get, r.get, ("R",), 1e-12, wp)
+        compare(ctx.get, r.get, RATES, 1e-12, nb)
+        compare(ctx.get, r.get, STATE, 1e-11, nb)
+        assert force_close(ctx.report_force(), r.report_force(), r.get("fc"), r.get("ft")), k
+    pt = orc.OrcTool()  # the product's tool after the steps, for the bitwise tool check
+    t = ctx.tool_get()
+    C.memmove(C.byref(pt), C.byref(t), C.sizeof(orc.OrcTool))
+    return pt
+
+
+@pytest.mark.parametrize("tensile", [False, True])
+def test_product_against_reference_pse_build(mf, orc, tensile):
+    """The PSE heat solver (interactions_gpu.cu:88-144, leap_frog.cu:122): five steps of the
+    product's FP64 form against the reference's own CUDA step built with its PSE solver, on the
+    same GPU; heat flows (T_t nonzero) on both sides."""
+    st = perturbed_scene(mf, ny=12, seed=34, tensile=tensile)
+    ctx = load_product(mf, st, thermal_solver=mf.THERMAL_PSE)
+    r = ref_gpu_from(orc, st, solver="pse")
+    pt = product_steps_against(orc, ctx, r, 5)
+    assert np.count_nonzero(r.get("T_t")) > 100
+    assert tool_bits(mf, pt, r.get_tool())
+    ctx.close()
+
+
+def test_product_against_reference_pse_build_500k(mf, orc):
+    """The ~500k-particle configuration (1290 x 387 lattice, dx = 1.55 um, 577,555 particles,
+    PSE heat, where the half-length binding of tool_particle, interactions_gpu.cu:405, splits the
+    particles at N/2): five steps of the product's FP64 form against the reference's PSE build."""
+    import bench
+
+    p, solver, _ = bench.config_params(mf, "c3")
+    assert solver == mf.THERMAL_PSE
+    sc = mf.Scene.from_params(p)
+    st = scene_state(mf, sc)
+    assert st["N"] > 500_000
+    ctx = load_product(mf, st, thermal_solver=solver)
+    r = ref_gpu_from(orc, st, solver="pse")
+    pt = product_steps_against(orc, ctx, r, 5)
+    assert tool_bits(mf, pt, r.get_tool())
     ctx.close()
