@@ -193,7 +193,8 @@ class ClockSampler:
 SORT_RATE_STEPS = 1000  # untimed steps over which the list form's sort rate is counted
 
 
-def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None, flags=0):
+def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None, flags=0,
+              sort_rate_steps=SORT_RATE_STEPS):
     """Per-step CUDA-event times (ms) of mf_step(1) with the L2 flushed between steps, then
     a few steps run kernel by kernel (mf_step_timed, L2 flushed) for the device time of each
     part: cell sort, predictor, interactions + rates (the pair kernel), corrector ..
@@ -236,9 +237,10 @@ def time_form(mf, torch, scene, precision, steps, warmup, device, state_in=None,
     if precision == mf.PRECISION_MIXED and flags & mf.OPT_NEIGHBOUR_LISTS:
         # the trajectory's sort rate over a window longer than the timed steps (untimed): the
         # sorting steps' extra time is amortised at this rate
-        ctx.step(SORT_RATE_STEPS)
+        if sort_rate_steps > 0:
+            ctx.step(sort_rate_steps)
         ctx.synchronize()
-        n_run = warmup + 2 * steps + SORT_RATE_STEPS
+        n_run = warmup + 2 * steps + sort_rate_steps
         extra["steps_per_sort"] = n_run / max(ctx.status()["sorts"], 1)
         extra["sort_rate_window_steps"] = n_run
     stages = []
@@ -930,6 +932,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sort-rate-steps", type=int, default=SORT_RATE_STEPS,
+                    help="untimed steps over which the neighbour-list form's sort rate is counted")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched form's 64-instance sweep that the benchmark line carries")
     ap.add_argument("--no-reference-gpu", action="store_true",
@@ -1026,7 +1030,7 @@ def main():
         torch.cuda.synchronize(device)
         with ClockSampler(device) as cs:
             step_ms, pair_ms, st, extra = time_form(mf, torch, scene, prec, args.steps, args.warmup, device,
-                                                    args.state_in, flags)
+                                                    args.state_in, flags, args.sort_rate_steps)
         if name == "mixed":
             clocks = cs.summary()
         total_ms = max_over_ranks(float(step_ms.sum()), world, device=f"cuda:{device}")
