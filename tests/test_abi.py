@@ -51,3 +51,14 @@ def test_argument_checks_without_device(mf):
     n = C.c_int()
     assert L.mf_tool_sample(C.byref(t), 0.0, None, 0, C.byref(n)) == -1
     assert L.mf_ctx_create(0, None) == -1
+
+
+def test_batch_form_entry_points_check_their_arguments(mf):
+    """The batch form entry points refuse a null batch before touching a device."""
+    L = mf.lib()
+    k = C.c_int()
+    assert L.mf_batch_set_form(None, mf.BATCH_PERSISTENT, 0, 4) == -1
+    assert L.mf_batch_form(None, C.byref(k), C.byref(k)) == -1
+    assert L.mf_batch_set_wait_limit(None, C.c_double(1.0)) == -1
+    assert L.mf_batch_step(None, 1) == -1
+    assert L.mf_batch_create(None, 1, 2, None) == -1
