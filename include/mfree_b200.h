@@ -191,6 +191,15 @@ int mf_get_constants(const mf_ctx *ctx, mf_phys_constants *phys, mf_corr_constan
                      mf_trml_constants *trml_wp, mf_trml_constants *trml_tool, int *has_joco);
 int mf_set_options(mf_ctx *ctx, int thermal_solver, int jc_model, int precision);
 int mf_set_dt(mf_ctx *ctx, double dt); /* global_dt (benchmarks.cpp:20) */
+/* Tool-workpiece contact conductance, an extension with no counterpart in the reference (whose
+   heat crosses the interface only through the sampled tool particles' conduction terms,
+   interactions_gpu.cu:314-326): each step, a workpiece particle that the contact treatment finds
+   inside the tool gains dt h (T_tool - T) / (cp sqrt(m rho)) in temperature, h in the library's
+   units (1e8 W/m^2K = 1e-7 g/(us^3 K)), sqrt(m / rho) being its contact length per unit depth;
+   applied after the friction heat, before the return map, where the workpiece's cp > 0.
+   h = 0 (the default) switches it off and leaves the reference's step unchanged. Contexts with
+   it on step in the child-graph batch form and have no differentiable step (MF_ERR_INVALID). */
+int mf_set_contact_conductance(mf_ctx *ctx, double h_contact, double T_tool);
 
 /* ---- tool: tool_gpu_set_up_tool (tool_gpu.cu:224-271); the per-step tool_gpu_update_tool
    (tool_gpu.cu:275-316) happens on the device inside mf_step. NULL or num_seg = 0: no tool. */

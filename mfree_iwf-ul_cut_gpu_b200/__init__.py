@@ -140,6 +140,7 @@ def lib():
         "mf_set_constants": ([vp, C.POINTER(Phys), C.POINTER(Corr), C.POINTER(Joco), C.POINTER(Trml),
                               C.POINTER(Trml)], i),
         "mf_set_options": ([vp, i, i, i], i), "mf_set_dt": ([vp, d], i),
+        "mf_set_contact_conductance": ([vp, d, d], i),
         "mf_tool_set": ([vp, C.POINTER(ToolState)], i), "mf_tool_get": ([vp, C.POINTER(ToolState)], i),
         "mf_step": ([vp, i], i), "mf_step_timed": ([vp, vp], i), "mf_step_stage": ([vp, i], i), "mf_report_force": ([vp, vp], i),
         "mf_tangent_mean_force": ([vp, i, i, i, vp, vp], i),
@@ -418,6 +419,11 @@ class Context:
 
     def set_dt(self, dt):
         self._check(self.L.mf_set_dt(self.h, dt), "mf_set_dt")
+
+    def set_contact_conductance(self, h_contact, T_tool):
+        """Tool-workpiece contact conductance (no reference counterpart; 0 = off)."""
+        self._check(self.L.mf_set_contact_conductance(self.h, float(h_contact), float(T_tool)),
+                    "mf_set_contact_conductance")
 
     def tool_set(self, tool: ToolState | None):
         self._check(self.L.mf_tool_set(self.h, C.byref(tool) if tool is not None else None), "mf_tool_set")

@@ -352,12 +352,22 @@ int launch_stage(mf_ctx *ctx, int stage) {
     case 3:
       {
         const int fb = (N + FINISH_BLOCK - 1) / FINISH_BLOCK;
-        if (ctx->P.fuse) {  // the next step's predictor runs here too
-          if (fused_step(ctx))
+        const bool hash = fused_step(ctx);
+        if (ctx->P.h_contact > 0.) {  // with contact conductance
+          if (ctx->P.fuse && hash)
+            TRY(launch_pdl(ctx, k_finish_flat<true, true, true>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+          else if (ctx->P.fuse)
+            TRY(launch_pdl(ctx, k_finish_flat<false, true, true>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+          else if (hash)
+            TRY(launch_pdl(ctx, k_finish_flat<true, false, true>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+          else
+            TRY(launch_pdl(ctx, k_finish_flat<false, false, true>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
+        } else if (ctx->P.fuse) {  // the next step's predictor runs here too
+          if (hash)
             TRY(launch_pdl(ctx, k_finish_flat<true, true>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
           else
             TRY(launch_pdl(ctx, k_finish_flat<false, true>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
-        } else if (fused_step(ctx)) {
+        } else if (hash) {
           TRY(launch_pdl(ctx, k_finish_flat<true, false>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
         } else {
           TRY(launch_pdl(ctx, k_finish_flat<false, false>, fb, FINISH_BLOCK, ctx->P, ctx->D, ctx->scan_tiles));
@@ -555,6 +565,14 @@ int mf_set_flags(mf_ctx *ctx, int flags) {
   ctx->flags = flags;
   ctx->P.keep_derivs = (flags & MF_OPT_KEEP_DERIVATIVES) ? 1 : 0;
   drop_graphs(ctx);
+  return MF_OK;
+}
+
+int mf_set_contact_conductance(mf_ctx *ctx, double h_contact, double T_tool) {
+  if (!ctx || !(h_contact >= 0.) || !std::isfinite(h_contact) || !std::isfinite(T_tool)) return MF_ERR_INVALID;
+  ctx->P.h_contact = h_contact;
+  ctx->P.T_contact = T_tool;
+  drop_graphs(ctx);  // a kernel variant and its parameters
   return MF_OK;
 }
 
@@ -1051,14 +1069,14 @@ void batch_release(mf_batch *b) {
 }
 
 // The batched kernels serve systems whose steps run the same kernel variants: locked grids,
-// steps launched whole (not staged), no neighbour lists, one precision, heat solver, yield
-// law and plasticity setting. Anything else keeps the child-graph batch.
+// steps launched whole (not staged), no neighbour lists or contact conductance, one precision,
+// heat solver, yield law and plasticity setting. Anything else keeps the child-graph batch.
 bool batch_can_fuse(mf_batch *b) {
   const params &P0 = b->ctx[0]->P;
   for (mf_ctx *c : b->ctx) {
     set_list_mode(c);
     const params &P = c->P;
-    if (!fused_step(c) || P.verlet || P.fuse || P.precision != P0.precision ||
+    if (!fused_step(c) || P.verlet || P.fuse || P.h_contact > 0. || P.precision != P0.precision ||
         P.thermal_solver != P0.thermal_solver || P.jc_model != P0.jc_model || P.plastic != P0.plastic ||
         (P.thermal_solver == MF_THERMAL_PSE && (P.thermal_wp != 0) != (P0.thermal_wp != 0)))
       return false;
@@ -1925,7 +1943,7 @@ int tangent_check(mf_ctx *ctx) {
   if (!ready(ctx) || ctx->mid_step) return MF_ERR_STATE;
   if (!(ctx->P.dt > 0.)) return MF_ERR_STATE;
   if (!ctx->G.locked || ctx->grid_kind != MF_GRID_GREEN || ctx->P.thermal_solver == MF_THERMAL_PSE ||
-      ctx->P.jc_model != MF_JC_JOHNSON_COOK || !ctx->P.plastic)
+      ctx->P.jc_model != MF_JC_JOHNSON_COOK || !ctx->P.plastic || ctx->P.h_contact > 0.)
     return MF_ERR_INVALID;
   return MF_OK;
 }

@@ -59,6 +59,10 @@ struct params {
   float skin;
   double eos_c0;  // (double)sqrtf((float)(K / rho0)), the EOS sound speed (actions_gpu.cu:41-51)
   double dt;
+  // tool-workpiece contact conductance (an extension without a reference counterpart, off at
+  // 0): a workpiece particle in contact with the tool exchanges h_contact (T_contact - T) per
+  // unit contact length with a tool surface at T_contact
+  double h_contact, T_contact;
   mf_phys_constants phys;
   mf_corr_constants corr;
   mf_joco_constants joco;

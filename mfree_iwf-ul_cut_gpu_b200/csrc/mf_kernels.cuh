@@ -857,7 +857,7 @@ static __global__ void __launch_bounds__(PAIR_BLOCK) k_pse(params P, dev_buffers
 // first, so the kernel runs with fewer registers and more warps per SM. (eps_pl is not touched
 // here: the corrector does not change it, the return map in k_plastic does.) With FUSE_PRED and
 // `fuse`, also the next step's predictor (neighbour lists, a step without a sort).
-template <bool FUSE_PRED>
+template <bool FUSE_PRED, bool CONDUCT>
 __device__ __forceinline__ void finish_particle_phased(const params &P, const dev_buffers &D,
                                                        const mf_tool_state &TL, int q, double2 &pos_out,
                                                        unsigned &f_out, double2 &fc_out, double2 &ft_out,
@@ -899,6 +899,7 @@ __device__ __forceinline__ void finish_particle_phased(const params &P, const de
     }
   }
   // tool particles move with the tool (tool_gpu.cu:210-221); contact (:151-207)
+  bool in_contact = false;
   if (P.has_tool) {
     if (tool) {
       pos.x += dt * TL.vel[0];
@@ -936,6 +937,7 @@ __device__ __forceinline__ void finish_particle_phased(const params &P, const de
         fc = fN;
         ft = fT;
         D.n[q] = make_double2(nx, ny);
+        in_contact = true;
       }
     }
   }
@@ -976,6 +978,11 @@ __device__ __forceinline__ void finish_particle_phased(const params &P, const de
     T = T + dt * T_t;
   }
   if (fric) T += dT_fric;
+  // contact conductance (no reference counterpart; off unless set): heat h (T_tool - T) per unit
+  // contact length, the contact length of a particle of mass m (per unit depth) at density rho
+  // being sqrt(m / rho), so dT/dt = h (T_tool - T) / (cp sqrt(m rho))
+  if (CONDUCT && in_contact && !blanked && P.trml_wp.cp > 0.)
+    T += dt * P.h_contact * (P.T_contact - T) / (P.trml_wp.cp * sqrt(P.phys.mass * rho));
   // JC plasticity, radial return (actions_gpu.cu:226-285): the elastic lower bound of
   // finish_particle, the rest in k_plastic
   bool elastic = false;
@@ -1120,7 +1127,7 @@ __device__ __forceinline__ void force_close_step(const params &P, const dev_buff
 #ifndef FINISH_FLAT_MIN_BLOCKS
 #define FINISH_FLAT_MIN_BLOCKS 3
 #endif
-template <bool FUSE_HASH, bool FUSE_PRED>
+template <bool FUSE_HASH, bool FUSE_PRED, bool CONDUCT = false>
 __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buffers &D,
                                                                                     int num_scan_tiles, blk bk) {
   __shared__ mf_tool_state s_tool;
@@ -1137,7 +1144,8 @@ __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buff
   if (q < P.N) {
     double2 pos;
     unsigned f;
-    finish_particle_phased<FUSE_PRED>(P, D, s_tool, q, pos, f, fc, ft, newly_blanked, want_sort, identity, fuse);
+    finish_particle_phased<FUSE_PRED, CONDUCT>(P, D, s_tool, q, pos, f, fc, ft, newly_blanked, want_sort, identity,
+                                               fuse);
     blanked_now = (f & FLAG_BLANKED) ? 1u : 0u;
     if (FUSE_HASH) {  // compute_hashes of the next step (grid.cu:34-51)
       const geom g = *D.g;
@@ -1239,11 +1247,11 @@ __device__ __forceinline__ void finish_flat_body(const params &P, const dev_buff
   if (lane_id() == 0) force_close_step(P, D, r, fuse, !identity);
 }
 
-template <bool FUSE_HASH, bool FUSE_PRED>
+template <bool FUSE_HASH, bool FUSE_PRED, bool CONDUCT = false>
 __global__ void __launch_bounds__(FINISH_BLOCK, FINISH_FLAT_MIN_BLOCKS) k_finish_flat(params P, dev_buffers D, int num_scan_tiles) {
   MF_PDL_WAIT();
   MF_PDL_TRIGGER();
-  finish_flat_body<FUSE_HASH, FUSE_PRED>(P, D, num_scan_tiles, grid_blk());
+  finish_flat_body<FUSE_HASH, FUSE_PRED, CONDUCT>(P, D, num_scan_tiles, grid_blk());
 }
 
 // JC plasticity (actions_gpu.cu:226-285) for the particles the finish kernel listed: the
