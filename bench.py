@@ -140,17 +140,57 @@ def sum_over_ranks(value: float, world: int, device=None) -> float:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML read from a thread
+    every 20 ms (reading only; nothing is set), else nvidia-smi every 200 ms."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
+        self.thread = None
+        self.samples = []  # (sm_mhz, max_mhz, set of reason names)
+
+    def _nvml_handle(self, nv):
+        try:  # the CUDA device's own GPU, whatever the visible-device order
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _poll(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self.stop.wait(0.02):
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except Exception:
+                continue
+            self.samples.append((sm, mx, {k for k, b in bits.items() if r & b}))
 
     def __enter__(self):
+        import threading
+
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = self._nvml_handle(nv)
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
                                           "-i", str(self.dev), "-lms", "200"], stdout=subprocess.PIPE,
@@ -160,7 +200,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
-        self.lines = []
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -168,26 +210,24 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
                 out, _ = self.proc.communicate()
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+            for ln in out.splitlines():
+                parts = [x.strip() for x in ln.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    self.samples.append((float(parts[1]), float(parts[2]),
+                                         {nm for nm, v in zip(self.NAMES, parts[5:9]) if v.lower() == "active"}))
+                except ValueError:
+                    continue
 
     def summary(self):
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in getattr(self, "lines", []):
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = max(mx, float(parts[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        sm = [x[0] for x in self.samples]
+        reasons = set().union(*[x[2] for x in self.samples])
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(x[1] for x in self.samples),
+                "sm_mhz_min": float(min(sm)), "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.thread is not None else "nvidia-smi"}
 
 
 SORT_RATE_STEPS = 1000  # untimed steps over which the list form's sort rate is counted
