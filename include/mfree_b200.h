@@ -400,8 +400,10 @@ int mf_batch_step(mf_batch *batch, int n_launches); /* n_launches x steps_per_la
    launch (captured in the batch's graph) of blocks_per_sm 256-thread blocks per SM (0: as many
    as are resident); its blocks take each phase's blocks of all instances in turn and meet at a
    grid-wide barrier between phases, every instance's results still equal to its own context's
-   bit for bit. Each barrier wait is bounded (mf_batch_set_wait_limit, default 2 s): if one
-   expires the launch ends early and every instance's mf_status.error_flags gets bit 3.
+   bit for bit. Each barrier wait is bounded (mf_batch_set_wait_limit, seconds in [0, 3600],
+   default 2 s; 0 makes the first wait give up at once): if one expires, that barrier releases no
+   block, the launch ends early with the instances' states part-stepped, and every instance's
+   mf_status.error_flags gets bit 3.
    The persistent form steps mixed-precision batches only (an FP64 build of it contracted the
    pair sums' multiply-adds differently, ~1e-16 relative off the single-system step).
    mf_batch_set_form rebuilds the batch's graph (MF_ERR_INVALID for a child-graph or FP64 batch
