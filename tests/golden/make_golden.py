@@ -269,9 +269,30 @@ def oracle_fixture():
     np.savez_compressed(HERE / "oracle_steps.npz", **oracle_steps.compute(mf, B))
 
 
+def ref_gpu_fixture():
+    """The reference's own CUDA step on a small scene (tests/golden/ref_gpu_steps.py); needs a CUDA
+    device and oracle/_ref/libref_gpu.so and libref_gpu_pse.so."""
+    import importlib.util
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import ref_gpu_steps
+
+    spec = importlib.util.spec_from_file_location("mfree_b200", ROOT / "mfree_iwf-ul_cut_gpu_b200" / "__init__.py",
+                                                  submodule_search_locations=[str(ROOT / "mfree_iwf-ul_cut_gpu_b200")])
+    mf = importlib.util.module_from_spec(spec)
+    sys.modules["mfree_b200"] = mf
+    spec.loader.exec_module(mf)
+    if B.ref_gpu() is None or B.ref_gpu("pse") is None:
+        raise SystemExit("the reference's GPU builds are missing (oracle/build_oracle.py on a machine with its tree)")
+    np.savez_compressed(HERE / "ref_gpu_steps.npz", **ref_gpu_steps.compute(mf, B))
+
+
 def main():
     if sys.argv[1:] == ["oracle"]:
         oracle_fixture()
+        return
+    if sys.argv[1:] == ["ref_gpu"]:
+        ref_gpu_fixture()
         return
     build_oracle.build_ref()
     R = B.ref()
