@@ -360,17 +360,25 @@ __device__ __forceinline__ void pair_mixed_particle(const params &P, const dev_b
     const int cnt = sorting ? build_list(D, R, q, I, g, gi, gj, dxc, P.skin) : D.ncount[q];
     const uint4 *row = reinterpret_cast<const uint4 *>(D.nlist + (size_t)q * LIST_CAP);
     uint4 e4 = row[0];  // (a row is LIST_CAP entries: the first four are always there)
+    const unsigned self = (unsigned)q | (3u << LIST_INDEX_BITS);
+    // software pipeline: the next entry's four record planes are in flight while one entry is
+    // summed (c0..c3 hold entry k's at the top of its iteration; past the count, the particle's
+    // own record, always a valid address). Measured on the ~150k-particle cut: pair kernel 48.1
+    // against 50.1 us at 5 blocks per SM (96 registers, 4 B of spills); at 4 blocks per SM (108
+    // registers) 54.2 us.
+    float4 c0, c1, c2, c3;
+    R.all((int)((cnt > 0 ? e4.x : self) & LIST_INDEX_MASK), c0, c1, c2, c3);
     for (int k0 = 0; k0 < cnt; k0 += 4) {
       const unsigned ev[4] = {e4.x, e4.y, e4.z, e4.w};
       if (k0 + 4 < cnt) e4 = row[(k0 >> 2) + 1];  // the next four, in flight during these
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         const bool live = k0 + u < cnt;
-        const unsigned e = live ? ev[u] : (unsigned)q | (3u << LIST_INDEX_BITS);
-        const int j = (int)(e & LIST_INDEX_MASK);
+        const unsigned e = live ? ev[u] : self;
+        const unsigned en = (k0 + u + 1 < cnt) ? (u < 3 ? ev[u + 1] : e4.x) : self;
         const float ox = fmaf((float)((int)(e >> LIST_INDEX_BITS) - 3), dxc, I.x);
-        float4 b0, b1, b2, b3;
-        R.all(j, b0, b1, b2, b3);
+        const float4 b0 = c0, b1 = c1, b2 = c2, b3 = c3;
+        R.all((int)(en & LIST_INDEX_MASK), c0, c1, c2, c3);
         const unsigned fjw = (unsigned)__float_as_int(b0.z);
         const float xij = ox - b0.x;
         const float yij = fmaf((float)(gj - (int)(fjw >> 8)), dxc, I.y - b0.y);
@@ -401,9 +409,9 @@ __device__ __forceinline__ void pair_mixed_body(const params &P, const dev_buffe
   pair_mixed_particle<LIST>(P, D, bk.x * blockDim.x + threadIdx.x);
 }
 
-// blocks per SM: the window kernel at 6 (80 registers, no spills); the list kernel at 5 (92
-// registers, no spills; at 6 it spills a little and ran ~1.5 us slower, at 9 with 56 registers
-// 13 us slower)
+// blocks per SM: the window kernel at 6 (80 registers, no spills); the list kernel at 5 (96
+// registers with its software pipeline, 4 B of spills; before the pipeline, at 6 it spilled a
+// little and ran ~1.5 us slower than at 5, at 9 with 56 registers 13 us slower)
 template <bool LIST>
 static __global__ void __launch_bounds__(PAIR_BLOCK, LIST ? 5 : 6) k_pair_mixed(params P, dev_buffers D) {
   MF_PDL_WAIT();
