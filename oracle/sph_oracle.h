@@ -11,9 +11,11 @@
  * Johnson-Cook yield/secant functions are checked bit-for-bit against the reference's own
  * sources compiled on the host (oracle/_ref/libref_host.so, see oracle/build_oracle.py).
  * The device-only kernel bodies (pair loop, per-particle actions, contact, sort/reorder)
- * are restated line by line from the reference source; the reference's GPU build cannot
- * be compiled with CUDA 12 (texture references were removed), so those bodies are pinned
- * by the restatement and by the host-compiled pieces they call.
+ * are restated line by line from the reference source and pinned against the reference's
+ * own CUDA build: its device sources compiled unchanged for sm_100a with a shim for the
+ * texture-reference API that CUDA 12 removed (oracle/ref_gpu, oracle/_ref/libref_gpu.so and
+ * the PSE build libref_gpu_pse.so), compared live on a GPU and through golden vectors of its
+ * outputs (tests/golden/ref_gpu_steps.npz) on any host.
  *
  * Layout mirrors particle_gpu (particle_gpu.h:33-87): SoA arrays of doubles, vector fields
  * interleaved (pos = x0 y0 x1 y1 ..., S = xx xy yy zz per particle), flags stored as

@@ -1,8 +1,8 @@
 """Regression fixtures of the oracle's own FP64 step (test infrastructure).
 
-The reference's step cannot run here (its GPU build is unbuildable and it has no CPU path), so
-the oracle's step is pinned piecewise against the reference's host-compiled functions and, as a
-whole, by these fixtures of its own outputs on the benchmark configurations: c1 (143 x 43,
+The reference's step has no CPU path; its CUDA build runs on a GPU only (oracle/_ref, pinned
+there and through tests/golden/ref_gpu_steps.npz). These fixtures of the oracle's own outputs
+hold its whole step fixed on the benchmark configurations, on any host: c1 (143 x 43,
 adiabatic, no tool particles, ~6k particles) after one step (full arrays) and after 1,000 steps (digest), and c2
 (the ~150k-particle cut) after one step (digest). Every per-particle result of the oracle is
 independent of the OpenMP thread count (particles are computed independently; the cell sort is
